@@ -1,0 +1,112 @@
+"""ctypes binding of libactfem_gpu.so (include/afem.h).
+
+The library is built in-tree by ``actfemtide_b200.build`` (or
+``__graft_entry__.build()``); this module never falls back to anything else:
+if the shared object is missing, loading raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libactfem_gpu.so")
+
+AFEM_OK = 0
+STATUS = {
+    0: "AFEM_OK", -1: "AFEM_EINVAL", -2: "AFEM_EVOLUME", -3: "AFEM_EPATTERN", -4: "AFEM_EMAXITER",
+    -5: "AFEM_EBREAKDOWN", -6: "AFEM_ENONFINITE", -7: "AFEM_ECUDA", -8: "AFEM_ESTATE", -9: "AFEM_ETIMEOUT",
+    -10: "AFEM_EIO", -11: "AFEM_ENOPRECOND", -12: "AFEM_ESITE", -13: "AFEM_ESTAGNATION",
+}
+PRECOND = {"IC": 0, "SSOR": 1, "DIAG": 2, "NONE": 3}
+PRECISION = {"fp64": 0, "mixed": 1}
+
+# Every entry point declared in include/afem.h.
+EXPORTS = (
+    "afem_create", "afem_destroy", "afem_last_error", "afem_stream", "afem_set_mesh", "afem_get_lines",
+    "afem_set_cond", "afem_set_sigma", "afem_set_source", "afem_set_bounds", "afem_assemble",
+    "afem_export_system", "afem_solve", "afem_get_solution", "afem_sites", "afem_site_coeffs", "afem_load_ctl",
+    "afem_ctl_info", "afem_run_ctl", "afem_fortran_g", "afem_set_profiling", "afem_profile_count",
+    "afem_profile_entry",
+)
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("precond", C.c_int), ("precision", C.c_int), ("tol", C.c_double), ("maxit", C.c_int),
+                ("sigma_diag", C.c_double), ("check_every", C.c_int), ("inner_tol", C.c_double),
+                ("use_graph", C.c_int)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("resid_recursive", C.c_double),
+                ("resid_true", C.c_double), ("seconds", C.c_double), ("status", C.c_int)]
+
+
+class AfemError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_LIB = None
+_vp = C.c_void_p
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+def lib():
+    """Load the in-tree library (raises OSError when it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise OSError(f"{LIB_PATH} is missing: run `python -m actfemtide_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    L.afem_create.restype = _vp
+    L.afem_create.argtypes = [C.c_int]
+    L.afem_destroy.argtypes = [_vp]
+    L.afem_last_error.restype = C.c_char_p
+    L.afem_last_error.argtypes = [_vp]
+    L.afem_stream.restype = _vp
+    L.afem_stream.argtypes = [_vp]
+    L.afem_set_mesh.argtypes = [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp, _vp]
+    L.afem_get_lines.argtypes = [_vp, C.POINTER(C.c_int), _vp, _vp]
+    L.afem_set_cond.argtypes = [_vp, C.c_double, C.c_double, C.c_int, C.c_int, _vp, C.c_int, _vp]
+    L.afem_set_sigma.argtypes = [_vp, _vp]
+    L.afem_set_source.argtypes = [_vp, C.c_int, C.c_int, _vp, _vp]
+    L.afem_set_bounds.argtypes = [_vp, C.c_double, C.c_double, C.c_double, C.c_double]
+    L.afem_assemble.argtypes = [_vp]
+    L.afem_export_system.argtypes = [_vp, C.c_double, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_long), _vp, _vp,
+                                     _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.afem_solve.argtypes = [_vp, C.c_int, _vp, _vp, C.POINTER(SolveOpts), C.POINTER(SolveStats)]
+    L.afem_get_solution.argtypes = [_vp, C.c_int, _vp]
+    L.afem_sites.argtypes = [_vp, C.c_int, _vp, _vp]
+    L.afem_site_coeffs.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp]
+    L.afem_load_ctl.argtypes = [_vp, C.c_char_p]
+    L.afem_ctl_info.argtypes = [_vp, C.POINTER(C.c_int), _vp, C.POINTER(C.c_int), _vp]
+    L.afem_run_ctl.argtypes = [_vp, C.POINTER(SolveOpts)]
+    L.afem_fortran_g.argtypes = [C.c_double, C.c_int, C.c_int, C.c_char_p, C.c_int]
+    L.afem_set_profiling.argtypes = [_vp, C.c_int]
+    L.afem_profile_count.argtypes = [_vp]
+    L.afem_profile_entry.argtypes = [_vp, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_long)]
+    for name in ("afem_set_mesh", "afem_get_lines", "afem_set_cond", "afem_set_sigma", "afem_set_source",
+                 "afem_set_bounds", "afem_assemble", "afem_export_system", "afem_solve", "afem_get_solution",
+                 "afem_sites", "afem_site_coeffs", "afem_load_ctl", "afem_ctl_info", "afem_run_ctl",
+                 "afem_fortran_g", "afem_set_profiling", "afem_profile_count", "afem_profile_entry"):
+        getattr(L, name).restype = C.c_int
+    _LIB = L
+    return L
+
+
+def ptr(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def fortran_g(x: float, w: int = 15, d: int = 7) -> str:
+    buf = C.create_string_buffer(64)
+    n = lib().afem_fortran_g(float(x), w, d, buf, 64)
+    if n < 0:
+        raise ValueError("format overflow")
+    return buf.value.decode()

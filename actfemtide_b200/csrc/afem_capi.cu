@@ -1,0 +1,374 @@
+// C ABI entry points (include/afem.h): context, inputs, assembly, solve, sites.
+#include <cmath>
+#include <cstring>
+#include <exception>
+
+#include "afem_internal.h"
+
+namespace afem {
+
+void reset_status(afem_ctx* c) { AFEM_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), c->stream)); }
+
+void check_status(afem_ctx* c, const char* what) {
+  DevStatus h{};
+  AFEM_CUDA(cudaMemcpyAsync(&h, c->status.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
+  AFEM_CUDA(cudaStreamSynchronize(c->stream));
+  AFEM_CUDA(cudaGetLastError());
+  if (h.code == DEV_OK) return;
+  reset_status(c);
+  int code = AFEM_EINVAL;
+  const char* kind = "error";
+  switch (h.code) {
+    case DEV_VOLUME: code = AFEM_EVOLUME; kind = "non-positive volume"; break;
+    case DEV_ROWLEN: code = AFEM_EPATTERN; kind = "row longer than 64 nonzeros"; break;
+    case DEV_TIMEOUT: code = AFEM_ETIMEOUT; kind = "device wait exceeded its bound"; break;
+    case DEV_NOTFOUND: code = AFEM_EPATTERN; kind = "id not found"; break;
+    case DEV_DEGREE: code = AFEM_EPATTERN; kind = "adjacency longer than the kernel limit"; break;
+    case DEV_NOSIGMA: code = AFEM_EINVAL; kind = "no conductivity for tag"; break;
+    default: break;
+  }
+  char buf[256];
+  snprintf(buf, sizeof(buf), "%s: %s (index %d, 0-based)", what, kind, h.where);
+  throw Error{code, buf};
+}
+
+}  // namespace afem
+
+using afem::Error;
+
+namespace {
+
+template <class F>
+int guarded(afem_ctx* c, F&& f) {
+  if (!c) return AFEM_EINVAL;
+  try {
+    cudaSetDevice(c->device);
+    int rc = f();
+    return rc;
+  } catch (const Error& e) {
+    c->err = e.msg;
+    return e.code;
+  } catch (const std::exception& e) {
+    c->err = e.what();
+    return AFEM_EINVAL;
+  }
+}
+
+void invalidate_assembly(afem_ctx* c) { c->assembled = false; }
+
+}  // namespace
+
+extern "C" {
+
+afem_ctx* afem_create(int device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return nullptr;
+  if (cudaSetDevice(device) != cudaSuccess) return nullptr;
+  afem_ctx* c = new afem_ctx();
+  c->device = device;
+  try {
+    AFEM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    AFEM_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+    c->status.alloc(1);
+    c->status.zero(c->stream);
+    AFEM_CUDA(cudaStreamSynchronize(c->stream));
+  } catch (const Error&) {
+    delete c;
+    return nullptr;
+  }
+  return c;
+}
+
+void afem_destroy(afem_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  afem::destroy_work(c);
+  afem::destroy_ctl(c);
+  for (auto* s : c->src) delete s;
+  c->src.clear();
+    if (c->stream) {
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+  }
+  delete c;
+}
+
+const char* afem_last_error(const afem_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+void* afem_stream(afem_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int afem_set_mesh(afem_ctx* c, int node, const double* xyz, int ntet, const int32_t* n4, const int32_t* tag,
+                  int nline, const int32_t* line, const int32_t* n6line) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(node > 0 && ntet > 0 && xyz && n4 && tag, AFEM_EINVAL, "set_mesh: empty mesh or null array");
+    AFEM_REQUIRE(nline >= 0, AFEM_EINVAL, "set_mesh: negative nline");
+    for (long i = 0; i < 4L * ntet; ++i)
+      AFEM_REQUIRE(n4[i] >= 1 && n4[i] <= node, AFEM_EINVAL, "set_mesh: node id outside 1..node in n4");
+    if (nline > 0) {
+      AFEM_REQUIRE(line && n6line, AFEM_EINVAL, "set_mesh: nline > 0 needs line and n6line");
+      for (long i = 0; i < 2L * nline; ++i)
+        AFEM_REQUIRE(line[i] >= 1 && line[i] <= node, AFEM_EINVAL, "set_mesh: node id outside 1..node in line");
+      for (long i = 0; i < 6L * ntet; ++i)
+        AFEM_REQUIRE(n6line[i] != 0 && std::abs(n6line[i]) <= nline, AFEM_EINVAL,
+                     "set_mesh: n6line entry outside +-1..nline");
+    }
+    cudaStream_t s = c->stream;
+    c->node = node;
+    c->ntet = ntet;
+    c->xyz.upload(xyz, 3L * node, s);
+    c->n4.upload(n4, 4L * ntet, s);
+    c->tag.upload(tag, ntet, s);
+    c->h_tag.assign(tag, tag + ntet);
+    c->pattern_ready = false;
+    c->assembled = false;
+    c->sigma_set = false;
+    afem::reset_status(c);
+    if (nline > 0) {
+      c->nline = nline;
+      c->line.upload(line, 2L * nline, s);
+      c->n6line.upload(n6line, 6L * ntet, s);
+    } else {
+      afem::build_lines_device(c);
+    }
+    AFEM_CUDA(cudaStreamSynchronize(s));
+    afem::build_pattern_device(c);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_get_lines(afem_ctx* c, int* nline, int32_t* line, int32_t* n6line) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(c->nline > 0, AFEM_ESTATE, "get_lines: no mesh");
+    if (nline) *nline = c->nline;
+    if (line) c->line.download(line, 2L * c->nline, c->stream);
+    if (n6line) c->n6line.download(n6line, 6L * c->ntet, c->stream);
+    AFEM_CUDA(cudaStreamSynchronize(c->stream));
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_set_cond(afem_ctx* c, double sigma_air, double sigma_ocean, int condflag, int nvolume,
+                  const double* sigma_land, int nphys2, const double* sigma_file) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(c->ntet > 0, AFEM_ESTATE, "set_cond: set the mesh first");
+    AFEM_REQUIRE(condflag == 0 || condflag == 1, AFEM_EINVAL, "set_cond: condflag must be 0 or 1");
+    const std::vector<int32_t>& tag = c->h_tag;
+    const long ntet = c->ntet;
+    long count3 = 0;
+    for (long t = 0; t < ntet; ++t) count3 += tag[t] >= 3;
+    if (condflag == 1) {
+      AFEM_REQUIRE(sigma_file && nphys2 == count3, AFEM_EINVAL,
+                   "set_cond: nphys2 differs from the number of tetrahedra with tag >= 3 (SETNPHYS1INDEX2COND)");
+    }
+    const long nphys1 = ntet - count3;
+    std::vector<double> sig(ntet);
+    for (long t = 0; t < ntet; ++t) {
+      const int j = tag[t];
+      if (j == 1) sig[t] = sigma_air;
+      else if (j == 2) sig[t] = sigma_ocean;
+      else if (j >= 3) {
+        if (condflag == 0) {
+          AFEM_REQUIRE(sigma_land && j - 1 <= nvolume, AFEM_EINVAL, "set_cond: tag beyond nvolume + 1");
+          sig[t] = sigma_land[j - 2];
+        } else {
+          AFEM_REQUIRE(t >= nphys1, AFEM_EINVAL, "set_cond: land tetrahedra must come last (sigma(iele - nphys1))");
+          sig[t] = sigma_file[t - nphys1];
+        }
+      } else {
+        throw Error{AFEM_EINVAL, "set_cond: tetrahedron tag < 1 selects no conductivity"};
+      }
+    }
+    c->sigma.upload(sig.data(), ntet, c->stream);
+    AFEM_CUDA(cudaStreamSynchronize(c->stream));
+    c->sigma_set = true;
+    invalidate_assembly(c);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_set_sigma(afem_ctx* c, const double* sigma_tet) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(c->ntet > 0 && sigma_tet, AFEM_EINVAL, "set_sigma: set the mesh first / null array");
+    c->sigma.upload(sigma_tet, c->ntet, c->stream);
+    AFEM_CUDA(cudaStreamSynchronize(c->stream));
+    c->sigma_set = true;
+    invalidate_assembly(c);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_set_source(afem_ctx* c, int isrc, int nodes, const double* F, const double* v) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(c->node > 0, AFEM_ESTATE, "set_source: set the mesh first");
+    AFEM_REQUIRE(isrc >= 0 && isrc < 16, AFEM_EINVAL, "set_source: isrc must be 0..15");
+    AFEM_REQUIRE(nodes >= 0 && nodes <= c->node, AFEM_EINVAL, "set_source: nodes must be 0..node");
+    AFEM_REQUIRE(nodes == 0 || (F && v), AFEM_EINVAL, "set_source: null F or v");
+    if ((int)c->src.size() <= isrc) c->src.resize(isrc + 1, nullptr);
+    if (!c->src[isrc]) c->src[isrc] = new afem::SourceSet();
+    afem::SourceSet* S = c->src[isrc];
+    S->nodes = nodes;
+    S->F.upload(F, 3L * nodes, c->stream);
+    S->v.upload(reinterpret_cast<const double2*>(v), 3L * nodes, c->stream);
+    AFEM_CUDA(cudaStreamSynchronize(c->stream));
+    invalidate_assembly(c);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_set_bounds(afem_ctx* c, double zmin, double zmax, double xout, double yout) {
+  return guarded(c, [&]() {
+    c->zmin = zmin; c->zmax = zmax; c->xout = xout; c->yout = yout;
+    c->bounds_set = true;
+    invalidate_assembly(c);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_assemble(afem_ctx* c) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(c->pattern_ready, AFEM_ESTATE, "assemble: set the mesh first");
+    afem::reset_status(c);
+    afem::assemble_device(c);
+    afem::invalidate_work(c);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_export_system(afem_ctx* c, double freq, int isrc, int* n_out, long* iau_tot, int32_t* INU, int32_t* IAU,
+                       int32_t* INL, int32_t* IAL, double* D, double* AU, double* AL, double* b, uint8_t* bc) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(c->pattern_ready, AFEM_ESTATE, "export: no pattern");
+    const int n = c->nline;
+    cudaStream_t s = c->stream;
+    std::vector<int32_t> rp(n + 1), cl(c->nnz), dp(n);
+    c->rowptr.download(rp.data(), n + 1, s);
+    c->col.download(cl.data(), c->nnz, s);
+    c->diagpos.download(dp.data(), n, s);
+    std::vector<double2> km;
+    std::vector<double2> rh;
+    if (c->assembled) {
+      km.resize(c->nnz);
+      c->km.download(km.data(), c->nnz, s);
+      AFEM_REQUIRE(isrc >= 0 && isrc < c->rhs_nsrc, AFEM_EINVAL, "export: isrc out of range");
+      rh.resize(n);
+      AFEM_CUDA(cudaMemcpyAsync(rh.data(), c->rhs.p + (long)isrc * n, sizeof(double2) * n, cudaMemcpyDeviceToHost, s));
+      if (bc) c->bc.download(bc, n, s);
+    } else {
+      AFEM_REQUIRE(!(D || AU || AL || b || bc), AFEM_ESTATE, "export: values requested before assembly");
+    }
+    AFEM_CUDA(cudaStreamSynchronize(s));
+    const double omega = 2.0 * (4.0 * std::atan(1.0)) * freq;
+    long tot = 0;
+    for (int i = 0; i < n; ++i) tot += rp[i + 1] - dp[i] - 1;
+    if (n_out) *n_out = n;
+    if (iau_tot) *iau_tot = tot;
+    long pu = 0, pl = 0;
+    if (INU) INU[0] = 0;
+    if (INL) INL[0] = 0;
+    for (int i = 0; i < n; ++i) {
+      for (int k = rp[i]; k < rp[i + 1]; ++k) {
+        const int j = cl[k];
+        double re = 0, im = 0;
+        if (!km.empty()) { re = km[k].x; im = omega * km[k].y; }
+        if (j < i) {
+          if (IAL) IAL[pl] = j + 1;
+          if (AL) { AL[2 * pl] = re; AL[2 * pl + 1] = im; }
+          ++pl;
+        } else if (j > i) {
+          if (IAU) IAU[pu] = j + 1;
+          if (AU) { AU[2 * pu] = re; AU[2 * pu + 1] = im; }
+          ++pu;
+        } else if (D) {
+          D[2 * i] = re; D[2 * i + 1] = im;
+        }
+      }
+      if (INU) INU[i + 1] = (int32_t)pu;
+      if (INL) INL[i + 1] = (int32_t)pl;
+      if (b && !rh.empty()) { b[2 * i] = rh[i].x; b[2 * i + 1] = rh[i].y; }
+    }
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_solve(afem_ctx* c, int nsys, const double* freq, const int* src, const afem_solve_opts* opts,
+               afem_solve_stats* stats) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(freq && opts, AFEM_EINVAL, "solve: null freq or opts");
+    AFEM_REQUIRE(opts->precond >= 0 && opts->precond <= 3, AFEM_EINVAL, "solve: unknown preconditioner");
+    afem::reset_status(c);
+    return afem::solve_device(c, nsys, freq, src, opts, stats);
+  });
+}
+
+int afem_get_solution(afem_ctx* c, int k, double* x) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(k >= 0 && k < c->nsys && x, AFEM_EINVAL, "get_solution: no such system");
+    // stored [row][system]
+    std::vector<double2> all((size_t)c->nline * c->nsys);
+    c->X.download(all.data(), all.size(), c->stream);
+    AFEM_CUDA(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < c->nline; ++i) {
+      x[2 * i] = all[(size_t)i * c->nsys + k].x;
+      x[2 * i + 1] = all[(size_t)i * c->nsys + k].y;
+    }
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_sites(afem_ctx* c, int nobs, const double* xyz_obs, double* out) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(nobs > 0 && xyz_obs && out, AFEM_EINVAL, "sites: empty or null");
+    afem::reset_status(c);
+    afem::sites_device(c, nobs, xyz_obs, out);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_site_coeffs(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item, double* val_e, double* val_f,
+                     int32_t* iele) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(nobs > 0 && xyz_obs, AFEM_EINVAL, "site_coeffs: empty or null");
+    AFEM_REQUIRE(c->ntet > 0 && c->nline > 0, AFEM_ESTATE, "site_coeffs: no mesh");
+    afem::reset_status(c);
+    afem::site_coeffs_device(c, nobs, xyz_obs, item, val_e, val_f, iele);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_set_profiling(afem_ctx* c, int enable) {
+  return guarded(c, [&]() {
+    c->prof.on = enable != 0;
+    c->prof.e.clear();
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_profile_count(afem_ctx* c) { return c ? (int)c->prof.e.size() : 0; }
+
+int afem_profile_entry(afem_ctx* c, int i, char* name, int cap, double* ms, long* launches) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(i >= 0 && i < (int)c->prof.e.size(), AFEM_EINVAL, "profile_entry: index out of range");
+    const afem::ProfEntry& e = c->prof.e[i];
+    if (name && cap > 0) {
+      std::strncpy(name, e.name.c_str(), cap - 1);
+      name[cap - 1] = 0;
+    }
+    if (ms) *ms = e.ms;
+    if (launches) *launches = e.launches;
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_load_ctl(afem_ctx* c, const char* path) {
+  return guarded(c, [&]() { return afem::load_ctl(c, path); });
+}
+
+int afem_ctl_info(afem_ctx* c, int* nfreq, double* freq, int* nobs, double* xyz) {
+  return guarded(c, [&]() { return afem::ctl_info(c, nfreq, freq, nobs, xyz); });
+}
+
+int afem_run_ctl(afem_ctx* c, const afem_solve_opts* o) {
+  return guarded(c, [&]() { return afem::run_ctl(c, o); });
+}
+
+}  // extern "C"

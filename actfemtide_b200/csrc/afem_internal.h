@@ -1,0 +1,241 @@
+// Internal declarations shared by the translation units of libactfem_gpu.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/afem.h"
+
+namespace afem {
+
+// ---------------------------------------------------------------- errors
+struct Error {
+  int code;
+  std::string msg;
+};
+
+#define AFEM_CUDA(call)                                                                       \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      throw ::afem::Error{AFEM_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)};   \
+  } while (0)
+
+#define AFEM_REQUIRE(cond, code, msg)                 \
+  do {                                                \
+    if (!(cond)) throw ::afem::Error{(code), (msg)};  \
+  } while (0)
+
+// ---------------------------------------------------------------- device buffer
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count == n && p) return;
+    release();
+    if (count == 0) return;
+    AFEM_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void upload(const T* h, size_t count, cudaStream_t s) {
+    alloc(count);
+    if (count) AFEM_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void download(T* h, size_t count, cudaStream_t s) const {
+    if (count) AFEM_CUDA(cudaMemcpyAsync(h, p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+  }
+  void zero(cudaStream_t s) {
+    if (n) AFEM_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// Error / status words written by kernels (never trap).
+enum DevErr : int {
+  DEV_OK = 0,
+  DEV_VOLUME = 1,      // non-positive volume
+  DEV_ROWLEN = 2,      // row longer than the kernel's limit
+  DEV_TIMEOUT = 3,     // bounded wait expired
+  DEV_NOTFOUND = 4,    // id missing (edge search / pattern slot)
+  DEV_DEGREE = 5,      // adjacency longer than the kernel's limit
+  DEV_NOSIGMA = 6      // tetrahedron tag selects no conductivity
+};
+
+struct DevStatus {
+  int code;   // first DevErr raised
+  int where;  // kernel-specific index (0-based row / tet) of the first error
+  int aux;
+  int pad;
+};
+
+// ---------------------------------------------------------------- limits
+constexpr int ROW_MAX = 64;      // maximum nonzeros of one matrix row (diagonal included)
+constexpr int EDGE_DEG_MAX = 64; // maximum tetrahedra sharing one edge
+constexpr int NODE_DEG_MAX = 100;// maximum tetrahedra sharing one node (MKLINE_V2 maxnele)
+constexpr int NODE_NBR_MAX = 128;// maximum edges leaving one node towards larger ids
+
+struct SourceSet {
+  int nodes = 0;
+  DBuf<double> F;   // 3*nodes
+  DBuf<double2> v;  // 3*nodes
+};
+
+struct CtlInfo;  // drop-in driver state (afem_io.cpp)
+
+// Per-kernel device time accumulated with CUDA events while profiling is on.
+struct ProfEntry {
+  std::string name;
+  double ms = 0.0;
+  long launches = 0;
+};
+struct Profile {
+  bool on = false;
+  std::vector<ProfEntry> e;
+  void add(const char* name, double ms, long n = 1) {
+    for (auto& x : e)
+      if (x.name == name) { x.ms += ms; x.launches += n; return; }
+    e.push_back(ProfEntry{name, ms, n});
+  }
+};
+
+struct SolverWork;  // afem_solver.cu
+
+}  // namespace afem
+
+struct afem_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int num_sms = 0;
+
+  // mesh
+  int node = 0, ntet = 0, nline = 0;
+  afem::DBuf<double> xyz;      // 3*node
+  afem::DBuf<int32_t> n4;      // 4*ntet, 1-based
+  afem::DBuf<int32_t> tag;     // ntet
+  std::vector<int32_t> h_tag;  // host copy of the tags (conductivity selection)
+  afem::DBuf<int32_t> line;    // 2*nline, 1-based
+  afem::DBuf<int32_t> n6line;  // 6*ntet, signed 1-based
+
+  // conductivity
+  afem::DBuf<double> sigma;  // ntet
+  bool sigma_set = false;
+
+  // sources
+  std::vector<afem::SourceSet*> src;
+
+  // Dirichlet bounds
+  double zmin = 0, zmax = 0, xout = 0, yout = 0;
+  bool bounds_set = false;
+
+  // pattern (full CSR, sorted columns, 0-based)
+  long nnz = 0;
+  afem::DBuf<int32_t> rowptr;   // nline+1
+  afem::DBuf<int32_t> col;      // nnz
+  afem::DBuf<int32_t> diagpos;  // nline
+  afem::DBuf<int32_t> etp;      // nline+1, edge -> (tet, local edge) adjacency
+  afem::DBuf<int32_t> etl;      // 6*ntet, value = tet*8 + local edge, ascending per edge
+  bool pattern_ready = false;
+
+  // values: A(omega) = K + i*omega*M, stored interleaved (K_k, M_k)
+  afem::DBuf<double2> km;       // nnz
+  afem::DBuf<uint8_t> bc;       // nline Dirichlet flags
+  afem::DBuf<double2> rhs;      // nline * nsrc
+  int rhs_nsrc = 0;
+  bool assembled = false;
+
+  // solutions of the last solve: x[k*nline + i]
+  afem::DBuf<double2> X;
+  std::vector<double> sol_freq;
+  int nsys = 0;
+
+  afem::SolverWork* work = nullptr;
+  afem::CtlInfo* ctl = nullptr;
+
+  afem::DBuf<afem::DevStatus> status;  // one status word
+  afem::Profile prof;
+};
+
+namespace afem {
+
+// afem_mesh.cu
+void build_lines_device(afem_ctx* c);     // MKLINE_V2 + MKN6 on the device
+void build_pattern_device(afem_ctx* c);   // adjacency + full CSR pattern
+void exclusive_scan(const int32_t* in, int32_t* out, int n, cudaStream_t s, long* total_host);
+
+// afem_assemble.cu
+void assemble_device(afem_ctx* c);        // K, M, rhs, bc (GENMAT + COPY_UL + GENBCCSEM + SET_BC)
+
+// afem_solver.cu
+int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, const afem_solve_opts* o,
+                 afem_solve_stats* st);
+void destroy_work(afem_ctx* c);
+void invalidate_work(afem_ctx* c);      // values changed: drop derived copies (FP32 matrix)
+
+// afem_sites.cu
+void site_coeffs_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item, double* val_e, double* val_f,
+                        int32_t* iele);
+void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out);
+
+// status helpers
+void reset_status(afem_ctx* c);
+void check_status(afem_ctx* c, const char* what);
+
+// afem_io.cpp
+int load_ctl(afem_ctx* c, const char* path);
+int ctl_info(afem_ctx* c, int* nfreq, double* freq, int* nobs, double* xyz);
+int run_ctl(afem_ctx* c, const afem_solve_opts* o);
+void destroy_ctl(afem_ctx* c);
+
+}  // namespace afem
+
+// ---------------------------------------------------------------- device helpers
+#ifdef __CUDACC__
+namespace afem {
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cscale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+// Smith's algorithm (R. L. Smith, CACM 5(8), 1962) for a / b.
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+  if (fabs(b.x) >= fabs(b.y)) {
+    double r = b.y / b.x, den = b.x + b.y * r;
+    return make_double2((a.x + a.y * r) / den, (a.y - a.x * r) / den);
+  } else {
+    double r = b.x / b.y, den = b.x * r + b.y;
+    return make_double2((a.x * r + a.y) / den, (a.y * r - a.x) / den);
+  }
+}
+
+__device__ __forceinline__ void raise_status(DevStatus* st, int code, int where) {
+  if (atomicCAS(&st->code, 0, code) == 0) st->where = where;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+}  // namespace afem
+#endif

@@ -1,0 +1,520 @@
+// Drop-in driver: the reference's forward ctl file and the files it names.
+//
+// Reference: src/common/m_param.f90:145-446 (readparam), :449-485 (READCOND),
+// :939-999 (readcontrolfile / subtractcommentout); src/common/
+// m_mesh_type.f90:379-468 (readmsh2); src/common/m_line_type.f90:28-48
+// (READLINE); src/src_tide/m_readfvxyz.f90:7-62 (readfxyz / readvxyz);
+// src/solver_mpi/n_ebfem_bxyz_mpi.f90:55-183 (driver), :937-1030
+// (PREPZSRCOBS), :470-527 (SETNPHYS1INDEX2COND), :570-626 (CALOBSRESP);
+// src/common/m_outresp.f90:221-262 (OUTOBSFILESFWD).
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "afem_internal.h"
+
+namespace afem {
+
+struct CtlInfo {
+  std::string dir;  // directory of the ctl file (relative paths resolve against the working directory, as in Fortran)
+  std::string g_meshfile, z_meshfile, lineinfofile, ocean_meshfile, meshctlfile, vxyz_file, fxyz_file,
+      outputfolder, header2d, header3d, condfile;
+  std::vector<double> freq;
+  double xbound[4] = {0, 0, 0, 0}, ybound[4] = {0, 0, 0, 0}, zbound[4] = {0, 0, 0, 0};
+  double lenout = 0, upzin = 0, downzin = 0, zmax = 0, zmin = 0;
+  int nobs = 0, lonlatflag = 2, ixyflag = 0, nsource = 0, condflag = 0, nvolume = 0;
+  double lonorigin = 0, latorigin = 0;
+  std::vector<std::string> obsname, sourcename;
+  std::vector<double> xyzobs;  // 3*nobs, after PREPZSRCOBS
+  double sigma_air = 1e-8;
+  std::vector<double> sigma_land;
+  int nodes = 0;
+};
+
+namespace {
+
+std::string rtrim(const std::string& s) {
+  size_t e = s.find_last_not_of(" \t\r\n");
+  return e == std::string::npos ? std::string() : s.substr(0, e + 1);
+}
+std::string ltrim(const std::string& s) {
+  size_t b = s.find_first_not_of(" \t\r\n");
+  return b == std::string::npos ? std::string() : s.substr(b);
+}
+std::string trim(const std::string& s) { return ltrim(rtrim(s)); }
+
+// Fortran list-directed tokens: blanks/commas separate; "(a,b)" is one complex item.
+std::vector<std::string> tokens(const std::string& line) {
+  std::vector<std::string> out;
+  size_t i = 0, n = line.size();
+  while (i < n) {
+    while (i < n && (line[i] == ' ' || line[i] == '\t' || line[i] == ',' || line[i] == '\r')) ++i;
+    if (i >= n) break;
+    if (line[i] == '/') break;  // list-directed terminator
+    size_t j = i;
+    if (line[i] == '(') {
+      while (j < n && line[j] != ')') ++j;
+      out.push_back(line.substr(i, j - i + 1));
+      i = j + 1;
+      continue;
+    }
+    if (line[i] == '\'' || line[i] == '"') {
+      char q = line[i];
+      j = i + 1;
+      while (j < n && line[j] != q) ++j;
+      out.push_back(line.substr(i + 1, j - i - 1));
+      i = j + 1;
+      continue;
+    }
+    while (j < n && line[j] != ' ' && line[j] != '\t' && line[j] != ',' && line[j] != '\r') ++j;
+    out.push_back(line.substr(i, j - i));
+    i = j;
+  }
+  return out;
+}
+
+double fnum(const std::string& t) {
+  std::string s = t;
+  for (auto& ch : s)
+    if (ch == 'd' || ch == 'D') ch = 'e';
+  char* end = nullptr;
+  double v = std::strtod(s.c_str(), &end);
+  if (end == s.c_str()) throw Error{AFEM_EIO, "cannot read a number from '" + t + "'"};
+  return v;
+}
+
+void fcomplex(const std::string& t, double* re, double* im) {
+  // "(re,im)"
+  std::string s = t;
+  if (s.size() < 5 || s.front() != '(' || s.back() != ')') throw Error{AFEM_EIO, "bad complex item '" + t + "'"};
+  s = s.substr(1, s.size() - 2);
+  size_t c = s.find(',');
+  if (c == std::string::npos) throw Error{AFEM_EIO, "bad complex item '" + t + "'"};
+  *re = fnum(trim(s.substr(0, c)));
+  *im = fnum(trim(s.substr(c + 1)));
+}
+
+// Sequential record reader over the ctl lines (after readcontrolfile's cut).
+struct Records {
+  std::vector<std::string> lines;
+  size_t pos = 0;
+  const std::string& next(const char* what) {
+    if (pos >= lines.size()) throw Error{AFEM_EIO, std::string("ctl file ends before ") + what};
+    return lines[pos++];
+  }
+  std::string str(const char* what) { return trim(next(what)); }          // '(a)' read, trimmed
+  std::string word(const char* what) {                                     // list-directed character item
+    auto t = tokens(next(what));
+    return t.empty() ? std::string() : t[0];
+  }
+  std::vector<double> nums(const char* what, size_t k) {
+    auto t = tokens(next(what));
+    if (t.size() < k) throw Error{AFEM_EIO, std::string("ctl: too few values for ") + what};
+    std::vector<double> v(k);
+    for (size_t i = 0; i < k; ++i) v[i] = fnum(t[i]);
+    return v;
+  }
+  double num(const char* what) { return nums(what, 1)[0]; }
+  void skip(const char* what) { next(what); }
+};
+
+// readcontrolfile + subtractcommentout (m_param.f90:939-999): drop "##"
+// lines, keep columns 21.. of the others.
+Records read_ctl_records(const std::string& path) {
+  std::ifstream f(path);
+  if (!f) throw Error{AFEM_EIO, "cannot open ctl file " + path};
+  Records r;
+  std::string line;
+  while (std::getline(f, line)) {
+    if (!line.empty() && line.back() == '\r') line.pop_back();
+    if (line.size() >= 2 && line[0] == '#' && line[1] == '#') continue;
+    r.lines.push_back(line.size() > 20 ? line.substr(20) : std::string());
+  }
+  return r;
+}
+
+struct Msh {
+  int node = 0;
+  std::vector<double> xyz;
+  std::vector<int32_t> n4, n4flag;  // n4flag: (physical, elementary) per tet
+  std::vector<int32_t> n3;          // triangles
+};
+
+// readmsh2 (m_mesh_type.f90:379-468): Gmsh 2.2 ASCII, two tags per element.
+Msh read_msh(const std::string& path, bool want_tets, bool want_tris) {
+  std::ifstream f(path);
+  if (!f) throw Error{AFEM_EIO, "cannot open mesh file " + path};
+  Msh m;
+  std::string line;
+  for (int i = 0; i < 4; ++i)
+    if (!std::getline(f, line)) throw Error{AFEM_EIO, "truncated mesh header in " + path};
+  if (!(f >> m.node)) throw Error{AFEM_EIO, "no node count in " + path};
+  m.xyz.resize(3L * m.node);
+  for (int i = 0; i < m.node; ++i) {
+    long id;
+    std::string a, b, c;
+    if (!(f >> id >> a >> b >> c)) throw Error{AFEM_EIO, "truncated node list in " + path};
+    m.xyz[3L * i] = fnum(a);
+    m.xyz[3L * i + 1] = fnum(b);
+    m.xyz[3L * i + 2] = fnum(c);
+  }
+  std::getline(f, line);
+  std::getline(f, line);  // $EndNodes
+  std::getline(f, line);  // $Elements
+  long nele = 0;
+  if (!(f >> nele)) throw Error{AFEM_EIO, "no element count in " + path};
+  static const int etype[16] = {0, 2, 3, 0, 4, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1};
+  for (long e = 0; e < nele; ++e) {
+    long id;
+    int itype, ntag, jj, kk;
+    if (!(f >> id >> itype >> ntag >> jj >> kk)) throw Error{AFEM_EIO, "truncated element list in " + path};
+    int nn = (itype >= 0 && itype < 16) ? etype[itype] : 0;
+    if (nn == 0) throw Error{AFEM_EIO, "unsupported element type in " + path};
+    int nd[4];
+    for (int k = 0; k < nn; ++k) f >> nd[k];
+    if (itype == 4 && want_tets) {
+      for (int k = 0; k < 4; ++k) m.n4.push_back(nd[k]);
+      m.n4flag.push_back(jj);
+      m.n4flag.push_back(kk);
+    } else if (itype == 2 && want_tris) {
+      for (int k = 0; k < 3; ++k) m.n3.push_back(nd[k]);
+    }
+  }
+  return m;
+}
+
+int count_msh_nodes(const std::string& path) {
+  std::ifstream f(path);
+  if (!f) throw Error{AFEM_EIO, "cannot open mesh file " + path};
+  std::string line;
+  for (int i = 0; i < 4; ++i) std::getline(f, line);
+  int n = 0;
+  if (!(f >> n)) throw Error{AFEM_EIO, "no node count in " + path};
+  return n;
+}
+
+// READLINE (m_line_type.f90:28-48)
+void read_lineinfo(const std::string& path, std::vector<int32_t>& line, std::vector<int32_t>& n6, int& nline,
+                   int& ntet) {
+  std::ifstream f(path);
+  if (!f) throw Error{AFEM_EIO, "cannot open line file " + path};
+  if (!(f >> nline)) throw Error{AFEM_EIO, "no nline in " + path};
+  line.resize(2L * nline);
+  for (long i = 0; i < 2L * nline; ++i)
+    if (!(f >> line[i])) throw Error{AFEM_EIO, "truncated line list in " + path};
+  if (!(f >> ntet)) throw Error{AFEM_EIO, "no ntet in " + path};
+  n6.resize(6L * ntet);
+  for (long i = 0; i < 6L * ntet; ++i)
+    if (!(f >> n6[i])) throw Error{AFEM_EIO, "truncated n6line in " + path};
+}
+
+// readfxyz / readvxyz (m_readfvxyz.f90:7-62): first `nodes` records.
+void read_fv(const std::string& fpath, const std::string& vpath, int nodes, std::vector<double>& F,
+             std::vector<double>& v) {
+  F.assign(3L * nodes, 0.0);
+  v.assign(6L * nodes, 0.0);
+  std::ifstream ff(fpath), fv(vpath);
+  if (!ff) throw Error{AFEM_EIO, "cannot open " + fpath};
+  if (!fv) throw Error{AFEM_EIO, "cannot open " + vpath};
+  std::string line;
+  for (int i = 0; i < nodes; ++i) {
+    if (!std::getline(ff, line)) throw Error{AFEM_EIO, "fxyz file has fewer than nodes records"};
+    auto t = tokens(line);
+    if (t.size() < 6) throw Error{AFEM_EIO, "fxyz record with fewer than 6 values"};
+    for (int c = 0; c < 3; ++c) F[3L * i + c] = fnum(t[3 + c]);
+  }
+  for (int i = 0; i < nodes; ++i) {
+    if (!std::getline(fv, line)) throw Error{AFEM_EIO, "vxyz file has fewer than nodes records"};
+    auto t = tokens(line);
+    if (t.size() < 5) throw Error{AFEM_EIO, "vxyz record with fewer than 5 values"};
+    fcomplex(t[3], &v[6L * i + 0], &v[6L * i + 1]);
+    fcomplex(t[4], &v[6L * i + 2], &v[6L * i + 3]);
+    v[6L * i + 4] = 0.0;
+    v[6L * i + 5] = 0.0;
+  }
+}
+
+// READCOND (m_param.f90:449-485): 11 header lines, nphys2, then "index rho".
+void read_cond(const std::string& path, std::vector<double>& sigma) {
+  std::ifstream f(path);
+  if (!f) throw Error{AFEM_EIO, "cannot open cond file " + path};
+  std::string line;
+  for (int i = 0; i < 11; ++i)
+    if (!std::getline(f, line)) throw Error{AFEM_EIO, "truncated cond header in " + path};
+  int nphys2 = 0;
+  if (!(f >> nphys2)) throw Error{AFEM_EIO, "no nphys2 in " + path};
+  sigma.assign(nphys2, -9999.0);
+  for (int i = 0; i < nphys2; ++i) {
+    long idx;
+    std::string r;
+    if (!(f >> idx >> r)) throw Error{AFEM_EIO, "truncated cond list in " + path};
+    const double rho = fnum(r);
+    if (std::fabs(rho) > 1e-10) sigma[i] = 1.0 / rho;
+  }
+}
+
+// PREPZSRCOBS (n_ebfem_bxyz_mpi.f90:976-998) with findtri's barycentrics
+// (m_triangle.f90:133-260): z += surface height interpolated in the first
+// triangle (id order) that contains (x, y).  The reference visits candidate
+// triangles bucket by bucket; on a shared edge both triangles give the same
+// height up to rounding.
+void lift_sites(const Msh& h, std::vector<double>& xyzobs) {
+  const long ntri = (long)h.n3.size() / 3;
+  const int nobs = (int)xyzobs.size() / 3;
+  for (int s = 0; s < nobs; ++s) {
+    const double x = xyzobs[3 * s], y = xyzobs[3 * s + 1];
+    bool found = false;
+    for (long t = 0; t < ntri && !found; ++t) {
+      const double* p[3];
+      for (int j = 0; j < 3; ++j) p[j] = &h.xyz[3L * (h.n3[3 * t + j] - 1)];
+      const double x12[2] = {p[1][0] - p[0][0], p[1][1] - p[0][1]};
+      const double x13[2] = {p[2][0] - p[0][0], p[2][1] - p[0][1]};
+      const double x23[2] = {p[2][0] - p[1][0], p[2][1] - p[1][1]};
+      const double v1[2] = {x - p[0][0], y - p[0][1]};
+      const double v2[2] = {x - p[1][0], y - p[1][1]};
+      const double a0 = (x13[0] * x12[1] - x13[1] * x12[0]);
+      double a[3];
+      a[1] = (x13[0] * v1[1] - x13[1] * v1[0]) / a0;
+      a[2] = (v1[0] * x12[1] - v1[1] * x12[0]) / a0;
+      a[0] = (v2[0] * x23[1] - v2[1] * x23[0]) / a0;
+      if (a[0] >= 0.0 && a[1] >= 0.0 && a[2] >= 0.0) {
+        xyzobs[3 * s + 2] = a[0] * p[0][2] + a[1] * p[1][2] + a[2] * p[2][2] + xyzobs[3 * s + 2];
+        found = true;
+      }
+    }
+    if (!found) throw Error{AFEM_EIO, "site outside the surface mesh (PREPZSRCOBS)"};
+  }
+}
+
+// Fortran Gw.d edit descriptor (G15.7 of OUTOBSFILESFWD) for finite values.
+std::string fortran_g(double x, int w, int d) {
+  char buf[64];
+  const double ax = std::fabs(x);
+  if (x == 0.0) {
+    std::snprintf(buf, sizeof(buf), "%*.*f%*s", w - 4, d - 1, 0.0, 4, "");
+    return buf;
+  }
+  // F editing when 0.1 - 0.5e-(d+1) <= |x| < 10^d - 0.5
+  if (ax >= 0.1 - 0.5 * std::pow(10.0, -(d + 1)) && ax < std::pow(10.0, d) - 0.5) {
+    int k = 0;
+    // smallest k with |x| < 10^k - 0.5*10^(k-d)
+    for (k = 0; k <= d; ++k)
+      if (ax < std::pow(10.0, k) - 0.5 * std::pow(10.0, k - d)) break;
+    std::snprintf(buf, sizeof(buf), "%*.*f%*s", w - 4, d - k, x, 4, "");
+    return buf;
+  }
+  // Ew.d: [-]0.ddddddE+ee
+  int e10 = (int)std::floor(std::log10(ax)) + 1;
+  double mant = ax / std::pow(10.0, e10);
+  double r = std::round(mant * std::pow(10.0, d)) / std::pow(10.0, d);
+  if (r >= 1.0) { r /= 10.0; e10 += 1; }
+  char mb[32];
+  std::snprintf(mb, sizeof(mb), "%.*f", d, r);  // "0.ddddddd"
+  char eb[16];
+  std::snprintf(eb, sizeof(eb), "E%c%02d", e10 < 0 ? '-' : '+', std::abs(e10));
+  std::string s = std::string(x < 0 ? "-" : "") + mb + eb;
+  if ((int)s.size() < w) s = std::string(w - s.size(), ' ') + s;
+  return s;
+}
+
+}  // namespace
+
+int load_ctl(afem_ctx* c, const char* path) {
+  AFEM_REQUIRE(path, AFEM_EINVAL, "load_ctl: null path");
+  destroy_ctl(c);
+  CtlInfo* ci = new CtlInfo();
+  c->ctl = ci;
+  Records r = read_ctl_records(path);
+  const int itopoflag = (int)r.num("itopoflag");
+  if (itopoflag == 1) {
+    const int nfile = (int)r.num("nfile");
+    for (int i = 0; i < nfile; ++i) {
+      r.skip("topofile");
+      r.skip("lonlatshift");
+    }
+  } else if (itopoflag != 0) {
+    throw Error{AFEM_EIO, "ctl: itopoflag should be 0 or 1"};
+  }
+  ci->g_meshfile = r.str("mesh file");
+  ci->z_meshfile = r.str("2d triangle z file");
+  ci->lineinfofile = r.str("line file");
+  ci->ocean_meshfile = r.str("ocean mesh file");
+  ci->meshctlfile = r.str("mesh ctl file");
+  ci->vxyz_file = r.str("vxyz file");
+  ci->fxyz_file = r.str("fxyz file");
+  ci->outputfolder = r.str("output folder");
+  ci->header2d = r.str("header2d");
+  ci->header3d = r.str("header3d");
+  const int nfreq = (int)r.num("nfreq");
+  for (int i = 0; i < nfreq; ++i) ci->freq.push_back(r.num("frequency"));
+  ci->xbound[1] = r.num("west bound");
+  ci->xbound[2] = r.num("east bound");
+  ci->ybound[1] = r.num("south bound");
+  ci->ybound[2] = r.num("north bound");
+  ci->lenout = r.num("lenout");
+  ci->upzin = r.num("upzin");
+  ci->downzin = r.num("downzin");
+  ci->zmax = r.num("zmax");
+  ci->zmin = r.num("zmin");
+  for (int i = 0; i < 7; ++i) r.skip("mesh size / obs / source parameters");
+  // zbound / xbound / ybound (m_param.f90:259-264)
+  ci->zbound[0] = ci->zmin; ci->zbound[1] = ci->downzin; ci->zbound[2] = ci->upzin; ci->zbound[3] = ci->zmax;
+  ci->xbound[0] = ci->xbound[1] - ci->lenout;
+  ci->xbound[3] = -ci->xbound[0];
+  ci->ybound[0] = ci->ybound[1] - ci->lenout;
+  ci->ybound[3] = -ci->ybound[0];
+  ci->nobs = (int)r.num("nobs");
+  ci->lonlatflag = (int)r.num("lonlatflag");
+  if (ci->lonlatflag == 1) throw Error{AFEM_EIO, "ctl: lonlatflag 1 (UTM sites) is not supported; give xyz (2) or local lon/lat (0)"};
+  r.skip("UTM zone line");
+  auto org = r.nums("lonlatorigin", 2);
+  ci->lonorigin = org[0];
+  ci->latorigin = org[1];
+  const double pi = 4.0 * std::atan(1.0), d2r = pi / 180.0, radius = 6371.2;
+  for (int i = 0; i < ci->nobs; ++i) {
+    ci->obsname.push_back(r.str("site name"));
+    auto v = r.nums("site coordinates", 3);
+    if (ci->lonlatflag == 0) {
+      ci->xyzobs.push_back((v[0] - ci->lonorigin) * d2r * radius * std::cos(ci->latorigin * d2r));
+      ci->xyzobs.push_back((v[1] - ci->latorigin) * d2r * radius);
+      ci->xyzobs.push_back(v[2]);
+    } else {
+      ci->xyzobs.insert(ci->xyzobs.end(), v.begin(), v.end());
+    }
+  }
+  ci->ixyflag = (int)r.num("ixyflag");
+  if (ci->ixyflag == 1) {
+    r.skip("xyfilehead");
+    r.skip("nx ny");
+    const int ixydepth = (int)r.num("ixydepth");
+    if (ixydepth == 1) r.skip("depth_xy");
+    r.skip("pokimsh");
+    r.skip("ki23dfile");
+  } else if (ci->ixyflag == 2) {
+    r.skip("xyfilehead");
+    r.skip("pokimsh");
+    r.skip("ki23dfile");
+  }
+  ci->nsource = (int)r.num("nsource");
+  for (int i = 0; i < ci->nsource; ++i) {
+    ci->sourcename.push_back(r.word("source name"));
+    r.skip("source start");
+    r.skip("source end");
+  }
+  r.skip("source current");
+  ci->sigma_air = r.num("sigma_air");
+  ci->condflag = (int)r.num("condflag");
+  std::vector<double> sigma_file;
+  if (ci->condflag == 0) {
+    ci->nvolume = (int)r.num("nvolume");
+    for (int i = 0; i < ci->nvolume; ++i) ci->sigma_land.push_back(r.num("sigma_land"));
+  } else if (ci->condflag == 1) {
+    ci->condfile = trim(r.next("condfile").substr(0, 50));
+    read_cond(ci->condfile, sigma_file);
+  } else {
+    throw Error{AFEM_EIO, "ctl: condflag should be 0 or 1"};
+  }
+  // mesh, surface, ocean node count, edges
+  Msh g = read_msh(ci->g_meshfile, true, false);
+  Msh h = read_msh(ci->z_meshfile, false, true);
+  ci->nodes = count_msh_nodes(ci->ocean_meshfile);
+  lift_sites(h, ci->xyzobs);
+  std::vector<int32_t> line, n6;
+  int nline = 0, ntet_l = 0;
+  read_lineinfo(ci->lineinfofile, line, n6, nline, ntet_l);
+  const int ntet = (int)g.n4.size() / 4;
+  AFEM_REQUIRE(ntet_l == ntet, AFEM_EIO, "lineinfo ntet differs from the mesh");
+  std::vector<int32_t> tag(ntet);
+  for (int t = 0; t < ntet; ++t) tag[t] = g.n4flag[2 * t + 1];  // n4flag(:,2): elementary tag
+  int rc = afem_set_mesh(c, g.node, g.xyz.data(), ntet, g.n4.data(), tag.data(), nline, line.data(), n6.data());
+  if (rc) throw Error{rc, c->err};
+  // GENMAT's ocean value is the default-real literal 3.33
+  rc = afem_set_cond(c, ci->sigma_air, (double)3.33f, ci->condflag, ci->nvolume,
+                     ci->sigma_land.empty() ? nullptr : ci->sigma_land.data(), (int)sigma_file.size(),
+                     sigma_file.empty() ? nullptr : sigma_file.data());
+  if (rc) throw Error{rc, c->err};
+  std::vector<double> F, v;
+  read_fv(ci->fxyz_file, ci->vxyz_file, ci->nodes, F, v);
+  rc = afem_set_source(c, 0, ci->nodes, F.data(), v.data());
+  if (rc) throw Error{rc, c->err};
+  // forward_bxyz: zmin = zbound(1), zmax = zbound(4), xout = xbound(4), yout = ybound(4)
+  rc = afem_set_bounds(c, ci->zbound[0], ci->zbound[3], ci->xbound[3], ci->ybound[3]);
+  if (rc) throw Error{rc, c->err};
+  return AFEM_OK;
+}
+
+int ctl_info(afem_ctx* c, int* nfreq, double* freq, int* nobs, double* xyz) {
+  AFEM_REQUIRE(c->ctl, AFEM_ESTATE, "ctl_info: no ctl loaded");
+  CtlInfo* ci = c->ctl;
+  if (nfreq) *nfreq = (int)ci->freq.size();
+  if (freq) std::memcpy(freq, ci->freq.data(), sizeof(double) * ci->freq.size());
+  if (nobs) *nobs = ci->nobs;
+  if (xyz) std::memcpy(xyz, ci->xyzobs.data(), sizeof(double) * ci->xyzobs.size());
+  return AFEM_OK;
+}
+
+// Frequency loop of n_ebfem_bxyz (n_ebfem_bxyz_mpi.f90:144-183): one forward
+// solve per frequency, CALOBSEBCOMP, then OUTOBSFILESFWD.  GENMAT fills
+// right-hand-side column 1 only, so sources 2..nsr have zero fields.
+int run_ctl(afem_ctx* c, const afem_solve_opts* o) {
+  AFEM_REQUIRE(c->ctl, AFEM_ESTATE, "run_ctl: no ctl loaded");
+  AFEM_REQUIRE(o, AFEM_EINVAL, "run_ctl: null options");
+  CtlInfo* ci = c->ctl;
+  int rc = afem_assemble(c);
+  if (rc) throw Error{rc, c->err};
+  const int nf = (int)ci->freq.size(), nobs = ci->nobs;
+  std::vector<double> amp((size_t)nf * 5 * nobs), ph((size_t)nf * 5 * nobs);
+  const double pi = 4.0 * std::atan(1.0), r2d = 180.0 / pi;
+  for (int i = 0; i < nf; ++i) {
+    if (ci->freq[i] < 0.0) continue;
+    afem_solve_stats st{};
+    rc = afem_solve(c, 1, &ci->freq[i], nullptr, o, &st);
+    if (rc) throw Error{rc, std::string("run_ctl: solve failed: ") + c->err};
+    std::vector<double> out(2L * 5 * nobs);
+    rc = afem_sites(c, nobs, ci->xyzobs.data(), out.data());
+    if (rc) throw Error{rc, c->err};
+    for (int comp = 0; comp < 5; ++comp)
+      for (int s = 0; s < nobs; ++s) {
+        const double re = out[2 * ((long)comp * nobs + s)], im = out[2 * ((long)comp * nobs + s) + 1];
+        amp[((size_t)i * 5 + comp) * nobs + s] = std::sqrt(std::pow(re, 2.0) + std::pow(im, 2.0));
+        ph[((size_t)i * 5 + comp) * nobs + s] = std::atan2(im, re) * r2d;
+      }
+  }
+  for (int l = 0; l < nobs; ++l)
+    for (int k = 0; k < ci->nsource; ++k) {
+      const std::string fn = rtrim(ci->outputfolder) + rtrim(ci->obsname[l]) + "_" + rtrim(ci->sourcename[k]) + ".dat";
+      FILE* f = std::fopen(fn.c_str(), "w");
+      if (!f) throw Error{AFEM_EIO, "cannot write " + fn};
+      for (int i = 0; i < nf; ++i) {
+        std::string row = fortran_g(ci->freq[i], 15, 7);
+        for (int comp = 0; comp < 5; ++comp) {
+          const double a = (k == 0) ? amp[((size_t)i * 5 + comp) * nobs + l] : 0.0;
+          const double p = (k == 0) ? ph[((size_t)i * 5 + comp) * nobs + l] : 0.0;
+          row += fortran_g(a, 15, 7) + fortran_g(p, 15, 7);
+        }
+        std::fprintf(f, "%s\n", row.c_str());
+      }
+      std::fclose(f);
+    }
+  return AFEM_OK;
+}
+
+void destroy_ctl(afem_ctx* c) {
+  delete c->ctl;
+  c->ctl = nullptr;
+}
+
+}  // namespace afem
+
+// Host-only helpers exported for the test-suite (no device work).
+extern "C" int afem_fortran_g(double x, int w, int d, char* out, int cap) {
+  std::string s = afem::fortran_g(x, w, d);
+  if ((int)s.size() + 1 > cap) return AFEM_EINVAL;
+  std::memcpy(out, s.c_str(), s.size() + 1);
+  return (int)s.size();
+}

@@ -1,0 +1,984 @@
+// Batched preconditioned COCG (COCG13_single) on the device.
+//
+// Reference: src/solver/COCG13_single.f90:9-340.  Per iteration the reference
+// does: z = M^-1 r (forward + backward sweep with DD), rho = r^T z, p = z +
+// (rho/rho1) p, q = A p, alpha = rho / p^T q, x += alpha p, r -= alpha q,
+// RESID = ||r|| / ||b||.  Here one iteration is four streaming kernels and
+// three single-block scalar kernels:
+//   k_fwd   : x += alpha p, r -= alpha q (previous iteration), ||r||^2, forward sweep
+//   k_scal_r: RESID, convergence / iteration cap / non-finite checks
+//   k_bwd   : backward sweep, rho = r^T z (unconjugated)
+//   k_scal_rho: beta = rho / rho1
+//   k_pupd  : p = z + beta p
+//   k_spmv  : q = A p, p^T q
+//   k_scal_pq: alpha = rho / p^T q, rho1 = rho, epoch++
+// Every kernel returns at once after the batch has finished, so a captured
+// chunk of iterations can run past convergence harmlessly.
+//
+// Storage: A(omega_s) = K + i omega_s M for system s; K and M are read once
+// per entry for all NS systems of a batch.  Vectors are laid out [row][system]
+// so the NS values of one row are contiguous.  A warp handles one row: lane =
+// g * NS + s works on system s and on entries g, g + G, ... (G = 32 / NS).
+//
+// The triangular sweeps are sync-free: each row waits (bounded) on a per-row
+// flag of every row it depends on.  Rows are statically interleaved over the
+// warps of a cooperative (co-resident) grid, each warp in increasing
+// dependency order, so the lowest unfinished row can always proceed.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "afem_internal.h"
+
+namespace afem {
+
+template <class T>
+struct Cx;
+template <>
+struct Cx<double> {
+  using V = double2;
+  __host__ __device__ static V make(double a, double b) { return make_double2(a, b); }
+};
+template <>
+struct Cx<float> {
+  using V = float2;
+  __host__ __device__ static V make(float a, float b) { return make_float2(a, b); }
+};
+
+constexpr int MAX_NS = 16;
+constexpr unsigned SPIN_LIMIT = 1u << 24;
+
+// per-system scalars (always FP64)
+struct SysScal {
+  double2 rho, rho1, alpha, beta, pq;
+  double rr, bnrm2, resid, omega;
+  int active;     // 1 while iterating
+  int status;     // afem_status of this system
+  int iter;       // iterations done
+  int pad;
+};
+
+struct Ctrl {
+  unsigned epoch;  // flag generation, increases by one per sweep pair, never reset
+  int done;        // all systems finished
+  int iter;        // iterations of the current inner solve
+  int maxit;
+  double tol;
+};
+
+struct SolverWork {
+  int n = 0, ns = 0, prec_bits = 64;
+  int nblocks = 0;  // persistent grid size (blocks of 256 threads)
+  DBuf<double2> x, b;               // FP64 solution and right-hand side [row][sys]
+  DBuf<double2> r64;                // FP64 true residual
+  DBuf<double2> r, z, p, q, dd;     // FP64 inner vectors
+  DBuf<float2> rf, zf, pf, qf, ddf; // FP32 inner vectors
+  DBuf<float2> kmf;                 // FP32 copy of (K, M)
+  bool kmf_valid = false;
+  DBuf<unsigned> flag_f, flag_b;
+  DBuf<double> part;                // partial sums [block][sys][4]
+  DBuf<SysScal> sc;
+  DBuf<Ctrl> ctrl;
+  Ctrl* h_ctrl = nullptr;           // pinned mirror
+  SysScal* h_sc = nullptr;          // pinned mirror
+  unsigned epoch_host = 0;
+  ~SolverWork() {
+    if (h_ctrl) cudaFreeHost(h_ctrl);
+    if (h_sc) cudaFreeHost(h_sc);
+  }
+};
+
+namespace {
+
+__device__ __forceinline__ bool wait_flag(const unsigned* f, unsigned epoch, DevStatus* st, int row) {
+  if (ld_acquire(f) >= epoch) return true;
+  unsigned spins = 0;
+  for (;;) {
+    if (ld_acquire(f) >= epoch) return true;
+    ++spins;
+    if (spins > 32) __nanosleep(spins > 4096 ? 256 : 32);
+    if ((spins & 255) == 0 && *(volatile int*)&st->code == DEV_TIMEOUT) return false;
+    if (spins > SPIN_LIMIT) {
+      raise_status(st, DEV_TIMEOUT, row);
+      return false;
+    }
+  }
+}
+
+template <class V>
+__device__ __forceinline__ V ldcg(const V* p);
+template <>
+__device__ __forceinline__ double2 ldcg<double2>(const double2* p) { return __ldcg(p); }
+template <>
+__device__ __forceinline__ float2 ldcg<float2>(const float2* p) { return __ldcg(p); }
+
+template <class T>
+__device__ __forceinline__ T shfl_xor(T v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+
+// Reduce complex (t1, t2) over the G lane groups of a warp (lanes differing in g).
+template <class T, int NS>
+__device__ __forceinline__ void group_reduce(T& a, T& b, T& c, T& d) {
+#pragma unroll
+  for (int m = NS; m < 32; m <<= 1) {
+    a += shfl_xor(a, m);
+    b += shfl_xor(b, m);
+    c += shfl_xor(c, m);
+    d += shfl_xor(d, m);
+  }
+}
+
+// Block-reduce NS-per-lane doubles into part[blockIdx][s*4 + slot]; lanes with g == 0 hold system s values.
+template <int NS, int NVAL>
+__device__ __forceinline__ void block_partials(const double (&v)[NVAL], double* part) {
+  __shared__ double red[8][32][NVAL];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < NVAL; ++k) red[w][lane][k] = v[k];
+  __syncthreads();
+  if (threadIdx.x < NS) {
+    const int s = threadIdx.x;
+    double acc[NVAL];
+#pragma unroll
+    for (int k = 0; k < NVAL; ++k) acc[k] = 0.0;
+    for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww)
+#pragma unroll
+      for (int k = 0; k < NVAL; ++k) acc[k] += red[ww][s][k];
+#pragma unroll
+    for (int k = 0; k < NVAL; ++k) part[((long)blockIdx.x * MAX_NS + s) * 4 + k] = acc[k];
+  }
+}
+
+// ------------------------------------------------------------------ forward sweep
+// For iteration > 1 first applies the previous update to the row, then
+// y_i = (r_i - sum_{j<i} A_ij y_j) * DD_i  (COCG13_single.f90:203-212, 304-307).
+template <class T, int NS>
+__global__ void __launch_bounds__(256)
+    k_fwd(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const int32_t* __restrict__ diagpos,
+          const typename Cx<T>::V* __restrict__ km, int n, typename Cx<T>::V* __restrict__ r,
+          typename Cx<T>::V* __restrict__ y, const typename Cx<T>::V* __restrict__ p,
+          const typename Cx<T>::V* __restrict__ q, double2* __restrict__ x, const typename Cx<T>::V* __restrict__ dd,
+          unsigned* __restrict__ flag, int mode, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl,
+          double* __restrict__ part, DevStatus* st) {
+  using V = typename Cx<T>::V;
+  if (ctrl->done) return;
+  constexpr int G = 32 / NS;
+  const unsigned epoch = ctrl->epoch;
+  const bool update = ctrl->iter > 0;
+  const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const double om = sc[s].omega;
+  const double2 al = sc[s].alpha;
+  const bool act = sc[s].active;
+  double rr = 0.0;
+  for (int row = warp; row < n; row += nwarps) {
+    V ri = r[(long)row * NS + s];
+    if (update && act && g == 0) {
+      const V qi = q[(long)row * NS + s], pi = p[(long)row * NS + s];
+      ri = Cx<T>::make((T)((double)ri.x - (al.x * (double)qi.x - al.y * (double)qi.y)),
+                       (T)((double)ri.y - (al.x * (double)qi.y + al.y * (double)qi.x)));
+      r[(long)row * NS + s] = ri;
+      double2 xi = x[(long)row * NS + s];
+      xi.x += al.x * (double)pi.x - al.y * (double)pi.y;
+      xi.y += al.x * (double)pi.y + al.y * (double)pi.x;
+      x[(long)row * NS + s] = xi;
+    }
+    if (g == 0) rr += (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
+    if (mode == 2) {  // DIAG: z = DD r
+      if (g == 0) {
+        const V d = dd[(long)row * NS + s];
+        y[(long)row * NS + s] = Cx<T>::make(ri.x * d.x - ri.y * d.y, ri.x * d.y + ri.y * d.x);
+      }
+      continue;
+    }
+    if (mode == 3) {  // no preconditioner
+      if (g == 0) y[(long)row * NS + s] = ri;
+      continue;
+    }
+    const int k0 = rowptr[row], k1 = diagpos[row];
+    T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
+    for (int k = k0 + g; k < k1; k += G) {
+      const int j = col[k];
+      const V a = km[k];
+      if (!wait_flag(flag + j, epoch, st, row)) break;
+      const V yj = ldcg(y + (long)j * NS + s);
+      t1x += a.x * yj.x; t1y += a.x * yj.y;
+      t2x += a.y * yj.x; t2y += a.y * yj.y;
+    }
+    group_reduce<T, NS>(t1x, t1y, t2x, t2y);
+    if (g == 0) {
+      const T o = (T)om;
+      const T ax = t1x - o * t2y, ay = t1y + o * t2x;
+      const T wx = ri.x - ax, wy = ri.y - ay;
+      const V d = dd[(long)row * NS + s];
+      y[(long)row * NS + s] = Cx<T>::make(wx * d.x - wy * d.y, wx * d.y + wy * d.x);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      st_release(flag + row, epoch);
+    }
+  }
+  double v[1] = {rr};
+  block_partials<NS, 1>(v, part);
+}
+
+// ------------------------------------------------------------------ backward sweep
+// z_i = y_i - DD_i * sum_{j>i} A_ij z_j (COCG13_single.f90:214-225), rho += r_i z_i.
+template <class T, int NS>
+__global__ void __launch_bounds__(256)
+    k_bwd(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const int32_t* __restrict__ diagpos,
+          const typename Cx<T>::V* __restrict__ km, int n, const typename Cx<T>::V* __restrict__ r,
+          typename Cx<T>::V* __restrict__ z, const typename Cx<T>::V* __restrict__ dd, unsigned* __restrict__ flag,
+          int mode, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl, double* __restrict__ part, DevStatus* st) {
+  using V = typename Cx<T>::V;
+  if (ctrl->done) return;
+  constexpr int G = 32 / NS;
+  const unsigned epoch = ctrl->epoch;
+  const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const double om = sc[s].omega;
+  double rx = 0.0, ry = 0.0;
+  for (int it = warp; it < n; it += nwarps) {
+    const int row = n - 1 - it;
+    V zi = z[(long)row * NS + s];
+    if (mode <= 1) {
+      const int k0 = diagpos[row] + 1, k1 = rowptr[row + 1];
+      T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
+      for (int k = k0 + g; k < k1; k += G) {
+        const int j = col[k];
+        const V a = km[k];
+        if (!wait_flag(flag + j, epoch, st, row)) break;
+        const V zj = ldcg(z + (long)j * NS + s);
+        t1x += a.x * zj.x; t1y += a.x * zj.y;
+        t2x += a.y * zj.x; t2y += a.y * zj.y;
+      }
+      group_reduce<T, NS>(t1x, t1y, t2x, t2y);
+      if (g == 0) {
+        const T o = (T)om;
+        const T swx = t1x - o * t2y, swy = t1y + o * t2x;
+        const V d = dd[(long)row * NS + s];
+        zi = Cx<T>::make(zi.x - (d.x * swx - d.y * swy), zi.y - (d.x * swy + d.y * swx));
+        z[(long)row * NS + s] = zi;
+      }
+      __syncwarp();
+      if (lane == 0) {
+        __threadfence();
+        st_release(flag + row, epoch);
+      }
+    }
+    if (g == 0) {
+      const V ri = r[(long)row * NS + s];
+      rx += (double)ri.x * (double)zi.x - (double)ri.y * (double)zi.y;
+      ry += (double)ri.x * (double)zi.y + (double)ri.y * (double)zi.x;
+    }
+  }
+  double v[2] = {rx, ry};
+  block_partials<NS, 2>(v, part);
+}
+
+// ------------------------------------------------------------------ p update, SpMV
+template <class T, int NS>
+__global__ void k_pupd(int n, const typename Cx<T>::V* __restrict__ z, typename Cx<T>::V* __restrict__ p,
+                       const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl) {
+  using V = typename Cx<T>::V;
+  if (ctrl->done) return;
+  const bool first = ctrl->iter == 0;
+  const long total = (long)n * NS;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int s = (int)(i % NS);
+    const V zi = z[i];
+    if (first) {
+      p[i] = zi;
+    } else {
+      const double2 be = sc[s].beta;
+      const V pi = p[i];
+      p[i] = Cx<T>::make((T)((double)zi.x + (be.x * (double)pi.x - be.y * (double)pi.y)),
+                         (T)((double)zi.y + (be.x * (double)pi.y + be.y * (double)pi.x)));
+    }
+  }
+}
+
+// q = A p (COCG13_single.f90:273-288) and p^T q partial sums.  With
+// resid_mode, computes r = b - A x in FP64 instead and ||r||^2 (and ||b||^2).
+template <class T, int NS>
+__global__ void __launch_bounds__(256)
+    k_spmv(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+           const typename Cx<T>::V* __restrict__ km, int n, const typename Cx<T>::V* __restrict__ p,
+           typename Cx<T>::V* __restrict__ q, const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl,
+           double* __restrict__ part, const typename Cx<T>::V* __restrict__ bvec) {
+  using V = typename Cx<T>::V;
+  if (ctrl && ctrl->done) return;
+  constexpr int G = 32 / NS;
+  const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const double om = sc[s].omega;
+  double ax = 0.0, ay = 0.0, bb = 0.0;
+  for (int row = warp; row < n; row += nwarps) {
+    const int k0 = rowptr[row], k1 = rowptr[row + 1];
+    T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
+    for (int k = k0 + g; k < k1; k += G) {
+      const int j = __ldg(col + k);
+      const V a = km[k];
+      const V pj = p[(long)j * NS + s];
+      t1x += a.x * pj.x; t1y += a.x * pj.y;
+      t2x += a.y * pj.x; t2y += a.y * pj.y;
+    }
+    group_reduce<T, NS>(t1x, t1y, t2x, t2y);
+    if (g == 0) {
+      const T o = (T)om;
+      const V qi = Cx<T>::make(t1x - o * t2y, t1y + o * t2x);
+      if (bvec) {  // r = b - A x
+        const V bi = bvec[(long)row * NS + s];
+        const V ri = Cx<T>::make(bi.x - qi.x, bi.y - qi.y);
+        q[(long)row * NS + s] = ri;
+        ax += (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
+        bb += (double)bi.x * (double)bi.x + (double)bi.y * (double)bi.y;
+      } else {
+        q[(long)row * NS + s] = qi;
+        const V pi = p[(long)row * NS + s];
+        ax += (double)pi.x * (double)qi.x - (double)pi.y * (double)qi.y;
+        ay += (double)pi.x * (double)qi.y + (double)pi.y * (double)qi.x;
+      }
+    }
+  }
+  double v[3] = {ax, ay, bb};
+  block_partials<NS, 3>(v, part);
+}
+
+// ------------------------------------------------------------------ scalar kernels
+__device__ __forceinline__ void sum_partials(const double* part, int nblocks, int s, int k, double* out,
+                                             int nvals) {
+  // one warp per system; deterministic order
+  __shared__ double sh[32][4];
+  const int lane = threadIdx.x & 31;
+  for (int v = 0; v < nvals; ++v) {
+    double acc = 0.0;
+    for (int b = lane; b < nblocks; b += 32) acc += part[((long)b * MAX_NS + s) * 4 + k + v];
+    for (int m = 16; m > 0; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+    sh[threadIdx.x >> 5][v] = acc;
+  }
+  __syncwarp();
+  for (int v = 0; v < nvals; ++v) out[v] = sh[threadIdx.x >> 5][v];
+}
+
+__global__ void k_scal_r(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns) {
+  if (ctrl->done) return;
+  const int s = threadIdx.x >> 5;
+  bool finished = true;
+  if (s < ns) {
+    double rr;
+    sum_partials(part, nblocks, s, 0, &rr, 1);
+    if ((threadIdx.x & 31) == 0) {
+      SysScal& S = sc[s];
+      if (S.active) {
+        S.rr = rr;
+        S.resid = sqrt(rr / S.bnrm2);
+        if (ctrl->iter > 0) S.iter += 1;
+        if (!isfinite(S.resid)) { S.active = 0; S.status = AFEM_ENONFINITE; }
+        else if (S.resid <= ctrl->tol && ctrl->iter > 0) { S.active = 0; S.status = AFEM_OK; }
+        else if (ctrl->iter >= ctrl->maxit) { S.active = 0; S.status = AFEM_EMAXITER; }
+      }
+    }
+  }
+  __syncthreads();
+  __shared__ int any_active;
+  if (threadIdx.x == 0) any_active = 0;
+  __syncthreads();
+  if (s < ns && (threadIdx.x & 31) == 0 && sc[s].active) atomicOr(&any_active, 1);
+  __syncthreads();
+  finished = !any_active;
+  if (threadIdx.x == 0 && finished) ctrl->done = 1;
+}
+
+__device__ __forceinline__ double2 d_cdiv(double2 a, double2 b) { return cdiv(a, b); }
+
+__global__ void k_scal_rho(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns) {
+  if (ctrl->done) return;
+  const int s = threadIdx.x >> 5;
+  if (s >= ns) return;
+  double v[2];
+  sum_partials(part, nblocks, s, 0, v, 2);
+  if ((threadIdx.x & 31) == 0) {
+    SysScal& S = sc[s];
+    S.rho = make_double2(v[0], v[1]);
+    if (S.active) {
+      if (S.rho.x == 0.0 && S.rho.y == 0.0) { S.active = 0; S.status = AFEM_EBREAKDOWN; }
+      else if (ctrl->iter > 0) S.beta = d_cdiv(S.rho, S.rho1);
+    }
+  }
+}
+
+__global__ void k_scal_pq(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns) {
+  if (ctrl->done) return;
+  const int s = threadIdx.x >> 5;
+  if (s < ns) {
+    double v[2];
+    sum_partials(part, nblocks, s, 0, v, 2);
+    if ((threadIdx.x & 31) == 0) {
+      SysScal& S = sc[s];
+      S.pq = make_double2(v[0], v[1]);
+      if (S.active) {
+        if (S.pq.x == 0.0 && S.pq.y == 0.0) { S.active = 0; S.status = AFEM_EBREAKDOWN; S.alpha = make_double2(0, 0); }
+        else S.alpha = d_cdiv(S.rho, S.pq);
+        S.rho1 = S.rho;
+      } else {
+        S.alpha = make_double2(0.0, 0.0);
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ctrl->iter += 1;
+    ctrl->epoch += 1;
+  }
+}
+
+// ------------------------------------------------------------------ preconditioner set-up
+// SSOR / DIAG: DD_i = 1 / (sd * D_i) (COCG13_single.f90:126-130).
+template <class T, int NS>
+__global__ void k_dd_diag(const typename Cx<T>::V* __restrict__ km, const int32_t* __restrict__ diagpos, int n,
+                          double sd, const SysScal* __restrict__ sc, typename Cx<T>::V* __restrict__ dd) {
+  const long total = (long)n * NS;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int row = (int)(i / NS), s = (int)(i % NS);
+    const double2 a = make_double2((double)km[diagpos[row]].x, (double)km[diagpos[row]].y);
+    const double om = sc[s].omega;
+    const double2 D = make_double2(sd * a.x, sd * om * a.y);
+    const double2 w = cdiv(make_double2(1.0, 0.0), D);
+    dd[i] = Cx<T>::make((T)w.x, (T)w.y);
+  }
+}
+
+// IC: DD_i = 1 / (sd*D_i - sum_{k in L(i)} AL_k * AL_k * DD_col(k)) (COCG13_single.f90:107-124, SIGMA = 0).
+template <class T, int NS>
+__global__ void __launch_bounds__(256)
+    k_dd_ic(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const int32_t* __restrict__ diagpos,
+            const typename Cx<T>::V* __restrict__ km, int n, double sd, const SysScal* __restrict__ sc,
+            typename Cx<T>::V* __restrict__ dd, unsigned* __restrict__ flag, const Ctrl* __restrict__ ctrl,
+            DevStatus* st) {
+  using V = typename Cx<T>::V;
+  constexpr int G = 32 / NS;
+  const unsigned epoch = ctrl->epoch;
+  const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const double om = sc[s].omega;
+  for (int row = warp; row < n; row += nwarps) {
+    const int k0 = rowptr[row], k1 = diagpos[row];
+    double wx = 0, wy = 0;
+    for (int k = k0 + g; k < k1; k += G) {
+      const int j = col[k];
+      const V a = km[k];
+      if (!wait_flag(flag + j, epoch, st, row)) break;
+      const V d = ldcg(dd + (long)j * NS + s);
+      const double2 al = make_double2((double)a.x, om * (double)a.y);
+      const double2 a2 = cmul(al, al);
+      const double2 t = cmul(a2, make_double2((double)d.x, (double)d.y));
+      wx += t.x; wy += t.y;
+    }
+    for (int m = NS; m < 32; m <<= 1) {
+      wx += __shfl_xor_sync(0xffffffffu, wx, m);
+      wy += __shfl_xor_sync(0xffffffffu, wy, m);
+    }
+    if (g == 0) {
+      const V a = km[diagpos[row]];
+      const double2 W = make_double2(sd * (double)a.x - wx, sd * om * (double)a.y - wy);
+      const double2 dv = cdiv(make_double2(1.0, 0.0), W);
+      dd[(long)row * NS + s] = Cx<T>::make((T)dv.x, (T)dv.y);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      st_release(flag + row, epoch);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ helpers
+template <class Vd, class Vs>
+__global__ void k_convert(const Vs* __restrict__ in, Vd* __restrict__ out, long total);
+template <>
+__global__ void k_convert<float2, double2>(const double2* __restrict__ in, float2* __restrict__ out, long total) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x)
+    out[i] = make_float2((float)in[i].x, (float)in[i].y);
+}
+
+__global__ void k_gather_rhs(const double2* __restrict__ rhs, int n, int ns, const int* __restrict__ src,
+                             double2* __restrict__ b) {
+  const long total = (long)n * ns;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int row = (int)(i / ns), s = (int)(i % ns);
+    b[i] = rhs[(long)src[s] * n + row];
+  }
+}
+
+__global__ void k_add_x(double2* __restrict__ x, const double2* __restrict__ dx, long total) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x)
+    x[i] = make_double2(x[i].x + dx[i].x, x[i].y + dx[i].y);
+}
+
+template <class V>
+__global__ void k_copy_r(const double2* __restrict__ in, V* __restrict__ out, long total);
+template <>
+__global__ void k_copy_r<double2>(const double2* __restrict__ in, double2* __restrict__ out, long total) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x)
+    out[i] = in[i];
+}
+template <>
+__global__ void k_copy_r<float2>(const double2* __restrict__ in, float2* __restrict__ out, long total) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x)
+    out[i] = make_float2((float)in[i].x, (float)in[i].y);
+}
+
+// Start of an inner solve: x_inner = 0, ||b||^2 from the partials of the residual SpMV.
+__global__ void k_init_sys(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns, double tol, int maxit,
+                           const double* omega) {
+  const int s = threadIdx.x >> 5;
+  if (s < ns) {
+    double v[1];
+    sum_partials(part, nblocks, s, 0, v, 1);
+    if ((threadIdx.x & 31) == 0) {
+      SysScal& S = sc[s];
+      S.omega = omega[s];
+      S.bnrm2 = v[0];
+      S.rr = v[0];
+      S.resid = 1.0;
+      S.rho = S.rho1 = S.alpha = S.beta = S.pq = make_double2(0.0, 0.0);
+      S.iter = 0;
+      S.active = v[0] > 0.0;
+      S.status = AFEM_OK;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ctrl->done = 0;
+    ctrl->iter = 0;
+    ctrl->tol = tol;
+    ctrl->maxit = maxit;
+  }
+}
+
+// Residual norms after a true-residual SpMV: part[.][0] = ||b - Ax||^2, part[.][2] = ||b||^2.
+__global__ void k_true_resid(const double* part, int nblocks, int ns, double* out /* 2*ns */) {
+  const int s = threadIdx.x >> 5;
+  if (s >= ns) return;
+  double v[3];
+  sum_partials(part, nblocks, s, 0, v, 3);
+  if ((threadIdx.x & 31) == 0) {
+    out[2 * s] = v[0];
+    out[2 * s + 1] = v[2];
+  }
+}
+
+}  // namespace
+
+// ======================================================================== host side
+namespace {
+
+struct Launch {
+  afem_ctx* c;
+  SolverWork* w;
+};
+
+template <class K, class... Args>
+void launch_coop(K kernel, int blocks, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(256);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  AFEM_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
+}
+
+template <class K>
+int coresident_blocks(K kernel, int num_sms) {
+  int per_sm = 0;
+  AFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0));
+  AFEM_REQUIRE(per_sm > 0, AFEM_ECUDA, "sweep kernel cannot be resident");
+  return per_sm * num_sms;
+}
+
+template <class T, int NS>
+struct Inner {
+  using V = typename Cx<T>::V;
+  static V* vec(SolverWork* w, int which);
+};
+template <int NS>
+struct Inner<double, NS> {
+  using V = double2;
+  static V* R(SolverWork* w) { return w->r.p; }
+  static V* Z(SolverWork* w) { return w->z.p; }
+  static V* P(SolverWork* w) { return w->p.p; }
+  static V* Q(SolverWork* w) { return w->q.p; }
+  static V* DD(SolverWork* w) { return w->dd.p; }
+  static const V* KM(afem_ctx* c, SolverWork*) { return c->km.p; }
+};
+template <int NS>
+struct Inner<float, NS> {
+  using V = float2;
+  static V* R(SolverWork* w) { return w->rf.p; }
+  static V* Z(SolverWork* w) { return w->zf.p; }
+  static V* P(SolverWork* w) { return w->pf.p; }
+  static V* Q(SolverWork* w) { return w->qf.p; }
+  static V* DD(SolverWork* w) { return w->ddf.p; }
+  static const V* KM(afem_ctx*, SolverWork* w) { return w->kmf.p; }
+};
+
+// One COCG iteration (7 launches).
+template <class T, int NS>
+void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, cudaEvent_t* ev) {
+  using I = Inner<T, NS>;
+  cudaStream_t s = c->stream;
+  const int n = w->n;
+  if (ev) AFEM_CUDA(cudaEventRecord(ev[0], s));
+  launch_coop(k_fwd<T, NS>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
+              (const int32_t*)c->diagpos.p, I::KM(c, w), n, I::R(w), I::Z(w), (const typename I::V*)I::P(w),
+              (const typename I::V*)I::Q(w), w->x.p, (const typename I::V*)I::DD(w), w->flag_f.p, mode, w->sc.p,
+              w->ctrl.p, w->part.p, c->status.p);
+  if (ev) AFEM_CUDA(cudaEventRecord(ev[1], s));
+  k_scal_r<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, sweep_blocks, NS);
+  if (ev) AFEM_CUDA(cudaEventRecord(ev[2], s));
+  launch_coop(k_bwd<T, NS>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
+              (const int32_t*)c->diagpos.p, I::KM(c, w), n, (const typename I::V*)I::R(w), I::Z(w),
+              (const typename I::V*)I::DD(w), w->flag_b.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p);
+  if (ev) AFEM_CUDA(cudaEventRecord(ev[3], s));
+  k_scal_rho<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, sweep_blocks, NS);
+  if (ev) AFEM_CUDA(cudaEventRecord(ev[4], s));
+  k_pupd<T, NS><<<c->num_sms * 8, 256, 0, s>>>(n, I::Z(w), I::P(w), w->sc.p, w->ctrl.p);
+  if (ev) AFEM_CUDA(cudaEventRecord(ev[5], s));
+  k_spmv<T, NS><<<w->nblocks, 256, 0, s>>>((const int32_t*)c->rowptr.p, (const int32_t*)c->col.p, I::KM(c, w), n,
+                                           (const typename I::V*)I::P(w), I::Q(w), w->sc.p, w->ctrl.p, w->part.p,
+                                           (const typename I::V*)nullptr);
+  if (ev) AFEM_CUDA(cudaEventRecord(ev[6], s));
+  k_scal_pq<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, NS);
+}
+
+// FP64 true residual r64 = b - A x; returns per-system ||r||^2 and ||b||^2 on the host.
+template <int NS>
+void true_residual(afem_ctx* c, SolverWork* w, std::vector<double>& rr, std::vector<double>& bb) {
+  cudaStream_t s = c->stream;
+  k_spmv<double, NS><<<w->nblocks, 256, 0, s>>>((const int32_t*)c->rowptr.p, (const int32_t*)c->col.p, c->km.p, w->n,
+                                                w->x.p, w->r64.p, w->sc.p, (const Ctrl*)nullptr, w->part.p, w->b.p);
+  DBuf<double> out;
+  out.alloc(2 * NS);
+  k_true_resid<<<1, 32 * MAX_NS, 0, s>>>(w->part.p, w->nblocks, NS, out.p);
+  std::vector<double> h(2 * NS);
+  out.download(h.data(), 2 * NS, s);
+  AFEM_CUDA(cudaStreamSynchronize(s));
+  rr.resize(NS);
+  bb.resize(NS);
+  for (int k = 0; k < NS; ++k) { rr[k] = h[2 * k]; bb[k] = h[2 * k + 1]; }
+}
+
+template <class T, int NS>
+void setup_dd(afem_ctx* c, SolverWork* w, int precond, double sd) {
+  using I = Inner<T, NS>;
+  cudaStream_t s = c->stream;
+  if (precond == AFEM_PRECOND_IC) {
+    // fresh epoch for the set-up recurrence
+    w->epoch_host += 1;
+    AFEM_CUDA(cudaMemcpyAsync(&w->ctrl.p->epoch, &w->epoch_host, sizeof(unsigned), cudaMemcpyHostToDevice, s));
+    const int blocks = coresident_blocks(k_dd_ic<T, NS>, c->num_sms);
+    launch_coop(k_dd_ic<T, NS>, blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
+                (const int32_t*)c->diagpos.p, I::KM(c, w), w->n, sd, (const SysScal*)w->sc.p, I::DD(w), w->flag_f.p,
+                (const Ctrl*)w->ctrl.p, c->status.p);
+    w->epoch_host += 1;
+    AFEM_CUDA(cudaMemcpyAsync(&w->ctrl.p->epoch, &w->epoch_host, sizeof(unsigned), cudaMemcpyHostToDevice, s));
+  } else if (precond == AFEM_PRECOND_SSOR || precond == AFEM_PRECOND_DIAG) {
+    k_dd_diag<T, NS><<<c->num_sms * 8, 256, 0, s>>>(I::KM(c, w), (const int32_t*)c->diagpos.p, w->n, sd,
+                                                    (const SysScal*)w->sc.p, I::DD(w));
+  }
+}
+
+// Inner COCG from x_inner = 0 on right-hand side r64 (FP64, converted to T).
+// Returns iterations; fills per-system status/resid.
+template <class T, int NS>
+int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, double tol, int maxit, int check_every,
+               const double* d_omega, std::vector<SysScal>& hs) {
+  using I = Inner<T, NS>;
+  cudaStream_t s = c->stream;
+  const int n = w->n;
+  const long total = (long)n * NS;
+  // r = rhs (as T), x = 0, ||b||^2
+  k_copy_r<typename I::V><<<c->num_sms * 8, 256, 0, s>>>(w->r64.p, I::R(w), total);
+  // ||r64||^2 via partials of a dedicated pass
+  {
+    // reuse SpMV-with-b path on x = 0: part[0] = ||b||^2
+    AFEM_CUDA(cudaMemsetAsync(w->x.p, 0, sizeof(double2) * total, s));
+    k_spmv<double, NS><<<w->nblocks, 256, 0, s>>>((const int32_t*)c->rowptr.p, (const int32_t*)c->col.p, c->km.p, n,
+                                                  w->x.p, w->q.p, w->sc.p, (const Ctrl*)nullptr, w->part.p, w->r64.p);
+  }
+  k_init_sys<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, NS, tol, maxit, d_omega);
+  setup_dd<T, NS>(c, w, o->precond, o->sigma_diag > 0 ? o->sigma_diag : 1.0);
+  const int mode = o->precond;
+  const int sweep_blocks = coresident_blocks(k_fwd<T, NS>, c->num_sms);
+  const int sb2 = coresident_blocks(k_bwd<T, NS>, c->num_sms);
+  const int sblocks = std::min(std::min(sweep_blocks, sb2), w->nblocks);
+  AFEM_CUDA(cudaMemcpyAsync(&w->ctrl.p->epoch, &w->epoch_host, sizeof(unsigned), cudaMemcpyHostToDevice, s));
+  int iters_done = 0;
+  const int chunk = check_every > 0 ? check_every : 32;
+  // profiling: 7 events per iteration of a chunk (fwd | scal | bwd | scal | pupd | spmv)
+  const bool prof = c->prof.on;
+  std::vector<cudaEvent_t> evs;
+  if (prof) {
+    evs.resize(7L * chunk);
+    for (auto& e : evs) AFEM_CUDA(cudaEventCreate(&e));
+  }
+  auto ev_of = [&](int k) -> cudaEvent_t* { return prof ? &evs[7L * k] : nullptr; };
+  cudaGraphExec_t gexec = nullptr;
+  bool use_graph = o->use_graph != 0;
+  if (use_graph) {
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      bool ok = true;
+      try {
+        for (int k = 0; k < chunk; ++k) enqueue_iteration<T, NS>(c, w, mode, sblocks, ev_of(k));
+      } catch (const Error&) {
+        ok = false;
+      }
+      e = cudaStreamEndCapture(s, &graph);
+      if (ok && e == cudaSuccess && graph) {
+        if (cudaGraphInstantiate(&gexec, graph, 0) != cudaSuccess) gexec = nullptr;
+      }
+      if (graph) cudaGraphDestroy(graph);
+    }
+    cudaGetLastError();
+    if (!gexec) use_graph = false;
+  }
+  int iter_before = 0;
+  for (;;) {
+    if (use_graph) {
+      AFEM_CUDA(cudaGraphLaunch(gexec, s));
+    } else {
+      for (int k = 0; k < chunk; ++k) enqueue_iteration<T, NS>(c, w, mode, sblocks, ev_of(k));
+    }
+    AFEM_CUDA(cudaMemcpyAsync(w->h_ctrl, w->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+    AFEM_CUDA(cudaStreamSynchronize(s));
+    check_status(c, "COCG iteration");
+    if (prof) {
+      // count only iterations that ran to their last kernel
+      const int executed = std::min(chunk, w->h_ctrl->iter - iter_before);
+      const char* tag = sizeof(T) == 8 ? "fp64" : "fp32";
+      char nf[48], nb[48], np_[48], ns_[48];
+      snprintf(nf, sizeof nf, "cocg_fwd_sweep_%s_ns%d", tag, NS);
+      snprintf(nb, sizeof nb, "cocg_bwd_sweep_%s_ns%d", tag, NS);
+      snprintf(np_, sizeof np_, "cocg_p_update_%s_ns%d", tag, NS);
+      snprintf(ns_, sizeof ns_, "cocg_spmv_%s_ns%d", tag, NS);
+      for (int k = 0; k < executed; ++k) {
+        float a = 0, b = 0, d = 0, e = 0;
+        cudaEvent_t* E = &evs[7L * k];
+        if (cudaEventElapsedTime(&a, E[0], E[1]) != cudaSuccess || cudaEventElapsedTime(&b, E[2], E[3]) != cudaSuccess ||
+            cudaEventElapsedTime(&d, E[4], E[5]) != cudaSuccess || cudaEventElapsedTime(&e, E[5], E[6]) != cudaSuccess) {
+          cudaGetLastError();
+          continue;
+        }
+        c->prof.add(nf, a);
+        c->prof.add(nb, b);
+        c->prof.add(np_, d);
+        c->prof.add(ns_, e);
+      }
+    }
+    iter_before = w->h_ctrl->iter;
+    if (w->h_ctrl->done) break;
+    if (w->h_ctrl->iter > maxit + 2 * chunk) break;  // safety: the scalar kernels stop at maxit
+  }
+  if (gexec) cudaGraphExecDestroy(gexec);
+  for (auto& e : evs) cudaEventDestroy(e);
+  w->epoch_host = w->h_ctrl->epoch;
+  hs.resize(NS);
+  AFEM_CUDA(cudaMemcpyAsync(w->h_sc, w->sc.p, sizeof(SysScal) * NS, cudaMemcpyDeviceToHost, s));
+  AFEM_CUDA(cudaStreamSynchronize(s));
+  for (int k = 0; k < NS; ++k) hs[k] = w->h_sc[k];
+  iters_done = 0;
+  for (int k = 0; k < NS; ++k) iters_done = std::max(iters_done, hs[k].iter);
+  return iters_done;
+}
+
+template <int NS>
+int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_opts* o, afem_solve_stats* st) {
+  SolverWork* w = c->work;
+  cudaStream_t s = c->stream;
+  const int n = c->nline;
+  const long total = (long)n * NS;
+  const bool mixed = o->precision == AFEM_MIXED;
+  // ---- workspace
+  if (!w) {
+    w = new SolverWork();
+    c->work = w;
+  }
+  if (w->n != n || w->ns != NS) {
+    w->n = n;
+    w->ns = NS;
+    w->x.alloc(total); w->b.alloc(total); w->r64.alloc(total);
+    w->r.alloc(total); w->z.alloc(total); w->p.alloc(total); w->q.alloc(total); w->dd.alloc(total);
+    w->rf.release(); w->zf.release(); w->pf.release(); w->qf.release(); w->ddf.release();
+    w->flag_f.alloc(n); w->flag_b.alloc(n);
+    w->flag_f.zero(s); w->flag_b.zero(s);
+    w->sc.alloc(MAX_NS);
+    w->ctrl.alloc(1);
+    w->ctrl.zero(s);
+    w->epoch_host = 1;
+    if (!w->h_ctrl) AFEM_CUDA(cudaMallocHost(&w->h_ctrl, sizeof(Ctrl)));
+    if (!w->h_sc) AFEM_CUDA(cudaMallocHost(&w->h_sc, sizeof(SysScal) * MAX_NS));
+  }
+  if (mixed && w->rf.n != (size_t)total) {
+    w->rf.alloc(total); w->zf.alloc(total); w->pf.alloc(total); w->qf.alloc(total); w->ddf.alloc(total);
+  }
+  if (mixed && (!w->kmf_valid || w->kmf.n != (size_t)c->nnz)) {
+    w->kmf.alloc(c->nnz);
+    k_convert<float2, double2><<<c->num_sms * 8, 256, 0, s>>>(c->km.p, w->kmf.p, c->nnz);
+    w->kmf_valid = true;
+  }
+  {
+    int b1 = 0;
+    AFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_spmv<double, NS>, 256, 0));
+    w->nblocks = std::max(1, b1) * c->num_sms;
+    int bf = coresident_blocks(k_fwd<double, NS>, c->num_sms);
+    int bb = coresident_blocks(k_bwd<double, NS>, c->num_sms);
+    w->nblocks = std::max(w->nblocks, std::max(bf, bb));
+    if (mixed) {
+      w->nblocks = std::max(w->nblocks, coresident_blocks(k_fwd<float, NS>, c->num_sms));
+      w->nblocks = std::max(w->nblocks, coresident_blocks(k_bwd<float, NS>, c->num_sms));
+    }
+    w->part.alloc((size_t)w->nblocks * MAX_NS * 4);
+  }
+  // ---- right-hand sides and omegas
+  {
+    DBuf<int> dsrc;
+    std::vector<int> hsrc(NS);
+    for (int k = 0; k < NS; ++k) {
+      hsrc[k] = srcs ? srcs[k] : 0;
+      AFEM_REQUIRE(hsrc[k] >= 0 && hsrc[k] < c->rhs_nsrc, AFEM_EINVAL, "solve: source index out of range");
+    }
+    dsrc.upload(hsrc.data(), NS, s);
+    k_gather_rhs<<<c->num_sms * 8, 256, 0, s>>>(c->rhs.p, n, NS, dsrc.p, w->b.p);
+    AFEM_CUDA(cudaStreamSynchronize(s));
+  }
+  std::vector<double> om(NS);
+  const double pi = 4.0 * std::atan(1.0);
+  for (int k = 0; k < NS; ++k) om[k] = 2.0 * pi * freq[k];
+  DBuf<double> d_om;
+  d_om.upload(om.data(), NS, s);
+  // SysScal.omega must be valid for the residual SpMV before k_init_sys runs
+  {
+    std::vector<SysScal> tmp(MAX_NS);
+    for (int k = 0; k < NS; ++k) { memset(&tmp[k], 0, sizeof(SysScal)); tmp[k].omega = om[k]; }
+    AFEM_CUDA(cudaMemcpyAsync(w->sc.p, tmp.data(), sizeof(SysScal) * NS, cudaMemcpyHostToDevice, s));
+    AFEM_CUDA(cudaStreamSynchronize(s));
+  }
+  cudaEvent_t e0, e1;
+  AFEM_CUDA(cudaEventCreate(&e0));
+  AFEM_CUDA(cudaEventCreate(&e1));
+  AFEM_CUDA(cudaEventRecord(e0, s));
+
+  DBuf<double2> xacc;  // accumulated FP64 solution
+  xacc.alloc(total);
+  xacc.zero(s);
+  // r64 = b (x = 0)
+  AFEM_CUDA(cudaMemcpyAsync(w->r64.p, w->b.p, sizeof(double2) * total, cudaMemcpyDeviceToDevice, s));
+  const double tol = o->tol > 0 ? o->tol : 1e-8;
+  const int maxit = o->maxit > 0 ? o->maxit : 100000;
+  int it_total = 0, refinements = 0;
+  std::vector<double> rr, bb;
+  std::vector<SysScal> hs;
+  std::vector<int> status(NS, AFEM_EMAXITER);
+  double worst = 0.0, rec = 0.0;
+  double prev = 1.0;  // current ||b - A x|| / ||b|| (worst system)
+  for (int outer = 0; outer < 64; ++outer) {
+    // The inner solve starts from x = 0 on r64 and stops at a recursive
+    // residual relative to ||r64||; ask for the reduction still missing,
+    // never below what FP32 can deliver in the mixed mode.
+    double inner_tol = std::min(0.5, 0.5 * tol / prev);
+    if (outer == 0) inner_tol = tol;
+    if (mixed) inner_tol = std::max(inner_tol, o->inner_tol > 0 ? o->inner_tol : 1e-5);
+    const int left = maxit - it_total;
+    if (left <= 0) break;
+    int its;
+    if (mixed) its = inner_cocg<float, NS>(c, w, o, inner_tol, left, o->check_every, d_om.p, hs);
+    else its = inner_cocg<double, NS>(c, w, o, inner_tol, left, o->check_every, d_om.p, hs);
+    it_total += its;
+    refinements += 1;
+    k_add_x<<<c->num_sms * 8, 256, 0, s>>>(xacc.p, w->x.p, total);
+    AFEM_CUDA(cudaMemcpyAsync(w->x.p, xacc.p, sizeof(double2) * total, cudaMemcpyDeviceToDevice, s));
+    true_residual<NS>(c, w, rr, bb);  // r64 = b - A x_acc
+    worst = 0.0;
+    rec = 0.0;
+    bool all_ok = true, any_fatal = false;
+    for (int k = 0; k < NS; ++k) {
+      const double rel = bb[k] > 0 ? std::sqrt(rr[k] / bb[k]) : 0.0;
+      worst = std::max(worst, rel);
+      rec = std::max(rec, hs[k].resid);
+      if (!(rel <= tol)) all_ok = false;
+      if (hs[k].status == AFEM_ENONFINITE || hs[k].status == AFEM_EBREAKDOWN) any_fatal = true;
+      status[k] = (rel <= tol) ? AFEM_OK : hs[k].status;
+    }
+    if (all_ok || any_fatal || !std::isfinite(worst)) break;
+    if (worst > 0.9 * prev && outer > 0) {  // no progress from a restart
+      for (int k = 0; k < NS; ++k)
+        if (status[k] == AFEM_OK || status[k] == AFEM_EMAXITER) status[k] = status[k] == AFEM_OK ? AFEM_OK : AFEM_ESTAGNATION;
+      break;
+    }
+    prev = worst;
+  }
+  AFEM_CUDA(cudaEventRecord(e1, s));
+  AFEM_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // keep solutions
+  c->X.alloc(total);
+  AFEM_CUDA(cudaMemcpyAsync(c->X.p, xacc.p, sizeof(double2) * total, cudaMemcpyDeviceToDevice, s));
+  AFEM_CUDA(cudaStreamSynchronize(s));
+  c->nsys = NS;
+  c->sol_freq.assign(freq, freq + NS);
+  int stat = AFEM_OK;
+  for (int k = 0; k < NS; ++k)
+    if (status[k] != AFEM_OK) { stat = status[k]; break; }
+  if (st) {
+    st->iterations = it_total;
+    st->refinements = refinements;
+    st->resid_recursive = rec;
+    st->resid_true = worst;
+    st->seconds = ms * 1e-3;
+    st->status = stat;
+  }
+  return stat;
+}
+
+}  // namespace
+
+int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, const afem_solve_opts* o,
+                 afem_solve_stats* st) {
+  AFEM_REQUIRE(c->assembled, AFEM_ESTATE, "solve: system not assembled");
+  switch (nsys) {
+    case 1: return solve_ns<1>(c, freq, src, o, st);
+    case 2: return solve_ns<2>(c, freq, src, o, st);
+    case 4: return solve_ns<4>(c, freq, src, o, st);
+    case 8: return solve_ns<8>(c, freq, src, o, st);
+    case 16: return solve_ns<16>(c, freq, src, o, st);
+    default: throw Error{AFEM_EINVAL, "solve: nsys must be 1, 2, 4, 8 or 16"};
+  }
+}
+
+void invalidate_work(afem_ctx* c) {
+  if (c->work) c->work->kmf_valid = false;
+}
+
+void destroy_work(afem_ctx* c) {
+  delete c->work;
+  c->work = nullptr;
+}
+
+}  // namespace afem

@@ -1,0 +1,224 @@
+"""Host-side API of the B200 tidal forward path, over the C ABI (include/afem.h).
+
+Mirrors the reference's seams (src/solver_mpi/forward_bxyz_mpi.f90:3,
+src/solver/COCG13_single.f90:9, src/solver_mpi/n_ebfem_bxyz_mpi.f90:397/653):
+a ``Forward`` object holds one device context with the mesh, conductivity,
+tidal source and Dirichlet bounds; ``assemble`` builds the system once for
+every frequency, ``solve`` runs batched COCG, ``sites`` evaluates B and E.
+Errors raise ``AfemError`` with the library's status code, as the reference
+reports ``ERROR`` / stops.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import capi
+from .capi import AfemError, SolveOpts, SolveStats, ptr
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+@dataclass
+class SolveResult:
+    iterations: int
+    refinements: int
+    resid_recursive: float
+    resid_true: float
+    seconds: float
+    status: int
+
+    @property
+    def ok(self) -> bool:
+        return self.status == capi.AFEM_OK
+
+
+class Forward:
+    """One device context (one CUDA stream) holding one forward problem."""
+
+    def __init__(self, device: int = 0):
+        self._L = capi.lib()
+        self.ctx = self._L.afem_create(device)
+        if not self.ctx:
+            raise AfemError(-7, f"afem_create({device}) failed: no usable CUDA device")
+        self.node = self.ntet = self.nline = 0
+
+    def close(self):
+        if self.ctx:
+            self._L.afem_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != capi.AFEM_OK:
+            raise AfemError(rc, self._L.afem_last_error(self.ctx).decode())
+
+    # ------------------------------------------------------------ inputs
+    def set_mesh(self, xyz, n4, tag, line=None, n6line=None):
+        """readmsh2 + READLINE; without line/n6line the MKLINE_V2 numbering is built on the device."""
+        xyz = _c(xyz, np.float64); n4 = _c(n4, np.int32); tag = _c(tag, np.int32)
+        self.node, self.ntet = xyz.shape[0], n4.shape[0]
+        if line is None:
+            self._check(self._L.afem_set_mesh(self.ctx, self.node, ptr(xyz), self.ntet, ptr(n4), ptr(tag), 0, None, None))
+        else:
+            line = _c(line, np.int32); n6line = _c(n6line, np.int32)
+            self._check(self._L.afem_set_mesh(self.ctx, self.node, ptr(xyz), self.ntet, ptr(n4), ptr(tag), line.shape[0],
+                                              ptr(line), ptr(n6line)))
+        n = C.c_int(0)
+        self._check(self._L.afem_get_lines(self.ctx, C.byref(n), None, None))
+        self.nline = n.value
+
+    def lines(self):
+        line = np.zeros((self.nline, 2), np.int32); n6 = np.zeros((self.ntet, 6), np.int32)
+        self._check(self._L.afem_get_lines(self.ctx, None, ptr(line), ptr(n6)))
+        return line, n6
+
+    def set_cond(self, sigma_air, sigma_ocean, condflag, sigma_land=None, sigma_file=None):
+        sl = None if sigma_land is None else _c(sigma_land, np.float64)
+        sf = None if sigma_file is None else _c(sigma_file, np.float64)
+        self._check(self._L.afem_set_cond(self.ctx, float(sigma_air), float(sigma_ocean), int(condflag),
+                                          0 if sl is None else len(sl), ptr(sl), 0 if sf is None else len(sf), ptr(sf)))
+
+    def set_sigma(self, sigma_tet):
+        s = _c(sigma_tet, np.float64)
+        self._check(self._L.afem_set_sigma(self.ctx, ptr(s)))
+
+    def set_source(self, F, v, isrc: int = 0):
+        F = _c(F, np.float64); v = _c(v, np.complex128)
+        self._check(self._L.afem_set_source(self.ctx, isrc, F.shape[0], ptr(F), ptr(v)))
+
+    def set_bounds(self, zmin, zmax, xout, yout):
+        self._check(self._L.afem_set_bounds(self.ctx, zmin, zmax, xout, yout))
+
+    def load_model(self, m, with_lines=None, sources=None):
+        """Load a synthetic TidalModel (actfemtide_b200.synth) with per-land-tetrahedron conductivity."""
+        if with_lines is not None:
+            self.set_mesh(m.xyz, m.n4, m.tag, *with_lines)
+        else:
+            self.set_mesh(m.xyz, m.n4, m.tag)
+        self.set_cond(m.sigma_air, m.sigma_ocean, 1, sigma_file=m.sigma_land)
+        if sources is None:
+            sources = [(m.F, m.v)]
+        for k, (F, v) in enumerate(sources):
+            self.set_source(F, v, k)
+        b = m.bounds
+        self.set_bounds(b["zmin"], b["zmax"], b["xout"], b["yout"])
+
+    # ------------------------------------------------------------ assembly
+    def assemble(self):
+        self._check(self._L.afem_assemble(self.ctx))
+
+    def export_system(self, freq: float, isrc: int = 0):
+        """The assembled system in the reference's split layout (type global_matrix)."""
+        n = C.c_int(0); tot = C.c_long(0)
+        self._check(self._L.afem_export_system(self.ctx, freq, isrc, C.byref(n), C.byref(tot), *([None] * 9)))
+        n, tot = n.value, tot.value
+        INU = np.zeros(n + 1, np.int32); INL = np.zeros(n + 1, np.int32)
+        IAU = np.zeros(tot, np.int32); IAL = np.zeros(tot, np.int32)
+        D = np.zeros(n, np.complex128); AU = np.zeros(tot, np.complex128); AL = np.zeros(tot, np.complex128)
+        b = np.zeros(n, np.complex128); bc = np.zeros(n, np.uint8)
+        self._check(self._L.afem_export_system(self.ctx, freq, isrc, None, None, ptr(INU), ptr(IAU), ptr(INL), ptr(IAL),
+                                               ptr(D), ptr(AU), ptr(AL), ptr(b), ptr(bc)))
+        return dict(INU=INU, IAU=IAU, INL=INL, IAL=IAL, D=D, AU=AU, AL=AL, b=b, bc=bc)
+
+    def export_pattern(self):
+        n = C.c_int(0); tot = C.c_long(0)
+        self._check(self._L.afem_export_system(self.ctx, 0.0, 0, C.byref(n), C.byref(tot), *([None] * 9)))
+        n, tot = n.value, tot.value
+        INU = np.zeros(n + 1, np.int32); INL = np.zeros(n + 1, np.int32)
+        IAU = np.zeros(tot, np.int32); IAL = np.zeros(tot, np.int32)
+        self._check(self._L.afem_export_system(self.ctx, 0.0, 0, None, None, ptr(INU), ptr(IAU), ptr(INL), ptr(IAL),
+                                               None, None, None, None, None))
+        return INU, IAU, INL, IAL
+
+    # ------------------------------------------------------------ solve
+    def solve(self, freqs, srcs=None, precond="SSOR", precision="fp64", tol=1e-8, maxit=100000, sigma_diag=1.0,
+              check_every=0, inner_tol=0.0, use_graph=True) -> SolveResult:
+        f = _c(np.atleast_1d(freqs), np.float64)
+        s = None if srcs is None else _c(srcs, np.int32)
+        o = SolveOpts(capi.PRECOND[precond], capi.PRECISION[precision], tol, maxit, sigma_diag, check_every, inner_tol,
+                      int(use_graph))
+        st = SolveStats()
+        rc = self._L.afem_solve(self.ctx, len(f), ptr(f), ptr(s), C.byref(o), C.byref(st))
+        res = SolveResult(st.iterations, st.refinements, st.resid_recursive, st.resid_true, st.seconds, st.status)
+        if rc not in (capi.AFEM_OK, -4, -13):  # max-iter / stagnation are reported in the result
+            self._check(rc)
+        res.status = rc
+        return res
+
+    def solution(self, k: int = 0):
+        x = np.zeros(self.nline, np.complex128)
+        self._check(self._L.afem_get_solution(self.ctx, k, ptr(x)))
+        return x
+
+    # ------------------------------------------------------------ sites
+    def sites(self, xyz_obs, nsys: int = 1):
+        """Complex (nsys, 5, nobs): bx, by, bz (B = curl A), ex, ey (E = -i omega A)."""
+        o = _c(xyz_obs, np.float64)
+        out = np.zeros((nsys, 5, o.shape[0]), np.complex128)
+        self._check(self._L.afem_sites(self.ctx, o.shape[0], ptr(o), ptr(out)))
+        return out
+
+    def site_coeffs(self, xyz_obs):
+        o = _c(xyz_obs, np.float64)
+        nobs = o.shape[0]
+        item = np.zeros((nobs, 6), np.int32); ve = np.zeros((3, nobs, 6)); vf = np.zeros((3, nobs, 6))
+        iele = np.zeros(nobs, np.int32)
+        self._check(self._L.afem_site_coeffs(self.ctx, nobs, ptr(o), ptr(item), ptr(ve), ptr(vf), ptr(iele)))
+        return item, ve, vf, iele
+
+    # ------------------------------------------------------------ measurement
+    def set_profiling(self, enable: bool):
+        self._check(self._L.afem_set_profiling(self.ctx, int(enable)))
+
+    def profile(self):
+        """{kernel name: (total ms, launches)} accumulated since profiling was enabled."""
+        out = {}
+        buf = C.create_string_buffer(64)
+        for i in range(self._L.afem_profile_count(self.ctx)):
+            ms = C.c_double(0); n = C.c_long(0)
+            self._check(self._L.afem_profile_entry(self.ctx, i, buf, 64, C.byref(ms), C.byref(n)))
+            out[buf.value.decode()] = (ms.value, n.value)
+        return out
+
+    def stream_ptr(self) -> int:
+        return int(self._L.afem_stream(self.ctx) or 0)
+
+    # ------------------------------------------------------------ drop-in driver
+    def load_ctl(self, path: str):
+        self._check(self._L.afem_load_ctl(self.ctx, path.encode()))
+        n = C.c_int(0)
+        self._check(self._L.afem_get_lines(self.ctx, C.byref(n), None, None))
+        self.nline = n.value
+
+    def ctl_info(self):
+        nf = C.c_int(0); no = C.c_int(0)
+        self._check(self._L.afem_ctl_info(self.ctx, C.byref(nf), None, C.byref(no), None))
+        f = np.zeros(nf.value); x = np.zeros((no.value, 3))
+        self._check(self._L.afem_ctl_info(self.ctx, None, ptr(f), None, ptr(x)))
+        return f, x
+
+    def run_ctl(self, precond="SSOR", precision="fp64", tol=1e-8, maxit=100000):
+        o = SolveOpts(capi.PRECOND[precond], capi.PRECISION[precision], tol, maxit, 1.0, 0, 0.0, 1)
+        self._check(self._L.afem_run_ctl(self.ctx, C.byref(o)))
+
+
+def amp_phase(c):
+    """CALOBSRESP's amplitude and phase in degrees (n_ebfem_bxyz_mpi.f90:611-626)."""
+    c = np.asarray(c)
+    return np.sqrt(c.real ** 2 + c.imag ** 2), np.arctan2(c.imag, c.real) * (180.0 / (4.0 * np.arctan(1.0)))

@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 tidal forward path: seconds per complex edge-FEM solve to a 1e-8 FP64 true residual.
+
+One step = one pass of the forward path over one batch: assemble the
+Nedelec system (K, M and the sigma(v x F) right-hand sides) from the
+resident mesh, solve it with COCG to a true residual <= 1e-8, evaluate B and
+E at the sites.  The workload is the 96x96x64-hex model (3,538,944 tets,
+4,193,536 edges, log-normal subsurface, M2 source, 400 sites), synthetic
+and seeded (no dataset exists for it).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--method plain|mixed|batched]
+  python bench.py --impl reference ...   # the CPU reference path (oracle restatement)
+
+Prints ONE JSON line on rank 0.  Under torchrun every rank solves its own
+independent systems (replicas; weak scaling), the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s per complex edge-FEM solve to 1e-8 residual: learned+batched vs plain COCG"
+UNIT = "s/solve"
+TOL = 1e-8
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ----------------------------------------------------------------------------- helpers
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1])); smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def kernel_bytes(name: str, n: int, nnz: int, ns: int, real_bytes: int, ntet: int = 0, nsrc: int = 1,
+                 node: int = 0, nodes: int = 0) -> float:
+    """Algorithmic bytes of one launch of the named kernel (values read/written once)."""
+    ent = 2 * real_bytes + 4          # (K, M) pair + column index per stored entry
+    vec = 2 * real_bytes * ns         # one complex value per system per row
+    off = (nnz - n) // 2              # strictly lower (= strictly upper) entries
+    if name.startswith("cocg_fwd_sweep"):
+        # L entries, rowptr+diagpos, flag write; r r/w, q, p, x r/w (FP64), DD, y write, y gather
+        return ent * off + 12 * n + n * (vec * 6 + 32 * ns)
+    if name.startswith("cocg_bwd_sweep"):
+        # U entries, rowptr+diagpos, flag write; y read, z write, DD, z gather, r read
+        return ent * off + 12 * n + n * vec * 5
+    if name.startswith("cocg_spmv"):
+        # all entries, rowptr; p gather, p own read (p^T q), q write
+        return ent * nnz + 4 * (n + 1) + n * vec * 3
+    if name.startswith("cocg_p_update"):
+        return n * vec * 3
+    if name.startswith("assemble_rows"):
+        # tetrahedron data (n4, n6line, tag, sigma), node coordinates, adjacency, pattern, values, rhs
+        return ntet * (16 + 24 + 4 + 8) + 24 * node + 24 * ntet + 4 * (n + 1) + 4 * nnz + 16 * nnz + 16 * n * nsrc \
+            + nodes * (24 + 48) * nsrc
+    return 0.0
+
+
+# ----------------------------------------------------------------------------- workloads
+def build_workload(method: str, rank: int):
+    from actfemtide_b200 import synth
+    m = synth.large_model(seed=rank)
+    if method == "batched":
+        m2 = synth.large_model(seed=1000 + rank)
+        freqs = 1.0 / (3600.0 * np.array(synth.BATCH_PERIODS_H))
+        f = np.concatenate([freqs, freqs])
+        src = np.repeat([0, 1], 8).astype(np.int32)
+        sources = [(m.F, m.v), (m2.F, m2.v)]
+    else:
+        f = np.array([1.0 / synth.M2_PERIOD_S])
+        src = np.zeros(1, np.int32)
+        sources = [(m.F, m.v)]
+    return m, f, src, sources
+
+
+def solve_kwargs(method: str):
+    if method == "mixed":
+        return dict(precond="SSOR", precision="mixed")
+    return dict(precond="SSOR", precision="fp64")
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def run_gpu(args):
+    import torch
+    ws, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    from actfemtide_b200.forward import Forward
+
+    m, freqs, srcs, sources = build_workload(args.method, rank)
+    fw = Forward(local)
+    fw.load_model(m, sources=sources)
+    line, n6 = fw.lines()
+    n, nnz_half = fw.nline, None
+    INU, IAU, INL, IAL = fw.export_pattern()
+    nnz = n + 2 * len(IAU)
+    ns = len(freqs)
+    kw = solve_kwargs(args.method)
+    stream = torch.cuda.ExternalStream(fw.stream_ptr(), device=local)
+
+    def step():
+        fw.assemble()
+        res = fw.solve(freqs, srcs=srcs, tol=TOL, maxit=args.maxit, **kw)
+        out = fw.sites(m.sites, nsys=ns)
+        return res, out
+
+    for _ in range(args.warmup):
+        res, _ = step()
+        if not res.ok:
+            raise SystemExit(f"warm-up solve failed: {res}")
+    fw.set_profiling(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    iters, resid = [], []
+    for _ in range(args.steps):
+        res, out = step()
+        iters.append(res.iterations)
+        resid.append(res.resid_true)
+        if not res.ok:
+            raise SystemExit(f"timed solve failed: {res}")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    prof = fw.profile()
+    fw.set_profiling(False)
+
+    # ---- end to end through the C ABI with pinned host buffers, copies inside the timed region
+    pin = lambda a: _pinned(torch, a)  # noqa: E731
+    h = dict(xyz=pin(m.xyz), n4=pin(m.n4), tag=pin(m.tag), line=pin(line), n6=pin(n6), sig=pin(m.sigma_land),
+             F=[pin(F) for F, _ in sources], v=[pin(v) for _, v in sources], sites=pin(m.sites))
+    h2d = sum(int(a.nbytes) for a in (h["xyz"], h["n4"], h["tag"], h["line"], h["n6"], h["sig"])) + \
+        sum(int(a.nbytes) for a in h["F"]) + sum(int(a.nbytes) for a in h["v"]) + int(h["sites"].nbytes)
+    d2h = 16 * 5 * m.sites.shape[0] * ns
+    e2e_steps = max(1, args.e2e_steps)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        fw.set_mesh(h["xyz"], h["n4"], h["tag"], h["line"], h["n6"])
+        fw.set_cond(m.sigma_air, m.sigma_ocean, 1, sigma_file=h["sig"])
+        for k in range(len(sources)):
+            fw.set_source(h["F"][k], h["v"][k], k)
+        fw.set_bounds(m.bounds["zmin"], m.bounds["zmax"], m.bounds["xout"], m.bounds["yout"])
+        fw.assemble()
+        r2 = fw.solve(freqs, srcs=srcs, tol=TOL, maxit=args.maxit, **kw)
+        out = fw.sites(h["sites"], nsys=ns)
+        if not r2.ok:
+            raise SystemExit(f"e2e solve failed: {r2}")
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    # max over ranks
+    times = np.array([ms / 1e3, e2e_s], dtype=np.float64)
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor(times, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        times = t.cpu().numpy()
+        dist.barrier()
+    total_solves = args.steps * ns * ws
+    value = times[0] / total_solves
+    e2e_value = times[1] / (e2e_steps * ns * ws)
+
+    # ---- roofline of the dominant kernel
+    peak, peak_kind = peaks()
+    real_bytes = 4 if args.method == "mixed" else 8
+    dom, dom_ms, dom_n = None, 0.0, 0
+    for name, (kms, cnt) in prof.items():
+        if kms > dom_ms:
+            dom, dom_ms, dom_n = name, kms, cnt
+    rb = 4 if "fp32" in (dom or "") else real_bytes
+    per_launch = kernel_bytes(dom or "", n, nnz, ns, rb, m.ntet, len(sources), m.node, m.nodes)
+    achieved = per_launch / (dom_ms / max(1, dom_n) / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    launches = sum(c for _, c in prof.values())
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(m, freqs[0], int(np.median(iters)), args.cpu_seconds)
+    line_out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "complex-f64" if args.method != "mixed" else "complex-f32 inner / f64 refinement",
+        "data": "synthetic (seeded Kuhn-split box, log-normal subsurface, M2 tidal source)",
+        "config": {"workload": f"96x96x64 hex box: {m.ntet} tets, {n} edges, nnz {nnz}, {m.sites.shape[0]} sites",
+                   "method": f"{args.method}: COCG-{kw['precond']} {kw['precision']}, {ns} system(s) per step",
+                   "solves_per_step": ns, "tol_true_residual": TOL, "iterations_median": int(np.median(iters)),
+                   "true_residual_max": float(max(resid)), "parallelism": f"replicas x{ws}",
+                   "l2": "working set > 126 MB L2 (matrix alone %.2f GB)" % (nnz * 20 / 1e9)},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps, "includes": "set_mesh (upload, pattern) + cond + source + assemble + solve + sites"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "peak_kind": peak_kind,
+                     "bytes_per_launch": per_launch, "avg_launch_ms": dom_ms / max(1, dom_n), "traffic": None,
+                     "kernel_share": {k: round(v[0] / max(1e-9, sum(x[0] for x in prof.values())), 4)
+                                      for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line_out), flush=True)
+    fw.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def _pinned(torch, a):
+    a = np.ascontiguousarray(a)
+    t = torch.empty(a.shape, dtype=getattr(torch, {"float64": "float64", "int32": "int32", "complex128": "complex128"}[
+        str(a.dtype)]), pin_memory=True)
+    out = t.numpy()
+    out[...] = a
+    out._keep = t  # keep the pinned tensor alive with the view
+    return out
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+def cpu_baseline(m, freq, gpu_iters, seconds, threads=1):
+    """The oracle's serial assembly + SSOR-COCG on the same model, on a bounded sample of iterations.
+
+    s/solve = assembly time + (time per COCG iteration) x (iterations the
+    solve needs, taken from the GPU run of the same system)."""
+    from oracle import oracle as O
+    of = O.OracleForward(m)
+    t0 = time.perf_counter()
+    A = of.assemble(freq)
+    t_asm = time.perf_counter() - t0
+    # time a few iterations to size the sample, then the sample
+    t0 = time.perf_counter()
+    O.cocg13_single(A, precond="SSOR", resid=1e-300, maxit=2)
+    per = (time.perf_counter() - t0) / 2
+    k = max(3, int(seconds / max(per, 1e-6)))
+    t0 = time.perf_counter()
+    if threads <= 1:
+        O.cocg13_single(A, precond="SSOR", resid=1e-300, maxit=k)
+        dt = time.perf_counter() - t0
+        per_it = dt / k
+        eff = 1
+    else:
+        ths = [threading.Thread(target=O.cocg13_single, args=(A,), kwargs=dict(precond="SSOR", resid=1e-300, maxit=k))
+               for _ in range(threads)]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        dt = time.perf_counter() - t0
+        per_it = dt / k / threads  # throughput: `threads` independent solves in parallel
+        eff = threads
+    value = t_asm / eff + per_it * gpu_iters
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"oracle GENMAT+COPY_UL+BC once ({t_asm:.2f} s) + {k} SSOR-COCG iterations "
+                      f"x {threads} thread(s) ({per_it * 1e3:.1f} ms/iteration/solve), extrapolated to "
+                      f"{gpu_iters} iterations"}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    ws, rank, _ = dist_info()
+    if rank != 0:
+        return
+    from actfemtide_b200 import synth
+    m = synth.large_model(seed=0)
+    threads = os.cpu_count() or 1
+    iters_needed = args.ref_iters
+    vals = []
+    t_all = time.perf_counter()
+    cb = None
+    for _ in range(args.warmup + args.steps):
+        cb = cpu_baseline(m, 1.0 / synth.M2_PERIOD_S, iters_needed, args.cpu_seconds / max(1, args.steps), threads)
+        vals.append(cb["value"])
+    vals = vals[args.warmup:]
+    value = float(np.median(vals))
+    cb["value"] = value
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": 1e3 * value, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+           "dtype": "complex-f64", "data": "synthetic (seeded Kuhn-split box, log-normal subsurface, M2 tidal source)",
+           "config": {"workload": f"96x96x64 hex box: {m.ntet} tets", "method": "plain: COCG-SSOR fp64 (CPU)",
+                      "iterations_assumed": iters_needed},
+           "impl": "reference", "cpu_baseline": cb,
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "wall_s": time.perf_counter() - t_all}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=2)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--method", default="plain", choices=["plain", "mixed", "batched"])
+    p.add_argument("--maxit", type=int, default=200000)
+    p.add_argument("--e2e-steps", type=int, default=1)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--ref-iters", type=int, default=6000,
+                   help="iterations of the plain solve on the 96x96x64 model (from the GPU run)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    args = p.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,184 @@
+/*
+ * afem.h -- C ABI of libactfem_gpu.so, the B200 (sm_100a) implementation of
+ * the ActFEMtide tidal forward path: assemble the complex-symmetric
+ * first-order Nedelec system, solve it with COCG, evaluate E/B at sites.
+ *
+ * The reference is a Fortran program with no plugin layer; its seams are the
+ * subroutines below.  Each entry point names the reference interface it
+ * replaces.  Conventions:
+ *   - node / edge / tetrahedron ids are 1-based, exactly as in the reference
+ *     files and arrays; 2-D Fortran arrays are passed element-major:
+ *     xyz[3*(i-1)+c] = xyz(c+1,i), n4[4*(t-1)+k] = n4(t,k+1),
+ *     n6line[6*(t-1)+j] = n6line(t,j+1), line[2*(e-1)+k] = line(k+1,e).
+ *   - complex numbers are interleaved doubles (re, im), i.e. C99
+ *     `double _Complex` / Fortran complex(8) layout.
+ *   - every call returns 0 (AFEM_OK) or a negative afem_status; the message of
+ *     the last failure on a context is afem_last_error(ctx).  No call exits.
+ *   - host pointers are borrowed for the duration of the call and copied;
+ *     device buffers belong to the context.  One context per host thread;
+ *     each context owns one CUDA stream on the device given to afem_create.
+ */
+#ifndef AFEM_H
+#define AFEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct afem_ctx afem_ctx;
+
+typedef enum afem_status {
+  AFEM_OK = 0,
+  AFEM_EINVAL = -1,         /* bad argument (null pointer, size, id out of range) */
+  AFEM_EVOLUME = -2,        /* non-positive tetrahedron volume (m_fem_util.f90:23) */
+  AFEM_EPATTERN = -3,       /* row longer than the pattern limit / dof not found */
+  AFEM_EMAXITER = -4,       /* iteration cap reached (COCG13_single ERROR = -100) */
+  AFEM_EBREAKDOWN = -5,     /* rho or p^T q vanished */
+  AFEM_ENONFINITE = -6,     /* NaN/Inf in the iterates */
+  AFEM_ECUDA = -7,          /* CUDA runtime error */
+  AFEM_ESTATE = -8,         /* call out of order (e.g. solve before assemble) */
+  AFEM_ETIMEOUT = -9,       /* a device wait exceeded its bound */
+  AFEM_EIO = -10,           /* file could not be read or parsed */
+  AFEM_ENOPRECOND = -11,    /* NSET = 0 (COCG13_single ERROR = 101) */
+  AFEM_ESITE = -12,         /* a site lies outside every tetrahedron (FINDELEMENT0) */
+  AFEM_ESTAGNATION = -13    /* residual stopped decreasing */
+} afem_status;
+
+/* Preconditioners of COCG13_single (COCG13_single.f90:107-130, 202-241). */
+typedef enum afem_precond {
+  AFEM_PRECOND_IC = 0,    /* diagonal-modified IC(0): DD_i = 1/(D_i*sd - sum AL_k^2 DD_col) */
+  AFEM_PRECOND_SSOR = 1,  /* DD_i = 1/(sd*D_i), same forward/backward sweeps */
+  AFEM_PRECOND_DIAG = 2,  /* z = DD * r */
+  AFEM_PRECOND_NONE = 3
+} afem_precond;
+
+typedef enum afem_precision {
+  AFEM_FP64 = 0,          /* every kernel in complex FP64 */
+  AFEM_MIXED = 1          /* inner COCG in complex FP32, FP64 iterative refinement outside */
+} afem_precision;
+
+typedef struct afem_solve_opts {
+  int precond;            /* afem_precond */
+  int precision;          /* afem_precision */
+  double tol;             /* relative FP64 true residual to reach, ||b-Ax||/||b|| (1e-8) */
+  int maxit;              /* total COCG iteration cap */
+  double sigma_diag;      /* SIGMA_DIAG of COCG13_single (1.0) */
+  int check_every;        /* iterations between host-visible convergence checks (0 = auto) */
+  double inner_tol;       /* MIXED: relative reduction per refinement step (0 = auto) */
+  int use_graph;          /* 1: capture the iteration loop in a CUDA graph */
+} afem_solve_opts;
+
+typedef struct afem_solve_stats {
+  int iterations;         /* COCG iterations (summed over refinement steps) */
+  int refinements;        /* MIXED: outer refinement steps */
+  double resid_recursive; /* last recursive ||r||/||b|| */
+  double resid_true;      /* FP64 ||b - A x|| / ||b|| computed on the device */
+  double seconds;         /* device time of the solve */
+  int status;             /* afem_status of the solve */
+} afem_solve_stats;
+
+/* ---- context -------------------------------------------------------------- */
+afem_ctx *afem_create(int device);
+void afem_destroy(afem_ctx *ctx);
+const char *afem_last_error(const afem_ctx *ctx);
+/* Device pointer of the context's stream (cudaStream_t), for callers that order work with it. */
+void *afem_stream(afem_ctx *ctx);
+
+/* ---- mesh, edges, conductivity, source ------------------------------------ */
+/* Replaces READMESH_TOTAL/readmsh2 (m_mesh_type.f90:281-468) + READLINE
+ * (m_line_type.f90:28-48): the em3d.msh tetrahedra with their elementary tag
+ * (n4flag(:,2)) and the lineinfo.dat edge list.  line/n6line may be NULL
+ * (nline = 0): the edge numbering of MKLINE_V2/MKN6 (tmtgem/common/
+ * m_line_type.f90:120-277) is then built on the device. */
+int afem_set_mesh(afem_ctx *ctx, int node, const double *xyz, int ntet, const int32_t *n4, const int32_t *tag,
+                  int nline, const int32_t *line, const int32_t *n6line);
+/* Number of edges and the numbering in use (line: 2*nline, n6line: 6*ntet; either may be NULL). */
+int afem_get_lines(afem_ctx *ctx, int *nline, int32_t *line, int32_t *n6line);
+
+/* Replaces param_cond + SETNPHYS1INDEX2COND + READCOND (m_param.f90:449-485,
+ * n_ebfem_bxyz_mpi.f90:470-527) and GENMAT's selection (forward_bxyz_mpi.f90:196-208):
+ * tag 1 -> sigma_air, tag 2 -> sigma_ocean (the reference hard-codes 3.33),
+ * tag j >= 3 -> sigma_land[j-2] (condflag 0, sigma_land(j-1) in Fortran) or
+ * sigma_file[t-nphys1-1] for 1-based tetrahedron t (condflag 1, nphys2 values). */
+int afem_set_cond(afem_ctx *ctx, double sigma_air, double sigma_ocean, int condflag, int nvolume,
+                  const double *sigma_land, int nphys2, const double *sigma_file);
+/* Direct per-tetrahedron conductivity override (ntet values, S/m). */
+int afem_set_sigma(afem_ctx *ctx, const double *sigma_tet);
+
+/* Replaces readfxyz/readvxyz (m_readfvxyz.f90:7-62): F (3*nodes, nT) and
+ * v (3*nodes complex, m/s) for mesh nodes 1..nodes; later nodes are zero.
+ * Several source patterns may be set (isrc = 0..), each one RHS column. */
+int afem_set_source(afem_ctx *ctx, int isrc, int nodes, const double *F, const double *v_complex);
+
+/* Replaces the bounds forward_bxyz passes to GENBCCSEM (forward_bxyz_mpi.f90:34-37,
+ * 467-519): zmin = zbound(1), zmax = zbound(4), xout = xbound(4), yout = ybound(4). */
+int afem_set_bounds(afem_ctx *ctx, double zmin, double zmax, double xout, double yout);
+
+/* ---- assembly ------------------------------------------------------------- */
+/* Replaces set_iccg_var7_dofn (m_iccg_var_takuto.f90:277-359) and, per call,
+ * INITIALIZE + GENMAT + COPY_UL_ICCG12 + GENBCCSEM + SET_BC_ICCG
+ * (forward_bxyz_mpi.f90:46-58).  The device keeps K (curl-curl) and
+ * M (sigma-weighted mass * mu0 * L0^2) so that A(omega) = K + i*omega*M
+ * serves every frequency without re-assembly. */
+int afem_assemble(afem_ctx *ctx);
+
+/* Export the assembled system for one frequency in the reference's split
+ * layout (type global_matrix, m_iccg_var_takuto.f90:9-18): INU/INL (n+1,
+ * INU[0] = 0), IAU/IAL 1-based columns, complex D (n), AU/AL (iau_tot),
+ * b (n, source isrc).  Any pointer may be NULL.  *n and *iau_tot receive sizes. */
+int afem_export_system(afem_ctx *ctx, double freq_hz, int isrc, int *n, long *iau_tot, int32_t *INU, int32_t *IAU,
+                       int32_t *INL, int32_t *IAL, double *D, double *AU, double *AL, double *b, uint8_t *bc);
+
+/* ---- solve ---------------------------------------------------------------- */
+/* Replaces solveCG -> COCG13_single (forward_bxyz_mpi.f90:70-94,
+ * COCG13_single.f90:9-340) and, as the production solver, solvePARDISO
+ * (forward_bxyz_mpi.f90:63).  Solves nsys systems A(freq[k]) x_k = b_{src[k]}
+ * in one batched launch sequence; src may be NULL (all source 0).  Solutions
+ * stay on the device (afem_get_solution copies them out). */
+int afem_solve(afem_ctx *ctx, int nsys, const double *freq_hz, const int *src, const afem_solve_opts *opts,
+               afem_solve_stats *stats);
+/* Solution of system k (n complex values, [nT*km] like bs in forward_bxyz). */
+int afem_get_solution(afem_ctx *ctx, int k, double *x_complex);
+
+/* ---- sites ---------------------------------------------------------------- */
+/* Replaces PREPOBSCOEFF (n_ebfem_bxyz_mpi.f90:653-726, FINDELEMENT0 +
+ * EDGEBASISFUN/FACEBASISFUN) and CALOBSEBCOMP/CALOBSRESP (:397-423, :570-626)
+ * with the primary field 0: for each solved system k and site s,
+ * out[(k*5 + c)*nobs + s] for c = bx, by, bz (B = curl A) and ex, ey
+ * (E = -i*omega*A), complex. */
+int afem_sites(afem_ctx *ctx, int nobs, const double *xyz_obs, double *out_complex);
+/* The site coefficient rows (item: 6*nobs 1-based edge ids ascending; val_e, val_f: 3*nobs*6,
+ * [(c*nobs + s)*6 + j]; iele: containing tetrahedron) for parity checks. */
+int afem_site_coeffs(afem_ctx *ctx, int nobs, const double *xyz_obs, int32_t *item, double *val_e, double *val_f,
+                     int32_t *iele);
+
+/* ---- measurement (no counterpart in the reference, which only prints banners) -- */
+/* Accumulate per-kernel device time (CUDA events on the context's stream)
+ * while enabled; enabling or disabling clears the table. */
+int afem_set_profiling(afem_ctx *ctx, int enable);
+int afem_profile_count(afem_ctx *ctx);
+/* Entry i: kernel name, total milliseconds, launches. */
+int afem_profile_entry(afem_ctx *ctx, int i, char *name, int cap, double *ms, long *launches);
+
+/* ---- drop-in driver --------------------------------------------------------- */
+/* Replaces the rank-0 input stage of program n_ebfem_bxyz (n_ebfem_bxyz_mpi.f90:55-90):
+ * reads the forward ctl file (readcontrolfile + readparam, m_param.f90:145-446,
+ * 939-999) and every file it names (mesh, polygonz surface, lineinfo, ocean
+ * mesh node count, vxyz/fxyz, cond file), lifts the sites onto the surface
+ * (PREPZSRCOBS, n_ebfem_bxyz_mpi.f90:937-1030) and loads it all. */
+int afem_load_ctl(afem_ctx *ctx, const char *ctl_path);
+/* Frequencies and sites from the last afem_load_ctl (either pointer may be NULL). */
+int afem_ctl_info(afem_ctx *ctx, int *nfreq, double *freq, int *nobs, double *xyz_obs);
+/* Run every frequency of the loaded ctl and write <outputfolder><site>_<src>.dat
+ * exactly as OUTOBSFILESFWD (m_outresp.f90:221-262). */
+int afem_run_ctl(afem_ctx *ctx, const afem_solve_opts *opts);
+/* Fortran Gw.d formatting of x as OUTOBSFILESFWD writes it ('(11g15.7)'); host only. */
+int afem_fortran_g(double x, int w, int d, char *out, int cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AFEM_H */

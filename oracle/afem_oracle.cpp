@@ -1,0 +1,711 @@
+// CPU oracle for the ActFEMtide tidal forward path -- TEST INFRASTRUCTURE ONLY.
+//
+// A statement-by-statement C++ restatement of the reference's Fortran path,
+// used by tests/ (as the parity checker) and by bench.py (the timed CPU
+// baseline).  Nothing in the product library links or calls this file.
+//
+// Parity status: the reference ships no tests, golden vectors or data for
+// this path and cannot be compiled here (Fortran + MKL), so this oracle is
+// pinned only by the two known-answer examples the reference carries in its
+// sources (SORT_INDEX, src/solver/sort_index.f90:3-10; the CRS product of
+// src/common/test.f90:5-20), by the reference-shipped tide files
+// (src/src_tide/{f,v}xyz_mesh, parsed by the product readers) and by
+// mathematical identities (curl-curl annihilates discrete gradients, direct
+// solves).  Parity against the reference itself is therefore "unpinned".
+//
+// Conventions: node / edge / tetrahedron ids are 1-based exactly as in the
+// reference; arrays that are 2-D in Fortran are passed row-major by element
+// (n4[t*4+k] = n4(t+1,k+1), n6line[t*6+j] = n6line(t+1,j+1),
+// xyz[3*(i-1)+c] = xyz(c+1,i)); complex arrays are interleaved (re, im).
+// Compile with -ffp-contract=off: the reference is built for AVX without FMA
+// (src/solver_mpi/Makefile:8), so products and sums round separately.
+
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+typedef std::complex<double> cplx;
+
+namespace {
+
+// edge table kl (src/solver/m_fem_edge_util.f90:5-11), 1-based local nodes
+const int KL[6][2] = {{1, 2}, {2, 3}, {1, 3}, {1, 4}, {2, 4}, {3, 4}};
+// face table lmn (m_fem_edge_util.f90:13-17)
+const int LMN[4][3] = {{2, 3, 4}, {1, 4, 3}, {1, 2, 4}, {1, 3, 2}};
+// rotation matrix C(4,6) (m_fem_edge_util.f90:19-23)
+const int CROT[4][6] = {{0, 1, 0, 0, -1, 1}, {0, 0, -1, 1, 0, -1}, {1, 0, 0, -1, 1, 0}, {-1, -1, 1, 0, 0, 0}};
+
+inline double PI() { return 4.0 * std::atan(1.0); }      // constants :: pi (m_constants.f90:6)
+inline double DMU() { return 4.0 * PI() * 1.0e-7; }     // constants :: dmu (m_constants.f90:9)
+
+struct V3 { double x[3]; };
+inline V3 sub(const double* a, const double* b) { return V3{{a[0] - b[0], a[1] - b[1], a[2] - b[2]}}; }
+inline V3 neg(const V3& a) { return V3{{-a.x[0], -a.x[1], -a.x[2]}}; }
+// outer / inner (src/common/m_outerinnerproduct.f90:4-19)
+inline V3 outer(const V3& a, const V3& b) {
+  return V3{{a.x[1] * b.x[2] - a.x[2] * b.x[1], a.x[2] * b.x[0] - a.x[0] * b.x[2], a.x[0] * b.x[1] - a.x[1] * b.x[0]}};
+}
+inline double inner(const V3& a, const V3& b) { return a.x[0] * b.x[0] + a.x[1] * b.x[1] + a.x[2] * b.x[2]; }
+inline V3 scale(double c, const V3& a) { return V3{{c * a.x[0], c * a.x[1], c * a.x[2]}}; }
+
+// volume (src/solver/m_fem_util.f90:101-109)
+inline double volume(const V3& a, const V3& b, const V3& c) { return 1.0 / 6.0 * inner(outer(a, b), c); }
+
+// calxmn (m_fem_util.f90:42-53): xx(:,1..6)
+inline void calxmn(const double e[4][3], V3 xx[6]) {
+  xx[0] = sub(e[3], e[2]);
+  xx[1] = sub(e[3], e[0]);
+  xx[2] = sub(e[1], e[3]);
+  xx[3] = sub(e[2], e[1]);
+  xx[4] = sub(e[0], e[2]);
+  xx[5] = sub(e[1], e[0]);
+}
+
+// gradnodebasisfun (m_fem_util.f90:12-40).  Returns false for v <= 0 (the reference stops).
+inline bool gradnodebasisfun(const double e[4][3], V3 gn[4], double* v) {
+  V3 xx[6];
+  calxmn(e, xx);
+  *v = volume(xx[0], xx[4], neg(xx[3]));
+  if (*v <= 0) return false;
+  const double c = 1.0 / 6.0 / *v;
+  gn[0] = scale(c, outer(sub(e[3], e[1]), sub(e[2], e[1])));
+  gn[1] = scale(c, outer(sub(e[2], e[0]), sub(e[3], e[0])));
+  gn[2] = scale(c, outer(sub(e[3], e[0]), sub(e[1], e[0])));
+  gn[3] = scale(c, outer(sub(e[1], e[0]), sub(e[2], e[0])));
+  return true;
+}
+
+// intv (m_fem_util.f90:86-96), k/m 1-based
+inline double intv(int k, int m, double v) { return (k != m) ? v / 20.0 : v / 10.0; }
+
+// nodebasisfun (m_fem_util.f90:56-83)
+inline void nodebasisfun(const double e[4][3], const double x3[3], double a[4]) {
+  V3 v[4];
+  for (int j = 0; j < 4; ++j) v[j] = sub(e[j], x3);
+  V3 x12 = sub(e[1], e[0]), x13 = sub(e[2], e[0]), x14 = sub(e[3], e[0]);
+  V3 x24 = sub(e[3], e[1]), x23 = sub(e[2], e[1]);
+  double a5 = volume(x12, x13, x14);
+  double a4 = volume(x12, x13, neg(v[0])) / a5;
+  double a3 = volume(x14, x12, neg(v[0])) / a5;
+  double a2 = volume(x13, x14, neg(v[0])) / a5;
+  double a1 = volume(x24, x23, neg(v[1])) / a5;
+  a[0] = a1; a[1] = a2; a[2] = a3; a[3] = a4;
+}
+
+inline void load_tet(const double* xyz, const int* n4, long t, double e[4][3]) {
+  for (int j = 0; j < 4; ++j) {
+    const double* p = xyz + 3 * (long)(n4[t * 4 + j] - 1);
+    e[j][0] = p[0]; e[j][1] = p[1]; e[j][2] = p[2];
+  }
+}
+
+// SORT_INDEX (src/solver/sort_index.f90:13-56): heap sort of RA carrying NA.
+void sort_index(int n, int* na, double* ra) {
+  // 1-based views
+  int* NA = na - 1;
+  double* RA = ra - 1;
+  if (n < 2) return;
+  int L = n / 2 + 1, IR = n, I, J;
+  double RRA; int IIA;
+  for (;;) {
+    if (L > 1) {
+      L = L - 1; RRA = RA[L]; IIA = NA[L];
+    } else {
+      RRA = RA[IR]; IIA = NA[IR];
+      RA[IR] = RA[1]; NA[IR] = NA[1];
+      IR = IR - 1;
+      if (IR == 1) { RA[1] = RRA; NA[1] = IIA; return; }
+    }
+    I = L; J = L + L;
+    while (J <= IR) {
+      if (J < IR) { if (RA[J] < RA[J + 1]) J = J + 1; }
+      if (RRA < RA[J]) { RA[I] = RA[J]; NA[I] = NA[J]; I = J; J = J + J; }
+      else J = IR + 1;
+    }
+    RA[I] = RRA; NA[I] = IIA;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_version() { return 1; }
+
+void orc_sort_index(int n, int* na, double* ra) { sort_index(n, na, ra); }
+
+// mul_matcrs_cv (src/common/m_matrix.f90:83-102): vout = crs * cv, 1-based items.
+void orc_mul_matcrs_cv(int nrow, const int* stack, const int* item, const double* val, const double* cv,
+                       double* vout) {
+  const cplx* x = reinterpret_cast<const cplx*>(cv);
+  cplx* y = reinterpret_cast<cplx*>(vout);
+  for (int r = 0; r < nrow; ++r) {
+    cplx s(0.0, 0.0);
+    for (int j = stack[r]; j < stack[r + 1]; ++j) s = s + val[j] * x[item[j] - 1];
+    y[r] = s;
+  }
+}
+
+// MKLINE_V2 + MKN6 (tmtgem/common/m_line_type.f90:120-222, 224-277).
+// Edges grouped by their smaller node n1 ascending; inside a group, in order
+// of first encounter scanning the tetrahedra that contain n1 by ascending id
+// and their local nodes 1..4.  n6line(t,j) = +-id, sign = orientation of kl(j).
+// Returns nline, or -1 if a node is shared by more than maxnele=100
+// tetrahedra, -2 if cap is too small, -3 if an edge is missing.
+long orc_mkline(int node, long ntet, const int* n4, long cap, int* line, int* n6line) {
+  const int maxnele = 100;
+  std::vector<int> nele(node + 1, 0);
+  std::vector<long> node2ele((size_t)maxnele * (node + 1));
+  for (long i = 0; i < ntet; ++i)
+    for (int j = 0; j < 4; ++j) {
+      int n1 = n4[i * 4 + j];
+      if (nele[n1] == maxnele) return -1;
+      nele[n1]++;
+      node2ele[(size_t)maxnele * n1 + nele[n1] - 1] = i;
+    }
+  std::vector<long> stack(node + 1, 0);
+  std::vector<int> item;
+  item.reserve((size_t)ntet * 2);
+  long nline = 0;
+  for (int n1 = 1; n1 <= node; ++n1) {
+    stack[n1] = stack[n1 - 1];
+    for (int j = 0; j < nele[n1]; ++j) {
+      long iele = node2ele[(size_t)maxnele * n1 + j];
+      for (int k = 0; k < 4; ++k) {
+        int n2 = n4[iele * 4 + k];
+        if (n2 <= n1) continue;
+        bool found = false;
+        for (long l = stack[n1 - 1]; l < stack[n1]; ++l)
+          if (item[l] == n2) { found = true; break; }
+        if (found) continue;
+        stack[n1]++;
+        item.push_back(n2);
+        nline++;
+      }
+    }
+  }
+  if (nline > cap) return -2;
+  for (int i = 1; i <= node; ++i)
+    for (long j = stack[i - 1]; j < stack[i]; ++j) { line[2 * j] = i; line[2 * j + 1] = item[j]; }
+  for (long i = 0; i < ntet; ++i)
+    for (int j = 0; j < 6; ++j) {
+      int n11 = n4[i * 4 + KL[j][0] - 1], n12 = n4[i * 4 + KL[j][1] - 1], dir = 1;
+      if (n11 > n12) { std::swap(n11, n12); dir = -1; }
+      long id = -1;
+      for (long k = stack[n11 - 1]; k < stack[n11]; ++k)
+        if (item[k] == n12) { id = k + 1; break; }
+      if (id < 0) return -3;
+      n6line[i * 6 + j] = (int)(dir * id);
+    }
+  return nline;
+}
+
+// set_iccg_var7_dofn / C_set_dof2 (src/solver/m_iccg_var_takuto.f90:277-485)
+// with table_dof = identity (n_ebfem_bxyz_mpi.f90:104-107).  Strictly upper
+// (IAU) and strictly lower (IAL) column lists per row, ascending, built by the
+// reference's search-then-insert.  INU/INL hold n+1 prefix counts (INU[0]=0),
+// IAU/IAL 1-based columns.  Call with IAU==NULL to get the counts only.
+// Returns iau_tot (== ial_tot), or -1 when a row exceeds max_inum = 1000.
+long orc_pattern(int n, long ntet, const int* n6line, int* INU, int* INL, int* IAU, int* IAL) {
+  const int max_inum = 1000;
+  std::vector<std::vector<int>> up(n + 1), lo(n + 1);
+  for (long elm = 0; elm < ntet; ++elm) {
+    int dof[6];
+    for (int j = 0; j < 6; ++j) dof[j] = std::abs(n6line[elm * 6 + j]);
+    for (int kf = 0; kf < 6; ++kf) {
+      int i = dof[kf];
+      for (int lf = 0; lf < 6; ++lf) {
+        int j = dof[lf];
+        if (i == j) continue;
+        std::vector<int>& row = (i < j) ? up[i] : lo[i];
+        bool exist = false;
+        for (size_t num = 0; num < row.size(); ++num) {
+          if (j == row[num]) { exist = true; break; }
+          else if (j < row[num]) break;
+        }
+        if (exist) continue;
+        if ((int)row.size() + 1 > max_inum) return -1;
+        size_t pos = row.size();
+        for (size_t num = 0; num < row.size(); ++num)
+          if (j < row[num]) { pos = num; break; }
+        row.insert(row.begin() + pos, j);
+      }
+    }
+  }
+  INU[0] = 0; INL[0] = 0;
+  for (int i = 1; i <= n; ++i) {
+    INU[i] = INU[i - 1] + (int)up[i].size();
+    INL[i] = INL[i - 1] + (int)lo[i].size();
+  }
+  if (IAU && IAL)
+    for (int i = 1; i <= n; ++i) {
+      std::copy(up[i].begin(), up[i].end(), IAU + INU[i - 1]);
+      std::copy(lo[i].begin(), lo[i].end(), IAL + INL[i - 1]);
+    }
+  return INU[n];
+}
+
+// Conductivity per tetrahedron as GENMAT selects it (forward_bxyz_mpi.f90:196-208):
+// tag 1 -> sigma_air; 2 -> sigma_ocean (the reference hard-codes the default-real
+// literal 3.33); >=3 -> sigma_land(tag-1) for condflag 0, sigma(iele-nphys1) for
+// condflag 1.  Returns 0, or -(t+1) for a tetrahedron whose tag selects nothing.
+long orc_resolve_sigma(long ntet, const int* tag, double sigma_air, double sigma_ocean, int condflag, int nvolume,
+                       const double* sigma_land, long nphys1, const double* sigma_file, double* sigma_tet) {
+  for (long t = 0; t < ntet; ++t) {
+    int j = tag[t];
+    if (j == 1) sigma_tet[t] = sigma_air;
+    else if (j == 2) sigma_tet[t] = sigma_ocean;
+    else if (j >= 3) {
+      if (condflag == 0) {
+        if (j - 1 > nvolume) return -(t + 1);
+        sigma_tet[t] = sigma_land[j - 2];
+      } else {
+        if (t + 1 - nphys1 < 1) return -(t + 1);
+        sigma_tet[t] = sigma_file[t - nphys1];
+      }
+    } else return -(t + 1);
+  }
+  return 0;
+}
+
+// INITIALIZE + GENMAT + COPY_UL_ICCG12 + GENBCCSEM + SET_BC_ICCG for one
+// frequency (forward_bxyz_mpi.f90:42-58, 99-311, 467-519, 567-636;
+// m_iccg_var_takuto.f90:23-37, 107-167).  sup_iccg's linear row search
+// (forward_bxyz_mpi.f90:642-699) scatters into D and AU.  Source: fxyz/vxyz
+// hold nodes 1..nodes, later nodes are zero (m_readfvxyz.f90:21,47).
+// Returns 0; -1 non-positive volume (tet id in *bad); -2 dof not found;
+// -3 copy_ul mismatch.
+int orc_forward_assemble(int node, const double* xyz, long ntet, const int* n4, const int* tag, int nline,
+                         const int* line, const int* n6line, const int* INU, const int* IAU, const int* INL,
+                         const int* IAL, const double* sigma_tet, int nodes, const double* F, const double* vc,
+                         double freq, double zmin, double zmax, double xout, double yout, int apply_bc,
+                         double* D_, double* AU_, double* AL_, double* b_, unsigned char* bc_flag, long* bad) {
+  const double pi = PI(), dmu = DMU();
+  const double omega = 2.0 * pi * freq;
+  const double L0 = 1.0e3;
+  cplx* D = reinterpret_cast<cplx*>(D_);
+  cplx* AU = reinterpret_cast<cplx*>(AU_);
+  cplx* AL = reinterpret_cast<cplx*>(AL_);
+  cplx* b = reinterpret_cast<cplx*>(b_);
+  const long iau_tot = INU[nline];
+  for (int i = 0; i < nline; ++i) { D[i] = 0.0; b[i] = 0.0; }
+  for (long i = 0; i < iau_tot; ++i) { AU[i] = 0.0; AL[i] = 0.0; }
+  const cplx* v = reinterpret_cast<const cplx*>(vc);
+  const cplx iunit(0.0, 1.0);
+  for (long iele = 0; iele < ntet; ++iele) {
+    int idir[6];
+    for (int j = 0; j < 6; ++j) idir[j] = (n6line[iele * 6 + j] < 0) ? -1 : 1;
+    double e[4][3];
+    load_tet(xyz, n4, iele, e);
+    V3 xx[6], gn[4];
+    double vol;
+    calxmn(e, xx);
+    if (!gradnodebasisfun(e, gn, &vol)) { if (bad) *bad = iele + 1; return -1; }
+    const double AA = 1.0 / 9.0 / vol;
+    double S[6][6];
+    for (int j = 0; j < 6; ++j)
+      for (int k = 0; k < 6; ++k) S[j][k] = inner(xx[j], xx[k]) * idir[j] * idir[k] * AA;
+    const double sigma = sigma_tet[iele];
+    const cplx BB = iunit * omega * dmu * sigma * std::pow(L0, 2.0);
+    cplx elm_k[6][6];
+    for (int i = 0; i < 6; ++i)
+      for (int j = 0; j < 6; ++j) {
+        int k = KL[i][0], l = KL[i][1], m = KL[j][0], n = KL[j][1];
+        double yy = intv(k, m, vol) * inner(gn[l - 1], gn[n - 1]) - intv(k, n, vol) * inner(gn[l - 1], gn[m - 1]) -
+                    intv(l, m, vol) * inner(gn[k - 1], gn[n - 1]) + intv(l, n, vol) * inner(gn[k - 1], gn[m - 1]);
+        cplx S1 = (yy * idir[i] * idir[j]) * BB;
+        elm_k[i][j] = S[i][j] + S1;
+      }
+    // sup_iccg
+    int tdof[6];
+    for (int i = 0; i < 6; ++i) tdof[i] = n6line[iele * 6 + i] * idir[i];
+    for (int ie = 0; ie < 6; ++ie) {
+      int igl = tdof[ie];
+      for (int je = 0; je < 6; ++je) {
+        int jgl = tdof[je];
+        if (igl == jgl) D[igl - 1] += elm_k[ie][je];
+        else if (igl < jgl) {
+          long pos = -1;
+          for (int num = INU[igl - 1]; num < INU[igl]; ++num)
+            if (jgl == IAU[num]) { pos = num; break; }
+          if (pos < 0) { if (bad) *bad = iele + 1; return -2; }
+          if (ie > je) AU[pos] += elm_k[ie][je];
+          else AU[pos] += elm_k[je][ie];
+        }
+      }
+    }
+    // right-hand side, ocean tetrahedra only (forward_bxyz_mpi.f90:267-299)
+    cplx S2[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (tag[iele] == 2) {
+      cplx vF[4][3];
+      for (int i = 0; i < 4; ++i) {
+        int no = n4[iele * 4 + i];
+        double Fv[3] = {0.0, 0.0, 0.0};
+        cplx vv[3] = {0.0, 0.0, 0.0};
+        if (no <= nodes) {
+          for (int c = 0; c < 3; ++c) { Fv[c] = F[3 * (no - 1) + c]; vv[c] = v[3 * (no - 1) + c]; }
+        }
+        // cr_outer (m_outerinnerproduct.f90:52-60)
+        vF[i][0] = vv[1] * Fv[2] - vv[2] * Fv[1];
+        vF[i][1] = vv[2] * Fv[0] - vv[0] * Fv[2];
+        vF[i][2] = vv[0] * Fv[1] - vv[1] * Fv[0];
+      }
+      for (int i = 0; i < 6; ++i) {
+        int k = KL[i][0], l = KL[i][1];
+        for (int j = 1; j <= 4; ++j) {
+          // rc_inner (m_outerinnerproduct.f90:78-84)
+          cplx gl = gn[l - 1].x[0] * vF[j - 1][0] + gn[l - 1].x[1] * vF[j - 1][1] + gn[l - 1].x[2] * vF[j - 1][2];
+          cplx gk = gn[k - 1].x[0] * vF[j - 1][0] + gn[k - 1].x[1] * vF[j - 1][1] + gn[k - 1].x[2] * vF[j - 1][2];
+          S2[i] = S2[i] + dmu * sigma * (intv(k, j, vol) * gl - intv(l, j, vol) * gk) * (double)idir[i] * 1.0e3;
+        }
+      }
+    }
+    for (int i = 0; i < 6; ++i) {
+      int ii = n6line[iele * 6 + i] * idir[i];
+      b[ii - 1] = b[ii - 1] + S2[i];
+    }
+  }
+  // COPY_UL_ICCG12
+  {
+    std::vector<char> assigned(iau_tot, 0);
+    for (int igl = 1; igl <= nline; ++igl)
+      for (int num = INU[igl - 1]; num < INU[igl]; ++num) {
+        int jgl = IAU[num];
+        long pos = -1;
+        for (int num2 = INL[jgl - 1]; num2 < INL[jgl]; ++num2)
+          if (igl == IAL[num2]) { pos = num2; break; }
+        if (pos < 0) return -3;
+        AL[pos] = AU[num];
+        assigned[pos] = 1;
+      }
+    for (long i = 0; i < INL[nline]; ++i)
+      if (!assigned[i]) return -3;
+  }
+  // GENBCCSEM
+  const double xout1 = xout - 1.0, yout1 = yout - 1.0, zmin1 = zmin + 1.0, zmax1 = zmax - 1.0;
+  for (int i = 0; i < nline; ++i) {
+    const double* p1 = xyz + 3 * (long)(line[2 * i] - 1);
+    const double* p2 = xyz + 3 * (long)(line[2 * i + 1] - 1);
+    int g = 0;
+    if (p1[0] <= -xout1 && p2[0] <= -xout1) g = 3;
+    else if (p1[0] >= xout1 && p2[0] >= xout1) g = 5;
+    else if (p1[1] <= -yout1 && p2[1] <= -yout1) g = 4;
+    else if (p1[1] >= yout1 && p2[1] >= yout1) g = 2;
+    else if (p1[2] <= zmin1 && p2[2] <= zmin1) g = 6;
+    else if (p1[2] >= zmax1 && p2[2] >= zmax1) g = 1;
+    bc_flag[i] = (g != 0);
+  }
+  if (!apply_bc) return 0;
+  // SET_BC_ICCG with Dirichlet value 0, one source column
+  for (int i = 0; i < nline; ++i) {
+    if (bc_flag[i]) b[i] = 0.0;
+    else {
+      cplx temp = D[i] * cplx(0.0, 0.0);
+      for (int p = INL[i]; p < INL[i + 1]; ++p) temp = temp + AL[p] * cplx(0.0, 0.0);
+      for (int p = INU[i]; p < INU[i + 1]; ++p) temp = temp + AU[p] * cplx(0.0, 0.0);
+      b[i] = b[i] - temp;
+    }
+  }
+  for (int i = 0; i < nline; ++i) {
+    if (bc_flag[i]) {
+      D[i] = 1.0;
+      for (int p = INL[i]; p < INL[i + 1]; ++p) AL[p] = 0.0;
+      for (int p = INU[i]; p < INU[i + 1]; ++p) AU[p] = 0.0;
+    } else {
+      for (int p = INL[i]; p < INL[i + 1]; ++p)
+        if (bc_flag[IAL[p] - 1]) AL[p] = 0.0;
+      for (int p = INU[i]; p < INU[i + 1]; ++p)
+        if (bc_flag[IAU[p] - 1]) AU[p] = 0.0;
+    }
+  }
+  return 0;
+}
+
+// Split assembly used to check the product's frequency-independent storage:
+// K (curl-curl, real) and Msig (sigma-weighted mass times mu0*L0^2, real),
+// with A(omega) = K + i*omega*Msig, in the same D/AU layout.
+int orc_assemble_split(long ntet, const double* xyz, const int* n4, const int* n6line, int nline, const int* INU,
+                       const int* IAU, const double* sigma_tet, double* Kd, double* Ku, double* Md, double* Mu) {
+  const double dmu = DMU(), L0 = 1.0e3;
+  const long tot = INU[nline];
+  std::fill(Kd, Kd + nline, 0.0); std::fill(Md, Md + nline, 0.0);
+  std::fill(Ku, Ku + tot, 0.0); std::fill(Mu, Mu + tot, 0.0);
+  for (long iele = 0; iele < ntet; ++iele) {
+    int idir[6];
+    for (int j = 0; j < 6; ++j) idir[j] = (n6line[iele * 6 + j] < 0) ? -1 : 1;
+    double e[4][3];
+    load_tet(xyz, n4, iele, e);
+    V3 xx[6], gn[4];
+    double vol;
+    calxmn(e, xx);
+    if (!gradnodebasisfun(e, gn, &vol)) return -1;
+    const double AA = 1.0 / 9.0 / vol;
+    const double ms = dmu * sigma_tet[iele] * L0 * L0;
+    for (int ie = 0; ie < 6; ++ie)
+      for (int je = 0; je < 6; ++je) {
+        int gi = std::abs(n6line[iele * 6 + ie]), gj = std::abs(n6line[iele * 6 + je]);
+        if (gi > gj) continue;
+        // sup_iccg adds elm_k(max(ie,je), min(ie,je)) to the upper entry
+        const int i = std::max(ie, je), j = std::min(ie, je);
+        int k = KL[i][0], l = KL[i][1], m = KL[j][0], n = KL[j][1];
+        double s = inner(xx[i], xx[j]) * idir[i] * idir[j] * AA;
+        double yy = intv(k, m, vol) * inner(gn[l - 1], gn[n - 1]) - intv(k, n, vol) * inner(gn[l - 1], gn[m - 1]) -
+                    intv(l, m, vol) * inner(gn[k - 1], gn[n - 1]) + intv(l, n, vol) * inner(gn[k - 1], gn[m - 1]);
+        double mm = yy * idir[i] * idir[j] * ms;
+        if (gi == gj) { Kd[gi - 1] += s; Md[gi - 1] += mm; }
+        else {
+          long pos = -1;
+          for (int num = INU[gi - 1]; num < INU[gi]; ++num)
+            if (gj == IAU[num]) { pos = num; break; }
+          if (pos < 0) return -2;
+          Ku[pos] += s; Mu[pos] += mm;
+        }
+      }
+  }
+  return 0;
+}
+
+// COCG13_single (src/solver/COCG13_single.f90:9-340): preconditioned COCG on
+// split D/L/U storage, unconjugated r^T z and p^T q, conjugated norms, stop on
+// the recursive residual ||r||/||b|| <= RESID.  PRECOND "IC" (diagonal-modified
+// IC(0)), "SSOR", "DIAG".  NSET 0 -> ERROR 101 on first use, 1 -> precondition,
+// 2 -> symmetric diagonal scaling as well.  ITER in: max iterations; out: count
+// (MAXIT+1 after a full loop, as the Fortran DO variable).  ERROR -100 at the cap.
+// The reference SAVEs DD/SCALE across calls; here they are fresh each call.
+void orc_cocg13_single(int NP, int NPL, int NPU, double* D_, double* AL_, const int* INL, const int* IAL,
+                       double* AU_, const int* INU, const int* IAU, double* B_, double* X_, const char* PRECOND,
+                       double SIGMA_DIAG, double SIGMA, double* RESID, int* ITER, int* ERROR, int NSET,
+                       double* history) {
+  (void)NPL; (void)NPU;
+  cplx* D = reinterpret_cast<cplx*>(D_);
+  cplx* AL = reinterpret_cast<cplx*>(AL_);
+  cplx* AU = reinterpret_cast<cplx*>(AU_);
+  cplx* B = reinterpret_cast<cplx*>(B_);
+  cplx* X = reinterpret_cast<cplx*>(X_);
+  *ERROR = 0;
+  if (NSET == 0) { *ERROR = 101; return; }
+  std::vector<cplx> R(NP), Z(NP), P(NP);
+  std::vector<cplx>& Q = Z;  // Q shares the Z column (COCG13_single.f90:64-67)
+  std::vector<cplx> DD(NP, 0.0);
+  std::vector<double> SCALE(NP, 1.0);
+  const int MAXIT = *ITER;
+  const double TOL = *RESID;
+  const bool ic = (std::strncmp(PRECOND, "IC", 2) == 0) || (std::strncmp(PRECOND, "ILU", 3) == 0);
+  const bool ssor = std::strncmp(PRECOND, "SSOR", 4) == 0;
+  const bool diag = std::strncmp(PRECOND, "DIAG", 4) == 0;
+  if (NSET >= 1) {
+    if (NSET == 2) {
+      for (int i = 0; i < NP; ++i) SCALE[i] = 1.0 / std::sqrt(std::abs(D[i]));
+      for (int j = 0; j < NP; ++j) {
+        D[j] = std::abs(D[j]) / D[j];
+        for (int i = INU[j]; i < INU[j + 1]; ++i) AU[i] = AU[i] * SCALE[IAU[i] - 1] * SCALE[j];
+        for (int i = INL[j]; i < INL[j + 1]; ++i) AL[i] = AL[i] * SCALE[IAL[i] - 1] * SCALE[j];
+      }
+    }
+    for (int i = 0; i < NP; ++i) B[i] = B[i] * SCALE[i];
+    for (int i = 0; i < NP; ++i) DD[i] = 0.0;
+    if (ic) {
+      for (int i = 0; i < NP; ++i) {
+        cplx W = D[i] * SIGMA_DIAG;
+        for (int k = INL[i]; k < INL[i + 1]; ++k) {
+          cplx SS = AL[k];
+          int id = IAL[k];
+          for (int kk = INU[id - 1]; kk < INU[id]; ++kk) SS = SS + AU[kk] * SIGMA;
+          W = W - AL[k] * SS * DD[id - 1];
+        }
+        DD[i] = cplx(1.0, 0.0) / W;
+      }
+    }
+    if (ssor || diag)
+      for (int i = 0; i < NP; ++i) DD[i] = cplx(1.0, 0.0) / (SIGMA_DIAG * D[i]);
+  }
+  for (int j = 0; j < NP; ++j) {
+    cplx W = B[j] - D[j] * X[j];
+    for (int i = INU[j]; i < INU[j + 1]; ++i) W = W - AU[i] * X[IAU[i] - 1];
+    for (int i = INL[j]; i < INL[j + 1]; ++i) W = W - AL[i] * X[IAL[i] - 1];
+    R[j] = W;
+  }
+  double BNRM2 = 0.0;
+  for (int i = 0; i < NP; ++i) BNRM2 = BNRM2 + (B[i] * std::conj(B[i])).real();
+  if (BNRM2 == 0.0) {
+    for (int i = 0; i < NP; ++i) X[i] = 0.0;
+    *RESID = 0.0; *ITER = 0;
+    return;
+  }
+  cplx RHO, RHO1 = 0.0, ALPHA;
+  int iter;
+  for (iter = 1; iter <= MAXIT; ++iter) {
+    for (int i = 0; i < NP; ++i) Z[i] = R[i];
+    if (ic || ssor) {
+      for (int i = 0; i < NP; ++i) {
+        cplx W = R[i];
+        for (int j = INL[i]; j < INL[i + 1]; ++j) W = W - AL[j] * Z[IAL[j] - 1];
+        Z[i] = W * DD[i];
+      }
+      for (int i = NP - 1; i >= 0; --i) {
+        cplx SW(0.0, 0.0);
+        for (int j = INU[i]; j < INU[i + 1]; ++j) SW = SW + AU[j] * Z[IAU[j] - 1];
+        Z[i] = Z[i] - DD[i] * SW;
+      }
+    }
+    if (diag)
+      for (int i = 0; i < NP; ++i) Z[i] = R[i] * DD[i];
+    cplx RHO0(0.0, 0.0);
+    for (int i = 0; i < NP; ++i) RHO0 = RHO0 + R[i] * Z[i];
+    RHO = RHO0;
+    if (iter == 1) {
+      for (int i = 0; i < NP; ++i) P[i] = Z[i];
+    } else {
+      cplx BETA = RHO / RHO1;
+      for (int i = 0; i < NP; ++i) P[i] = Z[i] + BETA * P[i];
+    }
+    for (int j = 0; j < NP; ++j) {
+      cplx W = D[j] * P[j];
+      for (int i = INU[j]; i < INU[j + 1]; ++i) W = W + AU[i] * P[IAU[i] - 1];
+      for (int i = INL[j]; i < INL[j + 1]; ++i) W = W + AL[i] * P[IAL[i] - 1];
+      Q[j] = W;
+    }
+    cplx C10(0.0, 0.0);
+    for (int i = 0; i < NP; ++i) C10 = C10 + P[i] * Q[i];
+    ALPHA = RHO / C10;
+    for (int i = 0; i < NP; ++i) {
+      X[i] = X[i] + ALPHA * P[i];
+      R[i] = R[i] - ALPHA * Q[i];
+    }
+    double DNRM2 = 0.0;
+    for (int i = 0; i < NP; ++i) DNRM2 = DNRM2 + (R[i] * std::conj(R[i])).real();
+    *RESID = std::sqrt(DNRM2 / BNRM2);
+    if (history) history[iter - 1] = *RESID;
+    if (*RESID <= TOL) break;
+    if (iter == MAXIT) *ERROR = -100;
+    RHO1 = RHO;
+  }
+  *ITER = iter;
+  for (int i = 0; i < NP; ++i) {
+    X[i] = X[i] * SCALE[i];
+    B[i] = B[i] / SCALE[i];
+  }
+}
+
+// ||b - A x|| / ||b|| on split storage (the build's acceptance criterion).
+double orc_true_residual(int NP, const double* D_, const double* AL_, const int* INL, const int* IAL,
+                         const double* AU_, const int* INU, const int* IAU, const double* B_, const double* X_) {
+  const cplx* D = reinterpret_cast<const cplx*>(D_);
+  const cplx* AL = reinterpret_cast<const cplx*>(AL_);
+  const cplx* AU = reinterpret_cast<const cplx*>(AU_);
+  const cplx* B = reinterpret_cast<const cplx*>(B_);
+  const cplx* X = reinterpret_cast<const cplx*>(X_);
+  double rn = 0.0, bn = 0.0;
+  for (int j = 0; j < NP; ++j) {
+    cplx W = B[j] - D[j] * X[j];
+    for (int i = INU[j]; i < INU[j + 1]; ++i) W = W - AU[i] * X[IAU[i] - 1];
+    for (int i = INL[j]; i < INL[j + 1]; ++i) W = W - AL[i] * X[IAL[i] - 1];
+    rn += std::norm(W);
+    bn += std::norm(B[j]);
+  }
+  return bn > 0 ? std::sqrt(rn / bn) : 0.0;
+}
+
+// FINDELEMENT0 (src/common/m_mesh_type.f90:697-734): first tetrahedron in id
+// order whose four barycentric coordinates are >= 0.  Returns 1-based id or 0.
+long orc_findelement0(const double* x3, const double* xyz, long ntet, const int* n4, double* a) {
+  for (long i = 0; i < ntet; ++i) {
+    double e[4][3];
+    load_tet(xyz, n4, i, e);
+    nodebasisfun(e, x3, a);
+    if (a[0] >= 0.0 && a[1] >= 0.0 && a[2] >= 0.0 && a[3] >= 0.0) return i + 1;
+  }
+  return 0;
+}
+
+// PREPOBSCOEFF (n_ebfem_bxyz_mpi.f90:653-726) with EDGEBASISFUN/FACEBASISFUN
+// (m_fem_edge_util.f90:27-82): per site, 6 entries sorted by edge id (item,
+// 1-based) with edge-basis values val_e (3 comps) and face-basis*C values val_f.
+// Layout: item[s*6+j], val_e[(c*nobs + s)*6 + j], val_f likewise (c = x,y,z).
+// Returns 0 or -(s+1) for a site outside the mesh.
+long orc_prepobscoeff(const double* xyz, long ntet, const int* n4, const int* n6line, int nobs,
+                      const double* xyzobs, int* item, double* val_e, double* val_f, int* iele_out) {
+  for (int s = 0; s < nobs; ++s) {
+    const double* x3 = xyzobs + 3 * s;
+    double a4[4];
+    long iele = orc_findelement0(x3, xyz, ntet, n4, a4);
+    if (iele == 0) return -(s + 1);
+    if (iele_out) iele_out[s] = (int)iele;
+    long t = iele - 1;
+    double e[4][3];
+    load_tet(xyz, n4, t, e);
+    V3 gn[4];
+    double vol, lam[4];
+    gradnodebasisfun(e, gn, &vol);
+    nodebasisfun(e, x3, lam);
+    double w[6][3], wf[4][3], wfe[6][3];
+    for (int i = 0; i < 6; ++i) {
+      int k = KL[i][0], l = KL[i][1];
+      for (int c = 0; c < 3; ++c) w[i][c] = lam[k - 1] * gn[l - 1].x[c] - lam[l - 1] * gn[k - 1].x[c];
+    }
+    for (int i = 0; i < 4; ++i) {
+      int l = LMN[i][0], m = LMN[i][1], n = LMN[i][2];
+      V3 o1 = outer(gn[m - 1], gn[n - 1]), o2 = outer(gn[l - 1], gn[m - 1]), o3 = outer(gn[n - 1], gn[l - 1]);
+      for (int c = 0; c < 3; ++c)
+        wf[i][c] = 2.0 * (lam[l - 1] * o1.x[c] + lam[n - 1] * o2.x[c] + lam[m - 1] * o3.x[c]);
+    }
+    for (int c = 0; c < 3; ++c)  // mul_ab (m_matrix.f90:1106-1126)
+      for (int j = 0; j < 6; ++j) {
+        double acc = 0.0;
+        for (int k = 0; k < 4; ++k) acc = acc + wf[k][c] * (CROT[k][j] * 1.0);
+        wfe[j][c] = acc;
+      }
+    double r6[6];
+    int n6[6];
+    double ce[6][3], cf[6][3];
+    for (int j = 0; j < 6; ++j) {
+      int sg = (n6line[t * 6 + j] < 0) ? -1 : 1;
+      for (int c = 0; c < 3; ++c) { ce[j][c] = w[j][c] * sg; cf[j][c] = wfe[j][c] * sg; }
+      r6[j] = std::abs(n6line[t * 6 + j]) * 1.0;
+      n6[j] = j + 1;
+    }
+    sort_index(6, n6, r6);
+    for (int j = 0; j < 6; ++j) {
+      int jj = std::abs(n6line[t * 6 + n6[j] - 1]);
+      item[s * 6 + j] = jj;
+      for (int c = 0; c < 3; ++c) {
+        val_e[((long)c * nobs + s) * 6 + j] = ce[n6[j] - 1][c];
+        val_f[((long)c * nobs + s) * 6 + j] = cf[n6[j] - 1][c];
+      }
+    }
+  }
+  return 0;
+}
+
+// CALOBSEBCOMP + CALOBSRESP (n_ebfem_bxyz_mpi.f90:397-423, 570-626) with the
+// primary field fp = 0: for each source column k, bx,by,bz = coeff(2,c)*A and
+// ex,ey = coeff(1,c)*(-i*omega*A).  out: complex [(k*5 + comp)*nobs + s];
+// amp/phase (deg) alongside, same indexing.
+void orc_calobsebcomp(int nline, int nsr, double omega, const double* fs_, int nobs, const int* item,
+                      const double* val_e, const double* val_f, double* out_, double* amp, double* phase) {
+  const cplx* fs = reinterpret_cast<const cplx*>(fs_);
+  cplx* out = reinterpret_cast<cplx*>(out_);
+  const double pi = 4.0 * std::atan(1.0), r2d = 180.0 / pi;
+  std::vector<cplx> fss(nline);
+  for (int k = 0; k < nsr; ++k) {
+    const cplx* f = fs + (long)k * nline;
+    for (int i = 0; i < nline; ++i) fss[i] = -(cplx(0.0, 1.0) * omega * f[i]);
+    for (int comp = 0; comp < 5; ++comp) {
+      const double* val = (comp < 3) ? val_f + (long)comp * nobs * 6 : val_e + (long)(comp - 3) * nobs * 6;
+      const cplx* src = (comp < 3) ? f : fss.data();
+      for (int s = 0; s < nobs; ++s) {
+        cplx acc(0.0, 0.0);
+        for (int j = 0; j < 6; ++j) acc = acc + val[s * 6 + j] * src[item[s * 6 + j] - 1];
+        long o = ((long)k * 5 + comp) * nobs + s;
+        out[o] = acc;
+        if (amp) amp[o] = std::sqrt(std::pow(acc.real(), 2.0) + std::pow(acc.imag(), 2.0));
+        if (phase) phase[o] = std::atan2(acc.imag(), acc.real()) * r2d;
+      }
+    }
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,255 @@
+"""ctypes front end of the CPU oracle (``afem_oracle.cpp``) -- TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` use this module, and only as the checker / timed CPU reference.
+Each function names the reference routine it restates; see the C++ source for
+file:line citations.  Parity status: unpinned against the reference itself
+(no compiler for it here, no golden data shipped with it); pinned by the
+reference's two in-source known-answer examples and by identities.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liborc.so")
+
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_c128p = np.ctypeslib.ndpointer(dtype=np.complex128, flags="C_CONTIGUOUS")
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(HERE, "afem_oracle.cpp")
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        build()
+        L = C.CDLL(LIB_PATH)
+        L.orc_sort_index.argtypes = [C.c_int, _i32p, _f64p]
+        L.orc_mul_matcrs_cv.argtypes = [C.c_int, _i32p, _i32p, _f64p, _c128p, _c128p]
+        L.orc_mkline.restype = C.c_long
+        L.orc_mkline.argtypes = [C.c_int, C.c_long, _i32p, C.c_long, _i32p, _i32p]
+        L.orc_pattern.restype = C.c_long
+        L.orc_pattern.argtypes = [C.c_int, C.c_long, _i32p, _i32p, _i32p, C.c_void_p, C.c_void_p]
+        L.orc_resolve_sigma.restype = C.c_long
+        L.orc_resolve_sigma.argtypes = [C.c_long, _i32p, C.c_double, C.c_double, C.c_int, C.c_int, _f64p, C.c_long,
+                                        _f64p, _f64p]
+        L.orc_forward_assemble.restype = C.c_int
+        L.orc_forward_assemble.argtypes = [C.c_int, _f64p, C.c_long, _i32p, _i32p, C.c_int, _i32p, _i32p, _i32p, _i32p,
+                                           _i32p, _i32p, _f64p, C.c_int, _f64p, _c128p, C.c_double, C.c_double,
+                                           C.c_double, C.c_double, C.c_double, C.c_int, _c128p, _c128p, _c128p, _c128p,
+                                           _u8p, C.POINTER(C.c_long)]
+        L.orc_assemble_split.restype = C.c_int
+        L.orc_assemble_split.argtypes = [C.c_long, _f64p, _i32p, _i32p, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p,
+                                         _f64p, _f64p]
+        L.orc_cocg13_single.restype = None
+        L.orc_cocg13_single.argtypes = [C.c_int, C.c_int, C.c_int, _c128p, _c128p, _i32p, _i32p, _c128p, _i32p, _i32p,
+                                        _c128p, _c128p, C.c_char_p, C.c_double, C.c_double, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.c_void_p]
+        L.orc_true_residual.restype = C.c_double
+        L.orc_true_residual.argtypes = [C.c_int, _c128p, _c128p, _i32p, _i32p, _c128p, _i32p, _i32p, _c128p, _c128p]
+        L.orc_findelement0.restype = C.c_long
+        L.orc_findelement0.argtypes = [_f64p, _f64p, C.c_long, _i32p, _f64p]
+        L.orc_prepobscoeff.restype = C.c_long
+        L.orc_prepobscoeff.argtypes = [_f64p, C.c_long, _i32p, _i32p, C.c_int, _f64p, _i32p, _f64p, _f64p, _i32p]
+        L.orc_calobsebcomp.restype = None
+        L.orc_calobsebcomp.argtypes = [C.c_int, C.c_int, C.c_double, _c128p, C.c_int, _i32p, _f64p, _f64p, _c128p,
+                                       _f64p, _f64p]
+        _LIB = L
+    return _LIB
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def sort_index(na, ra):
+    """SORT_INDEX: heap sort of ra carrying na (src/solver/sort_index.f90:13-56)."""
+    na = _c(na, np.int32).copy(); ra = _c(ra, np.float64).copy()
+    lib().orc_sort_index(len(na), na, ra)
+    return na, ra
+
+
+def mul_matcrs_cv(stack, item, val, cv):
+    """mul_matcrs_cv (src/common/m_matrix.f90:83-102); stack 0-based prefix, item 1-based."""
+    stack = _c(stack, np.int32); out = np.zeros(len(stack) - 1, dtype=np.complex128)
+    lib().orc_mul_matcrs_cv(len(stack) - 1, stack, _c(item, np.int32), _c(val, np.float64), _c(cv, np.complex128), out)
+    return out
+
+
+def mkline(node: int, n4):
+    """MKLINE_V2 + MKN6: returns line (nline, 2) and n6line (ntet, 6), 1-based."""
+    n4 = _c(n4, np.int32)
+    ntet = n4.shape[0]
+    cap = 6 * ntet + 6
+    line = np.zeros((cap, 2), dtype=np.int32)
+    n6 = np.zeros((ntet, 6), dtype=np.int32)
+    nline = lib().orc_mkline(node, ntet, n4, cap, line, n6)
+    if nline < 0:
+        raise RuntimeError(f"orc_mkline failed: {nline}")
+    return np.ascontiguousarray(line[:nline]), n6
+
+
+def pattern(nline: int, n6line):
+    """set_iccg_var7_dofn/C_set_dof2: INU, IAU, INL, IAL (prefix arrays length n+1, columns 1-based)."""
+    n6 = _c(n6line, np.int32)
+    INU = np.zeros(nline + 1, dtype=np.int32); INL = np.zeros(nline + 1, dtype=np.int32)
+    tot = lib().orc_pattern(nline, n6.shape[0], n6, INU, INL, None, None)
+    if tot < 0:
+        raise RuntimeError("orc_pattern overflow")
+    IAU = np.zeros(tot, dtype=np.int32); IAL = np.zeros(tot, dtype=np.int32)
+    lib().orc_pattern(nline, n6.shape[0], n6, INU, INL, IAU.ctypes.data, IAL.ctypes.data)
+    return INU, IAU, INL, IAL
+
+
+def resolve_sigma(tag, sigma_air, sigma_ocean, condflag, sigma_land=None, nphys1=0, sigma_file=None):
+    """Per-tetrahedron sigma as GENMAT selects it (forward_bxyz_mpi.f90:196-208)."""
+    tag = _c(tag, np.int32)
+    sl = _c(sigma_land if sigma_land is not None else [0.0], np.float64)
+    sf = _c(sigma_file if sigma_file is not None else [0.0], np.float64)
+    out = np.zeros(tag.shape[0], dtype=np.float64)
+    rc = lib().orc_resolve_sigma(tag.shape[0], tag, sigma_air, sigma_ocean, condflag, len(sl), sl, nphys1, sf, out)
+    if rc != 0:
+        raise RuntimeError(f"resolve_sigma: tetrahedron {-rc} has no conductivity")
+    return out
+
+
+class Assembled:
+    def __init__(self, D, AU, AL, b, bc, INU, IAU, INL, IAL):
+        self.D, self.AU, self.AL, self.b, self.bc = D, AU, AL, b, bc
+        self.INU, self.IAU, self.INL, self.IAL = INU, IAU, INL, IAL
+
+    @property
+    def n(self):
+        return self.D.shape[0]
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        n = self.n
+        rows_u = np.repeat(np.arange(n), np.diff(self.INU))
+        rows_l = np.repeat(np.arange(n), np.diff(self.INL))
+        r = np.concatenate([np.arange(n), rows_u, rows_l])
+        c = np.concatenate([np.arange(n), self.IAU - 1, self.IAL - 1])
+        v = np.concatenate([self.D, self.AU, self.AL])
+        return sp.csr_matrix((v, (r, c)), shape=(n, n))
+
+
+def forward_assemble(m, line, n6line, pat, freq, sigma_tet, apply_bc=True) -> Assembled:
+    """INITIALIZE+GENMAT+COPY_UL_ICCG12+GENBCCSEM+SET_BC_ICCG for one frequency."""
+    INU, IAU, INL, IAL = pat
+    n = line.shape[0]
+    D = np.zeros(n, np.complex128); b = np.zeros(n, np.complex128)
+    AU = np.zeros(len(IAU), np.complex128); AL = np.zeros(len(IAL), np.complex128)
+    bc = np.zeros(n, np.uint8)
+    bad = C.c_long(0)
+    F = _c(m.F, np.float64).reshape(-1)
+    v = _c(m.v, np.complex128).reshape(-1)
+    rc = lib().orc_forward_assemble(m.node, _c(m.xyz, np.float64).reshape(-1), m.ntet, _c(m.n4, np.int32), _c(m.tag, np.int32),
+                                    n, _c(line, np.int32), _c(n6line, np.int32), INU, IAU, INL, IAL,
+                                    _c(sigma_tet, np.float64), m.nodes, F, v, float(freq), m.bounds["zmin"],
+                                    m.bounds["zmax"], m.bounds["xout"], m.bounds["yout"], int(apply_bc), D, AU, AL, b,
+                                    bc, C.byref(bad))
+    if rc != 0:
+        raise RuntimeError(f"orc_forward_assemble failed rc={rc} at element {bad.value}")
+    return Assembled(D, AU, AL, b, bc, INU, IAU, INL, IAL)
+
+
+def assemble_split(m, n6line, pat, sigma_tet):
+    INU, IAU, _, _ = pat
+    n = len(INU) - 1
+    Kd = np.zeros(n); Md = np.zeros(n); Ku = np.zeros(len(IAU)); Mu = np.zeros(len(IAU))
+    rc = lib().orc_assemble_split(m.ntet, _c(m.xyz, np.float64).reshape(-1), _c(m.n4, np.int32), _c(n6line, np.int32),
+                                  n, INU, IAU, _c(sigma_tet, np.float64), Kd, Ku, Md, Mu)
+    if rc != 0:
+        raise RuntimeError(f"orc_assemble_split rc={rc}")
+    return Kd, Ku, Md, Mu
+
+
+def cocg13_single(A: Assembled, b=None, x0=None, precond="IC", resid=1e-8, maxit=20000, sigma_diag=1.0, sigma=0.0,
+                  nset=1, history=False):
+    """COCG13_single on copies of A (the reference mutates its arguments)."""
+    n = A.n
+    D = A.D.copy(); AL = A.AL.copy(); AU = A.AU.copy()
+    B = (A.b if b is None else np.asarray(b, np.complex128)).copy()
+    X = np.zeros(n, np.complex128) if x0 is None else np.asarray(x0, np.complex128).copy()
+    R = C.c_double(resid); IT = C.c_int(maxit); ER = C.c_int(0)
+    hist = np.zeros(maxit + 1) if history else None
+    lib().orc_cocg13_single(n, len(AL), len(AU), D, AL, A.INL, A.IAL, AU, A.INU, A.IAU, B, X, precond.encode(),
+                            sigma_diag, sigma, C.byref(R), C.byref(IT), C.byref(ER), nset,
+                            hist.ctypes.data if history else None)
+    out = dict(x=X, resid=R.value, iter=IT.value, error=ER.value)
+    if history:
+        out["history"] = hist[: min(IT.value, maxit)]
+    return out
+
+
+def true_residual(A: Assembled, x, b=None):
+    B = A.b if b is None else _c(b, np.complex128)
+    return lib().orc_true_residual(A.n, A.D, A.AL, A.INL, A.IAL, A.AU, A.INU, A.IAU, _c(B, np.complex128),
+                                   _c(x, np.complex128))
+
+
+def findelement0(m, x3):
+    a = np.zeros(4)
+    i = lib().orc_findelement0(_c(x3, np.float64), _c(m.xyz, np.float64).reshape(-1), m.ntet, _c(m.n4, np.int32), a)
+    return int(i), a
+
+
+def prepobscoeff(m, n6line, sites):
+    """PREPOBSCOEFF: item (nobs,6) 1-based sorted edge ids; val_e/val_f (3, nobs, 6); iele (nobs,)."""
+    sites = _c(sites, np.float64)
+    nobs = sites.shape[0]
+    item = np.zeros((nobs, 6), np.int32)
+    ve = np.zeros((3, nobs, 6)); vf = np.zeros((3, nobs, 6)); iele = np.zeros(nobs, np.int32)
+    rc = lib().orc_prepobscoeff(_c(m.xyz, np.float64).reshape(-1), m.ntet, _c(m.n4, np.int32), _c(n6line, np.int32), nobs,
+                                sites.reshape(-1), item, ve, vf, iele)
+    if rc != 0:
+        raise RuntimeError(f"site {-rc} is outside the mesh")
+    return item, ve, vf, iele
+
+
+def calobsebcomp(fs, omega, item, ve, vf):
+    """CALOBSEBCOMP with fp = 0: returns complex (nsr, 5, nobs) [bx,by,bz,ex,ey], amp, phase (deg)."""
+    fs = np.asarray(fs, np.complex128)
+    if fs.ndim == 1:
+        fs = fs[None, :]
+    nsr, nline = fs.shape
+    nobs = item.shape[0]
+    out = np.zeros((nsr, 5, nobs), np.complex128); amp = np.zeros((nsr, 5, nobs)); ph = np.zeros((nsr, 5, nobs))
+    lib().orc_calobsebcomp(nline, nsr, float(omega), _c(fs, np.complex128), nobs, _c(item, np.int32),
+                           _c(ve, np.float64), _c(vf, np.float64), out, amp, ph)
+    return out, amp, ph
+
+
+class OracleForward:
+    """The whole reference path for one model on the CPU: numbering, pattern, assembly, COCG, sites."""
+
+    def __init__(self, m, line=None, n6line=None):
+        self.m = m
+        if line is None:
+            line, n6line = mkline(m.node, m.n4)
+        self.line, self.n6line = line, n6line
+        self.pat = pattern(line.shape[0], n6line)
+        self.sigma_tet = m.sigma_per_tet()
+
+    def assemble(self, freq, apply_bc=True) -> Assembled:
+        return forward_assemble(self.m, self.line, self.n6line, self.pat, freq, self.sigma_tet, apply_bc)
+
+    def sites(self, x, freq):
+        item, ve, vf, _ = prepobscoeff(self.m, self.n6line, self.m.sites)
+        omega = 2.0 * (4.0 * np.arctan(1.0)) * freq
+        return calobsebcomp(x, omega, item, ve, vf)

@@ -1,0 +1,224 @@
+"""GPU parity: every device stage of the path against the CPU oracle, through the C ABI.
+
+Tolerances: integer work (numbering, pattern, Dirichlet flags, site element
+and column order) is bit-exact; assembled entries within 1e-12 relative to
+the largest entry of their row; site coefficients within 1e-14; solved site
+fields within 1e-6 relative of the oracle's own solve, and every solve must
+reach an FP64 true residual <= 1e-8.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from actfemtide_b200 import synth
+from actfemtide_b200.capi import AfemError
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def fw(gpulib):
+    from actfemtide_b200.forward import Forward
+    f = Forward(0)
+    yield f
+    f.close()
+
+
+@pytest.fixture(scope="module")
+def box20(oracle):
+    """The 20x20x20 model with the oracle's assembly and a 1e-10 SSOR-COCG reference solve."""
+    m = synth.small_model()
+    of = oracle.OracleForward(m)
+    A = of.assemble(m.freqs[0])
+    r = oracle.cocg13_single(A, precond="SSOR", resid=1e-10, maxit=100000)
+    ref, _, _ = of.sites(r["x"], m.freqs[0])
+    return m, of, A, ref
+
+
+def assert_system_close(sys_gpu, A, rtol=1e-12):
+    n = A.n
+    # per-row scale: largest |entry| of the row
+    scale = np.abs(A.D).copy()
+    for i in range(n):
+        for k in range(A.INU[i], A.INU[i + 1]):
+            scale[i] = max(scale[i], abs(A.AU[k]))
+        for k in range(A.INL[i], A.INL[i + 1]):
+            scale[i] = max(scale[i], abs(A.AL[k]))
+    ru = np.repeat(np.arange(n), np.diff(A.INU))
+    rl = np.repeat(np.arange(n), np.diff(A.INL))
+    assert np.all(np.abs(sys_gpu["D"] - A.D) <= rtol * scale)
+    assert np.all(np.abs(sys_gpu["AU"] - A.AU) <= rtol * scale[ru])
+    assert np.all(np.abs(sys_gpu["AL"] - A.AL) <= rtol * scale[rl])
+    # real part (curl-curl) is computed in the reference's operation order: bit-exact
+    assert np.array_equal(sys_gpu["D"].real, A.D.real)
+    assert np.array_equal(sys_gpu["AU"].real, A.AU.real)
+    bscale = np.abs(A.b).max()
+    assert np.all(np.abs(sys_gpu["b"] - A.b) <= rtol * bscale)
+
+
+@pytest.mark.parametrize("maker", [synth.tiny_model, synth.small_model])
+def test_device_numbering_pattern_assembly(fw, oracle, maker):
+    m = maker()
+    of = oracle.OracleForward(m)
+    fw.load_model(m)  # numbering built on the device
+    line, n6 = fw.lines()
+    assert np.array_equal(line, of.line)
+    assert np.array_equal(n6, of.n6line)
+    INU, IAU, INL, IAL = fw.export_pattern()
+    for a, b in zip((INU, IAU, INL, IAL), of.pat):
+        assert np.array_equal(a, b)
+    fw.assemble()
+    A = of.assemble(m.freqs[0])
+    sg = fw.export_system(m.freqs[0])
+    assert np.array_equal(sg["bc"], A.bc)
+    assert_system_close(sg, A)
+    # the same with the reference's lineinfo given explicitly
+    fw.load_model(m, with_lines=(of.line, of.n6line))
+    fw.assemble()
+    sg2 = fw.export_system(m.freqs[0])
+    assert np.array_equal(sg2["D"], sg["D"]) and np.array_equal(sg2["AU"], sg["AU"])
+
+
+@pytest.mark.parametrize("name", ["tiny_2x2x4", "box4x4x6"])
+def test_golden_fixtures_on_device(fw, name):
+    from test_oracle import fixture_model
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    m = fixture_model(g)
+    fw.load_model(m)
+    line, n6 = fw.lines()
+    assert np.array_equal(line, g["line"]) and np.array_equal(n6, g["n6line"])
+    fw.assemble()
+    sg = fw.export_system(float(g["freq"]))
+
+    class A:  # golden system in the oracle's layout
+        pass
+    A.n = g["D"].shape[0]
+    for k in ("D", "AU", "AL", "b", "INU", "INL", "IAU", "IAL"):
+        setattr(A, k, g[k])
+    assert_system_close(sg, A)
+    item, ve, vf, iele = fw.site_coeffs(g["sites"])
+    assert np.array_equal(item, g["item"]) and np.array_equal(iele, g["iele"])
+    np.testing.assert_allclose(ve, g["val_e"], rtol=0, atol=1e-14 * np.abs(g["val_e"]).max())
+    np.testing.assert_allclose(vf, g["val_f"], rtol=0, atol=1e-14 * np.abs(g["val_f"]).max())
+    res = fw.solve(float(g["freq"]), precond="SSOR", tol=1e-12)
+    assert res.ok and res.resid_true <= 1e-12
+    out = fw.sites(g["sites"])
+    ref = g["site_field"]
+    assert np.abs(out - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+def test_site_coefficients_box20(fw, oracle):
+    m = synth.small_model()
+    of = oracle.OracleForward(m)
+    fw.load_model(m, with_lines=(of.line, of.n6line))
+    item, ve, vf, iele = fw.site_coeffs(m.sites)
+    i2, v2, f2, e2 = oracle.prepobscoeff(m, of.n6line, m.sites)
+    assert np.array_equal(iele, e2) and np.array_equal(item, i2)
+    assert np.abs(ve - v2).max() <= 1e-14 * np.abs(v2).max()
+    assert np.abs(vf - f2).max() <= 1e-14 * np.abs(f2).max()
+
+
+def test_ssor_cocg_box20_sites(fw, oracle, box20):
+    """Plain FP64 SSOR-COCG on the 20x20x20 model: true residual <= 1e-8, sites within 1e-6 of the oracle's solve."""
+    m, of, A, ref = box20
+    fw.load_model(m)
+    fw.assemble()
+    res = fw.solve(m.freqs[0], precond="SSOR", tol=1e-8)
+    assert res.ok, res
+    assert res.resid_true <= 1e-8
+    x = fw.solution(0)
+    assert oracle.true_residual(A, x) <= 1.01e-8
+    out = fw.sites(m.sites)
+    assert np.abs(out - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("precond", ["IC", "SSOR", "DIAG", "NONE"])
+def test_preconditioners_first_iterations(fw, oracle, precond):
+    """A few iterations of each preconditioner track the oracle's COCG13_single iterates."""
+    m = synth.tiny_model()
+    of = oracle.OracleForward(m)
+    fw.load_model(m)
+    fw.assemble()
+    A = of.assemble(m.freqs[0])
+    for its in (1, 2, 5):
+        res = fw.solve(m.freqs[0], precond=precond, tol=1e-30, maxit=its)
+        assert res.iterations == its
+        x = fw.solution(0)
+        r = oracle.cocg13_single(A, precond=precond if precond != "NONE" else "none", resid=1e-30, maxit=its)
+        assert np.abs(x - r["x"]).max() <= 1e-9 * np.abs(r["x"]).max()
+
+
+def test_batched_systems_match_single(fw):
+    """Frequencies x source patterns in one batch equal the one-by-one solves."""
+    m = synth.tidal_box(4, 4, 6, seed=3, site_grid=(-6.0, 0.0, 6.0), half_km=12.0)
+    m2 = synth.tidal_box(4, 4, 6, seed=3, vel_seed=7, site_grid=(-6.0, 0.0, 6.0), half_km=12.0)
+    fw.load_model(m, sources=[(m.F, m.v), (m2.F, m2.v)])
+    fw.assemble()
+    freqs = 1.0 / (3600.0 * np.array(synth.BATCH_PERIODS_H[:4]))
+    for ns in (2, 4, 8):
+        f = np.resize(freqs, ns)
+        src = np.arange(ns) % 2
+        res = fw.solve(f, srcs=src, precond="SSOR", tol=1e-10)
+        assert res.ok and res.resid_true <= 1e-10
+        xs = [fw.solution(k) for k in range(ns)]
+        sites_b = fw.sites(m.sites, nsys=ns)
+        for k in range(ns):
+            r1 = fw.solve(f[k], srcs=[src[k]], precond="SSOR", tol=1e-10)
+            assert r1.ok
+            s1 = fw.sites(m.sites)
+            assert np.abs(sites_b[k] - s1[0]).max() <= 1e-6 * np.abs(s1).max()
+
+
+def test_mixed_precision_box20(fw, oracle, box20):
+    m, of, A, ref = box20
+    fw.load_model(m)
+    fw.assemble()
+    res = fw.solve(m.freqs[0], precond="SSOR", precision="mixed", tol=1e-8)
+    assert res.ok and res.resid_true <= 1e-8
+    out = fw.sites(m.sites)
+    assert np.abs(out - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+def test_error_paths(fw):
+    m = synth.tiny_model()
+    bad = m.n4.copy()
+    bad[0, 0] = m.node + 5
+    with pytest.raises(AfemError) as e:
+        fw.set_mesh(m.xyz, bad, m.tag)
+    assert e.value.code == -1
+    # inverted tetrahedron -> non-positive volume
+    inv = m.n4.copy()
+    inv[3, [0, 1]] = inv[3, [1, 0]]
+    fw.set_mesh(m.xyz, inv, m.tag)
+    fw.set_cond(m.sigma_air, m.sigma_ocean, 1, sigma_file=m.sigma_land)
+    fw.set_source(m.F, m.v)
+    fw.set_bounds(**m.bounds)
+    with pytest.raises(AfemError) as e:
+        fw.assemble()
+    assert e.value.code == -2 and "index 3" in str(e.value)
+    # cond file size must match the land tetrahedra (SETNPHYS1INDEX2COND)
+    with pytest.raises(AfemError):
+        fw.set_cond(m.sigma_air, m.sigma_ocean, 1, sigma_file=m.sigma_land[:-1])
+    # solve before assemble
+    fw.load_model(m)
+    with pytest.raises(AfemError) as e:
+        fw.solve(m.freqs[0])
+    assert e.value.code == -8
+    # iteration cap is reported, not raised
+    fw.assemble()
+    res = fw.solve(m.freqs[0], precond="SSOR", tol=1e-30, maxit=3)
+    assert res.status == -4 and res.iterations == 3
+
+
+def test_repeated_solves_are_reproducible(fw):
+    m = synth.tiny_model()
+    fw.load_model(m)
+    fw.assemble()
+    fw.solve(m.freqs[0], precond="SSOR", tol=1e-10)
+    x1 = fw.solution(0)
+    fw.assemble()
+    fw.solve(m.freqs[0], precond="SSOR", tol=1e-10)
+    x2 = fw.solution(0)
+    assert np.array_equal(x1, x2)
