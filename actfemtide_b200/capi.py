@@ -29,7 +29,7 @@ EXPORTS = (
     "afem_set_cond", "afem_set_sigma", "afem_set_source", "afem_set_bounds", "afem_assemble",
     "afem_export_system", "afem_solve", "afem_get_solution", "afem_sites", "afem_site_coeffs", "afem_load_ctl",
     "afem_ctl_info", "afem_run_ctl", "afem_fortran_g", "afem_set_profiling", "afem_profile_count",
-    "afem_profile_entry",
+    "afem_profile_entry", "afem_cocg13_single", "afem_set_system",
 )
 
 
@@ -88,13 +88,18 @@ def lib():
     L.afem_ctl_info.argtypes = [_vp, C.POINTER(C.c_int), _vp, C.POINTER(C.c_int), _vp]
     L.afem_run_ctl.argtypes = [_vp, C.POINTER(SolveOpts)]
     L.afem_fortran_g.argtypes = [C.c_double, C.c_int, C.c_int, C.c_char_p, C.c_int]
+    L.afem_cocg13_single.argtypes = [_vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                     C.c_char_p, C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int), C.c_int]
+    L.afem_set_system.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.afem_set_profiling.argtypes = [_vp, C.c_int]
     L.afem_profile_count.argtypes = [_vp]
     L.afem_profile_entry.argtypes = [_vp, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_long)]
     for name in ("afem_set_mesh", "afem_get_lines", "afem_set_cond", "afem_set_sigma", "afem_set_source",
                  "afem_set_bounds", "afem_assemble", "afem_export_system", "afem_solve", "afem_get_solution",
                  "afem_sites", "afem_site_coeffs", "afem_load_ctl", "afem_ctl_info", "afem_run_ctl",
-                 "afem_fortran_g", "afem_set_profiling", "afem_profile_count", "afem_profile_entry"):
+                 "afem_fortran_g", "afem_set_profiling", "afem_profile_count", "afem_profile_entry", "afem_cocg13_single",
+                 "afem_set_system"):
         getattr(L, name).restype = C.c_int
     _LIB = L
     return L

@@ -1,4 +1,5 @@
 // C ABI entry points (include/afem.h): context, inputs, assembly, solve, sites.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <exception>
@@ -35,6 +36,65 @@ void check_status(afem_ctx* c, const char* what) {
 }  // namespace afem
 
 using afem::Error;
+
+namespace afem {
+
+// A complex system given in the reference's split storage (type global_matrix,
+// m_iccg_var_takuto.f90:9-18) becomes the device CSR with (K, M) = (Re, Im)
+// and omega = 1.  Rows keep their column order sorted ascending.
+void load_split_system(afem_ctx* c, int n, const int32_t* INU, const int32_t* IAU, const int32_t* INL,
+                       const int32_t* IAL, const double* D, const double* AU, const double* AL, const double* b) {
+  AFEM_REQUIRE(n > 0 && INU && IAU && INL && IAL && D && AU && AL && b, AFEM_EINVAL, "split system: null array");
+  AFEM_REQUIRE(INU[0] == 0 && INL[0] == 0, AFEM_EINVAL, "split system: INU(0) and INL(0) must be 0");
+  std::vector<int32_t> rp(n + 1), cl, dp(n);
+  std::vector<double2> km;
+  const long tot = (long)INU[n] + INL[n] + n;
+  cl.reserve(tot);
+  km.reserve(tot);
+  rp[0] = 0;
+  std::vector<std::pair<int, double2>> row;
+  for (int i = 0; i < n; ++i) {
+    row.clear();
+    for (int k = INL[i]; k < INL[i + 1]; ++k) {
+      const int j = IAL[k] - 1;
+      AFEM_REQUIRE(j >= 0 && j < i, AFEM_EINVAL, "split system: IAL column not below the diagonal");
+      row.push_back({j, make_double2(AL[2L * k], AL[2L * k + 1])});
+    }
+    row.push_back({i, make_double2(D[2L * i], D[2L * i + 1])});
+    for (int k = INU[i]; k < INU[i + 1]; ++k) {
+      const int j = IAU[k] - 1;
+      AFEM_REQUIRE(j > i && j < n, AFEM_EINVAL, "split system: IAU column not above the diagonal");
+      row.push_back({j, make_double2(AU[2L * k], AU[2L * k + 1])});
+    }
+    std::stable_sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    AFEM_REQUIRE((long)row.size() <= ROW_MAX, AFEM_EPATTERN, "split system: row longer than 64 entries");
+    for (auto& e : row) {
+      if (e.first == i) dp[i] = (int32_t)cl.size();
+      cl.push_back(e.first);
+      km.push_back(e.second);
+    }
+    rp[i + 1] = (int32_t)cl.size();
+  }
+  cudaStream_t s = c->stream;
+  c->nline = n;
+  c->ntet = 0;
+  c->node = 0;
+  c->nnz = (long)cl.size();
+  c->rowptr.upload(rp.data(), n + 1, s);
+  c->col.upload(cl.data(), cl.size(), s);
+  c->diagpos.upload(dp.data(), n, s);
+  c->km.upload(km.data(), km.size(), s);
+  c->rhs.upload(reinterpret_cast<const double2*>(b), n, s);
+  c->rhs_nsrc = 1;
+  c->bc.alloc(n);
+  c->bc.zero(s);
+  AFEM_CUDA(cudaStreamSynchronize(s));
+  c->pattern_ready = true;
+  c->assembled = true;
+  invalidate_work(c);
+}
+
+}  // namespace afem
 
 namespace {
 
@@ -331,6 +391,103 @@ int afem_site_coeffs(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item
     AFEM_REQUIRE(c->ntet > 0 && c->nline > 0, AFEM_ESTATE, "site_coeffs: no mesh");
     afem::reset_status(c);
     afem::site_coeffs_device(c, nobs, xyz_obs, item, val_e, val_f, iele);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_set_system(afem_ctx* c, int n, const int32_t* INU, const int32_t* IAU, const int32_t* INL,
+                    const int32_t* IAL, const double* D, const double* AU, const double* AL, const double* b) {
+  return guarded(c, [&]() {
+    afem::load_split_system(c, n, INU, IAU, INL, IAL, D, AU, AL, b);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_cocg13_single(afem_ctx* c, int NP, int NPL, int NPU, double* D, double* AL, const int32_t* INL,
+                       const int32_t* IAL, double* AU, const int32_t* INU, const int32_t* IAU, double* B, double* X,
+                       const char* PRECOND, double SIGMA_DIAG, double SIGMA, double* RESID, int* ITER, int* ERROR,
+                       int NSET) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(RESID && ITER && ERROR && PRECOND && B && X, AFEM_EINVAL, "cocg13_single: null argument");
+    (void)NPL;
+    (void)NPU;
+    *ERROR = 0;
+    if (NSET == 0) {  // COCG13_single.f90:49-52
+      *ERROR = 101;
+      return (int)AFEM_OK;
+    }
+    int prec = AFEM_PRECOND_NONE;
+    if (!std::strncmp(PRECOND, "IC", 2) || !std::strncmp(PRECOND, "ILU", 3)) prec = AFEM_PRECOND_IC;
+    else if (!std::strncmp(PRECOND, "SSOR", 4)) prec = AFEM_PRECOND_SSOR;
+    else if (!std::strncmp(PRECOND, "DIAG", 4)) prec = AFEM_PRECOND_DIAG;
+    AFEM_REQUIRE(!(prec == AFEM_PRECOND_IC && SIGMA != 0.0), AFEM_EINVAL,
+                 "cocg13_single: IC with SIGMA != 0 is not supported on the device");
+    std::vector<double> scale(NP, 1.0);
+    if (NSET == 2) {  // COCG13_single.f90:77-97, the caller's arrays are scaled in place
+      for (int i = 0; i < NP; ++i) scale[i] = 1.0 / std::sqrt(std::hypot(D[2 * i], D[2 * i + 1]));
+      for (int j = 0; j < NP; ++j) {
+        const double a = std::hypot(D[2 * j], D[2 * j + 1]);
+        const double dr = D[2 * j], di = D[2 * j + 1], den = dr * dr + di * di;
+        D[2 * j] = a * dr / den;
+        D[2 * j + 1] = -a * di / den;
+        for (int k = INU[j]; k < INU[j + 1]; ++k) {
+          const double f = scale[IAU[k] - 1] * scale[j];
+          AU[2L * k] *= f;
+          AU[2L * k + 1] *= f;
+        }
+        for (int k = INL[j]; k < INL[j + 1]; ++k) {
+          const double f = scale[IAL[k] - 1] * scale[j];
+          AL[2L * k] *= f;
+          AL[2L * k + 1] *= f;
+        }
+      }
+    }
+    double bn = 0.0;
+    for (int i = 0; i < NP; ++i) {
+      B[2 * i] *= scale[i];
+      B[2 * i + 1] *= scale[i];
+      bn += B[2 * i] * B[2 * i] + B[2 * i + 1] * B[2 * i + 1];
+    }
+    const int maxit = *ITER;
+    if (bn == 0.0) {  // COCG13_single.f90:171-177
+      for (int i = 0; i < 2 * NP; ++i) X[i] = 0.0;
+      *RESID = 0.0;
+      *ITER = 0;
+      for (int i = 0; i < NP; ++i) { B[2 * i] /= scale[i]; B[2 * i + 1] /= scale[i]; }
+      return (int)AFEM_OK;
+    }
+    afem::load_split_system(c, NP, INU, IAU, INL, IAL, D, AU, AL, B);
+    afem_solve_opts o{};
+    o.precond = prec;
+    o.precision = AFEM_FP64;
+    o.tol = *RESID;
+    o.maxit = maxit;
+    o.sigma_diag = SIGMA_DIAG;
+    o.use_graph = 1;
+    afem::SolveExtra ex;
+    ex.x0 = X;
+    ex.recursive_only = true;
+    afem_solve_stats st{};
+    const double freq = 1.0 / (8.0 * std::atan(1.0));  // omega = 1: the values are A itself
+    afem::reset_status(c);
+    const int rc = afem::solve_device(c, 1, &freq, nullptr, &o, &st, &ex);
+    if (rc != AFEM_OK && rc != AFEM_EMAXITER) return rc;
+    std::vector<double2> x(NP);
+    c->X.download(x.data(), NP, c->stream);
+    AFEM_CUDA(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < NP; ++i) {
+      X[2 * i] = x[i].x * scale[i];
+      X[2 * i + 1] = x[i].y * scale[i];
+      B[2 * i] /= scale[i];
+      B[2 * i + 1] /= scale[i];
+    }
+    *RESID = st.resid_recursive;
+    if (rc == AFEM_EMAXITER) {
+      *ERROR = -100;
+      *ITER = maxit + 1;  // value of the Fortran DO variable after a full loop
+    } else {
+      *ITER = st.iterations;
+    }
     return (int)AFEM_OK;
   });
 }

@@ -181,8 +181,14 @@ void exclusive_scan(const int32_t* in, int32_t* out, int n, cudaStream_t s, long
 void assemble_device(afem_ctx* c);        // K, M, rhs, bc (GENMAT + COPY_UL + GENBCCSEM + SET_BC)
 
 // afem_solver.cu
+struct SolveExtra {
+  const double* x0 = nullptr;   // initial guess, [row][system] interleaved complex (host)
+  bool recursive_only = false;  // stop on the recursive residual, no refinement (COCG13_single)
+};
 int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, const afem_solve_opts* o,
-                 afem_solve_stats* st);
+                 afem_solve_stats* st, const SolveExtra* ex = nullptr);
+void load_split_system(afem_ctx* c, int n, const int32_t* INU, const int32_t* IAU, const int32_t* INL,
+                       const int32_t* IAL, const double* D, const double* AU, const double* AL, const double* b);
 void destroy_work(afem_ctx* c);
 void invalidate_work(afem_ctx* c);      // values changed: drop derived copies (FP32 matrix)
 

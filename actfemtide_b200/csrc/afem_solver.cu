@@ -806,7 +806,8 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, double tol,
 }
 
 template <int NS>
-int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_opts* o, afem_solve_stats* st) {
+int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_opts* o, afem_solve_stats* st,
+             const SolveExtra* ex) {
   SolverWork* w = c->work;
   cudaStream_t s = c->stream;
   const int n = c->nline;
@@ -884,13 +885,25 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
 
   DBuf<double2> xacc;  // accumulated FP64 solution
   xacc.alloc(total);
-  xacc.zero(s);
-  // r64 = b (x = 0)
-  AFEM_CUDA(cudaMemcpyAsync(w->r64.p, w->b.p, sizeof(double2) * total, cudaMemcpyDeviceToDevice, s));
+  std::vector<double> rr, bb;
+  double tol_scale = 1.0;  // inner tolerances are relative to ||r0||; the target is relative to ||b||
+  if (ex && ex->x0) {
+    xacc.upload(reinterpret_cast<const double2*>(ex->x0), total, s);
+    AFEM_CUDA(cudaMemcpyAsync(w->x.p, xacc.p, sizeof(double2) * total, cudaMemcpyDeviceToDevice, s));
+    true_residual<NS>(c, w, rr, bb);  // r64 = b - A x0
+    double worst_r = 0.0;
+    for (int k = 0; k < NS; ++k)
+      if (bb[k] > 0) worst_r = std::max(worst_r, std::sqrt(rr[k] / bb[k]));
+    if (worst_r > 0) tol_scale = 1.0 / worst_r;
+  } else {
+    xacc.zero(s);
+    // r64 = b (x = 0)
+    AFEM_CUDA(cudaMemcpyAsync(w->r64.p, w->b.p, sizeof(double2) * total, cudaMemcpyDeviceToDevice, s));
+  }
+  const bool recursive_only = ex && ex->recursive_only;
   const double tol = o->tol > 0 ? o->tol : 1e-8;
   const int maxit = o->maxit > 0 ? o->maxit : 100000;
   int it_total = 0, refinements = 0;
-  std::vector<double> rr, bb;
   std::vector<SysScal> hs;
   std::vector<int> status(NS, AFEM_EMAXITER);
   double worst = 0.0, rec = 0.0;
@@ -900,7 +913,7 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     // residual relative to ||r64||; ask for the reduction still missing,
     // never below what FP32 can deliver in the mixed mode.
     double inner_tol = std::min(0.5, 0.5 * tol / prev);
-    if (outer == 0) inner_tol = tol;
+    if (outer == 0) inner_tol = tol * tol_scale;
     if (mixed) inner_tol = std::max(inner_tol, o->inner_tol > 0 ? o->inner_tol : 1e-5);
     const int left = maxit - it_total;
     if (left <= 0) break;
@@ -922,6 +935,13 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
       if (!(rel <= tol)) all_ok = false;
       if (hs[k].status == AFEM_ENONFINITE || hs[k].status == AFEM_EBREAKDOWN) any_fatal = true;
       status[k] = (rel <= tol) ? AFEM_OK : hs[k].status;
+    }
+    if (recursive_only) {
+      // COCG13_single semantics: one Krylov run judged on its recursive residual
+      for (int k = 0; k < NS; ++k) status[k] = hs[k].status;
+      rec = 0.0;
+      for (int k = 0; k < NS; ++k) rec = std::max(rec, hs[k].resid / tol_scale);
+      break;
     }
     if (all_ok || any_fatal || !std::isfinite(worst)) break;
     if (worst > 0.9 * prev && outer > 0) {  // no progress from a restart
@@ -960,14 +980,14 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
 }  // namespace
 
 int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, const afem_solve_opts* o,
-                 afem_solve_stats* st) {
+                 afem_solve_stats* st, const SolveExtra* ex) {
   AFEM_REQUIRE(c->assembled, AFEM_ESTATE, "solve: system not assembled");
   switch (nsys) {
-    case 1: return solve_ns<1>(c, freq, src, o, st);
-    case 2: return solve_ns<2>(c, freq, src, o, st);
-    case 4: return solve_ns<4>(c, freq, src, o, st);
-    case 8: return solve_ns<8>(c, freq, src, o, st);
-    case 16: return solve_ns<16>(c, freq, src, o, st);
+    case 1: return solve_ns<1>(c, freq, src, o, st, ex);
+    case 2: return solve_ns<2>(c, freq, src, o, st, ex);
+    case 4: return solve_ns<4>(c, freq, src, o, st, ex);
+    case 8: return solve_ns<8>(c, freq, src, o, st, ex);
+    case 16: return solve_ns<16>(c, freq, src, o, st, ex);
     default: throw Error{AFEM_EINVAL, "solve: nsys must be 1, 2, 4, 8 or 16"};
   }
 }

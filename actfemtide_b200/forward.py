@@ -161,6 +161,21 @@ class Forward:
         res.status = rc
         return res
 
+    def cocg13_single(self, INU, IAU, INL, IAL, D, AU, AL, B, X=None, precond="IC", resid=1e-8, maxit=3000,
+                      sigma_diag=1.0, sigma=0.0, nset=1):
+        """COCG13_single with the reference's argument list, on the device (arrays are copied, not mutated)."""
+        n = len(D)
+        D = _c(D, np.complex128).copy(); AU = _c(AU, np.complex128).copy(); AL = _c(AL, np.complex128).copy()
+        B = _c(B, np.complex128).copy()
+        X = np.zeros(n, np.complex128) if X is None else _c(X, np.complex128).copy()
+        INU = _c(INU, np.int32); IAU = _c(IAU, np.int32); INL = _c(INL, np.int32); IAL = _c(IAL, np.int32)
+        R = C.c_double(resid); IT = C.c_int(maxit); ER = C.c_int(0)
+        self._check(self._L.afem_cocg13_single(self.ctx, n, len(AL), len(AU), ptr(D), ptr(AL), ptr(INL), ptr(IAL),
+                                               ptr(AU), ptr(INU), ptr(IAU), ptr(B), ptr(X), precond.encode(),
+                                               sigma_diag, sigma, C.byref(R), C.byref(IT), C.byref(ER), nset))
+        self.nline = n
+        return dict(x=X, resid=R.value, iter=IT.value, error=ER.value)
+
     def solution(self, k: int = 0):
         x = np.zeros(self.nline, np.complex128)
         self._check(self._L.afem_get_solution(self.ctx, k, ptr(x)))

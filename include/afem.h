@@ -140,6 +140,22 @@ int afem_export_system(afem_ctx *ctx, double freq_hz, int isrc, int *n, long *ia
  * stay on the device (afem_get_solution copies them out). */
 int afem_solve(afem_ctx *ctx, int nsys, const double *freq_hz, const int *src, const afem_solve_opts *opts,
                afem_solve_stats *stats);
+/* The solver seam with the reference's own argument list: COCG13_single
+ * (src/solver/COCG13_single.f90:9-12) on the device.  D/AL/AU/B/X complex
+ * (interleaved), INL/INU (0:NP) prefix arrays, IAL/IAU 1-based columns;
+ * PRECOND "IC" / "SSOR" / "DIAG" (anything else: none); X is the initial
+ * guess and the solution; RESID in: tolerance on the recursive residual,
+ * out: reached value; ITER in: MAXIT, out: iterations (MAXIT+1 at the cap,
+ * as the Fortran loop variable); ERROR 0, 101 (NSET = 0) or -100 (cap).
+ * NSET = 2 scales D/AL/AU/B in place as the reference does.  IC with
+ * SIGMA != 0 is rejected (AFEM_EINVAL).  Returns an afem_status. */
+int afem_cocg13_single(afem_ctx *ctx, int NP, int NPL, int NPU, double *D, double *AL, const int32_t *INL,
+                       const int32_t *IAL, double *AU, const int32_t *INU, const int32_t *IAU, double *B, double *X,
+                       const char *PRECOND, double SIGMA_DIAG, double SIGMA, double *RESID, int *ITER, int *ERROR,
+                       int NSET);
+/* Load a system in the same split layout for afem_solve (freq_hz = 1/(2*pi) gives A itself). */
+int afem_set_system(afem_ctx *ctx, int n, const int32_t *INU, const int32_t *IAU, const int32_t *INL,
+                    const int32_t *IAL, const double *D, const double *AU, const double *AL, const double *b);
 /* Solution of system k (n complex values, [nT*km] like bs in forward_bxyz). */
 int afem_get_solution(afem_ctx *ctx, int k, double *x_complex);
 

@@ -222,3 +222,34 @@ def test_repeated_solves_are_reproducible(fw):
     fw.solve(m.freqs[0], precond="SSOR", tol=1e-10)
     x2 = fw.solution(0)
     assert np.array_equal(x1, x2)
+
+
+def test_cocg13_single_seam(fw, oracle):
+    """afem_cocg13_single with the reference's argument list against the oracle's COCG13_single."""
+    m = synth.tiny_model()
+    of = oracle.OracleForward(m)
+    A = of.assemble(m.freqs[0])
+    args = (A.INU, A.IAU, A.INL, A.IAL, A.D, A.AU, A.AL, A.b)
+    for prec in ("IC", "SSOR", "DIAG", "NONE"):
+        g = fw.cocg13_single(*args, precond=prec, resid=1e-30, maxit=4)
+        r = oracle.cocg13_single(A, precond=prec, resid=1e-30, maxit=4)
+        assert g["error"] == r["error"] == -100 and g["iter"] == r["iter"] == 5
+        assert np.abs(g["x"] - r["x"]).max() <= 1e-9 * np.abs(r["x"]).max()
+    g = fw.cocg13_single(*args, precond="SSOR", resid=1e-10, maxit=10000)
+    r = oracle.cocg13_single(A, precond="SSOR", resid=1e-10, maxit=10000)
+    assert g["error"] == 0 and r["error"] == 0 and abs(g["iter"] - r["iter"]) <= 3
+    assert g["resid"] <= 1e-10
+    o1, _, _ = of.sites(g["x"], m.freqs[0]); o2, _, _ = of.sites(r["x"], m.freqs[0])
+    assert np.abs(o1 - o2).max() <= 1e-6 * np.abs(o2).max()
+    # NSET = 0 -> ERROR 101; zero right-hand side -> X = 0, ITER = 0
+    assert fw.cocg13_single(*args, nset=0)["error"] == 101
+    z = fw.cocg13_single(*args[:7], np.zeros_like(A.b))
+    assert z["iter"] == 0 and np.all(z["x"] == 0)
+    # NSET = 2: symmetric diagonal scaling
+    g = fw.cocg13_single(*args, precond="SSOR", resid=1e-10, maxit=10000, nset=2)
+    r = oracle.cocg13_single(A, precond="SSOR", resid=1e-10, maxit=10000, nset=2)
+    o1, _, _ = of.sites(g["x"], m.freqs[0]); o2, _, _ = of.sites(r["x"], m.freqs[0])
+    assert np.abs(o1 - o2).max() <= 1e-6 * np.abs(o2).max()
+    # an initial guess is honoured: starting from the solution converges at once
+    g2 = fw.cocg13_single(*args, X=r["x"], precond="SSOR", resid=1e-8, maxit=10000)
+    assert g2["iter"] <= 2

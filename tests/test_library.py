@@ -1,0 +1,54 @@
+"""The C-ABI library builds, loads on CPU and exports every entry point include/afem.h declares."""
+import os
+import re
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "afem.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(afem_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_header(gpulib):
+    from actfemtide_b200 import capi
+    names = declared_symbols()
+    assert len(names) >= 20
+    out = subprocess.run(["nm", "-D", "--defined-only", capi.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\sT\s(afem_\w+)", out))
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    for n in names:
+        assert hasattr(gpulib, n)
+    assert set(capi.EXPORTS) >= set(names)
+
+
+def test_fortran_g_edit_descriptor(gpulib):
+    # OUTOBSFILESFWD writes '(11g15.7)' (src/common/m_outresp.f90:251)
+    from actfemtide_b200.capi import fortran_g
+    assert fortran_g(1.0 / 44714.0) == "  0.2236436E-04"
+    assert fortran_g(3.14159) == "   3.141590    "
+    assert fortran_g(-123.456) == "  -123.4560    "
+    assert fortran_g(0.0) == "   0.000000    "
+    assert fortran_g(12345678.9) == "  0.1234568E+08"
+    assert fortran_g(0.5) == "  0.5000000    "
+    assert fortran_g(-179.99999999) == "  -180.0000    "
+    for x in np.logspace(-6, 9, 40):
+        s = fortran_g(x)
+        assert len(s) == 15 and abs(float(s) - x) <= 1e-6 * abs(x)
+
+
+def test_no_device_no_context(gpulib):
+    # without a CUDA device afem_create returns NULL instead of crashing
+    from actfemtide_b200 import capi
+    try:
+        import torch
+        has = torch.cuda.is_available()
+    except Exception:
+        has = False
+    if not has:
+        assert not capi.lib().afem_create(0)
