@@ -19,7 +19,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3"]
 # Files whose arithmetic must round like the serial reference (no FMA contraction).
 NOFMA = {"afem_assemble.cu", "afem_sites.cu"}
-SOURCES = ["afem_capi.cu", "afem_mesh.cu", "afem_assemble.cu", "afem_solver.cu", "afem_sites.cu", "afem_io.cpp"]
+SOURCES = ["afem_capi.cu", "afem_mesh.cu", "afem_assemble.cu", "afem_solver.cu", "afem_sites.cu", "afem_mpnn.cu",
+           "afem_io.cpp"]
 HEADERS = ["afem_internal.h", os.path.join("..", "..", "include", "afem.h")]
 
 

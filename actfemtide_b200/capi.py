@@ -20,7 +20,7 @@ STATUS = {
     -5: "AFEM_EBREAKDOWN", -6: "AFEM_ENONFINITE", -7: "AFEM_ECUDA", -8: "AFEM_ESTATE", -9: "AFEM_ETIMEOUT",
     -10: "AFEM_EIO", -11: "AFEM_ENOPRECOND", -12: "AFEM_ESITE", -13: "AFEM_ESTAGNATION",
 }
-PRECOND = {"IC": 0, "SSOR": 1, "DIAG": 2, "NONE": 3}
+PRECOND = {"IC": 0, "SSOR": 1, "DIAG": 2, "NONE": 3, "LEARNED": 4}
 PRECISION = {"fp64": 0, "mixed": 1}
 
 # Every entry point declared in include/afem.h.
@@ -29,7 +29,8 @@ EXPORTS = (
     "afem_set_cond", "afem_set_sigma", "afem_set_source", "afem_set_bounds", "afem_assemble",
     "afem_export_system", "afem_solve", "afem_get_solution", "afem_sites", "afem_site_coeffs", "afem_load_ctl",
     "afem_ctl_info", "afem_run_ctl", "afem_fortran_g", "afem_set_profiling", "afem_profile_count",
-    "afem_profile_entry", "afem_cocg13_single", "afem_set_system",
+    "afem_profile_entry", "afem_cocg13_single", "afem_set_system", "afem_get_residual", "afem_mpnn_nparam",
+    "afem_mpnn_set_params", "afem_mpnn_get_params", "afem_mpnn_forward", "afem_mpnn_loss_grad", "afem_mpnn_train",
 )
 
 
@@ -92,6 +93,13 @@ def lib():
                                      C.c_char_p, C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_int),
                                      C.POINTER(C.c_int), C.c_int]
     L.afem_set_system.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.afem_get_residual.argtypes = [_vp, C.c_int, _vp]
+    L.afem_mpnn_nparam.argtypes = []
+    L.afem_mpnn_set_params.argtypes = [_vp, _vp, C.c_int]
+    L.afem_mpnn_get_params.argtypes = [_vp, _vp]
+    L.afem_mpnn_forward.argtypes = [_vp, C.c_int, _vp, _vp, _vp]
+    L.afem_mpnn_loss_grad.argtypes = [_vp, C.c_double, C.c_int, _vp, C.POINTER(C.c_double), _vp]
+    L.afem_mpnn_train.argtypes = [_vp, C.c_double, C.c_int, _vp, C.c_int, C.c_float, _vp]
     L.afem_set_profiling.argtypes = [_vp, C.c_int]
     L.afem_profile_count.argtypes = [_vp]
     L.afem_profile_entry.argtypes = [_vp, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_long)]
@@ -99,7 +107,8 @@ def lib():
                  "afem_set_bounds", "afem_assemble", "afem_export_system", "afem_solve", "afem_get_solution",
                  "afem_sites", "afem_site_coeffs", "afem_load_ctl", "afem_ctl_info", "afem_run_ctl",
                  "afem_fortran_g", "afem_set_profiling", "afem_profile_count", "afem_profile_entry", "afem_cocg13_single",
-                 "afem_set_system"):
+                 "afem_set_system", "afem_get_residual", "afem_mpnn_nparam", "afem_mpnn_set_params",
+                 "afem_mpnn_get_params", "afem_mpnn_forward", "afem_mpnn_loss_grad", "afem_mpnn_train"):
         getattr(L, name).restype = C.c_int
     _LIB = L
     return L

@@ -144,6 +144,7 @@ void afem_destroy(afem_ctx* c) {
   cudaSetDevice(c->device);
   afem::destroy_work(c);
   afem::destroy_ctl(c);
+  afem::mpnn_destroy(c);
   for (auto* s : c->src) delete s;
   c->src.clear();
     if (c->stream) {
@@ -375,6 +376,14 @@ int afem_get_solution(afem_ctx* c, int k, double* x) {
   });
 }
 
+int afem_get_residual(afem_ctx* c, int k, double* r) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(r, AFEM_EINVAL, "get_residual: null output");
+    afem::get_residual(c, k, r);
+    return (int)AFEM_OK;
+  });
+}
+
 int afem_sites(afem_ctx* c, int nobs, const double* xyz_obs, double* out) {
   return guarded(c, [&]() {
     AFEM_REQUIRE(nobs > 0 && xyz_obs && out, AFEM_EINVAL, "sites: empty or null");
@@ -488,6 +497,50 @@ int afem_cocg13_single(afem_ctx* c, int NP, int NPL, int NPU, double* D, double*
     } else {
       *ITER = st.iterations;
     }
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_mpnn_nparam(void) { return afem::mpnn_nparam(); }
+
+int afem_mpnn_set_params(afem_ctx* c, const float* p, int np) {
+  return guarded(c, [&]() {
+    afem::mpnn_set_params(c, p, np);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_mpnn_get_params(afem_ctx* c, float* p) {
+  return guarded(c, [&]() {
+    afem::mpnn_get_params(c, p);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_mpnn_forward(afem_ctx* c, int nsys, const double* freq, const double* r, double* z) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(c->assembled, AFEM_ESTATE, "mpnn_forward: system not assembled");
+    AFEM_REQUIRE(nsys >= 1 && nsys <= 16 && freq && r && z, AFEM_EINVAL, "mpnn_forward: bad arguments");
+    afem::mpnn_forward_host(c, nsys, freq, r, z);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_mpnn_loss_grad(afem_ctx* c, double freq, int nsamp, const double* r, double* loss, float* grad) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(c->assembled, AFEM_ESTATE, "mpnn_loss_grad: system not assembled");
+    AFEM_REQUIRE(nsamp >= 1 && r, AFEM_EINVAL, "mpnn_loss_grad: bad arguments");
+    const double L = afem::mpnn_loss_grad_host(c, freq, nsamp, r, grad);
+    if (loss) *loss = L;
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_mpnn_train(afem_ctx* c, double freq, int nsamp, const double* r, int steps, float lr, double* hist) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(c->assembled, AFEM_ESTATE, "mpnn_train: system not assembled");
+    AFEM_REQUIRE(nsamp >= 1 && r && steps >= 1, AFEM_EINVAL, "mpnn_train: bad arguments");
+    afem::mpnn_train_host(c, freq, nsamp, r, steps, lr, hist);
     return (int)AFEM_OK;
   });
 }

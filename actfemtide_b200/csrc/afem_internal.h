@@ -113,6 +113,7 @@ struct Profile {
 };
 
 struct SolverWork;  // afem_solver.cu
+struct MpnnState;   // afem_mpnn.cu
 
 }  // namespace afem
 
@@ -164,6 +165,8 @@ struct afem_ctx {
   int nsys = 0;
 
   afem::SolverWork* work = nullptr;
+  afem::MpnnState* mpnn = nullptr;
+  int last_learned_its = 0;  // iterations the last solve ran with the learned preconditioner
   afem::CtlInfo* ctl = nullptr;
 
   afem::DBuf<afem::DevStatus> status;  // one status word
@@ -190,7 +193,22 @@ int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, cons
 void load_split_system(afem_ctx* c, int n, const int32_t* INU, const int32_t* IAU, const int32_t* INL,
                        const int32_t* IAL, const double* D, const double* AU, const double* AL, const double* b);
 void destroy_work(afem_ctx* c);
-void invalidate_work(afem_ctx* c);      // values changed: drop derived copies (FP32 matrix)
+void invalidate_work(afem_ctx* c);
+void get_residual(afem_ctx* c, int k, double* r);  // b - A x of system k after the last solve      // values changed: drop derived copies (FP32 matrix)
+
+// afem_mpnn.cu (learned preconditioner)
+void mpnn_destroy(afem_ctx* c);
+int mpnn_nparam();
+void mpnn_set_params(afem_ctx* c, const float* p, int np);
+void mpnn_get_params(afem_ctx* c, float* p);
+bool mpnn_ready(afem_ctx* c);
+void mpnn_prepare(afem_ctx* c, int ns, const double* d_omega);
+template <class V>
+void mpnn_run(afem_ctx* c, int ns, const double* d_rms, const V* r, V* z, const int* skip);
+void mpnn_forward_host(afem_ctx* c, int ns, const double* freq, const double* r_host, double* z_host);
+double mpnn_loss_grad_host(afem_ctx* c, double freq, int nsamp, const double* r_host, float* grad_host);
+double mpnn_train_host(afem_ctx* c, double freq, int nsamp, const double* r_host, int steps, float lr,
+                       double* hist);
 
 // afem_sites.cu
 void site_coeffs_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item, double* val_e, double* val_f,

@@ -77,6 +77,9 @@ struct SolverWork {
   DBuf<double2> r, z, p, q, dd;     // FP64 inner vectors
   DBuf<float2> rf, zf, pf, qf, ddf; // FP32 inner vectors
   DBuf<float2> kmf;                 // FP32 copy of (K, M)
+  DBuf<double2> rprev;              // flexible COCG: previous residual (FP64 inner)
+  DBuf<float2> rprevf;              // flexible COCG: previous residual (FP32 inner)
+  DBuf<double> rms;                 // per-system rms(r) for the learned preconditioner
   bool kmf_valid = false;
   DBuf<unsigned> flag_f, flag_b;
   DBuf<double> part;                // partial sums [block][sys][4]
@@ -161,7 +164,7 @@ __global__ void __launch_bounds__(256)
           typename Cx<T>::V* __restrict__ y, const typename Cx<T>::V* __restrict__ p,
           const typename Cx<T>::V* __restrict__ q, double2* __restrict__ x, const typename Cx<T>::V* __restrict__ dd,
           unsigned* __restrict__ flag, int mode, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl,
-          double* __restrict__ part, DevStatus* st) {
+          double* __restrict__ part, DevStatus* st, typename Cx<T>::V* __restrict__ rprev) {
   using V = typename Cx<T>::V;
   if (ctrl->done) return;
   constexpr int G = 32 / NS;
@@ -176,6 +179,7 @@ __global__ void __launch_bounds__(256)
   double rr = 0.0;
   for (int row = warp; row < n; row += nwarps) {
     V ri = r[(long)row * NS + s];
+    if (rprev && g == 0) rprev[(long)row * NS + s] = ri;  // flexible COCG keeps r_k
     if (update && act && g == 0) {
       const V qi = q[(long)row * NS + s], pi = p[(long)row * NS + s];
       ri = Cx<T>::make((T)((double)ri.x - (al.x * (double)qi.x - al.y * (double)qi.y)),
@@ -194,7 +198,7 @@ __global__ void __launch_bounds__(256)
       }
       continue;
     }
-    if (mode == 3) {  // no preconditioner
+    if (mode >= 3) {  // no preconditioner (3) / learned network applied after this kernel (4)
       if (g == 0) y[(long)row * NS + s] = ri;
       continue;
     }
@@ -233,7 +237,8 @@ __global__ void __launch_bounds__(256)
     k_bwd(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const int32_t* __restrict__ diagpos,
           const typename Cx<T>::V* __restrict__ km, int n, const typename Cx<T>::V* __restrict__ r,
           typename Cx<T>::V* __restrict__ z, const typename Cx<T>::V* __restrict__ dd, unsigned* __restrict__ flag,
-          int mode, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl, double* __restrict__ part, DevStatus* st) {
+          int mode, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl, double* __restrict__ part, DevStatus* st,
+          const typename Cx<T>::V* __restrict__ rprev) {
   using V = typename Cx<T>::V;
   if (ctrl->done) return;
   constexpr int G = 32 / NS;
@@ -242,7 +247,7 @@ __global__ void __launch_bounds__(256)
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const double om = sc[s].omega;
-  double rx = 0.0, ry = 0.0;
+  double rx = 0.0, ry = 0.0, px = 0.0, py = 0.0;
   for (int it = warp; it < n; it += nwarps) {
     const int row = n - 1 - it;
     V zi = z[(long)row * NS + s];
@@ -275,10 +280,15 @@ __global__ void __launch_bounds__(256)
       const V ri = r[(long)row * NS + s];
       rx += (double)ri.x * (double)zi.x - (double)ri.y * (double)zi.y;
       ry += (double)ri.x * (double)zi.y + (double)ri.y * (double)zi.x;
+      if (rprev) {
+        const V rp = rprev[(long)row * NS + s];
+        px += (double)rp.x * (double)zi.x - (double)rp.y * (double)zi.y;
+        py += (double)rp.x * (double)zi.y + (double)rp.y * (double)zi.x;
+      }
     }
   }
-  double v[2] = {rx, ry};
-  block_partials<NS, 2>(v, part);
+  double v[4] = {rx, ry, px, py};
+  block_partials<NS, 4>(v, part);
 }
 
 // ------------------------------------------------------------------ p update, SpMV
@@ -367,7 +377,7 @@ __device__ __forceinline__ void sum_partials(const double* part, int nblocks, in
   for (int v = 0; v < nvals; ++v) out[v] = sh[threadIdx.x >> 5][v];
 }
 
-__global__ void k_scal_r(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns) {
+__global__ void k_scal_r(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns, double* rms, int n) {
   if (ctrl->done) return;
   const int s = threadIdx.x >> 5;
   bool finished = true;
@@ -378,6 +388,7 @@ __global__ void k_scal_r(SysScal* sc, Ctrl* ctrl, const double* part, int nblock
       SysScal& S = sc[s];
       if (S.active) {
         S.rr = rr;
+        if (rms) rms[s] = sqrt(rr / n) > 0.0 ? sqrt(rr / n) : 1.0;
         S.resid = sqrt(rr / S.bnrm2);
         if (ctrl->iter > 0) S.iter += 1;
         if (!isfinite(S.resid)) { S.active = 0; S.status = AFEM_ENONFINITE; }
@@ -398,18 +409,22 @@ __global__ void k_scal_r(SysScal* sc, Ctrl* ctrl, const double* part, int nblock
 
 __device__ __forceinline__ double2 d_cdiv(double2 a, double2 b) { return cdiv(a, b); }
 
-__global__ void k_scal_rho(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns) {
+__global__ void k_scal_rho(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns, int flexible) {
   if (ctrl->done) return;
   const int s = threadIdx.x >> 5;
   if (s >= ns) return;
-  double v[2];
-  sum_partials(part, nblocks, s, 0, v, 2);
+  double v[4];
+  sum_partials(part, nblocks, s, 0, v, 4);
   if ((threadIdx.x & 31) == 0) {
     SysScal& S = sc[s];
     S.rho = make_double2(v[0], v[1]);
     if (S.active) {
       if (S.rho.x == 0.0 && S.rho.y == 0.0) { S.active = 0; S.status = AFEM_EBREAKDOWN; }
-      else if (ctrl->iter > 0) S.beta = d_cdiv(S.rho, S.rho1);
+      else if (ctrl->iter > 0) {
+        // flexible (Polak-Ribiere) form for a variable preconditioner: z^T (r_k+1 - r_k) / z_k^T r_k
+        const double2 num = flexible ? make_double2(S.rho.x - v[2], S.rho.y - v[3]) : S.rho;
+        S.beta = d_cdiv(num, S.rho1);
+      }
     }
   }
 }
@@ -621,6 +636,7 @@ struct Inner<double, NS> {
   static V* P(SolverWork* w) { return w->p.p; }
   static V* Q(SolverWork* w) { return w->q.p; }
   static V* DD(SolverWork* w) { return w->dd.p; }
+  static V* RP(SolverWork* w) { return w->rprev.p; }
   static const V* KM(afem_ctx* c, SolverWork*) { return c->km.p; }
 };
 template <int NS>
@@ -631,34 +647,38 @@ struct Inner<float, NS> {
   static V* P(SolverWork* w) { return w->pf.p; }
   static V* Q(SolverWork* w) { return w->qf.p; }
   static V* DD(SolverWork* w) { return w->ddf.p; }
+  static V* RP(SolverWork* w) { return w->rprevf.p; }
   static const V* KM(afem_ctx*, SolverWork* w) { return w->kmf.p; }
 };
 
-// One COCG iteration (7 launches).
+// One COCG iteration (7 launches; the learned preconditioner adds the network's 8).
 template <class T, int NS>
 void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, cudaEvent_t* ev) {
   using I = Inner<T, NS>;
+  using V = typename I::V;
   cudaStream_t s = c->stream;
   const int n = w->n;
+  const bool learned = mode == AFEM_PRECOND_LEARNED;
+  V* rp = learned ? I::RP(w) : nullptr;
   if (ev) AFEM_CUDA(cudaEventRecord(ev[0], s));
   launch_coop(k_fwd<T, NS>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
-              (const int32_t*)c->diagpos.p, I::KM(c, w), n, I::R(w), I::Z(w), (const typename I::V*)I::P(w),
-              (const typename I::V*)I::Q(w), w->x.p, (const typename I::V*)I::DD(w), w->flag_f.p, mode, w->sc.p,
-              w->ctrl.p, w->part.p, c->status.p);
+              (const int32_t*)c->diagpos.p, I::KM(c, w), n, I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w),
+              w->x.p, (const V*)I::DD(w), w->flag_f.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, rp);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[1], s));
-  k_scal_r<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, sweep_blocks, NS);
+  k_scal_r<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, sweep_blocks, NS, learned ? w->rms.p : nullptr,
+                                     n);
+  if (learned) mpnn_run<V>(c, NS, w->rms.p, (const V*)I::R(w), I::Z(w), &w->ctrl.p->done);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[2], s));
   launch_coop(k_bwd<T, NS>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
-              (const int32_t*)c->diagpos.p, I::KM(c, w), n, (const typename I::V*)I::R(w), I::Z(w),
-              (const typename I::V*)I::DD(w), w->flag_b.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p);
+              (const int32_t*)c->diagpos.p, I::KM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w),
+              w->flag_b.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, (const V*)rp);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[3], s));
-  k_scal_rho<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, sweep_blocks, NS);
+  k_scal_rho<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, sweep_blocks, NS, learned ? 1 : 0);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[4], s));
   k_pupd<T, NS><<<c->num_sms * 8, 256, 0, s>>>(n, I::Z(w), I::P(w), w->sc.p, w->ctrl.p);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[5], s));
   k_spmv<T, NS><<<w->nblocks, 256, 0, s>>>((const int32_t*)c->rowptr.p, (const int32_t*)c->col.p, I::KM(c, w), n,
-                                           (const typename I::V*)I::P(w), I::Q(w), w->sc.p, w->ctrl.p, w->part.p,
-                                           (const typename I::V*)nullptr);
+                                           (const V*)I::P(w), I::Q(w), w->sc.p, w->ctrl.p, w->part.p, (const V*)nullptr);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[6], s));
   k_scal_pq<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, NS);
 }
@@ -703,8 +723,8 @@ void setup_dd(afem_ctx* c, SolverWork* w, int precond, double sd) {
 // Inner COCG from x_inner = 0 on right-hand side r64 (FP64, converted to T).
 // Returns iterations; fills per-system status/resid.
 template <class T, int NS>
-int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, double tol, int maxit, int check_every,
-               const double* d_omega, std::vector<SysScal>& hs) {
+int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond, double tol, int maxit,
+               int check_every, const double* d_omega, std::vector<SysScal>& hs, bool* stalled) {
   using I = Inner<T, NS>;
   cudaStream_t s = c->stream;
   const int n = w->n;
@@ -719,8 +739,17 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, double tol,
                                                   w->x.p, w->q.p, w->sc.p, (const Ctrl*)nullptr, w->part.p, w->r64.p);
   }
   k_init_sys<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, NS, tol, maxit, d_omega);
-  setup_dd<T, NS>(c, w, o->precond, o->sigma_diag > 0 ? o->sigma_diag : 1.0);
-  const int mode = o->precond;
+  setup_dd<T, NS>(c, w, precond, o->sigma_diag > 0 ? o->sigma_diag : 1.0);
+  const int mode = precond;
+  const bool learned = mode == AFEM_PRECOND_LEARNED;
+  if (learned) {
+    using V = typename I::V;
+    if (sizeof(V) == 8) w->rprevf.alloc(total); else w->rprev.alloc(total);
+    w->rms.alloc(NS);
+    mpnn_prepare(c, NS, d_omega);
+  }
+  if (stalled) *stalled = false;
+  double watch = 1e300;  // learned mode: residual at the last stall check
   const int sweep_blocks = coresident_blocks(k_fwd<T, NS>, c->num_sms);
   const int sb2 = coresident_blocks(k_bwd<T, NS>, c->num_sms);
   const int sblocks = std::min(std::min(sweep_blocks, sb2), w->nblocks);
@@ -790,6 +819,24 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, double tol,
       }
     }
     iter_before = w->h_ctrl->iter;
+    if (learned && !w->h_ctrl->done && w->h_ctrl->iter >= 2 * chunk) {
+      // stall detector: the learned preconditioner must halve the residual every two chunks
+      AFEM_CUDA(cudaMemcpyAsync(w->h_sc, w->sc.p, sizeof(SysScal) * NS, cudaMemcpyDeviceToHost, s));
+      AFEM_CUDA(cudaStreamSynchronize(s));
+      double worst = 0.0;
+      for (int k = 0; k < NS; ++k)
+        if (w->h_sc[k].active) worst = std::max(worst, w->h_sc[k].resid);
+      if ((w->h_ctrl->iter / chunk) % 2 == 0) {
+        if (!(worst < 0.5 * watch) && watch < 1e300) {
+          const int one = 1;
+          AFEM_CUDA(cudaMemcpyAsync(&w->ctrl.p->done, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+          AFEM_CUDA(cudaStreamSynchronize(s));
+          if (stalled) *stalled = true;
+          break;
+        }
+        watch = worst;
+      }
+    }
     if (w->h_ctrl->done) break;
     if (w->h_ctrl->iter > maxit + 2 * chunk) break;  // safety: the scalar kernels stop at maxit
   }
@@ -908,6 +955,11 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
   std::vector<int> status(NS, AFEM_EMAXITER);
   double worst = 0.0, rec = 0.0;
   double prev = 1.0;  // current ||b - A x|| / ||b|| (worst system)
+  int precond_now = o->precond;
+  int learned_its = 0;
+  bool fell_back = false;
+  if (precond_now == AFEM_PRECOND_LEARNED)
+    AFEM_REQUIRE(mpnn_ready(c), AFEM_ESTATE, "solve: the learned preconditioner has no weights");
   for (int outer = 0; outer < 64; ++outer) {
     // The inner solve starts from x = 0 on r64 and stops at a recursive
     // residual relative to ||r64||; ask for the reduction still missing,
@@ -918,8 +970,17 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     const int left = maxit - it_total;
     if (left <= 0) break;
     int its;
-    if (mixed) its = inner_cocg<float, NS>(c, w, o, inner_tol, left, o->check_every, d_om.p, hs);
-    else its = inner_cocg<double, NS>(c, w, o, inner_tol, left, o->check_every, d_om.p, hs);
+    bool stalled = false;
+    if (mixed) its = inner_cocg<float, NS>(c, w, o, precond_now, inner_tol, left, o->check_every, d_om.p, hs, &stalled);
+    else its = inner_cocg<double, NS>(c, w, o, precond_now, inner_tol, left, o->check_every, d_om.p, hs, &stalled);
+    if (precond_now == AFEM_PRECOND_LEARNED) {
+      learned_its += its;
+      if (stalled) {
+        // fallback: continue from the current iterate with SSOR-COCG
+        precond_now = AFEM_PRECOND_SSOR;
+        fell_back = true;
+      }
+    }
     it_total += its;
     refinements += 1;
     k_add_x<<<c->num_sms * 8, 256, 0, s>>>(xacc.p, w->x.p, total);
@@ -944,12 +1005,13 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
       break;
     }
     if (all_ok || any_fatal || !std::isfinite(worst)) break;
-    if (worst > 0.9 * prev && outer > 0) {  // no progress from a restart
+    if (worst > 0.9 * prev && outer > 0 && !fell_back) {  // no progress from a restart
       for (int k = 0; k < NS; ++k)
         if (status[k] == AFEM_OK || status[k] == AFEM_EMAXITER) status[k] = status[k] == AFEM_OK ? AFEM_OK : AFEM_ESTAGNATION;
       break;
     }
     prev = worst;
+    fell_back = false;
   }
   AFEM_CUDA(cudaEventRecord(e1, s));
   AFEM_CUDA(cudaEventSynchronize(e1));
@@ -966,6 +1028,7 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
   int stat = AFEM_OK;
   for (int k = 0; k < NS; ++k)
     if (status[k] != AFEM_OK) { stat = status[k]; break; }
+  c->last_learned_its = learned_its;
   if (st) {
     st->iterations = it_total;
     st->refinements = refinements;
@@ -989,6 +1052,18 @@ int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, cons
     case 8: return solve_ns<8>(c, freq, src, o, st, ex);
     case 16: return solve_ns<16>(c, freq, src, o, st, ex);
     default: throw Error{AFEM_EINVAL, "solve: nsys must be 1, 2, 4, 8 or 16"};
+  }
+}
+
+void get_residual(afem_ctx* c, int k, double* r) {
+  SolverWork* w = c->work;
+  AFEM_REQUIRE(w && c->nsys > 0 && k >= 0 && k < c->nsys, AFEM_ESTATE, "get_residual: no such system");
+  std::vector<double2> all((size_t)w->n * w->ns);
+  w->r64.download(all.data(), all.size(), c->stream);
+  AFEM_CUDA(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < w->n; ++i) {
+    r[2 * i] = all[(size_t)i * w->ns + k].x;
+    r[2 * i + 1] = all[(size_t)i * w->ns + k].y;
   }
 }
 

@@ -176,6 +176,43 @@ class Forward:
         self.nline = n
         return dict(x=X, resid=R.value, iter=IT.value, error=ER.value)
 
+    def residual(self, k: int = 0):
+        """FP64 b - A x of system k after the last solve."""
+        r = np.zeros(self.nline, np.complex128)
+        self._check(self._L.afem_get_residual(self.ctx, k, ptr(r)))
+        return r
+
+    # ------------------------------------------------------------ learned preconditioner
+    def mpnn_set_params(self, p):
+        p = _c(p, np.float32)
+        self._check(self._L.afem_mpnn_set_params(self.ctx, ptr(p), len(p)))
+
+    def mpnn_get_params(self):
+        p = np.zeros(self._L.afem_mpnn_nparam(), np.float32)
+        self._check(self._L.afem_mpnn_get_params(self.ctx, ptr(p)))
+        return p
+
+    def mpnn_forward(self, freqs, r):
+        """z = P(r); r (n,) or (n, nsys) complex."""
+        f = _c(np.atleast_1d(freqs), np.float64)
+        r2 = _c(np.asarray(r).reshape(self.nline, len(f)), np.complex128)
+        z = np.zeros_like(r2)
+        self._check(self._L.afem_mpnn_forward(self.ctx, len(f), ptr(f), ptr(r2), ptr(z)))
+        return z.reshape(np.asarray(r).shape)
+
+    def mpnn_loss_grad(self, freq, samples):
+        s = _c(np.atleast_2d(samples), np.complex128)
+        g = np.zeros(self._L.afem_mpnn_nparam(), np.float32)
+        loss = C.c_double(0)
+        self._check(self._L.afem_mpnn_loss_grad(self.ctx, float(freq), s.shape[0], ptr(s), C.byref(loss), ptr(g)))
+        return loss.value, g
+
+    def mpnn_train(self, freq, samples, steps, lr=1e-3):
+        s = _c(np.atleast_2d(samples), np.complex128)
+        hist = np.zeros(steps)
+        self._check(self._L.afem_mpnn_train(self.ctx, float(freq), s.shape[0], ptr(s), steps, lr, ptr(hist)))
+        return hist
+
     def solution(self, k: int = 0):
         x = np.zeros(self.nline, np.complex128)
         self._check(self._L.afem_get_solution(self.ctx, k, ptr(x)))

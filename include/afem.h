@@ -52,7 +52,8 @@ typedef enum afem_precond {
   AFEM_PRECOND_IC = 0,    /* diagonal-modified IC(0): DD_i = 1/(D_i*sd - sum AL_k^2 DD_col) */
   AFEM_PRECOND_SSOR = 1,  /* DD_i = 1/(sd*D_i), same forward/backward sweeps */
   AFEM_PRECOND_DIAG = 2,  /* z = DD * r */
-  AFEM_PRECOND_NONE = 3
+  AFEM_PRECOND_NONE = 3,
+  AFEM_PRECOND_LEARNED = 4  /* flexible COCG with the learned network; SSOR-COCG restart when it stalls */
 } afem_precond;
 
 typedef enum afem_precision {
@@ -156,6 +157,8 @@ int afem_cocg13_single(afem_ctx *ctx, int NP, int NPL, int NPU, double *D, doubl
 /* Load a system in the same split layout for afem_solve (freq_hz = 1/(2*pi) gives A itself). */
 int afem_set_system(afem_ctx *ctx, int n, const int32_t *INU, const int32_t *IAU, const int32_t *INL,
                     const int32_t *IAL, const double *D, const double *AU, const double *AL, const double *b);
+/* FP64 true residual b - A x of system k after the last afem_solve (n complex values). */
+int afem_get_residual(afem_ctx *ctx, int k, double *r_complex);
 /* Solution of system k (n complex values, [nT*km] like bs in forward_bxyz). */
 int afem_get_solution(afem_ctx *ctx, int k, double *x_complex);
 
@@ -170,6 +173,22 @@ int afem_sites(afem_ctx *ctx, int nobs, const double *xyz_obs, double *out_compl
  * [(c*nobs + s)*6 + j]; iele: containing tetrahedron) for parity checks. */
 int afem_site_coeffs(afem_ctx *ctx, int nobs, const double *xyz_obs, int32_t *item, double *val_e, double *val_f,
                      int32_t *iele);
+
+/* ---- learned preconditioner (no counterpart in the reference) ---------------- */
+/* A message-passing network over the matrix graph (6 layers, width 48, BF16
+ * weights, FP32 accumulation) that maps a residual r to z ~ A^-1 r; used by
+ * afem_solve with AFEM_PRECOND_LEARNED inside flexible COCG.  Parameters are
+ * one flat FP32 vector of afem_mpnn_nparam() values (W_in 8x48, then per
+ * layer W 144x48 and c 48, then W_out 48x2, all row-major). */
+int afem_mpnn_nparam(void);
+int afem_mpnn_set_params(afem_ctx *ctx, const float *params, int nparam);
+int afem_mpnn_get_params(afem_ctx *ctx, float *params);
+/* z = P(r) for nsys systems at freq[k]; r, z: [row][system] interleaved complex. */
+int afem_mpnn_forward(afem_ctx *ctx, int nsys, const double *freq, const double *r, double *z);
+/* Sum over nsamp residuals (each n complex values) of ||A P(r) - r||^2/||r||^2 and its gradient. */
+int afem_mpnn_loss_grad(afem_ctx *ctx, double freq_hz, int nsamp, const double *r, double *loss, float *grad);
+/* steps Adam updates (lr) on the mean loss over the samples; hist[steps] receives the loss per step. */
+int afem_mpnn_train(afem_ctx *ctx, double freq_hz, int nsamp, const double *r, int steps, float lr, double *hist);
 
 /* ---- measurement (no counterpart in the reference, which only prints banners) -- */
 /* Accumulate per-kernel device time (CUDA events on the context's stream)
