@@ -31,6 +31,7 @@ EXPORTS = (
     "afem_ctl_info", "afem_run_ctl", "afem_fortran_g", "afem_set_profiling", "afem_profile_count",
     "afem_profile_entry", "afem_cocg13_single", "afem_set_system", "afem_get_residual", "afem_mpnn_nparam",
     "afem_mpnn_set_params", "afem_mpnn_get_params", "afem_mpnn_forward", "afem_mpnn_loss_grad", "afem_mpnn_train",
+    "afem_solve_rhs", "afem_jacobian", "afem_sweep_schedule",
 )
 
 
@@ -94,6 +95,9 @@ def lib():
                                      C.POINTER(C.c_int), C.c_int]
     L.afem_set_system.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.afem_get_residual.argtypes = [_vp, C.c_int, _vp]
+    L.afem_sweep_schedule.argtypes = [C.c_int, _vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.afem_solve_rhs.argtypes = [_vp, C.c_int, _vp, _vp, C.POINTER(SolveOpts), C.POINTER(SolveStats)]
+    L.afem_jacobian.argtypes = [_vp, C.c_double, _vp, C.c_int, _vp]
     L.afem_mpnn_nparam.argtypes = []
     L.afem_mpnn_set_params.argtypes = [_vp, _vp, C.c_int]
     L.afem_mpnn_get_params.argtypes = [_vp, _vp]
@@ -108,7 +112,8 @@ def lib():
                  "afem_sites", "afem_site_coeffs", "afem_load_ctl", "afem_ctl_info", "afem_run_ctl",
                  "afem_fortran_g", "afem_set_profiling", "afem_profile_count", "afem_profile_entry", "afem_cocg13_single",
                  "afem_set_system", "afem_get_residual", "afem_mpnn_nparam", "afem_mpnn_set_params",
-                 "afem_mpnn_get_params", "afem_mpnn_forward", "afem_mpnn_loss_grad", "afem_mpnn_train"):
+                 "afem_mpnn_get_params", "afem_mpnn_forward", "afem_mpnn_loss_grad", "afem_mpnn_train",
+                 "afem_solve_rhs", "afem_jacobian", "afem_sweep_schedule"):
         getattr(L, name).restype = C.c_int
     _LIB = L
     return L

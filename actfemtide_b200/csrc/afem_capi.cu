@@ -90,6 +90,7 @@ void load_split_system(afem_ctx* c, int n, const int32_t* INU, const int32_t* IA
   c->bc.zero(s);
   AFEM_CUDA(cudaStreamSynchronize(s));
   c->pattern_ready = true;
+  c->schedule_ready = false;
   c->assembled = true;
   invalidate_work(c);
 }
@@ -355,7 +356,7 @@ int afem_solve(afem_ctx* c, int nsys, const double* freq, const int* src, const 
                afem_solve_stats* stats) {
   return guarded(c, [&]() {
     AFEM_REQUIRE(freq && opts, AFEM_EINVAL, "solve: null freq or opts");
-    AFEM_REQUIRE(opts->precond >= 0 && opts->precond <= 3, AFEM_EINVAL, "solve: unknown preconditioner");
+    AFEM_REQUIRE(opts->precond >= 0 && opts->precond <= 4, AFEM_EINVAL, "solve: unknown preconditioner");
     afem::reset_status(c);
     return afem::solve_device(c, nsys, freq, src, opts, stats);
   });
@@ -372,6 +373,26 @@ int afem_get_solution(afem_ctx* c, int k, double* x) {
       x[2 * i] = all[(size_t)i * c->nsys + k].x;
       x[2 * i + 1] = all[(size_t)i * c->nsys + k].y;
     }
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_solve_rhs(afem_ctx* c, int nsys, const double* freq, const double* rhs, const afem_solve_opts* opts,
+                   afem_solve_stats* stats) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(freq && opts && rhs, AFEM_EINVAL, "solve_rhs: null argument");
+    afem::reset_status(c);
+    afem::SolveExtra ex;
+    ex.rhs = rhs;
+    return afem::solve_device(c, nsys, freq, nullptr, opts, stats, &ex);
+  });
+}
+
+int afem_jacobian(afem_ctx* c, double freq, const double* x, int nadj, double* J) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(x && J && nadj > 0, AFEM_EINVAL, "jacobian: null argument");
+    afem::reset_status(c);
+    afem::jacobian_device(c, freq, x, nadj, J);
     return (int)AFEM_OK;
   });
 }

@@ -151,6 +151,11 @@ struct afem_ctx {
   afem::DBuf<int32_t> etp;      // nline+1, edge -> (tet, local edge) adjacency
   afem::DBuf<int32_t> etl;      // 6*ntet, value = tet*8 + local edge, ascending per edge
   bool pattern_ready = false;
+  // triangular-sweep schedules: rows in dependency-level order (a topological order)
+  afem::DBuf<int32_t> perm_f;   // forward sweep: lower-triangle levels ascending, ties by row
+  afem::DBuf<int32_t> perm_b;   // backward sweep: upper-triangle levels ascending, ties by row descending
+  int levels_f = 0, levels_b = 0;
+  bool schedule_ready = false;
 
   // values: A(omega) = K + i*omega*M, stored interleaved (K_k, M_k)
   afem::DBuf<double2> km;       // nnz
@@ -178,6 +183,7 @@ namespace afem {
 // afem_mesh.cu
 void build_lines_device(afem_ctx* c);     // MKLINE_V2 + MKN6 on the device
 void build_pattern_device(afem_ctx* c);   // adjacency + full CSR pattern
+void build_schedule(afem_ctx* c);         // sweep level schedules from the pattern
 void exclusive_scan(const int32_t* in, int32_t* out, int n, cudaStream_t s, long* total_host);
 
 // afem_assemble.cu
@@ -187,6 +193,7 @@ void assemble_device(afem_ctx* c);        // K, M, rhs, bc (GENMAT + COPY_UL + G
 struct SolveExtra {
   const double* x0 = nullptr;   // initial guess, [row][system] interleaved complex (host)
   bool recursive_only = false;  // stop on the recursive residual, no refinement (COCG13_single)
+  const double* rhs = nullptr;  // caller right-hand sides, [row][system] interleaved complex (host)
 };
 int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, const afem_solve_opts* o,
                  afem_solve_stats* st, const SolveExtra* ex = nullptr);
@@ -209,6 +216,9 @@ void mpnn_forward_host(afem_ctx* c, int ns, const double* freq, const double* r_
 double mpnn_loss_grad_host(afem_ctx* c, double freq, int nsamp, const double* r_host, float* grad_host);
 double mpnn_train_host(afem_ctx* c, double freq, int nsamp, const double* r_host, int steps, float lr,
                        double* hist);
+
+// afem_adjoint.cu
+void jacobian_device(afem_ctx* c, double freq, const double* x_host, int nadj, double* J_host);
 
 // afem_sites.cu
 void site_coeffs_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item, double* val_e, double* val_f,
@@ -255,6 +265,14 @@ __device__ __forceinline__ void raise_status(DevStatus* st, int code, int where)
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+// Polling load: coherent at GPU scope (served by L2), no fence.  The data a
+// flag publishes is read after the poll loop exits (control dependency) with
+// ld.global.cg, and the writer fences before it stores the flag.
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
 __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {

@@ -3,6 +3,9 @@
 // Integer work only: every output is bit-identical to the reference's
 // serial construction (tmtgem/common/m_line_type.f90:120-277 for the
 // numbering, src/solver/m_iccg_var_takuto.f90:277-485 for the pattern).
+#include <algorithm>
+#include <vector>
+
 #include "afem_internal.h"
 
 namespace afem {
@@ -319,6 +322,71 @@ void build_pattern_device(afem_ctx* c) {
                                                                   c->rowptr.p, c->col.p, c->diagpos.p, c->status.p);
   check_status(c, "pattern: fill");
   c->pattern_ready = true;
+  c->schedule_ready = false;
+}
+
+// Dependency levels of the two triangular sweeps (computed once per pattern on
+// the host: one pass over the strictly lower / upper parts) and the processing
+// orders the sweep kernels walk: rows sorted by level.  Every row's formula is
+// unchanged, only the order in which rows are visited; a row's dependencies
+// always have a smaller level, so the order is topological.
+void compute_schedule(int n, const int32_t* rp, const int32_t* dp, const int32_t* cl, int32_t* perm_f,
+                      int32_t* perm_b, int* levels_f, int* levels_b) {
+  std::vector<int32_t> lev(n);
+  auto order = [&](bool forward, int32_t* perm, int* nlev) {
+    int mx = 0;
+    if (forward) {
+      for (int i = 0; i < n; ++i) {
+        int l = 0;
+        for (int k = rp[i]; k < dp[i]; ++k) l = std::max(l, lev[cl[k]] + 1);
+        lev[i] = l;
+        mx = std::max(mx, l);
+      }
+    } else {
+      for (int i = n - 1; i >= 0; --i) {
+        int l = 0;
+        for (int k = dp[i] + 1; k < rp[i + 1]; ++k) l = std::max(l, lev[cl[k]] + 1);
+        lev[i] = l;
+        mx = std::max(mx, l);
+      }
+    }
+    *nlev = n > 0 ? mx + 1 : 0;
+    std::vector<int32_t> cnt(mx + 2, 0);
+    for (int i = 0; i < n; ++i) cnt[lev[i] + 1]++;
+    for (int l = 0; l <= mx; ++l) cnt[l + 1] += cnt[l];
+    if (forward) {
+      for (int i = 0; i < n; ++i) perm[cnt[lev[i]]++] = i;
+    } else {
+      for (int i = n - 1; i >= 0; --i) perm[cnt[lev[i]]++] = i;
+    }
+  };
+  order(true, perm_f, levels_f);
+  order(false, perm_b, levels_b);
+}
+
+void build_schedule(afem_ctx* c) {
+  if (c->schedule_ready) return;
+  const int n = c->nline;
+  cudaStream_t s = c->stream;
+  std::vector<int32_t> rp(n + 1), dp(n), cl(c->nnz), pf(n), pb(n);
+  c->rowptr.download(rp.data(), n + 1, s);
+  c->diagpos.download(dp.data(), n, s);
+  c->col.download(cl.data(), c->nnz, s);
+  AFEM_CUDA(cudaStreamSynchronize(s));
+  compute_schedule(n, rp.data(), dp.data(), cl.data(), pf.data(), pb.data(), &c->levels_f, &c->levels_b);
+  c->perm_f.upload(pf.data(), n, s);
+  c->perm_b.upload(pb.data(), n, s);
+  AFEM_CUDA(cudaStreamSynchronize(s));
+  c->schedule_ready = true;
 }
 
 }  // namespace afem
+
+// Host-only: the sweep schedules of a CSR pattern (diagonal included, columns
+// ascending, 0-based) for tests and tools.
+extern "C" int afem_sweep_schedule(int n, const int32_t* rowptr, const int32_t* col, const int32_t* diagpos,
+                                   int32_t* perm_f, int32_t* perm_b, int* levels_f, int* levels_b) {
+  if (n < 0 || !rowptr || !col || !diagpos || !perm_f || !perm_b) return AFEM_EINVAL;
+  afem::compute_schedule(n, rowptr, col, diagpos, perm_f, perm_b, levels_f, levels_b);
+  return AFEM_OK;
+}

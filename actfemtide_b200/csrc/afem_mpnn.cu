@@ -313,28 +313,32 @@ __global__ void k_loss_grad(const int32_t* __restrict__ rowptr, const int32_t* _
 }
 
 // ------------------------------------------------------------------ training: backward
-// dh = do W_out^T; dW_out += h^T do   (rows system-major)
+// dh = do W_out^T; dW_out += h^T do   (rows system-major; warp per row, lane = features 2l, 2l+1)
 __global__ void k_decode_bwd(const __nv_bfloat16* __restrict__ h, long rows, const float* __restrict__ dout,
                              const float* __restrict__ wout, float* __restrict__ dh, float* __restrict__ gwout) {
   __shared__ float red[H * 2];
   for (int k = threadIdx.x; k < H * 2; k += blockDim.x) red[k] = 0.f;
   __syncthreads();
-  float loc[H * 2];
-  for (int k = 0; k < H * 2; ++k) loc[k] = 0.f;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < rows; i += (long)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const long warp = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * (long)blockDim.x) >> 5;
+  float g00 = 0.f, g01 = 0.f, g10 = 0.f, g11 = 0.f;  // dW_out rows 2l, 2l+1, cols 0, 1
+  const int c = 2 * lane;
+  float w00 = 0.f, w01 = 0.f, w10 = 0.f, w11 = 0.f;
+  if (lane < 24) { w00 = wout[c * 2]; w01 = wout[c * 2 + 1]; w10 = wout[(c + 1) * 2]; w11 = wout[(c + 1) * 2 + 1]; }
+  for (long i = warp; i < rows; i += nw) {
     const float d0 = dout[2 * i], d1 = dout[2 * i + 1];
-    const unsigned* hv = reinterpret_cast<const unsigned*>(h + i * H);
-    for (int c = 0; c < H; c += 2) {
-      const float2 v = unpack_bf16(hv[c / 2]);
-      dh[i * H + c] = d0 * wout[c * 2] + d1 * wout[c * 2 + 1];
-      dh[i * H + c + 1] = d0 * wout[(c + 1) * 2] + d1 * wout[(c + 1) * 2 + 1];
-      loc[c * 2] += v.x * d0;
-      loc[c * 2 + 1] += v.x * d1;
-      loc[(c + 1) * 2] += v.y * d0;
-      loc[(c + 1) * 2 + 1] += v.y * d1;
+    if (lane < 24) {
+      const float2 v = unpack_bf16(reinterpret_cast<const unsigned*>(h + i * H)[lane]);
+      dh[i * H + c] = d0 * w00 + d1 * w01;
+      dh[i * H + c + 1] = d0 * w10 + d1 * w11;
+      g00 += v.x * d0; g01 += v.x * d1;
+      g10 += v.y * d0; g11 += v.y * d1;
     }
   }
-  for (int k = 0; k < H * 2; ++k) atomicAdd(&red[k], loc[k]);
+  if (lane < 24) {
+    atomicAdd(&red[c * 2], g00); atomicAdd(&red[c * 2 + 1], g01);
+    atomicAdd(&red[(c + 1) * 2], g10); atomicAdd(&red[(c + 1) * 2 + 1], g11);
+  }
   __syncthreads();
   for (int k = threadIdx.x; k < H * 2; k += blockDim.x) atomicAdd(&gwout[k], red[k]);
 }
@@ -468,7 +472,7 @@ __global__ void k_agg_bwd(const int32_t* __restrict__ rowptr, const int32_t* __r
   }
 }
 
-// dW_in += x^T dh0 with x rebuilt from r (K = 8)
+// dW_in += x^T dh0 with x rebuilt from r (K = 8); warp per row, lane = features lane, lane + 32
 template <class V>
 __global__ void k_encode_bwd(const V* __restrict__ r, int n, int ns, const float* __restrict__ s,
                              const float4* __restrict__ feat, const double* __restrict__ rms,
@@ -476,16 +480,24 @@ __global__ void k_encode_bwd(const V* __restrict__ r, int n, int ns, const float
   __shared__ float red[FIN * H];
   for (int k = threadIdx.x; k < FIN * H; k += blockDim.x) red[k] = 0.f;
   __syncthreads();
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < (long)n * ns; i += (long)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const long warp = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * (long)blockDim.x) >> 5;
+  float acc0[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, acc1[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  for (long i = warp; i < (long)n * ns; i += nw) {
     const int row = (int)(i % n), sy = (int)(i / n);
     const V ri = r[(long)row * ns + sy];
     const float inv = (float)(1.0 / rms[sy]) / s[i];
     const float4 f = feat[i];
     const float x[6] = {(float)ri.x * inv, (float)ri.y * inv, f.x, f.y, f.z, f.w};
-    for (int c = 0; c < H; ++c) {
-      const float d = dh[i * H + c];
-      for (int k = 0; k < 6; ++k) atomicAdd(&red[k * H + c], x[k] * d);
-    }
+    const float d0 = dh[i * H + lane];
+    const float d1 = (lane + 32 < H) ? dh[i * H + lane + 32] : 0.f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) { acc0[k] += x[k] * d0; acc1[k] += x[k] * d1; }
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    atomicAdd(&red[k * H + lane], acc0[k]);
+    if (lane + 32 < H) atomicAdd(&red[k * H + lane + 32], acc1[k]);
   }
   __syncthreads();
   for (int k = threadIdx.x; k < FIN * H; k += blockDim.x) atomicAdd(&gwin[k], red[k]);
@@ -618,6 +630,7 @@ void forward(afem_ctx* c, MpnnState* S, int ns, const V* r, V* z, bool train, co
   const __nv_bfloat16* hl = train ? S->h[L].p : S->h[L & 1].p;
   k_decode<V><<<blocks(rows, 256), 256, 0, st>>>(hl, n, ns, S->s.p, R, S->small.p + FIN * H + L * H, r, z,
                                                  nullptr, skip);
+  AFEM_CUDA(cudaGetLastError());
 }
 
 // Loss ||A z - r||^2/||r||^2 (summed over systems) and the gradient added to S->grad.
@@ -655,6 +668,7 @@ double loss_backward(afem_ctx* c, MpnnState* S, int ns, const double2* r) {
   }
   k_encode_bwd<double2><<<std::min(1024u, blocks(rows, 256)), 256, 0, st>>>(r, n, ns, S->s.p, S->feat.p, S->rms.p,
                                                                             S->dh.p, G + off_win());
+  AFEM_CUDA(cudaGetLastError());
   std::vector<double> h(2 * ns);
   AFEM_CUDA(cudaMemcpyAsync(h.data(), S->sums.p, sizeof(double) * 2 * ns, cudaMemcpyDeviceToHost, st));
   AFEM_CUDA(cudaStreamSynchronize(st));

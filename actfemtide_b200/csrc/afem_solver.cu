@@ -49,7 +49,7 @@ struct Cx<float> {
 };
 
 constexpr int MAX_NS = 16;
-constexpr unsigned SPIN_LIMIT = 1u << 24;
+constexpr unsigned SPIN_LIMIT = 1u << 21;  // x ~1 us back-off: a wait gives up after ~2 s
 
 // per-system scalars (always FP64)
 struct SysScal {
@@ -80,6 +80,7 @@ struct SolverWork {
   DBuf<double2> rprev;              // flexible COCG: previous residual (FP64 inner)
   DBuf<float2> rprevf;              // flexible COCG: previous residual (FP32 inner)
   DBuf<double> rms;                 // per-system rms(r) for the learned preconditioner
+  int rpw64 = 0, rpw32 = 0;         // SpMV rows per warp chosen by tune_spmv (0 = not tuned)
   bool kmf_valid = false;
   DBuf<unsigned> flag_f, flag_b;
   DBuf<double> part;                // partial sums [block][sys][4]
@@ -97,13 +98,15 @@ struct SolverWork {
 namespace {
 
 __device__ __forceinline__ bool wait_flag(const unsigned* f, unsigned epoch, DevStatus* st, int row) {
-  if (ld_acquire(f) >= epoch) return true;
-  unsigned spins = 0;
+  if (ld_relaxed(f) >= epoch) return true;
+  // exponential back-off keeps the poll traffic from crowding L2
+  unsigned spins = 0, ns = 32;
   for (;;) {
-    if (ld_acquire(f) >= epoch) return true;
+    __nanosleep(ns);
+    if (ns < 1024) ns <<= 1;
+    if (ld_relaxed(f) >= epoch) return true;
     ++spins;
-    if (spins > 32) __nanosleep(spins > 4096 ? 256 : 32);
-    if ((spins & 255) == 0 && *(volatile int*)&st->code == DEV_TIMEOUT) return false;
+    if ((spins & 63) == 0 && *(volatile int*)&st->code == DEV_TIMEOUT) return false;
     if (spins > SPIN_LIMIT) {
       raise_status(st, DEV_TIMEOUT, row);
       return false;
@@ -164,7 +167,8 @@ __global__ void __launch_bounds__(256)
           typename Cx<T>::V* __restrict__ y, const typename Cx<T>::V* __restrict__ p,
           const typename Cx<T>::V* __restrict__ q, double2* __restrict__ x, const typename Cx<T>::V* __restrict__ dd,
           unsigned* __restrict__ flag, int mode, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl,
-          double* __restrict__ part, DevStatus* st, typename Cx<T>::V* __restrict__ rprev) {
+          double* __restrict__ part, DevStatus* st, typename Cx<T>::V* __restrict__ rprev,
+          const int32_t* __restrict__ perm) {
   using V = typename Cx<T>::V;
   if (ctrl->done) return;
   constexpr int G = 32 / NS;
@@ -177,7 +181,8 @@ __global__ void __launch_bounds__(256)
   const double2 al = sc[s].alpha;
   const bool act = sc[s].active;
   double rr = 0.0;
-  for (int row = warp; row < n; row += nwarps) {
+  for (int pos = warp; pos < n; pos += nwarps) {
+    const int row = __ldg(perm + pos);
     V ri = r[(long)row * NS + s];
     if (rprev && g == 0) rprev[(long)row * NS + s] = ri;  // flexible COCG keeps r_k
     if (update && act && g == 0) {
@@ -221,10 +226,7 @@ __global__ void __launch_bounds__(256)
       y[(long)row * NS + s] = Cx<T>::make(wx * d.x - wy * d.y, wx * d.y + wy * d.x);
     }
     __syncwarp();
-    if (lane == 0) {
-      __threadfence();
-      st_release(flag + row, epoch);
-    }
+    if (lane == 0) st_release(flag + row, epoch);  // release: the row's values are visible first
   }
   double v[1] = {rr};
   block_partials<NS, 1>(v, part);
@@ -238,7 +240,7 @@ __global__ void __launch_bounds__(256)
           const typename Cx<T>::V* __restrict__ km, int n, const typename Cx<T>::V* __restrict__ r,
           typename Cx<T>::V* __restrict__ z, const typename Cx<T>::V* __restrict__ dd, unsigned* __restrict__ flag,
           int mode, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl, double* __restrict__ part, DevStatus* st,
-          const typename Cx<T>::V* __restrict__ rprev) {
+          const typename Cx<T>::V* __restrict__ rprev, const int32_t* __restrict__ perm) {
   using V = typename Cx<T>::V;
   if (ctrl->done) return;
   constexpr int G = 32 / NS;
@@ -248,8 +250,8 @@ __global__ void __launch_bounds__(256)
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const double om = sc[s].omega;
   double rx = 0.0, ry = 0.0, px = 0.0, py = 0.0;
-  for (int it = warp; it < n; it += nwarps) {
-    const int row = n - 1 - it;
+  for (int pos = warp; pos < n; pos += nwarps) {
+    const int row = __ldg(perm + pos);
     V zi = z[(long)row * NS + s];
     if (mode <= 1) {
       const int k0 = diagpos[row] + 1, k1 = rowptr[row + 1];
@@ -271,10 +273,7 @@ __global__ void __launch_bounds__(256)
         z[(long)row * NS + s] = zi;
       }
       __syncwarp();
-      if (lane == 0) {
-        __threadfence();
-        st_release(flag + row, epoch);
-      }
+      if (lane == 0) st_release(flag + row, epoch);
     }
     if (g == 0) {
       const V ri = r[(long)row * NS + s];
@@ -315,22 +314,28 @@ __global__ void k_pupd(int n, const typename Cx<T>::V* __restrict__ z, typename 
 
 // q = A p (COCG13_single.f90:273-288) and p^T q partial sums.  With
 // resid_mode, computes r = b - A x in FP64 instead and ||r||^2 (and ||b||^2).
-template <class T, int NS>
+// RPW rows per warp: lane = sub * (32/RPW) + g * NS + s, so rows of ~16
+// nonzeros do not leave half a warp idle (RPW is picked by tune_spmv).
+template <class T, int NS, int RPW = 1>
 __global__ void __launch_bounds__(256)
     k_spmv(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
            const typename Cx<T>::V* __restrict__ km, int n, const typename Cx<T>::V* __restrict__ p,
            typename Cx<T>::V* __restrict__ q, const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl,
            double* __restrict__ part, const typename Cx<T>::V* __restrict__ bvec) {
   using V = typename Cx<T>::V;
+  static_assert(NS * RPW <= 32, "rows per warp times systems must fit a warp");
   if (ctrl && ctrl->done) return;
-  constexpr int G = 32 / NS;
-  const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
+  constexpr int LPR = 32 / RPW;  // lanes per row
+  constexpr int G = LPR / NS;    // entry groups per row
+  const int lane = threadIdx.x & 31, sub = lane / LPR, s = lane % NS, g = (lane % LPR) / NS;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const double om = sc[s].omega;
   double ax = 0.0, ay = 0.0, bb = 0.0;
-  for (int row = warp; row < n; row += nwarps) {
-    const int k0 = rowptr[row], k1 = rowptr[row + 1];
+  for (int row0 = warp * RPW; row0 < n; row0 += nwarps * RPW) {
+    const int row = row0 + sub;
+    const bool live = row < n;
+    const int k0 = live ? rowptr[row] : 0, k1 = live ? rowptr[row + 1] : 0;
     T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
     for (int k = k0 + g; k < k1; k += G) {
       const int j = __ldg(col + k);
@@ -339,8 +344,12 @@ __global__ void __launch_bounds__(256)
       t1x += a.x * pj.x; t1y += a.x * pj.y;
       t2x += a.y * pj.x; t2y += a.y * pj.y;
     }
-    group_reduce<T, NS>(t1x, t1y, t2x, t2y);
-    if (g == 0) {
+#pragma unroll
+    for (int m = NS; m < LPR; m <<= 1) {
+      t1x += shfl_xor(t1x, m); t1y += shfl_xor(t1y, m);
+      t2x += shfl_xor(t2x, m); t2y += shfl_xor(t2y, m);
+    }
+    if (g == 0 && live) {
       const T o = (T)om;
       const V qi = Cx<T>::make(t1x - o * t2y, t1y + o * t2x);
       if (bvec) {  // r = b - A x
@@ -356,6 +365,13 @@ __global__ void __launch_bounds__(256)
         ay += (double)pi.x * (double)qi.y + (double)pi.y * (double)qi.x;
       }
     }
+  }
+  // fold the RPW rows of the warp onto lanes 0..NS-1
+#pragma unroll
+  for (int m = LPR; m < 32; m <<= 1) {
+    ax += shfl_xor(ax, m);
+    ay += shfl_xor(ay, m);
+    bb += shfl_xor(bb, m);
   }
   double v[3] = {ax, ay, bb};
   block_partials<NS, 3>(v, part);
@@ -476,7 +492,7 @@ __global__ void __launch_bounds__(256)
     k_dd_ic(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const int32_t* __restrict__ diagpos,
             const typename Cx<T>::V* __restrict__ km, int n, double sd, const SysScal* __restrict__ sc,
             typename Cx<T>::V* __restrict__ dd, unsigned* __restrict__ flag, const Ctrl* __restrict__ ctrl,
-            DevStatus* st) {
+            DevStatus* st, const int32_t* __restrict__ perm) {
   using V = typename Cx<T>::V;
   constexpr int G = 32 / NS;
   const unsigned epoch = ctrl->epoch;
@@ -484,7 +500,8 @@ __global__ void __launch_bounds__(256)
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const double om = sc[s].omega;
-  for (int row = warp; row < n; row += nwarps) {
+  for (int pos = warp; pos < n; pos += nwarps) {
+    const int row = __ldg(perm + pos);
     const int k0 = rowptr[row], k1 = diagpos[row];
     double wx = 0, wy = 0;
     for (int k = k0 + g; k < k1; k += G) {
@@ -508,10 +525,7 @@ __global__ void __launch_bounds__(256)
       dd[(long)row * NS + s] = Cx<T>::make((T)dv.x, (T)dv.y);
     }
     __syncwarp();
-    if (lane == 0) {
-      __threadfence();
-      st_release(flag + row, epoch);
-    }
+    if (lane == 0) st_release(flag + row, epoch);  // release: the row's values are visible first
   }
 }
 
@@ -651,6 +665,51 @@ struct Inner<float, NS> {
   static const V* KM(afem_ctx*, SolverWork* w) { return w->kmf.p; }
 };
 
+template <class T, int NS>
+void launch_spmv(afem_ctx* c, SolverWork* w, int rpw, const typename Cx<T>::V* km, const typename Cx<T>::V* p,
+                 typename Cx<T>::V* q, const Ctrl* ctrl, const typename Cx<T>::V* bvec) {
+  cudaStream_t s = c->stream;
+  const int n = w->n;
+  const int32_t* rp = c->rowptr.p;
+  const int32_t* cl = c->col.p;
+  if (rpw == 4 && NS * 4 <= 32)
+    k_spmv<T, NS, (NS * 4 <= 32 ? 4 : 1)><<<w->nblocks, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p, bvec);
+  else if (rpw == 2 && NS * 2 <= 32)
+    k_spmv<T, NS, (NS * 2 <= 32 ? 2 : 1)><<<w->nblocks, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p, bvec);
+  else
+    k_spmv<T, NS, 1><<<w->nblocks, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p, bvec);
+}
+
+// Rows-per-warp autotuner: times each variant on this matrix (q = A p with the
+// current p) and keeps the fastest; cached per workspace and precision.
+template <class T, int NS>
+int tune_spmv(afem_ctx* c, SolverWork* w) {
+  using I = Inner<T, NS>;
+  int& slot = sizeof(T) == 8 ? w->rpw64 : w->rpw32;
+  if (slot) return slot;
+  cudaStream_t s = c->stream;
+  cudaEvent_t a, b;
+  AFEM_CUDA(cudaEventCreate(&a));
+  AFEM_CUDA(cudaEventCreate(&b));
+  float best = 1e30f;
+  int pick = 1;
+  for (int rpw : {1, 2, 4}) {
+    if (NS * rpw > 32) break;
+    launch_spmv<T, NS>(c, w, rpw, I::KM(c, w), I::P(w), I::Q(w), nullptr, nullptr);  // warm
+    AFEM_CUDA(cudaEventRecord(a, s));
+    for (int k = 0; k < 3; ++k) launch_spmv<T, NS>(c, w, rpw, I::KM(c, w), I::P(w), I::Q(w), nullptr, nullptr);
+    AFEM_CUDA(cudaEventRecord(b, s));
+    AFEM_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    AFEM_CUDA(cudaEventElapsedTime(&ms, a, b));
+    if (ms < best * 0.97f) { best = ms; pick = rpw; }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  slot = pick;
+  return pick;
+}
+
 // One COCG iteration (7 launches; the learned preconditioner adds the network's 8).
 template <class T, int NS>
 void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, cudaEvent_t* ev) {
@@ -663,7 +722,8 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
   if (ev) AFEM_CUDA(cudaEventRecord(ev[0], s));
   launch_coop(k_fwd<T, NS>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
               (const int32_t*)c->diagpos.p, I::KM(c, w), n, I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w),
-              w->x.p, (const V*)I::DD(w), w->flag_f.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, rp);
+              w->x.p, (const V*)I::DD(w), w->flag_f.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, rp,
+              (const int32_t*)c->perm_f.p);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[1], s));
   k_scal_r<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, sweep_blocks, NS, learned ? w->rms.p : nullptr,
                                      n);
@@ -671,14 +731,15 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
   if (ev) AFEM_CUDA(cudaEventRecord(ev[2], s));
   launch_coop(k_bwd<T, NS>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
               (const int32_t*)c->diagpos.p, I::KM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w),
-              w->flag_b.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, (const V*)rp);
+              w->flag_b.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, (const V*)rp,
+              (const int32_t*)c->perm_b.p);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[3], s));
   k_scal_rho<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, sweep_blocks, NS, learned ? 1 : 0);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[4], s));
   k_pupd<T, NS><<<c->num_sms * 8, 256, 0, s>>>(n, I::Z(w), I::P(w), w->sc.p, w->ctrl.p);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[5], s));
-  k_spmv<T, NS><<<w->nblocks, 256, 0, s>>>((const int32_t*)c->rowptr.p, (const int32_t*)c->col.p, I::KM(c, w), n,
-                                           (const V*)I::P(w), I::Q(w), w->sc.p, w->ctrl.p, w->part.p, (const V*)nullptr);
+  launch_spmv<T, NS>(c, w, sizeof(T) == 8 ? w->rpw64 : w->rpw32, I::KM(c, w), (const V*)I::P(w), I::Q(w), w->ctrl.p,
+                     (const V*)nullptr);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[6], s));
   k_scal_pq<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, NS);
 }
@@ -711,7 +772,7 @@ void setup_dd(afem_ctx* c, SolverWork* w, int precond, double sd) {
     const int blocks = coresident_blocks(k_dd_ic<T, NS>, c->num_sms);
     launch_coop(k_dd_ic<T, NS>, blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
                 (const int32_t*)c->diagpos.p, I::KM(c, w), w->n, sd, (const SysScal*)w->sc.p, I::DD(w), w->flag_f.p,
-                (const Ctrl*)w->ctrl.p, c->status.p);
+                (const Ctrl*)w->ctrl.p, c->status.p, (const int32_t*)c->perm_f.p);
     w->epoch_host += 1;
     AFEM_CUDA(cudaMemcpyAsync(&w->ctrl.p->epoch, &w->epoch_host, sizeof(unsigned), cudaMemcpyHostToDevice, s));
   } else if (precond == AFEM_PRECOND_SSOR || precond == AFEM_PRECOND_DIAG) {
@@ -741,6 +802,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   k_init_sys<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, NS, tol, maxit, d_omega);
   setup_dd<T, NS>(c, w, precond, o->sigma_diag > 0 ? o->sigma_diag : 1.0);
   const int mode = precond;
+  tune_spmv<T, NS>(c, w);
   const bool learned = mode == AFEM_PRECOND_LEARNED;
   if (learned) {
     using V = typename I::V;
@@ -749,10 +811,13 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
     mpnn_prepare(c, NS, d_omega);
   }
   if (stalled) *stalled = false;
-  double watch = 1e300;  // learned mode: residual at the last stall check
+  double watch = 1e300, win_min = 1e300;  // stagnation windows (see below)
   const int sweep_blocks = coresident_blocks(k_fwd<T, NS>, c->num_sms);
   const int sb2 = coresident_blocks(k_bwd<T, NS>, c->num_sms);
   const int sblocks = std::min(std::min(sweep_blocks, sb2), w->nblocks);
+  // every solve starts a fresh flag generation: a solve that stopped inside a
+  // chunk left its last forward-sweep flags at the epoch it ended on
+  w->epoch_host += 1;
   AFEM_CUDA(cudaMemcpyAsync(&w->ctrl.p->epoch, &w->epoch_host, sizeof(unsigned), cudaMemcpyHostToDevice, s));
   int iters_done = 0;
   const int chunk = check_every > 0 ? check_every : 32;
@@ -765,7 +830,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   }
   auto ev_of = [&](int k) -> cudaEvent_t* { return prof ? &evs[7L * k] : nullptr; };
   cudaGraphExec_t gexec = nullptr;
-  bool use_graph = o->use_graph != 0;
+  bool use_graph = o->use_graph != 0 && !prof;
   if (use_graph) {
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
@@ -819,26 +884,30 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
       }
     }
     iter_before = w->h_ctrl->iter;
-    if (learned && !w->h_ctrl->done && w->h_ctrl->iter >= 2 * chunk) {
-      // stall detector: the learned preconditioner must halve the residual every two chunks
+    // stagnation detector: the smallest worst-system residual seen in a window
+    // of `win` chunks (learned: 4, FP32 inner: 8, FP64: 32) must be 10% below
+    // the previous window's, else the inner solve ends and the refinement /
+    // fallback loop takes over (COCG residuals oscillate: windows, not samples)
+    const int win = learned ? 4 : (sizeof(T) == 4 ? 8 : 32);
+    if (!w->h_ctrl->done) {
       AFEM_CUDA(cudaMemcpyAsync(w->h_sc, w->sc.p, sizeof(SysScal) * NS, cudaMemcpyDeviceToHost, s));
       AFEM_CUDA(cudaStreamSynchronize(s));
       double worst = 0.0;
       for (int k = 0; k < NS; ++k)
         if (w->h_sc[k].active) worst = std::max(worst, w->h_sc[k].resid);
-      if ((w->h_ctrl->iter / chunk) % 2 == 0) {
-        if (!(worst < 0.5 * watch) && watch < 1e300) {
+      win_min = std::min(win_min, worst);
+      if ((w->h_ctrl->iter / chunk) % win == 0) {
+        if (!(win_min < 0.9 * watch) && watch < 1e300) {
           const int one = 1;
           AFEM_CUDA(cudaMemcpyAsync(&w->ctrl.p->done, &one, sizeof(int), cudaMemcpyHostToDevice, s));
           AFEM_CUDA(cudaStreamSynchronize(s));
           if (stalled) *stalled = true;
           break;
         }
-        watch = worst;
+        watch = win_min;
+        win_min = 1e300;
       }
     }
-    if (w->h_ctrl->done) break;
-    if (w->h_ctrl->iter > maxit + 2 * chunk) break;  // safety: the scalar kernels stop at maxit
   }
   if (gexec) cudaGraphExecDestroy(gexec);
   for (auto& e : evs) cudaEventDestroy(e);
@@ -872,6 +941,7 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     w->r.alloc(total); w->z.alloc(total); w->p.alloc(total); w->q.alloc(total); w->dd.alloc(total);
     w->rf.release(); w->zf.release(); w->pf.release(); w->qf.release(); w->ddf.release();
     w->flag_f.alloc(n); w->flag_b.alloc(n);
+    w->rpw64 = w->rpw32 = 0;
     w->flag_f.zero(s); w->flag_b.zero(s);
     w->sc.alloc(MAX_NS);
     w->ctrl.alloc(1);
@@ -907,10 +977,15 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     std::vector<int> hsrc(NS);
     for (int k = 0; k < NS; ++k) {
       hsrc[k] = srcs ? srcs[k] : 0;
-      AFEM_REQUIRE(hsrc[k] >= 0 && hsrc[k] < c->rhs_nsrc, AFEM_EINVAL, "solve: source index out of range");
+      AFEM_REQUIRE((ex && ex->rhs) || (hsrc[k] >= 0 && hsrc[k] < c->rhs_nsrc), AFEM_EINVAL,
+                   "solve: source index out of range");
     }
-    dsrc.upload(hsrc.data(), NS, s);
-    k_gather_rhs<<<c->num_sms * 8, 256, 0, s>>>(c->rhs.p, n, NS, dsrc.p, w->b.p);
+    if (ex && ex->rhs) {
+      w->b.upload(reinterpret_cast<const double2*>(ex->rhs), total, s);
+    } else {
+      dsrc.upload(hsrc.data(), NS, s);
+      k_gather_rhs<<<c->num_sms * 8, 256, 0, s>>>(c->rhs.p, n, NS, dsrc.p, w->b.p);
+    }
     AFEM_CUDA(cudaStreamSynchronize(s));
   }
   std::vector<double> om(NS);
@@ -973,6 +1048,10 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     bool stalled = false;
     if (mixed) its = inner_cocg<float, NS>(c, w, o, precond_now, inner_tol, left, o->check_every, d_om.p, hs, &stalled);
     else its = inner_cocg<double, NS>(c, w, o, precond_now, inner_tol, left, o->check_every, d_om.p, hs, &stalled);
+    if (precond_now != AFEM_PRECOND_LEARNED && stalled) {
+      for (int k = 0; k < NS; ++k)
+        if (hs[k].active) hs[k].status = AFEM_ESTAGNATION;
+    }
     if (precond_now == AFEM_PRECOND_LEARNED) {
       learned_its += its;
       if (stalled) {
@@ -1045,6 +1124,7 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
 int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, const afem_solve_opts* o,
                  afem_solve_stats* st, const SolveExtra* ex) {
   AFEM_REQUIRE(c->assembled, AFEM_ESTATE, "solve: system not assembled");
+  build_schedule(c);
   switch (nsys) {
     case 1: return solve_ns<1>(c, freq, src, o, st, ex);
     case 2: return solve_ns<2>(c, freq, src, o, st, ex);
@@ -1068,7 +1148,10 @@ void get_residual(afem_ctx* c, int k, double* r) {
 }
 
 void invalidate_work(afem_ctx* c) {
-  if (c->work) c->work->kmf_valid = false;
+  if (c->work) {
+    c->work->kmf_valid = false;
+    c->work->rpw64 = c->work->rpw32 = 0;
+  }
 }
 
 void destroy_work(afem_ctx* c) {

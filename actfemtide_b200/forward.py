@@ -176,6 +176,39 @@ class Forward:
         self.nline = n
         return dict(x=X, resid=R.value, iter=IT.value, error=ER.value)
 
+    def solve_rhs(self, freqs, rhs, precond="SSOR", precision="fp64", tol=1e-8, maxit=100000) -> SolveResult:
+        """Solve A(freq_k) u_k = rhs[:, k] for caller right-hand sides rhs (n, nsys)."""
+        f = _c(np.atleast_1d(freqs), np.float64)
+        b = _c(np.asarray(rhs).reshape(self.nline, len(f)), np.complex128)
+        o = SolveOpts(capi.PRECOND[precond], capi.PRECISION[precision], tol, maxit, 1.0, 0, 0.0, 1)
+        st = SolveStats()
+        rc = self._L.afem_solve_rhs(self.ctx, len(f), ptr(f), ptr(b), C.byref(o), C.byref(st))
+        if rc not in (capi.AFEM_OK, -4, -13):
+            self._check(rc)
+        return SolveResult(st.iterations, st.refinements, st.resid_recursive, st.resid_true, st.seconds, rc)
+
+    def jacobian(self, freq, x, nadj):
+        """J[k, t] = d(datum k)/d log(sigma_t) from the nadj adjoint solutions of the last solve_rhs."""
+        xx = _c(x, np.complex128)
+        J = np.zeros((nadj, self.ntet), np.complex128)
+        self._check(self._L.afem_jacobian(self.ctx, float(freq), ptr(xx), nadj, ptr(J)))
+        return J
+
+    def adjoint_sources(self, freq, sites, comps=(3, 4)):
+        """Adjoint right-hand sides c with datum = c^T x for the site components (0..2 = B, 3..4 = E)."""
+        item, ve, vf, _ = self.site_coeffs(sites)
+        om = 2.0 * (4.0 * np.arctan(1.0)) * freq
+        cols = []
+        for s_ in range(len(sites)):
+            for comp in comps:
+                c = np.zeros(self.nline, np.complex128)
+                if comp < 3:
+                    c[item[s_] - 1] += vf[comp, s_]
+                else:
+                    c[item[s_] - 1] += -1j * om * ve[comp - 3, s_]
+                cols.append(c)
+        return np.stack(cols, axis=1)
+
     def residual(self, k: int = 0):
         """FP64 b - A x of system k after the last solve."""
         r = np.zeros(self.nline, np.complex128)

@@ -244,3 +244,103 @@ def tiny_model(nx=2, ny=2, nz=4, seed: int = 0) -> TidalModel:
     """A few hexes over [-10,10]^3 km (5 km cells, so the sea layer holds whole cells)."""
     return tidal_box(nx, ny, nz, seed=seed, block=False, site_grid=(-5.0, 5.0), half_km=10.0,
                      name=f"box{nx}x{ny}x{nz}")
+
+
+# ----------------------------------------------------------------------------- reference file formats
+def _write_msh(path, xyz, elems, etype):
+    """Gmsh 2.2 ASCII as readmsh2 reads it (src/common/m_mesh_type.f90:379-468): two tags per element."""
+    with open(path, "w") as f:
+        f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n")
+        f.write(f"{xyz.shape[0]}\n")
+        for i, p in enumerate(xyz):
+            f.write(f"{i + 1} {float(p[0])!r} {float(p[1])!r} {float(p[2])!r}\n")
+        f.write("$EndNodes\n$Elements\n")
+        f.write(f"{len(elems)}\n")
+        for k, (tag, nodes) in enumerate(elems):
+            f.write(f"{k + 1} {etype} 2 {tag} {tag} " + " ".join(str(int(n)) for n in nodes) + "\n")
+        f.write("$EndElements\n")
+
+
+def write_reference_inputs(m: TidalModel, outdir: str, line=None, n6line=None, site_names=None) -> str:
+    """Write model m as the files the reference's tide forward reads; returns the ctl path.
+
+    em3d.msh (tetrahedra, tags = elementary volume), polygonz.msh (top-of-earth
+    triangles with z), ocean.msh (only its node count is used), lineinfo.dat
+    (READLINE's layout; numbering from line/n6line when given), fxyz_mesh /
+    vxyz_mesh (readfxyz / readvxyz records), cond_test.msh (READCOND: 11 header
+    lines, nphys2, index and resistivity), tide_fwd.ctl (readparam's record
+    order, labels in the first 20 columns, xyz sites given 1 m below the surface).
+    """
+    import os
+    os.makedirs(outdir, exist_ok=True)
+    p = lambda name: os.path.join(outdir, name)  # noqa: E731
+    _write_msh(p("em3d.msh"), m.xyz, [(int(t), nd) for t, nd in zip(m.tag, m.n4)], 4)
+    # surface: nodes of the top grid with the solid-earth height
+    nx, ny, _ = m.dims
+    half = m.bounds["xout"]
+    xs = np.linspace(-half, half, nx + 1)
+    ys = np.linspace(-half, half, ny + 1)
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    sxyz = np.stack([X.ravel(), Y.ravel(), surface_z(X.ravel(), Y.ravel())], axis=1)
+    tris = []
+    for i in range(nx):
+        for j in range(ny):
+            a = i * (ny + 1) + j + 1
+            b = (i + 1) * (ny + 1) + j + 1
+            tris.append((1, (a, b, b + 1)))
+            tris.append((1, (a, b + 1, a + 1)))
+    _write_msh(p("polygonz.msh"), sxyz, tris, 2)
+    _write_msh(p("ocean.msh"), m.xyz[: m.nodes], [], 4)
+    if line is not None:
+        with open(p("lineinfo.dat"), "w") as f:
+            f.write(f"{line.shape[0]:12d}\n")
+            for a, b in line:
+                f.write(f"{a:10d}{b:10d}\n")
+            f.write(f"{n6line.shape[0]:12d}\n")
+            for r in n6line:
+                f.write("".join(f"{v:10d}" for v in r) + "\n")
+    with open(p("fxyz_mesh"), "w") as f:
+        for i in range(m.nodes):
+            F = m.F[i]
+            f.write(f"  0.0 0.0 {float(m.xyz[i, 2])!r} {float(F[0])!r} {float(F[1])!r} {float(F[2])!r} "
+                    f"{float(np.linalg.norm(F))!r}\n")
+    with open(p("vxyz_mesh"), "w") as f:
+        for i in range(m.nodes):
+            v = m.v[i]
+            f.write(f"  0.0 0.0 {float(m.xyz[i, 2])!r} ({float(v[0].real)!r},{float(v[0].imag)!r}) "
+                    f"({float(v[1].real)!r},{float(v[1].imag)!r}) {i + 1}\n")
+    with open(p("cond_test.msh"), "w") as f:
+        for k in range(11):
+            f.write(f"# header line {k + 1}\n")
+        f.write(f"{len(m.sigma_land)}\n")
+        for k, s in enumerate(m.sigma_land):
+            f.write(f"{m.nphys1 + k + 1} {float(1.0 / s)!r}\n")
+    names = site_names or [f"S{k + 1:03d}" for k in range(m.sites.shape[0])]
+    lab = lambda s: (s + " " * 20)[:20]  # noqa: E731
+    rows = [lab("itopoflag") + "0",
+            lab("mesh file") + p("em3d.msh"), lab("2d triangle z file") + p("polygonz.msh"),
+            lab("local line file") + p("lineinfo.dat"), lab("Ocean mesh file.") + p("ocean.msh"),
+            lab("mesh ctl file") + p("mesh.ctl"), lab("Vxyzfile") + p("vxyz_mesh"), lab("Fxyzfile") + p("fxyz_mesh"),
+            lab("output folder") + outdir.rstrip("/") + "/", lab("header2d  (a50)") + "h2d", lab("header3d  (a50)") + "h3d",
+            lab("# of frequency") + str(len(m.freqs))]
+    rows += [lab("Frequency [Hz]") + repr(float(fr)) for fr in m.freqs]
+    xb = float(half) - 10.0
+    rows += [lab("west bound") + repr(-xb), lab("east bound") + repr(xb), lab("south bound") + repr(-xb),
+             lab("north bound") + repr(xb), lab("lenout [km]") + "10.0", lab("upz in [km]  (>0)") + "5.0",
+             lab("downz in [km](<0)") + "-5.0", lab("zmax   [km]") + repr(float(m.bounds["zmax"])),
+             lab("zmin   [km]") + repr(float(m.bounds["zmin"]))]
+    rows += [lab(k) + "0.1" for k in ("sizein [km]", "sizebo [km]", "sigma_obs [km]", "A_obs     [km]",
+                                       "dlen_source [km]", "sigma_src [km]", "A_src     [km]")]
+    rows += [lab("# of observatory") + str(m.sites.shape[0]), lab("lonlat(1),xyz (2)") + "2",
+             lab("UTM ZONE") + "none", lab("lonlatorigin") + "0.0 0.0"]
+    for nm, s in zip(names, m.sites):
+        rows += [lab("Name") + nm, lab("xyz") + f"{float(s[0])!r} {float(s[1])!r} {-SITE_DEPTH_KM!r}"]
+    rows += [lab("0:no,1:nxny,2:ntrik") + "0", lab("# of sources") + "1", lab("Source Name") + "S1",
+             lab("source start point") + "0.0 0.0 -0.001", lab("source end   point") + "0.1 0.0 -0.001",
+             lab("Elcetric current[A]") + "0.0", lab("sigma_air    [S/m]") + repr(float(m.sigma_air)),
+             lab("condflag 0:home,1:") + "1", lab("condfile") + p("cond_test.msh")]
+    ctl = p("tide_fwd.ctl")
+    with open(ctl, "w") as f:
+        f.write("## forward control file written by actfemtide_b200.synth\n")
+        f.write("\n".join(rows) + "\n")
+    return ctl

@@ -157,6 +157,14 @@ int afem_cocg13_single(afem_ctx *ctx, int NP, int NPL, int NPU, double *D, doubl
 /* Load a system in the same split layout for afem_solve (freq_hz = 1/(2*pi) gives A itself). */
 int afem_set_system(afem_ctx *ctx, int n, const int32_t *INU, const int32_t *IAU, const int32_t *INL,
                     const int32_t *IAL, const double *D, const double *AU, const double *AL, const double *b);
+/* afem_solve with caller right-hand sides rhs[(row*nsys + k)] (complex), e.g. adjoint
+ * sources P^T of site data (src/src_inv/solvePARDISOinv.f90:154-196). */
+int afem_solve_rhs(afem_ctx *ctx, int nsys, const double *freq_hz, const double *rhs, const afem_solve_opts *opts,
+                   afem_solve_stats *stats);
+/* Sensitivities of nadj site data to log(sigma) of every tetrahedron (m_jacobian.f90:120-218):
+ * after afem_solve_rhs solved the nadj adjoint systems A u_k = c_k at freq_hz,
+ * J[k*ntet + t] = -u_k^T (dA/dlog sigma_t) x for the forward solution x (n complex). */
+int afem_jacobian(afem_ctx *ctx, double freq_hz, const double *x_complex, int nadj, double *J_complex);
 /* FP64 true residual b - A x of system k after the last afem_solve (n complex values). */
 int afem_get_residual(afem_ctx *ctx, int k, double *r_complex);
 /* Solution of system k (n complex values, [nT*km] like bs in forward_bxyz). */
@@ -197,6 +205,13 @@ int afem_set_profiling(afem_ctx *ctx, int enable);
 int afem_profile_count(afem_ctx *ctx);
 /* Entry i: kernel name, total milliseconds, launches. */
 int afem_profile_entry(afem_ctx *ctx, int i, char *name, int cap, double *ms, long *launches);
+
+/* Host only: the triangular-sweep schedules of a CSR pattern (0-based columns
+ * ascending, diagonal included): rows sorted by dependency level of the
+ * forward (lower) and backward (upper) sweeps; the sweep kernels visit rows
+ * in these orders.  No counterpart in the reference (its sweeps are serial). */
+int afem_sweep_schedule(int n, const int32_t *rowptr, const int32_t *col, const int32_t *diagpos, int32_t *perm_f,
+                        int32_t *perm_b, int *levels_f, int *levels_b);
 
 /* ---- drop-in driver --------------------------------------------------------- */
 /* Replaces the rank-0 input stage of program n_ebfem_bxyz (n_ebfem_bxyz_mpi.f90:55-90):

@@ -1,0 +1,43 @@
+"""Drop-in driver: the reference's ctl file and input files in, <site>_<src>.dat files out (GPU)."""
+import os
+
+import numpy as np
+import pytest
+
+from actfemtide_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def test_ctl_driver_matches_oracle(gpulib, oracle, tmp_path):
+    from actfemtide_b200.forward import Forward, amp_phase
+    m = synth.tidal_box(4, 4, 6, seed=3, site_grid=(-6.0, 0.0, 6.0), half_km=12.0)
+    m.freqs = np.array([1.0 / 44714.0, 1.0 / 43200.0])
+    of = oracle.OracleForward(m)
+    ctl = synth.write_reference_inputs(m, str(tmp_path), of.line, of.n6line)
+    with Forward(0) as fw:
+        fw.load_ctl(ctl)
+        freqs, xyz = fw.ctl_info()
+        assert np.allclose(freqs, m.freqs)
+        # PREPZSRCOBS: z = interpolated surface height - 1 m
+        assert np.allclose(xyz, m.sites, atol=1e-12)
+        line, n6 = fw.lines()
+        assert np.array_equal(line, of.line) and np.array_equal(n6, of.n6line)
+        fw.run_ctl(precond="SSOR", tol=1e-12)
+    # the ctl path uses GENMAT's ocean conductivity, the default-real literal 3.33
+    m33 = synth.TidalModel(**{**m.__dict__, "sigma_ocean": float(np.float32(3.33)), "sites": xyz})
+    of33 = oracle.OracleForward(m33, of.line, of.n6line)
+    for fi, fr in enumerate(m.freqs):
+        A = of33.assemble(fr)
+        r = oracle.cocg13_single(A, precond="SSOR", resid=1e-12, maxit=100000)
+        out, amp, ph = of33.sites(r["x"], fr)
+        for s in range(xyz.shape[0]):
+            path = os.path.join(str(tmp_path), f"S{s + 1:03d}_S1.dat")
+            rows = [list(map(float, ln.split())) for ln in open(path).read().splitlines()]
+            assert len(rows) == len(m.freqs) and all(len(rw) == 11 for rw in rows)
+            vals = np.array(rows[fi][1:]).reshape(5, 2)
+            assert abs(rows[fi][0] - fr) <= 1e-6 * fr
+            np.testing.assert_allclose(vals[:, 0], amp[0, :, s], rtol=2e-6, atol=1e-6 * amp[0].max())
+            big = amp[0, :, s] > 1e-3 * amp[0].max()
+            dphi = (vals[big, 1] - ph[0, big, s] + 180.0) % 360.0 - 180.0
+            assert np.all(np.abs(dphi) <= 1e-3)

@@ -52,3 +52,36 @@ def test_no_device_no_context(gpulib):
         has = False
     if not has:
         assert not capi.lib().afem_create(0)
+
+
+def test_sweep_schedule_is_topological(gpulib, oracle):
+    """The level orders the sweep kernels walk are permutations in which every dependency comes first."""
+    import ctypes as C
+    from actfemtide_b200 import synth
+    from actfemtide_b200.capi import ptr
+    m = synth.small_model()
+    line, n6 = oracle.mkline(m.node, m.n4)
+    INU, IAU, INL, IAL = oracle.pattern(line.shape[0], n6)
+    n = line.shape[0]
+    rows, cols = [], []
+    for i in range(n):
+        cs = sorted([c - 1 for c in IAL[INL[i]:INL[i + 1]]] + [i] + [c - 1 for c in IAU[INU[i]:INU[i + 1]]])
+        cols += cs
+        rows.append(len(cs))
+    rowptr = np.concatenate([[0], np.cumsum(rows)]).astype(np.int32)
+    col = np.array(cols, np.int32)
+    diagpos = np.array([rowptr[i] + list(col[rowptr[i]:rowptr[i + 1]]).index(i) for i in range(n)], np.int32)
+    pf = np.zeros(n, np.int32); pb = np.zeros(n, np.int32)
+    lf = C.c_int(0); lb = C.c_int(0)
+    assert gpulib.afem_sweep_schedule(n, ptr(rowptr), ptr(col), ptr(diagpos), ptr(pf), ptr(pb), C.byref(lf),
+                                      C.byref(lb)) == 0
+    assert sorted(pf) == list(range(n)) and sorted(pb) == list(range(n))
+    pos_f = np.empty(n, int); pos_f[pf] = np.arange(n)
+    pos_b = np.empty(n, int); pos_b[pb] = np.arange(n)
+    for i in range(n):
+        lower = col[rowptr[i]:diagpos[i]]
+        upper = col[diagpos[i] + 1:rowptr[i + 1]]
+        assert np.all(pos_f[lower] < pos_f[i])
+        assert np.all(pos_b[upper] < pos_b[i])
+    # far fewer levels than rows: the sweep parallelism the schedule exposes
+    assert 10 < lf.value < n // 50 and 10 < lb.value < n // 50
