@@ -387,6 +387,6 @@ void build_schedule(afem_ctx* c) {
 extern "C" int afem_sweep_schedule(int n, const int32_t* rowptr, const int32_t* col, const int32_t* diagpos,
                                    int32_t* perm_f, int32_t* perm_b, int* levels_f, int* levels_b) {
   if (n < 0 || !rowptr || !col || !diagpos || !perm_f || !perm_b) return AFEM_EINVAL;
-  afem::compute_schedule(n, rowptr, col, diagpos, perm_f, perm_b, levels_f, levels_b);
+  afem::compute_schedule(n, rowptr, diagpos, col, perm_f, perm_b, levels_f, levels_b);
   return AFEM_OK;
 }
