@@ -20,7 +20,7 @@ STATUS = {
     -5: "AFEM_EBREAKDOWN", -6: "AFEM_ENONFINITE", -7: "AFEM_ECUDA", -8: "AFEM_ESTATE", -9: "AFEM_ETIMEOUT",
     -10: "AFEM_EIO", -11: "AFEM_ENOPRECOND", -12: "AFEM_ESITE", -13: "AFEM_ESTAGNATION",
 }
-PRECOND = {"IC": 0, "SSOR": 1, "DIAG": 2, "NONE": 3, "LEARNED": 4}
+PRECOND = {"IC": 0, "SSOR": 1, "DIAG": 2, "NONE": 3, "LEARNED": 4, "SSOR_MC": 5}
 PRECISION = {"fp64": 0, "mixed": 1}
 
 # Every entry point declared in include/afem.h.
@@ -31,7 +31,7 @@ EXPORTS = (
     "afem_ctl_info", "afem_run_ctl", "afem_fortran_g", "afem_set_profiling", "afem_profile_count",
     "afem_profile_entry", "afem_cocg13_single", "afem_set_system", "afem_get_residual", "afem_mpnn_nparam",
     "afem_mpnn_set_params", "afem_mpnn_get_params", "afem_mpnn_forward", "afem_mpnn_loss_grad", "afem_mpnn_train",
-    "afem_solve_rhs", "afem_jacobian", "afem_sweep_schedule",
+    "afem_solve_rhs", "afem_jacobian", "afem_sweep_schedule", "afem_coloring",
 )
 
 
@@ -95,6 +95,8 @@ def lib():
                                      C.POINTER(C.c_int), C.c_int]
     L.afem_set_system.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.afem_get_residual.argtypes = [_vp, C.c_int, _vp]
+    L.afem_coloring.argtypes = [C.c_int, _vp, _vp, _vp, _vp, _vp]
+    L.afem_coloring.restype = C.c_int
     L.afem_sweep_schedule.argtypes = [C.c_int, _vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.afem_solve_rhs.argtypes = [_vp, C.c_int, _vp, _vp, C.POINTER(SolveOpts), C.POINTER(SolveStats)]
     L.afem_jacobian.argtypes = [_vp, C.c_double, _vp, C.c_int, _vp]

@@ -356,7 +356,7 @@ int afem_solve(afem_ctx* c, int nsys, const double* freq, const int* src, const 
                afem_solve_stats* stats) {
   return guarded(c, [&]() {
     AFEM_REQUIRE(freq && opts, AFEM_EINVAL, "solve: null freq or opts");
-    AFEM_REQUIRE(opts->precond >= 0 && opts->precond <= 4, AFEM_EINVAL, "solve: unknown preconditioner");
+    AFEM_REQUIRE(opts->precond >= 0 && opts->precond <= 5, AFEM_EINVAL, "solve: unknown preconditioner");
     afem::reset_status(c);
     return afem::solve_device(c, nsys, freq, src, opts, stats);
   });

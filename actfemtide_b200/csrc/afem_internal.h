@@ -155,6 +155,11 @@ struct afem_ctx {
   afem::DBuf<int32_t> perm_f;   // forward sweep: lower-triangle levels ascending, ties by row
   afem::DBuf<int32_t> perm_b;   // backward sweep: upper-triangle levels ascending, ties by row descending
   int levels_f = 0, levels_b = 0;
+  // multicolour sweeps: greedy colouring, rows sorted by colour
+  afem::DBuf<uint8_t> color;    // nline
+  afem::DBuf<int32_t> perm_mc;  // nline
+  afem::DBuf<int32_t> color_ptr;// ncolors + 1
+  int ncolors = 0;
   bool schedule_ready = false;
 
   // values: A(omega) = K + i*omega*M, stored interleaved (K_k, M_k)

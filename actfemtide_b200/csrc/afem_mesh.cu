@@ -364,6 +364,33 @@ void compute_schedule(int n, const int32_t* rp, const int32_t* dp, const int32_t
   order(false, perm_b, levels_b);
 }
 
+// Greedy distance-1 colouring of the matrix graph in row order (each row takes
+// the smallest colour none of its already-coloured neighbours has), then the
+// rows sorted by colour.  Rows of one colour share no nonzero, so a
+// Gauss-Seidel pass can update all of them at once.
+int compute_coloring(int n, const int32_t* rp, const int32_t* cl, uint8_t* color, int32_t* perm, int32_t* cptr,
+                     int max_colors) {
+  std::vector<int> mark(max_colors + 1, -1);
+  int nc = 0;
+  for (int i = 0; i < n; ++i) {
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      const int j = cl[k];
+      if (j < i) mark[color[j]] = i;
+    }
+    int cidx = 0;
+    while (cidx < max_colors && mark[cidx] == i) ++cidx;
+    if (cidx >= max_colors) return -1;
+    color[i] = (uint8_t)cidx;
+    nc = std::max(nc, cidx + 1);
+  }
+  std::vector<int32_t> cnt(nc + 1, 0);
+  for (int i = 0; i < n; ++i) cnt[color[i] + 1]++;
+  for (int c = 0; c < nc; ++c) cnt[c + 1] += cnt[c];
+  for (int c = 0; c <= nc; ++c) cptr[c] = cnt[c];
+  for (int i = 0; i < n; ++i) perm[cnt[color[i]]++] = i;
+  return nc;
+}
+
 void build_schedule(afem_ctx* c) {
   if (c->schedule_ready) return;
   const int n = c->nline;
@@ -376,11 +403,26 @@ void build_schedule(afem_ctx* c) {
   compute_schedule(n, rp.data(), dp.data(), cl.data(), pf.data(), pb.data(), &c->levels_f, &c->levels_b);
   c->perm_f.upload(pf.data(), n, s);
   c->perm_b.upload(pb.data(), n, s);
+  std::vector<uint8_t> color(n);
+  std::vector<int32_t> pm(n), cptr(256);
+  const int nc = compute_coloring(n, rp.data(), cl.data(), color.data(), pm.data(), cptr.data(), 255);
+  AFEM_REQUIRE(nc > 0, AFEM_EPATTERN, "colouring: more than 255 colours");
+  c->ncolors = nc;
+  c->color.upload(color.data(), n, s);
+  c->perm_mc.upload(pm.data(), n, s);
+  c->color_ptr.upload(cptr.data(), nc + 1, s);
   AFEM_CUDA(cudaStreamSynchronize(s));
   c->schedule_ready = true;
 }
 
 }  // namespace afem
+
+// Host-only: greedy colouring of a CSR pattern (rows sorted by colour), for tests.
+extern "C" int afem_coloring(int n, const int32_t* rowptr, const int32_t* col, uint8_t* color, int32_t* perm,
+                             int32_t* cptr) {
+  if (n < 0 || !rowptr || !col || !color || !perm || !cptr) return AFEM_EINVAL;
+  return afem::compute_coloring(n, rowptr, col, color, perm, cptr, 255);
+}
 
 // Host-only: the sweep schedules of a CSR pattern (diagonal included, columns
 // ascending, 0-based) for tests and tools.

@@ -81,6 +81,7 @@ struct SolverWork {
   DBuf<float2> rprevf;              // flexible COCG: previous residual (FP32 inner)
   DBuf<double> rms;                 // per-system rms(r) for the learned preconditioner
   int rpw64 = 0, rpw32 = 0;         // SpMV rows per warp chosen by tune_spmv (0 = not tuned)
+  int mc_blocks = 0;                // co-resident grid of the multicolour sweeps
   bool kmf_valid = false;
   DBuf<unsigned> flag_f, flag_b;
   DBuf<double> part;                // partial sums [block][sys][4]
@@ -287,6 +288,119 @@ __global__ void __launch_bounds__(256)
     }
   }
   double v[4] = {rx, ry, px, py};
+  block_partials<NS, 4>(v, part);
+}
+
+// ------------------------------------------------------------------ multicolour sweeps
+// SSOR of the colour-permuted matrix: rows of one colour share no nonzero, so
+// the forward sweep updates colour 0, 1, ... in turn (each a parallel pass over
+// its rows, summing only entries of earlier colours) and the backward sweep
+// goes through the colours in reverse.  One persistent cooperative kernel per
+// sweep with a grid barrier between colours; no flags, no waits.
+template <class T, int NS>
+__global__ void __launch_bounds__(256)
+    k_fwd_mc(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const typename Cx<T>::V* __restrict__ km,
+             int n, typename Cx<T>::V* __restrict__ r, typename Cx<T>::V* __restrict__ y,
+             const typename Cx<T>::V* __restrict__ p, const typename Cx<T>::V* __restrict__ q, double2* __restrict__ x,
+             const typename Cx<T>::V* __restrict__ dd, const uint8_t* __restrict__ color,
+             const int32_t* __restrict__ perm, const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc,
+             Ctrl* __restrict__ ctrl, double* __restrict__ part) {
+  using V = typename Cx<T>::V;
+  if (ctrl->done) return;  // uniform over the grid
+  cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+  constexpr int G = 32 / NS;
+  const bool update = ctrl->iter > 0;
+  const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const double om = sc[s].omega;
+  const double2 al = sc[s].alpha;
+  const bool act = sc[s].active;
+  double rr = 0.0;
+  for (int c = 0; c < ncolors; ++c) {
+    const int p0 = cptr[c], p1 = cptr[c + 1];
+    for (int pos = p0 + warp; pos < p1; pos += nwarps) {
+      const int row = __ldg(perm + pos);
+      V ri = r[(long)row * NS + s];
+      if (update && act && g == 0) {
+        const V qi = q[(long)row * NS + s], pi = p[(long)row * NS + s];
+        ri = Cx<T>::make((T)((double)ri.x - (al.x * (double)qi.x - al.y * (double)qi.y)),
+                         (T)((double)ri.y - (al.x * (double)qi.y + al.y * (double)qi.x)));
+        r[(long)row * NS + s] = ri;
+        double2 xi = x[(long)row * NS + s];
+        xi.x += al.x * (double)pi.x - al.y * (double)pi.y;
+        xi.y += al.x * (double)pi.y + al.y * (double)pi.x;
+        x[(long)row * NS + s] = xi;
+      }
+      if (g == 0) rr += (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
+      T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
+      for (int k = rowptr[row] + g; k < rowptr[row + 1]; k += G) {
+        const int j = __ldg(col + k);
+        if (__ldg(color + j) >= c) continue;
+        const V a = km[k];
+        const V yj = ldcg(y + (long)j * NS + s);
+        t1x += a.x * yj.x; t1y += a.x * yj.y;
+        t2x += a.y * yj.x; t2y += a.y * yj.y;
+      }
+      group_reduce<T, NS>(t1x, t1y, t2x, t2y);
+      if (g == 0) {
+        const T o = (T)om;
+        const T wx = ri.x - (t1x - o * t2y), wy = ri.y - (t1y + o * t2x);
+        const V d = dd[(long)row * NS + s];
+        y[(long)row * NS + s] = Cx<T>::make(wx * d.x - wy * d.y, wx * d.y + wy * d.x);
+      }
+    }
+    grid.sync();
+  }
+  double v[1] = {rr};
+  block_partials<NS, 1>(v, part);
+}
+
+template <class T, int NS>
+__global__ void __launch_bounds__(256)
+    k_bwd_mc(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const typename Cx<T>::V* __restrict__ km,
+             int n, const typename Cx<T>::V* __restrict__ r, typename Cx<T>::V* __restrict__ z,
+             const typename Cx<T>::V* __restrict__ dd, const uint8_t* __restrict__ color,
+             const int32_t* __restrict__ perm, const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc,
+             Ctrl* __restrict__ ctrl, double* __restrict__ part) {
+  using V = typename Cx<T>::V;
+  if (ctrl->done) return;
+  cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+  constexpr int G = 32 / NS;
+  const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const double om = sc[s].omega;
+  double rx = 0.0, ry = 0.0;
+  for (int c = ncolors - 1; c >= 0; --c) {
+    const int p0 = cptr[c], p1 = cptr[c + 1];
+    for (int pos = p0 + warp; pos < p1; pos += nwarps) {
+      const int row = __ldg(perm + pos);
+      T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
+      for (int k = rowptr[row] + g; k < rowptr[row + 1]; k += G) {
+        const int j = __ldg(col + k);
+        if (__ldg(color + j) <= c) continue;
+        const V a = km[k];
+        const V zj = ldcg(z + (long)j * NS + s);
+        t1x += a.x * zj.x; t1y += a.x * zj.y;
+        t2x += a.y * zj.x; t2y += a.y * zj.y;
+      }
+      group_reduce<T, NS>(t1x, t1y, t2x, t2y);
+      if (g == 0) {
+        V zi = z[(long)row * NS + s];
+        const T o = (T)om;
+        const T swx = t1x - o * t2y, swy = t1y + o * t2x;
+        const V d = dd[(long)row * NS + s];
+        zi = Cx<T>::make(zi.x - (d.x * swx - d.y * swy), zi.y - (d.x * swy + d.y * swx));
+        z[(long)row * NS + s] = zi;
+        const V ri = r[(long)row * NS + s];
+        rx += (double)ri.x * (double)zi.x - (double)ri.y * (double)zi.y;
+        ry += (double)ri.x * (double)zi.y + (double)ri.y * (double)zi.x;
+      }
+    }
+    grid.sync();
+  }
+  double v[4] = {rx, ry, 0.0, 0.0};
   block_partials<NS, 4>(v, part);
 }
 
@@ -719,22 +833,34 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
   const int n = w->n;
   const bool learned = mode == AFEM_PRECOND_LEARNED;
   V* rp = learned ? I::RP(w) : nullptr;
+  const bool mc = mode == AFEM_PRECOND_SSOR_MC;
   if (ev) AFEM_CUDA(cudaEventRecord(ev[0], s));
-  launch_coop(k_fwd<T, NS>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
-              (const int32_t*)c->diagpos.p, I::KM(c, w), n, I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w),
-              w->x.p, (const V*)I::DD(w), w->flag_f.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, rp,
-              (const int32_t*)c->perm_f.p);
+  if (mc)
+    launch_coop(k_fwd_mc<T, NS>, w->mc_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p, I::KM(c, w), n,
+                I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w), w->x.p, (const V*)I::DD(w),
+                (const uint8_t*)c->color.p, (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors,
+                w->sc.p, w->ctrl.p, w->part.p);
+  else
+    launch_coop(k_fwd<T, NS>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
+                (const int32_t*)c->diagpos.p, I::KM(c, w), n, I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w),
+                w->x.p, (const V*)I::DD(w), w->flag_f.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, rp,
+                (const int32_t*)c->perm_f.p);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[1], s));
-  k_scal_r<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, sweep_blocks, NS, learned ? w->rms.p : nullptr,
-                                     n);
+  const int swb = mc ? w->mc_blocks : sweep_blocks;
+  k_scal_r<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, swb, NS, learned ? w->rms.p : nullptr, n);
   if (learned) mpnn_run<V>(c, NS, w->rms.p, (const V*)I::R(w), I::Z(w), &w->ctrl.p->done);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[2], s));
-  launch_coop(k_bwd<T, NS>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
-              (const int32_t*)c->diagpos.p, I::KM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w),
-              w->flag_b.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, (const V*)rp,
-              (const int32_t*)c->perm_b.p);
+  if (mc)
+    launch_coop(k_bwd_mc<T, NS>, w->mc_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p, I::KM(c, w), n,
+                (const V*)I::R(w), I::Z(w), (const V*)I::DD(w), (const uint8_t*)c->color.p,
+                (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p);
+  else
+    launch_coop(k_bwd<T, NS>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
+                (const int32_t*)c->diagpos.p, I::KM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w),
+                w->flag_b.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, (const V*)rp,
+                (const int32_t*)c->perm_b.p);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[3], s));
-  k_scal_rho<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, sweep_blocks, NS, learned ? 1 : 0);
+  k_scal_rho<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, swb, NS, learned ? 1 : 0);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[4], s));
   k_pupd<T, NS><<<c->num_sms * 8, 256, 0, s>>>(n, I::Z(w), I::P(w), w->sc.p, w->ctrl.p);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[5], s));
@@ -775,7 +901,7 @@ void setup_dd(afem_ctx* c, SolverWork* w, int precond, double sd) {
                 (const Ctrl*)w->ctrl.p, c->status.p, (const int32_t*)c->perm_f.p);
     w->epoch_host += 1;
     AFEM_CUDA(cudaMemcpyAsync(&w->ctrl.p->epoch, &w->epoch_host, sizeof(unsigned), cudaMemcpyHostToDevice, s));
-  } else if (precond == AFEM_PRECOND_SSOR || precond == AFEM_PRECOND_DIAG) {
+  } else if (precond == AFEM_PRECOND_SSOR || precond == AFEM_PRECOND_DIAG || precond == AFEM_PRECOND_SSOR_MC) {
     k_dd_diag<T, NS><<<c->num_sms * 8, 256, 0, s>>>(I::KM(c, w), (const int32_t*)c->diagpos.p, w->n, sd,
                                                     (const SysScal*)w->sc.p, I::DD(w));
   }
@@ -815,6 +941,9 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   const int sweep_blocks = coresident_blocks(k_fwd<T, NS>, c->num_sms);
   const int sb2 = coresident_blocks(k_bwd<T, NS>, c->num_sms);
   const int sblocks = std::min(std::min(sweep_blocks, sb2), w->nblocks);
+  if (mode == AFEM_PRECOND_SSOR_MC)
+    w->mc_blocks = std::min(std::min(coresident_blocks(k_fwd_mc<T, NS>, c->num_sms),
+                                     coresident_blocks(k_bwd_mc<T, NS>, c->num_sms)), w->nblocks);
   // every solve starts a fresh flag generation: a solve that stopped inside a
   // chunk left its last forward-sweep flags at the epoch it ended on
   w->epoch_host += 1;
@@ -885,11 +1014,12 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
     }
     iter_before = w->h_ctrl->iter;
     // stagnation detector: the smallest worst-system residual seen in a window
-    // of `win` chunks (learned: 4, FP32 inner: 8, FP64: 32) must be 10% below
+    // of `win` chunks (learned: 4, FP32 inner: 16) must be 10% below
     // the previous window's, else the inner solve ends and the refinement /
     // fallback loop takes over (COCG residuals oscillate: windows, not samples)
-    const int win = learned ? 4 : (sizeof(T) == 4 ? 8 : 32);
-    if (!w->h_ctrl->done) {
+    // (FP64 inner solves have no window: like COCG13_single they run to the cap)
+    const int win = learned ? 4 : 16;
+    if (!w->h_ctrl->done && (learned || sizeof(T) == 4)) {
       AFEM_CUDA(cudaMemcpyAsync(w->h_sc, w->sc.p, sizeof(SysScal) * NS, cudaMemcpyDeviceToHost, s));
       AFEM_CUDA(cudaStreamSynchronize(s));
       double worst = 0.0;
@@ -962,6 +1092,7 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     int b1 = 0;
     AFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_spmv<double, NS>, 256, 0));
     w->nblocks = std::max(1, b1) * c->num_sms;
+    w->nblocks = std::max(w->nblocks, coresident_blocks(k_fwd_mc<double, NS>, c->num_sms));
     int bf = coresident_blocks(k_fwd<double, NS>, c->num_sms);
     int bb = coresident_blocks(k_bwd<double, NS>, c->num_sms);
     w->nblocks = std::max(w->nblocks, std::max(bf, bb));

@@ -53,7 +53,8 @@ typedef enum afem_precond {
   AFEM_PRECOND_SSOR = 1,  /* DD_i = 1/(sd*D_i), same forward/backward sweeps */
   AFEM_PRECOND_DIAG = 2,  /* z = DD * r */
   AFEM_PRECOND_NONE = 3,
-  AFEM_PRECOND_LEARNED = 4  /* flexible COCG with the learned network; SSOR-COCG restart when it stalls */
+  AFEM_PRECOND_LEARNED = 4,  /* flexible COCG with the learned network; SSOR-COCG restart when it stalls */
+  AFEM_PRECOND_SSOR_MC = 5   /* SSOR of the colour-permuted matrix: every sweep is ~20 parallel passes */
 } afem_precond;
 
 typedef enum afem_precision {
@@ -212,6 +213,10 @@ int afem_profile_entry(afem_ctx *ctx, int i, char *name, int cap, double *ms, lo
  * in these orders.  No counterpart in the reference (its sweeps are serial). */
 int afem_sweep_schedule(int n, const int32_t *rowptr, const int32_t *col, const int32_t *diagpos, int32_t *perm_f,
                         int32_t *perm_b, int *levels_f, int *levels_b);
+
+/* Host only: greedy distance-1 colouring of a CSR pattern; color[n], perm[n]
+ * (rows sorted by colour), cptr[ncolors+1] (cptr must hold 256).  Returns ncolors. */
+int afem_coloring(int n, const int32_t *rowptr, const int32_t *col, uint8_t *color, int32_t *perm, int32_t *cptr);
 
 /* ---- drop-in driver --------------------------------------------------------- */
 /* Replaces the rank-0 input stage of program n_ebfem_bxyz (n_ebfem_bxyz_mpi.f90:55-90):

@@ -85,3 +85,28 @@ def test_sweep_schedule_is_topological(gpulib, oracle):
         assert np.all(pos_b[upper] < pos_b[i])
     # far fewer levels than rows: the sweep parallelism the schedule exposes
     assert 10 < lf.value < n // 50 and 10 < lb.value < n // 50
+
+
+def test_coloring_is_proper(gpulib, oracle):
+    """Rows of one colour share no nonzero; the colour-sorted order is a permutation."""
+    from actfemtide_b200 import synth
+    from actfemtide_b200.capi import ptr
+    m = synth.tidal_box(8, 8, 6, seed=1)
+    line, n6 = oracle.mkline(m.node, m.n4)
+    INU, IAU, INL, IAL = oracle.pattern(line.shape[0], n6)
+    n = line.shape[0]
+    rows, cols = [], []
+    for i in range(n):
+        cs = sorted([c - 1 for c in IAL[INL[i]:INL[i + 1]]] + [i] + [c - 1 for c in IAU[INU[i]:INU[i + 1]]])
+        cols += cs
+        rows.append(len(cs))
+    rowptr = np.concatenate([[0], np.cumsum(rows)]).astype(np.int32)
+    col = np.array(cols, np.int32)
+    color = np.zeros(n, np.uint8); perm = np.zeros(n, np.int32); cptr = np.zeros(256, np.int32)
+    nc = gpulib.afem_coloring(n, ptr(rowptr), ptr(col), ptr(color), ptr(perm), ptr(cptr))
+    assert 2 <= nc <= 40
+    rr = np.repeat(np.arange(n), np.diff(rowptr))
+    off = col != rr
+    assert not np.any(color[rr[off]] == color[col[off]])
+    assert sorted(perm) == list(range(n))
+    assert np.all(np.diff(color[perm]) >= 0) and cptr[nc] == n
