@@ -82,6 +82,7 @@ struct SolverWork {
   DBuf<double> rms;                 // per-system rms(r) for the learned preconditioner
   int rpw64 = 0, rpw32 = 0;         // SpMV rows per warp chosen by tune_spmv (0 = not tuned)
   int mc_blocks = 0;                // co-resident grid of the multicolour sweeps
+  bool no_window = false;           // COCG13_single semantics: no stagnation window, run to the cap
   bool kmf_valid = false;
   DBuf<unsigned> flag_f, flag_b;
   DBuf<double> part;                // partial sums [block][sys][4]
@@ -1017,9 +1018,11 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
     // of `win` chunks (learned: 4, FP32 inner: 16) must be 10% below
     // the previous window's, else the inner solve ends and the refinement /
     // fallback loop takes over (COCG residuals oscillate: windows, not samples)
-    // (FP64 inner solves have no window: like COCG13_single they run to the cap)
-    const int win = learned ? 4 : 16;
-    if (!w->h_ctrl->done && (learned || sizeof(T) == 4)) {
+    // FP64 inner solves get a long window (64 chunks, 2048 iterations): on the
+    // air-dominated systems the recursive residual can flatten out near 1e-7,
+    // and a restart from the true residual resumes the descent
+    const int win = learned ? 4 : (sizeof(T) == 4 ? 16 : 64);
+    if (!w->h_ctrl->done && !w->no_window) {
       AFEM_CUDA(cudaMemcpyAsync(w->h_sc, w->sc.p, sizeof(SysScal) * NS, cudaMemcpyDeviceToHost, s));
       AFEM_CUDA(cudaStreamSynchronize(s));
       double worst = 0.0;
@@ -1154,6 +1157,7 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     AFEM_CUDA(cudaMemcpyAsync(w->r64.p, w->b.p, sizeof(double2) * total, cudaMemcpyDeviceToDevice, s));
   }
   const bool recursive_only = ex && ex->recursive_only;
+  w->no_window = recursive_only;
   const double tol = o->tol > 0 ? o->tol : 1e-8;
   const int maxit = o->maxit > 0 ? o->maxit : 100000;
   int it_total = 0, refinements = 0;

@@ -23,13 +23,13 @@ def test_ctl_driver_matches_oracle(gpulib, oracle, tmp_path):
         assert np.allclose(xyz, m.sites, atol=1e-12)
         line, n6 = fw.lines()
         assert np.array_equal(line, of.line) and np.array_equal(n6, of.n6line)
-        fw.run_ctl(precond="SSOR", tol=1e-12)
+        fw.run_ctl(precond="SSOR", tol=1e-10)
     # the ctl path uses GENMAT's ocean conductivity, the default-real literal 3.33
     m33 = synth.TidalModel(**{**m.__dict__, "sigma_ocean": float(np.float32(3.33)), "sites": xyz})
     of33 = oracle.OracleForward(m33, of.line, of.n6line)
     for fi, fr in enumerate(m.freqs):
         A = of33.assemble(fr)
-        r = oracle.cocg13_single(A, precond="SSOR", resid=1e-12, maxit=100000)
+        r = oracle.cocg13_single(A, precond="SSOR", resid=1e-11, maxit=100000)
         out, amp, ph = of33.sites(r["x"], fr)
         for s in range(xyz.shape[0]):
             path = os.path.join(str(tmp_path), f"S{s + 1:03d}_S1.dat")
