@@ -981,7 +981,11 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
     if (!gexec) use_graph = false;
   }
   int iter_before = 0;
-  for (;;) {
+  // every chunk either advances the iteration count or ends the solve; the
+  // chunk budget is a host-side backstop against a device state that does neither
+  const long chunk_budget = (long)maxit / chunk + 4;
+  for (long nchunk = 0;; ++nchunk) {
+    AFEM_REQUIRE(nchunk < chunk_budget, AFEM_ESTATE, "COCG: inner solve made no progress");
     if (use_graph) {
       AFEM_CUDA(cudaGraphLaunch(gexec, s));
     } else {
@@ -1014,6 +1018,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
       }
     }
     iter_before = w->h_ctrl->iter;
+    if (w->h_ctrl->done) break;
     // stagnation detector: the smallest worst-system residual seen in a window
     // of `win` chunks (learned: 4, FP32 inner: 16) must be 10% below
     // the previous window's, else the inner solve ends and the refinement /
@@ -1022,7 +1027,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
     // air-dominated systems the recursive residual can flatten out near 1e-7,
     // and a restart from the true residual resumes the descent
     const int win = learned ? 4 : (sizeof(T) == 4 ? 16 : 64);
-    if (!w->h_ctrl->done && !w->no_window) {
+    if (!w->no_window) {
       AFEM_CUDA(cudaMemcpyAsync(w->h_sc, w->sc.p, sizeof(SysScal) * NS, cudaMemcpyDeviceToHost, s));
       AFEM_CUDA(cudaStreamSynchronize(s));
       double worst = 0.0;
