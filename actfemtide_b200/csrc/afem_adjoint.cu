@@ -102,7 +102,8 @@ __global__ void k_jacobian(const double* __restrict__ xyz, const int32_t* __rest
 
 void jacobian_device(afem_ctx* c, double freq, const double* x_host, int nadj, double* J_host) {
   AFEM_REQUIRE(c->assembled && c->ntet > 0, AFEM_ESTATE, "jacobian: no assembled mesh system");
-  AFEM_REQUIRE(c->nsys == nadj && c->X.p, AFEM_ESTATE, "jacobian: solve the nadj adjoint systems first");
+  AFEM_REQUIRE(c->nsys == nadj && c->X.p && !c->sol_packed, AFEM_ESTATE,
+               "jacobian: solve the nadj adjoint systems first");
   cudaStream_t s = c->stream;
   DBuf<double2> x;
   x.upload(reinterpret_cast<const double2*>(x_host), c->nline, s);

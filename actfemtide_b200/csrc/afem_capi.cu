@@ -46,6 +46,7 @@ void load_split_system(afem_ctx* c, int n, const int32_t* INU, const int32_t* IA
                        const int32_t* IAL, const double* D, const double* AU, const double* AL, const double* b) {
   AFEM_REQUIRE(n > 0 && INU && IAU && INL && IAL && D && AU && AL && b, AFEM_EINVAL, "split system: null array");
   AFEM_REQUIRE(INU[0] == 0 && INL[0] == 0, AFEM_EINVAL, "split system: INU(0) and INL(0) must be 0");
+  clear_segments(c);
   std::vector<int32_t> rp(n + 1), cl, dp(n);
   std::vector<double2> km;
   const long tot = (long)INU[n] + INL[n] + n;
@@ -184,6 +185,7 @@ int afem_set_mesh(afem_ctx* c, int node, const double* xyz, int ntet, const int3
     c->pattern_ready = false;
     c->assembled = false;
     c->sigma_set = false;
+    afem::clear_segments(c);
     afem::reset_status(c);
     if (nline > 0) {
       c->nline = nline;
@@ -205,6 +207,76 @@ int afem_get_lines(afem_ctx* c, int* nline, int32_t* line, int32_t* n6line) {
     if (line) c->line.download(line, 2L * c->nline, c->stream);
     if (n6line) c->n6line.download(n6line, 6L * c->ntet, c->stream);
     AFEM_CUDA(cudaStreamSynchronize(c->stream));
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_set_segments(afem_ctx* c, int nseg, const int32_t* node_ptr) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(c->nline > 0 && c->ntet > 0, AFEM_ESTATE, "set_segments: set the mesh first");
+    AFEM_REQUIRE(nseg >= 0 && nseg <= 32, AFEM_EINVAL, "set_segments: nseg must be 0..32");
+    afem::clear_segments(c);
+    if (nseg == 0) return (int)AFEM_OK;
+    AFEM_REQUIRE(node_ptr, AFEM_EINVAL, "set_segments: null node_ptr");
+    AFEM_REQUIRE(node_ptr[0] == 0 && node_ptr[nseg] == c->node, AFEM_EINVAL,
+                 "set_segments: node_ptr must run from 0 to node");
+    for (int k = 0; k < nseg; ++k)
+      AFEM_REQUIRE(node_ptr[k + 1] > node_ptr[k], AFEM_EINVAL, "set_segments: empty or decreasing node range");
+    cudaStream_t s = c->stream;
+    // segment of a 1-based node id
+    auto seg_of = [&](int32_t id) {
+      return (int)(std::upper_bound(node_ptr, node_ptr + nseg + 1, id - 1) - node_ptr) - 1;
+    };
+    // tetrahedra: all four nodes in one mesh, meshes in order
+    std::vector<int32_t> n4(4L * c->ntet);
+    c->n4.download(n4.data(), n4.size(), s);
+    std::vector<int32_t> line(2L * c->nline);
+    c->line.download(line.data(), line.size(), s);
+    AFEM_CUDA(cudaStreamSynchronize(s));
+    std::vector<int32_t> tet_ptr(nseg + 1, 0), row_ptr(nseg + 1, 0);
+    int prev = 0;
+    for (long t = 0; t < c->ntet; ++t) {
+      const int k = seg_of(n4[4 * t]);
+      for (int j = 1; j < 4; ++j)
+        AFEM_REQUIRE(seg_of(n4[4 * t + j]) == k, AFEM_EINVAL, "set_segments: a tetrahedron joins two meshes");
+      AFEM_REQUIRE(k >= prev, AFEM_EINVAL, "set_segments: tetrahedra are not grouped mesh by mesh");
+      prev = k;
+      tet_ptr[k + 1] += 1;
+    }
+    std::vector<uint8_t> seg(c->nline);
+    prev = 0;
+    for (long e = 0; e < c->nline; ++e) {
+      const int k = seg_of(line[2 * e]);
+      AFEM_REQUIRE(seg_of(line[2 * e + 1]) == k, AFEM_EINVAL, "set_segments: an edge joins two meshes");
+      AFEM_REQUIRE(k >= prev, AFEM_EINVAL, "set_segments: edges are not numbered mesh by mesh");
+      prev = k;
+      row_ptr[k + 1] += 1;
+      seg[e] = (uint8_t)k;
+    }
+    for (int k = 0; k < nseg; ++k) {
+      AFEM_REQUIRE(tet_ptr[k + 1] > 0 && row_ptr[k + 1] > 0, AFEM_EINVAL, "set_segments: a mesh has no tetrahedra");
+      tet_ptr[k + 1] += tet_ptr[k];
+      row_ptr[k + 1] += row_ptr[k];
+    }
+    c->seg_node_ptr.assign(node_ptr, node_ptr + nseg + 1);
+    c->seg_tet_ptr = tet_ptr;
+    c->seg_row_ptr = row_ptr;
+    c->seg_of_row.upload(seg.data(), seg.size(), s);
+    AFEM_CUDA(cudaStreamSynchronize(s));
+    c->nseg = nseg;
+    afem::invalidate_work(c);
+    c->nsys = 0;
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_segment_info(afem_ctx* c, int* nseg, int32_t* row_ptr, int32_t* tet_ptr) {
+  return guarded(c, [&]() {
+    if (nseg) *nseg = c->nseg;
+    if (c->nseg > 0) {
+      if (row_ptr) std::copy(c->seg_row_ptr.begin(), c->seg_row_ptr.end(), row_ptr);
+      if (tet_ptr) std::copy(c->seg_tet_ptr.begin(), c->seg_tet_ptr.end(), tet_ptr);
+    }
     return (int)AFEM_OK;
   });
 }
@@ -365,6 +437,12 @@ int afem_solve(afem_ctx* c, int nsys, const double* freq, const int* src, const 
 int afem_get_solution(afem_ctx* c, int k, double* x) {
   return guarded(c, [&]() {
     AFEM_REQUIRE(k >= 0 && k < c->nsys && x, AFEM_EINVAL, "get_solution: no such system");
+    if (c->sol_packed) {  // packed batch: the rows of mesh k
+      const int r0 = c->seg_row_ptr[k], r1 = c->seg_row_ptr[k + 1];
+      AFEM_CUDA(cudaMemcpyAsync(x, c->X.p + r0, sizeof(double2) * (r1 - r0), cudaMemcpyDeviceToHost, c->stream));
+      AFEM_CUDA(cudaStreamSynchronize(c->stream));
+      return (int)AFEM_OK;
+    }
     // stored [row][system]
     std::vector<double2> all((size_t)c->nline * c->nsys);
     c->X.download(all.data(), all.size(), c->stream);

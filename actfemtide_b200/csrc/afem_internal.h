@@ -169,10 +169,18 @@ struct afem_ctx {
   int rhs_nsrc = 0;
   bool assembled = false;
 
+  // packed batch of independent meshes (segments): mesh k owns nodes
+  // [seg_node_ptr[k], seg_node_ptr[k+1]), tetrahedra [seg_tet_ptr[k], ..) and
+  // rows [seg_row_ptr[k], ..) of the union; system k of a solve is mesh k
+  int nseg = 0;
+  std::vector<int32_t> seg_node_ptr, seg_tet_ptr, seg_row_ptr;
+  afem::DBuf<uint8_t> seg_of_row;  // nline: segment of each row
+
   // solutions of the last solve: x[k*nline + i]
   afem::DBuf<double2> X;
   std::vector<double> sol_freq;
   int nsys = 0;
+  bool sol_packed = false;  // X holds a packed batch: one system per row, x[i]
 
   afem::SolverWork* work = nullptr;
   afem::MpnnState* mpnn = nullptr;
@@ -193,6 +201,15 @@ void exclusive_scan(const int32_t* in, int32_t* out, int n, cudaStream_t s, long
 
 // afem_assemble.cu
 void assemble_device(afem_ctx* c);        // K, M, rhs, bc (GENMAT + COPY_UL + GENBCCSEM + SET_BC)
+
+// packed batches
+inline void clear_segments(afem_ctx* c) {
+  c->nseg = 0;
+  c->seg_node_ptr.clear();
+  c->seg_tet_ptr.clear();
+  c->seg_row_ptr.clear();
+  c->seg_of_row.release();
+}
 
 // afem_solver.cu
 struct SolveExtra {

@@ -54,12 +54,13 @@ __device__ __forceinline__ void nodebasis(const V3 e[4], const V3& x3, double a[
   a[0] = a1; a[1] = a2; a[2] = a3; a[3] = a4;
 }
 
-__global__ void k_find(const double* __restrict__ xyz, const int32_t* __restrict__ n4, int ntet,
+// Searches tetrahedra t0 <= t < t1 (a packed batch restricts the search to one mesh).
+__global__ void k_find(const double* __restrict__ xyz, const int32_t* __restrict__ n4, long t0, long t1,
                        const double* __restrict__ obs, int nobs, int* __restrict__ best) {
   const int s = blockIdx.y;
   if (s >= nobs) return;
   const V3 x3{obs[3 * s], obs[3 * s + 1], obs[3 * s + 2]};
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < ntet; t += (long)gridDim.x * blockDim.x) {
+  for (long t = t0 + blockIdx.x * (long)blockDim.x + threadIdx.x; t < t1; t += (long)gridDim.x * blockDim.x) {
     if (t >= *(volatile int*)(best + s)) break;
     V3 e[4];
     load_tet(xyz, n4, t, e);
@@ -170,8 +171,10 @@ __global__ void k_eval(const double2* __restrict__ X, int nline, int nsys, const
 
 }  // namespace
 
-void site_coeffs_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item, double* val_e, double* val_f,
-                        int32_t* iele) {
+namespace {
+
+void site_coeffs_range(afem_ctx* c, int nobs, const double* xyz_obs, long t0, long t1, int32_t* item, double* val_e,
+                       double* val_f, int32_t* iele) {
   cudaStream_t s = c->stream;
   DBuf<double> obs;
   obs.upload(xyz_obs, 3L * nobs, s);
@@ -179,8 +182,8 @@ void site_coeffs_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* i
   best.alloc(nobs);
   std::vector<int> init(nobs, 0x7fffffff);
   AFEM_CUDA(cudaMemcpyAsync(best.p, init.data(), sizeof(int) * nobs, cudaMemcpyHostToDevice, s));
-  dim3 grid(std::max(1, std::min(2 * c->num_sms, (c->ntet + 255) / 256)), nobs);
-  k_find<<<grid, 256, 0, s>>>(c->xyz.p, c->n4.p, c->ntet, obs.p, nobs, best.p);
+  dim3 grid(std::max(1, std::min(2 * c->num_sms, (int)((t1 - t0 + 255) / 256))), nobs);
+  k_find<<<grid, 256, 0, s>>>(c->xyz.p, c->n4.p, t0, t1, obs.p, nobs, best.p);
   DBuf<int32_t> ditem;
   DBuf<double> dve, dvf;
   ditem.alloc(6L * nobs);
@@ -201,9 +204,43 @@ void site_coeffs_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* i
   AFEM_CUDA(cudaStreamSynchronize(s));
 }
 
+}  // namespace
+
+void site_coeffs_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item, double* val_e, double* val_f,
+                        int32_t* iele) {
+  site_coeffs_range(c, nobs, xyz_obs, 0, c->ntet, item, val_e, val_f, iele);
+}
+
 void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out) {
   AFEM_REQUIRE(c->nsys > 0 && c->X.p, AFEM_ESTATE, "sites: no solution");
   cudaStream_t s = c->stream;
+  if (c->sol_packed) {
+    // packed batch: system k is mesh k; its sites are searched in its own tetrahedra
+    AFEM_REQUIRE((int)c->seg_tet_ptr.size() == c->nsys + 1, AFEM_ESTATE, "sites: the packed meshes changed");
+    const double pi = 4.0 * std::atan(1.0);
+    std::vector<int32_t> item(6L * nobs);
+    std::vector<double> ve(18L * nobs), vf(18L * nobs);
+    DBuf<int32_t> ditem;
+    DBuf<double> dve, dvf, dom;
+    DBuf<double2> dout;
+    dout.alloc((long)c->nsys * 5 * nobs);
+    for (int k = 0; k < c->nsys; ++k) {
+      site_coeffs_range(c, nobs, xyz_obs, c->seg_tet_ptr[k], c->seg_tet_ptr[k + 1], item.data(), ve.data(), vf.data(),
+                        nullptr);
+      ditem.upload(item.data(), item.size(), s);
+      dve.upload(ve.data(), ve.size(), s);
+      dvf.upload(vf.data(), vf.size(), s);
+      const double om = 2.0 * pi * c->sol_freq[k];
+      dom.upload(&om, 1, s);
+      const long tot = 5L * nobs;
+      k_eval<<<(unsigned)((tot + 127) / 128), 128, 0, s>>>(c->X.p, c->nline, 1, dom.p, nobs, ditem.p, dve.p, dvf.p,
+                                                           dout.p + (long)k * 5 * nobs);
+      AFEM_CUDA(cudaStreamSynchronize(s));
+    }
+    dout.download(reinterpret_cast<double2*>(out), (long)c->nsys * 5 * nobs, s);
+    AFEM_CUDA(cudaStreamSynchronize(s));
+    return;
+  }
   std::vector<int32_t> item(6L * nobs);
   std::vector<double> ve(18L * nobs), vf(18L * nobs);
   site_coeffs_device(c, nobs, xyz_obs, item.data(), ve.data(), vf.data(), nullptr);

@@ -48,7 +48,8 @@ struct Cx<float> {
   __host__ __device__ static V make(float a, float b) { return make_float2(a, b); }
 };
 
-constexpr int MAX_NS = 16;
+constexpr int MAX_NS = 16;   // systems sharing one matrix (lanes of a warp)
+constexpr int MAX_SYS = 32;  // systems of one solve: NS, or the meshes of a packed batch
 constexpr unsigned SPIN_LIMIT = 1u << 21;  // x ~1 us back-off: a wait gives up after ~2 s
 
 // per-system scalars (always FP64)
@@ -71,6 +72,8 @@ struct Ctrl {
 
 struct SolverWork {
   int n = 0, ns = 0, prec_bits = 64;
+  int nsys = 0;     // systems of the current solve: ns, or the meshes of a packed batch
+  bool seg = false; // packed batch: vectors hold one system per row
   int nblocks = 0;  // persistent grid size (blocks of 256 threads)
   DBuf<double2> x, b;               // FP64 solution and right-hand side [row][sys]
   DBuf<double2> r64;                // FP64 true residual
@@ -155,14 +158,37 @@ __device__ __forceinline__ void block_partials(const double (&v)[NVAL], double* 
 #pragma unroll
       for (int k = 0; k < NVAL; ++k) acc[k] += red[ww][s][k];
 #pragma unroll
-    for (int k = 0; k < NVAL; ++k) part[((long)blockIdx.x * MAX_NS + s) * 4 + k] = acc[k];
+    for (int k = 0; k < NVAL; ++k) part[((long)blockIdx.x * MAX_SYS + s) * 4 + k] = acc[k];
+  }
+}
+
+// Packed batches of independent meshes (NS = 1, SEG): the system of a row is
+// seg[row].  Each warp slot adds its rows' values to its own per-system sums
+// in shared memory; the block then adds the slots in a fixed order, so the
+// partial sums stay deterministic.
+template <int SLOTS, int NVAL>
+__device__ __forceinline__ double (*seg_sums())[MAX_SYS][NVAL] {
+  __shared__ double red[SLOTS][MAX_SYS][NVAL];
+  for (int i = threadIdx.x; i < SLOTS * MAX_SYS * NVAL; i += blockDim.x) (&red[0][0][0])[i] = 0.0;
+  __syncthreads();
+  return red;
+}
+
+template <int SLOTS, int NVAL>
+__device__ __forceinline__ void seg_partials(double (*red)[MAX_SYS][NVAL], double* part) {
+  __syncthreads();
+  for (int t = threadIdx.x; t < MAX_SYS * NVAL; t += blockDim.x) {
+    const int sid = t / NVAL, k = t % NVAL;
+    double acc = 0.0;
+    for (int sl = 0; sl < SLOTS; ++sl) acc += red[sl][sid][k];
+    part[((long)blockIdx.x * MAX_SYS + sid) * 4 + k] = acc;
   }
 }
 
 // ------------------------------------------------------------------ forward sweep
 // For iteration > 1 first applies the previous update to the row, then
 // y_i = (r_i - sum_{j<i} A_ij y_j) * DD_i  (COCG13_single.f90:203-212, 304-307).
-template <class T, int NS>
+template <class T, int NS, bool SEG = false>
 __global__ void __launch_bounds__(256)
     k_fwd(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const int32_t* __restrict__ diagpos,
           const typename Cx<T>::V* __restrict__ km, int n, typename Cx<T>::V* __restrict__ r,
@@ -170,8 +196,9 @@ __global__ void __launch_bounds__(256)
           const typename Cx<T>::V* __restrict__ q, double2* __restrict__ x, const typename Cx<T>::V* __restrict__ dd,
           unsigned* __restrict__ flag, int mode, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl,
           double* __restrict__ part, DevStatus* st, typename Cx<T>::V* __restrict__ rprev,
-          const int32_t* __restrict__ perm) {
+          const int32_t* __restrict__ perm, const uint8_t* __restrict__ seg) {
   using V = typename Cx<T>::V;
+  static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;
   constexpr int G = 32 / NS;
   const unsigned epoch = ctrl->epoch;
@@ -179,12 +206,21 @@ __global__ void __launch_bounds__(256)
   const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const double om = sc[s].omega;
-  const double2 al = sc[s].alpha;
-  const bool act = sc[s].active;
+  double om = sc[s].omega;
+  double2 al = sc[s].alpha;
+  bool act = sc[s].active;
   double rr = 0.0;
+  double (*red)[MAX_SYS][1] = nullptr;
+  if constexpr (SEG) red = seg_sums<8, 1>();
   for (int pos = warp; pos < n; pos += nwarps) {
     const int row = __ldg(perm + pos);
+    int sid = s;
+    if constexpr (SEG) {
+      sid = __ldg(seg + row);
+      om = sc[sid].omega;
+      al = sc[sid].alpha;
+      act = sc[sid].active;
+    }
     V ri = r[(long)row * NS + s];
     if (rprev && g == 0) rprev[(long)row * NS + s] = ri;  // flexible COCG keeps r_k
     if (update && act && g == 0) {
@@ -197,7 +233,11 @@ __global__ void __launch_bounds__(256)
       xi.y += al.x * (double)pi.y + al.y * (double)pi.x;
       x[(long)row * NS + s] = xi;
     }
-    if (g == 0) rr += (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
+    if (g == 0) {
+      const double v = (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
+      if constexpr (SEG) red[threadIdx.x >> 5][sid][0] += v;
+      else rr += v;
+    }
     if (mode == 2) {  // DIAG: z = DD r
       if (g == 0) {
         const V d = dd[(long)row * NS + s];
@@ -230,30 +270,43 @@ __global__ void __launch_bounds__(256)
     __syncwarp();
     if (lane == 0) st_release(flag + row, epoch);  // release: the row's values are visible first
   }
-  double v[1] = {rr};
-  block_partials<NS, 1>(v, part);
+  if constexpr (SEG) {
+    seg_partials<8, 1>(red, part);
+  } else {
+    double v[1] = {rr};
+    block_partials<NS, 1>(v, part);
+  }
 }
 
 // ------------------------------------------------------------------ backward sweep
 // z_i = y_i - DD_i * sum_{j>i} A_ij z_j (COCG13_single.f90:214-225), rho += r_i z_i.
-template <class T, int NS>
+template <class T, int NS, bool SEG = false>
 __global__ void __launch_bounds__(256)
     k_bwd(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const int32_t* __restrict__ diagpos,
           const typename Cx<T>::V* __restrict__ km, int n, const typename Cx<T>::V* __restrict__ r,
           typename Cx<T>::V* __restrict__ z, const typename Cx<T>::V* __restrict__ dd, unsigned* __restrict__ flag,
           int mode, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl, double* __restrict__ part, DevStatus* st,
-          const typename Cx<T>::V* __restrict__ rprev, const int32_t* __restrict__ perm) {
+          const typename Cx<T>::V* __restrict__ rprev, const int32_t* __restrict__ perm,
+          const uint8_t* __restrict__ seg) {
   using V = typename Cx<T>::V;
+  static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;
   constexpr int G = 32 / NS;
   const unsigned epoch = ctrl->epoch;
   const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const double om = sc[s].omega;
+  double om = sc[s].omega;
   double rx = 0.0, ry = 0.0, px = 0.0, py = 0.0;
+  double (*red)[MAX_SYS][4] = nullptr;
+  if constexpr (SEG) red = seg_sums<8, 4>();
   for (int pos = warp; pos < n; pos += nwarps) {
     const int row = __ldg(perm + pos);
+    int sid = s;
+    if constexpr (SEG) {
+      sid = __ldg(seg + row);
+      om = sc[sid].omega;
+    }
     V zi = z[(long)row * NS + s];
     if (mode <= 1) {
       const int k0 = diagpos[row] + 1, k1 = rowptr[row + 1];
@@ -279,17 +332,28 @@ __global__ void __launch_bounds__(256)
     }
     if (g == 0) {
       const V ri = r[(long)row * NS + s];
-      rx += (double)ri.x * (double)zi.x - (double)ri.y * (double)zi.y;
-      ry += (double)ri.x * (double)zi.y + (double)ri.y * (double)zi.x;
-      if (rprev) {
-        const V rp = rprev[(long)row * NS + s];
-        px += (double)rp.x * (double)zi.x - (double)rp.y * (double)zi.y;
-        py += (double)rp.x * (double)zi.y + (double)rp.y * (double)zi.x;
+      const double ex = (double)ri.x * (double)zi.x - (double)ri.y * (double)zi.y;
+      const double ey = (double)ri.x * (double)zi.y + (double)ri.y * (double)zi.x;
+      if constexpr (SEG) {
+        red[threadIdx.x >> 5][sid][0] += ex;
+        red[threadIdx.x >> 5][sid][1] += ey;
+      } else {
+        rx += ex;
+        ry += ey;
+        if (rprev) {
+          const V rp = rprev[(long)row * NS + s];
+          px += (double)rp.x * (double)zi.x - (double)rp.y * (double)zi.y;
+          py += (double)rp.x * (double)zi.y + (double)rp.y * (double)zi.x;
+        }
       }
     }
   }
-  double v[4] = {rx, ry, px, py};
-  block_partials<NS, 4>(v, part);
+  if constexpr (SEG) {
+    seg_partials<8, 4>(red, part);
+  } else {
+    double v[4] = {rx, ry, px, py};
+    block_partials<NS, 4>(v, part);
+  }
 }
 
 // ------------------------------------------------------------------ multicolour sweeps
@@ -298,15 +362,16 @@ __global__ void __launch_bounds__(256)
 // its rows, summing only entries of earlier colours) and the backward sweep
 // goes through the colours in reverse.  One persistent cooperative kernel per
 // sweep with a grid barrier between colours; no flags, no waits.
-template <class T, int NS>
+template <class T, int NS, bool SEG = false>
 __global__ void __launch_bounds__(256)
     k_fwd_mc(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const typename Cx<T>::V* __restrict__ km,
              int n, typename Cx<T>::V* __restrict__ r, typename Cx<T>::V* __restrict__ y,
              const typename Cx<T>::V* __restrict__ p, const typename Cx<T>::V* __restrict__ q, double2* __restrict__ x,
              const typename Cx<T>::V* __restrict__ dd, const uint8_t* __restrict__ color,
              const int32_t* __restrict__ perm, const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc,
-             Ctrl* __restrict__ ctrl, double* __restrict__ part) {
+             Ctrl* __restrict__ ctrl, double* __restrict__ part, const uint8_t* __restrict__ seg) {
   using V = typename Cx<T>::V;
+  static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;  // uniform over the grid
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
   constexpr int G = 32 / NS;
@@ -314,14 +379,23 @@ __global__ void __launch_bounds__(256)
   const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const double om = sc[s].omega;
-  const double2 al = sc[s].alpha;
-  const bool act = sc[s].active;
+  double om = sc[s].omega;
+  double2 al = sc[s].alpha;
+  bool act = sc[s].active;
   double rr = 0.0;
+  double (*red)[MAX_SYS][1] = nullptr;
+  if constexpr (SEG) red = seg_sums<8, 1>();
   for (int c = 0; c < ncolors; ++c) {
     const int p0 = cptr[c], p1 = cptr[c + 1];
     for (int pos = p0 + warp; pos < p1; pos += nwarps) {
       const int row = __ldg(perm + pos);
+      int sid = s;
+      if constexpr (SEG) {
+        sid = __ldg(seg + row);
+        om = sc[sid].omega;
+        al = sc[sid].alpha;
+        act = sc[sid].active;
+      }
       V ri = r[(long)row * NS + s];
       if (update && act && g == 0) {
         const V qi = q[(long)row * NS + s], pi = p[(long)row * NS + s];
@@ -333,7 +407,11 @@ __global__ void __launch_bounds__(256)
         xi.y += al.x * (double)pi.y + al.y * (double)pi.x;
         x[(long)row * NS + s] = xi;
       }
-      if (g == 0) rr += (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
+      if (g == 0) {
+        const double v = (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
+        if constexpr (SEG) red[threadIdx.x >> 5][sid][0] += v;
+        else rr += v;
+      }
       T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
       for (int k = rowptr[row] + g; k < rowptr[row + 1]; k += G) {
         const int j = __ldg(col + k);
@@ -353,30 +431,42 @@ __global__ void __launch_bounds__(256)
     }
     grid.sync();
   }
-  double v[1] = {rr};
-  block_partials<NS, 1>(v, part);
+  if constexpr (SEG) {
+    seg_partials<8, 1>(red, part);
+  } else {
+    double v[1] = {rr};
+    block_partials<NS, 1>(v, part);
+  }
 }
 
-template <class T, int NS>
+template <class T, int NS, bool SEG = false>
 __global__ void __launch_bounds__(256)
     k_bwd_mc(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const typename Cx<T>::V* __restrict__ km,
              int n, const typename Cx<T>::V* __restrict__ r, typename Cx<T>::V* __restrict__ z,
              const typename Cx<T>::V* __restrict__ dd, const uint8_t* __restrict__ color,
              const int32_t* __restrict__ perm, const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc,
-             Ctrl* __restrict__ ctrl, double* __restrict__ part) {
+             Ctrl* __restrict__ ctrl, double* __restrict__ part, const uint8_t* __restrict__ seg) {
   using V = typename Cx<T>::V;
+  static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
   constexpr int G = 32 / NS;
   const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const double om = sc[s].omega;
+  double om = sc[s].omega;
   double rx = 0.0, ry = 0.0;
+  double (*red)[MAX_SYS][4] = nullptr;
+  if constexpr (SEG) red = seg_sums<8, 4>();
   for (int c = ncolors - 1; c >= 0; --c) {
     const int p0 = cptr[c], p1 = cptr[c + 1];
     for (int pos = p0 + warp; pos < p1; pos += nwarps) {
       const int row = __ldg(perm + pos);
+      int sid = s;
+      if constexpr (SEG) {
+        sid = __ldg(seg + row);
+        om = sc[sid].omega;
+      }
       T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
       for (int k = rowptr[row] + g; k < rowptr[row + 1]; k += G) {
         const int j = __ldg(col + k);
@@ -395,26 +485,37 @@ __global__ void __launch_bounds__(256)
         zi = Cx<T>::make(zi.x - (d.x * swx - d.y * swy), zi.y - (d.x * swy + d.y * swx));
         z[(long)row * NS + s] = zi;
         const V ri = r[(long)row * NS + s];
-        rx += (double)ri.x * (double)zi.x - (double)ri.y * (double)zi.y;
-        ry += (double)ri.x * (double)zi.y + (double)ri.y * (double)zi.x;
+        const double ex = (double)ri.x * (double)zi.x - (double)ri.y * (double)zi.y;
+        const double ey = (double)ri.x * (double)zi.y + (double)ri.y * (double)zi.x;
+        if constexpr (SEG) {
+          red[threadIdx.x >> 5][sid][0] += ex;
+          red[threadIdx.x >> 5][sid][1] += ey;
+        } else {
+          rx += ex;
+          ry += ey;
+        }
       }
     }
     grid.sync();
   }
-  double v[4] = {rx, ry, 0.0, 0.0};
-  block_partials<NS, 4>(v, part);
+  if constexpr (SEG) {
+    seg_partials<8, 4>(red, part);
+  } else {
+    double v[4] = {rx, ry, 0.0, 0.0};
+    block_partials<NS, 4>(v, part);
+  }
 }
 
 // ------------------------------------------------------------------ p update, SpMV
-template <class T, int NS>
+template <class T, int NS, bool SEG = false>
 __global__ void k_pupd(int n, const typename Cx<T>::V* __restrict__ z, typename Cx<T>::V* __restrict__ p,
-                       const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl) {
+                       const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl, const uint8_t* __restrict__ seg) {
   using V = typename Cx<T>::V;
   if (ctrl->done) return;
   const bool first = ctrl->iter == 0;
   const long total = (long)n * NS;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-    const int s = (int)(i % NS);
+    const int s = SEG ? (int)__ldg(seg + i) : (int)(i % NS);
     const V zi = z[i];
     if (first) {
       p[i] = zi;
@@ -431,25 +532,34 @@ __global__ void k_pupd(int n, const typename Cx<T>::V* __restrict__ z, typename 
 // resid_mode, computes r = b - A x in FP64 instead and ||r||^2 (and ||b||^2).
 // RPW rows per warp: lane = sub * (32/RPW) + g * NS + s, so rows of ~16
 // nonzeros do not leave half a warp idle (RPW is picked by tune_spmv).
-template <class T, int NS, int RPW = 1>
+template <class T, int NS, int RPW = 1, bool SEG = false>
 __global__ void __launch_bounds__(256)
     k_spmv(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
            const typename Cx<T>::V* __restrict__ km, int n, const typename Cx<T>::V* __restrict__ p,
            typename Cx<T>::V* __restrict__ q, const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl,
-           double* __restrict__ part, const typename Cx<T>::V* __restrict__ bvec) {
+           double* __restrict__ part, const typename Cx<T>::V* __restrict__ bvec, const uint8_t* __restrict__ seg) {
   using V = typename Cx<T>::V;
   static_assert(NS * RPW <= 32, "rows per warp times systems must fit a warp");
+  static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl && ctrl->done) return;
   constexpr int LPR = 32 / RPW;  // lanes per row
   constexpr int G = LPR / NS;    // entry groups per row
   const int lane = threadIdx.x & 31, sub = lane / LPR, s = lane % NS, g = (lane % LPR) / NS;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const double om = sc[s].omega;
+  double om = sc[s].omega;
   double ax = 0.0, ay = 0.0, bb = 0.0;
+  double (*red)[MAX_SYS][3] = nullptr;
+  if constexpr (SEG) red = seg_sums<8 * RPW, 3>();
+  const int slot = (threadIdx.x >> 5) * RPW + sub;
   for (int row0 = warp * RPW; row0 < n; row0 += nwarps * RPW) {
     const int row = row0 + sub;
     const bool live = row < n;
+    int sid = s;
+    if constexpr (SEG) {
+      sid = live ? (int)__ldg(seg + row) : 0;
+      om = sc[sid].omega;
+    }
     const int k0 = live ? rowptr[row] : 0, k1 = live ? rowptr[row + 1] : 0;
     T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
     for (int k = k0 + g; k < k1; k += G) {
@@ -467,19 +577,33 @@ __global__ void __launch_bounds__(256)
     if (g == 0 && live) {
       const T o = (T)om;
       const V qi = Cx<T>::make(t1x - o * t2y, t1y + o * t2x);
+      double e0, e1 = 0.0, e2 = 0.0;
       if (bvec) {  // r = b - A x
         const V bi = bvec[(long)row * NS + s];
         const V ri = Cx<T>::make(bi.x - qi.x, bi.y - qi.y);
         q[(long)row * NS + s] = ri;
-        ax += (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
-        bb += (double)bi.x * (double)bi.x + (double)bi.y * (double)bi.y;
+        e0 = (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
+        e2 = (double)bi.x * (double)bi.x + (double)bi.y * (double)bi.y;
       } else {
         q[(long)row * NS + s] = qi;
         const V pi = p[(long)row * NS + s];
-        ax += (double)pi.x * (double)qi.x - (double)pi.y * (double)qi.y;
-        ay += (double)pi.x * (double)qi.y + (double)pi.y * (double)qi.x;
+        e0 = (double)pi.x * (double)qi.x - (double)pi.y * (double)qi.y;
+        e1 = (double)pi.x * (double)qi.y + (double)pi.y * (double)qi.x;
+      }
+      if constexpr (SEG) {
+        red[slot][sid][0] += e0;
+        red[slot][sid][1] += e1;
+        red[slot][sid][2] += e2;
+      } else {
+        ax += e0;
+        ay += e1;
+        bb += e2;
       }
     }
+  }
+  if constexpr (SEG) {
+    seg_partials<8 * RPW, 3>(red, part);
+    return;
   }
   // fold the RPW rows of the warp onto lanes 0..NS-1
 #pragma unroll
@@ -500,7 +624,7 @@ __device__ __forceinline__ void sum_partials(const double* part, int nblocks, in
   const int lane = threadIdx.x & 31;
   for (int v = 0; v < nvals; ++v) {
     double acc = 0.0;
-    for (int b = lane; b < nblocks; b += 32) acc += part[((long)b * MAX_NS + s) * 4 + k + v];
+    for (int b = lane; b < nblocks; b += 32) acc += part[((long)b * MAX_SYS + s) * 4 + k + v];
     for (int m = 16; m > 0; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
     sh[threadIdx.x >> 5][v] = acc;
   }
@@ -589,10 +713,11 @@ __global__ void k_scal_pq(SysScal* sc, Ctrl* ctrl, const double* part, int nbloc
 // SSOR / DIAG: DD_i = 1 / (sd * D_i) (COCG13_single.f90:126-130).
 template <class T, int NS>
 __global__ void k_dd_diag(const typename Cx<T>::V* __restrict__ km, const int32_t* __restrict__ diagpos, int n,
-                          double sd, const SysScal* __restrict__ sc, typename Cx<T>::V* __restrict__ dd) {
+                          double sd, const SysScal* __restrict__ sc, typename Cx<T>::V* __restrict__ dd,
+                          const uint8_t* __restrict__ seg) {
   const long total = (long)n * NS;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-    const int row = (int)(i / NS), s = (int)(i % NS);
+    const int row = (int)(i / NS), s = seg ? (int)__ldg(seg + row) : (int)(i % NS);
     const double2 a = make_double2((double)km[diagpos[row]].x, (double)km[diagpos[row]].y);
     const double om = sc[s].omega;
     const double2 D = make_double2(sd * a.x, sd * om * a.y);
@@ -607,16 +732,17 @@ __global__ void __launch_bounds__(256)
     k_dd_ic(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const int32_t* __restrict__ diagpos,
             const typename Cx<T>::V* __restrict__ km, int n, double sd, const SysScal* __restrict__ sc,
             typename Cx<T>::V* __restrict__ dd, unsigned* __restrict__ flag, const Ctrl* __restrict__ ctrl,
-            DevStatus* st, const int32_t* __restrict__ perm) {
+            DevStatus* st, const int32_t* __restrict__ perm, const uint8_t* __restrict__ seg) {
   using V = typename Cx<T>::V;
   constexpr int G = 32 / NS;
   const unsigned epoch = ctrl->epoch;
   const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const double om = sc[s].omega;
+  double om = sc[s].omega;
   for (int pos = warp; pos < n; pos += nwarps) {
     const int row = __ldg(perm + pos);
+    if (seg) om = sc[__ldg(seg + row)].omega;  // packed batch (NS = 1)
     const int k0 = rowptr[row], k1 = diagpos[row];
     double wx = 0, wy = 0;
     for (int k = k0 + g; k < k1; k += G) {
@@ -654,10 +780,10 @@ __global__ void k_convert<float2, double2>(const double2* __restrict__ in, float
 }
 
 __global__ void k_gather_rhs(const double2* __restrict__ rhs, int n, int ns, const int* __restrict__ src,
-                             double2* __restrict__ b) {
+                             double2* __restrict__ b, const uint8_t* __restrict__ seg) {
   const long total = (long)n * ns;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-    const int row = (int)(i / ns), s = (int)(i % ns);
+    const int row = (int)(i / ns), s = seg ? (int)seg[row] : (int)(i % ns);
     b[i] = rhs[(long)src[s] * n + row];
   }
 }
@@ -780,24 +906,27 @@ struct Inner<float, NS> {
   static const V* KM(afem_ctx*, SolverWork* w) { return w->kmf.p; }
 };
 
-template <class T, int NS>
+template <class T, int NS, bool SEG>
 void launch_spmv(afem_ctx* c, SolverWork* w, int rpw, const typename Cx<T>::V* km, const typename Cx<T>::V* p,
                  typename Cx<T>::V* q, const Ctrl* ctrl, const typename Cx<T>::V* bvec) {
   cudaStream_t s = c->stream;
   const int n = w->n;
   const int32_t* rp = c->rowptr.p;
   const int32_t* cl = c->col.p;
+  const uint8_t* sg = SEG ? c->seg_of_row.p : nullptr;
   if (rpw == 4 && NS * 4 <= 32)
-    k_spmv<T, NS, (NS * 4 <= 32 ? 4 : 1)><<<w->nblocks, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p, bvec);
+    k_spmv<T, NS, (NS * 4 <= 32 ? 4 : 1), SEG><<<w->nblocks, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p,
+                                                                           bvec, sg);
   else if (rpw == 2 && NS * 2 <= 32)
-    k_spmv<T, NS, (NS * 2 <= 32 ? 2 : 1)><<<w->nblocks, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p, bvec);
+    k_spmv<T, NS, (NS * 2 <= 32 ? 2 : 1), SEG><<<w->nblocks, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p,
+                                                                           bvec, sg);
   else
-    k_spmv<T, NS, 1><<<w->nblocks, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p, bvec);
+    k_spmv<T, NS, 1, SEG><<<w->nblocks, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p, bvec, sg);
 }
 
 // Rows-per-warp autotuner: times each variant on this matrix (q = A p with the
 // current p) and keeps the fastest; cached per workspace and precision.
-template <class T, int NS>
+template <class T, int NS, bool SEG>
 int tune_spmv(afem_ctx* c, SolverWork* w) {
   using I = Inner<T, NS>;
   int& slot = sizeof(T) == 8 ? w->rpw64 : w->rpw32;
@@ -810,9 +939,9 @@ int tune_spmv(afem_ctx* c, SolverWork* w) {
   int pick = 1;
   for (int rpw : {1, 2, 4}) {
     if (NS * rpw > 32) break;
-    launch_spmv<T, NS>(c, w, rpw, I::KM(c, w), I::P(w), I::Q(w), nullptr, nullptr);  // warm
+    launch_spmv<T, NS, SEG>(c, w, rpw, I::KM(c, w), I::P(w), I::Q(w), nullptr, nullptr);  // warm
     AFEM_CUDA(cudaEventRecord(a, s));
-    for (int k = 0; k < 3; ++k) launch_spmv<T, NS>(c, w, rpw, I::KM(c, w), I::P(w), I::Q(w), nullptr, nullptr);
+    for (int k = 0; k < 3; ++k) launch_spmv<T, NS, SEG>(c, w, rpw, I::KM(c, w), I::P(w), I::Q(w), nullptr, nullptr);
     AFEM_CUDA(cudaEventRecord(b, s));
     AFEM_CUDA(cudaEventSynchronize(b));
     float ms = 0;
@@ -826,72 +955,78 @@ int tune_spmv(afem_ctx* c, SolverWork* w) {
 }
 
 // One COCG iteration (7 launches; the learned preconditioner adds the network's 8).
-template <class T, int NS>
+template <class T, int NS, bool SEG>
 void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, cudaEvent_t* ev) {
   using I = Inner<T, NS>;
   using V = typename I::V;
   cudaStream_t s = c->stream;
   const int n = w->n;
+  const int nsys = w->nsys;
+  const uint8_t* sg = SEG ? c->seg_of_row.p : nullptr;
   const bool learned = mode == AFEM_PRECOND_LEARNED;
   V* rp = learned ? I::RP(w) : nullptr;
   const bool mc = mode == AFEM_PRECOND_SSOR_MC;
   if (ev) AFEM_CUDA(cudaEventRecord(ev[0], s));
   if (mc)
-    launch_coop(k_fwd_mc<T, NS>, w->mc_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p, I::KM(c, w), n,
-                I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w), w->x.p, (const V*)I::DD(w),
+    launch_coop(k_fwd_mc<T, NS, SEG>, w->mc_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
+                I::KM(c, w), n, I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w), w->x.p, (const V*)I::DD(w),
                 (const uint8_t*)c->color.p, (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors,
-                w->sc.p, w->ctrl.p, w->part.p);
+                w->sc.p, w->ctrl.p, w->part.p, sg);
   else
-    launch_coop(k_fwd<T, NS>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
+    launch_coop(k_fwd<T, NS, SEG>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
                 (const int32_t*)c->diagpos.p, I::KM(c, w), n, I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w),
                 w->x.p, (const V*)I::DD(w), w->flag_f.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, rp,
-                (const int32_t*)c->perm_f.p);
+                (const int32_t*)c->perm_f.p, sg);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[1], s));
   const int swb = mc ? w->mc_blocks : sweep_blocks;
-  k_scal_r<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, swb, NS, learned ? w->rms.p : nullptr, n);
+  k_scal_r<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, swb, nsys, learned ? w->rms.p : nullptr, n);
   if (learned) mpnn_run<V>(c, NS, w->rms.p, (const V*)I::R(w), I::Z(w), &w->ctrl.p->done);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[2], s));
   if (mc)
-    launch_coop(k_bwd_mc<T, NS>, w->mc_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p, I::KM(c, w), n,
-                (const V*)I::R(w), I::Z(w), (const V*)I::DD(w), (const uint8_t*)c->color.p,
-                (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p);
+    launch_coop(k_bwd_mc<T, NS, SEG>, w->mc_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
+                I::KM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w), (const uint8_t*)c->color.p,
+                (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p,
+                sg);
   else
-    launch_coop(k_bwd<T, NS>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
+    launch_coop(k_bwd<T, NS, SEG>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
                 (const int32_t*)c->diagpos.p, I::KM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w),
                 w->flag_b.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, (const V*)rp,
-                (const int32_t*)c->perm_b.p);
+                (const int32_t*)c->perm_b.p, sg);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[3], s));
-  k_scal_rho<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, swb, NS, learned ? 1 : 0);
+  k_scal_rho<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, swb, nsys, learned ? 1 : 0);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[4], s));
-  k_pupd<T, NS><<<c->num_sms * 8, 256, 0, s>>>(n, I::Z(w), I::P(w), w->sc.p, w->ctrl.p);
+  k_pupd<T, NS, SEG><<<c->num_sms * 8, 256, 0, s>>>(n, I::Z(w), I::P(w), w->sc.p, w->ctrl.p, sg);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[5], s));
-  launch_spmv<T, NS>(c, w, sizeof(T) == 8 ? w->rpw64 : w->rpw32, I::KM(c, w), (const V*)I::P(w), I::Q(w), w->ctrl.p,
-                     (const V*)nullptr);
+  launch_spmv<T, NS, SEG>(c, w, sizeof(T) == 8 ? w->rpw64 : w->rpw32, I::KM(c, w), (const V*)I::P(w), I::Q(w),
+                          w->ctrl.p, (const V*)nullptr);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[6], s));
-  k_scal_pq<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, NS);
+  k_scal_pq<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, nsys);
 }
 
 // FP64 true residual r64 = b - A x; returns per-system ||r||^2 and ||b||^2 on the host.
-template <int NS>
+template <int NS, bool SEG>
 void true_residual(afem_ctx* c, SolverWork* w, std::vector<double>& rr, std::vector<double>& bb) {
   cudaStream_t s = c->stream;
-  k_spmv<double, NS><<<w->nblocks, 256, 0, s>>>((const int32_t*)c->rowptr.p, (const int32_t*)c->col.p, c->km.p, w->n,
-                                                w->x.p, w->r64.p, w->sc.p, (const Ctrl*)nullptr, w->part.p, w->b.p);
+  const int nsys = w->nsys;
+  k_spmv<double, NS, 1, SEG><<<w->nblocks, 256, 0, s>>>((const int32_t*)c->rowptr.p, (const int32_t*)c->col.p, c->km.p,
+                                                        w->n, w->x.p, w->r64.p, w->sc.p, (const Ctrl*)nullptr,
+                                                        w->part.p, w->b.p, SEG ? c->seg_of_row.p : nullptr);
   DBuf<double> out;
-  out.alloc(2 * NS);
-  k_true_resid<<<1, 32 * MAX_NS, 0, s>>>(w->part.p, w->nblocks, NS, out.p);
-  std::vector<double> h(2 * NS);
-  out.download(h.data(), 2 * NS, s);
+  out.alloc(2 * nsys);
+  k_true_resid<<<1, 32 * MAX_SYS, 0, s>>>(w->part.p, w->nblocks, nsys, out.p);
+  std::vector<double> h(2 * nsys);
+  out.download(h.data(), 2 * nsys, s);
   AFEM_CUDA(cudaStreamSynchronize(s));
-  rr.resize(NS);
-  bb.resize(NS);
-  for (int k = 0; k < NS; ++k) { rr[k] = h[2 * k]; bb[k] = h[2 * k + 1]; }
+  rr.resize(nsys);
+  bb.resize(nsys);
+  for (int k = 0; k < nsys; ++k) { rr[k] = h[2 * k]; bb[k] = h[2 * k + 1]; }
 }
 
-template <class T, int NS>
+template <class T, int NS, bool SEG>
 void setup_dd(afem_ctx* c, SolverWork* w, int precond, double sd) {
   using I = Inner<T, NS>;
   cudaStream_t s = c->stream;
+  const uint8_t* sg = SEG ? c->seg_of_row.p : nullptr;
   if (precond == AFEM_PRECOND_IC) {
     // fresh epoch for the set-up recurrence
     w->epoch_host += 1;
@@ -899,23 +1034,24 @@ void setup_dd(afem_ctx* c, SolverWork* w, int precond, double sd) {
     const int blocks = coresident_blocks(k_dd_ic<T, NS>, c->num_sms);
     launch_coop(k_dd_ic<T, NS>, blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
                 (const int32_t*)c->diagpos.p, I::KM(c, w), w->n, sd, (const SysScal*)w->sc.p, I::DD(w), w->flag_f.p,
-                (const Ctrl*)w->ctrl.p, c->status.p, (const int32_t*)c->perm_f.p);
+                (const Ctrl*)w->ctrl.p, c->status.p, (const int32_t*)c->perm_f.p, sg);
     w->epoch_host += 1;
     AFEM_CUDA(cudaMemcpyAsync(&w->ctrl.p->epoch, &w->epoch_host, sizeof(unsigned), cudaMemcpyHostToDevice, s));
   } else if (precond == AFEM_PRECOND_SSOR || precond == AFEM_PRECOND_DIAG || precond == AFEM_PRECOND_SSOR_MC) {
     k_dd_diag<T, NS><<<c->num_sms * 8, 256, 0, s>>>(I::KM(c, w), (const int32_t*)c->diagpos.p, w->n, sd,
-                                                    (const SysScal*)w->sc.p, I::DD(w));
+                                                    (const SysScal*)w->sc.p, I::DD(w), sg);
   }
 }
 
 // Inner COCG from x_inner = 0 on right-hand side r64 (FP64, converted to T).
 // Returns iterations; fills per-system status/resid.
-template <class T, int NS>
+template <class T, int NS, bool SEG>
 int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond, double tol, int maxit,
                int check_every, const double* d_omega, std::vector<SysScal>& hs, bool* stalled) {
   using I = Inner<T, NS>;
   cudaStream_t s = c->stream;
   const int n = w->n;
+  const int nsys = w->nsys;
   const long total = (long)n * NS;
   // r = rhs (as T), x = 0, ||b||^2
   k_copy_r<typename I::V><<<c->num_sms * 8, 256, 0, s>>>(w->r64.p, I::R(w), total);
@@ -923,13 +1059,14 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   {
     // reuse SpMV-with-b path on x = 0: part[0] = ||b||^2
     AFEM_CUDA(cudaMemsetAsync(w->x.p, 0, sizeof(double2) * total, s));
-    k_spmv<double, NS><<<w->nblocks, 256, 0, s>>>((const int32_t*)c->rowptr.p, (const int32_t*)c->col.p, c->km.p, n,
-                                                  w->x.p, w->q.p, w->sc.p, (const Ctrl*)nullptr, w->part.p, w->r64.p);
+    k_spmv<double, NS, 1, SEG><<<w->nblocks, 256, 0, s>>>((const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
+                                                          c->km.p, n, w->x.p, w->q.p, w->sc.p, (const Ctrl*)nullptr,
+                                                          w->part.p, w->r64.p, SEG ? c->seg_of_row.p : nullptr);
   }
-  k_init_sys<<<1, 32 * MAX_NS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, NS, tol, maxit, d_omega);
-  setup_dd<T, NS>(c, w, precond, o->sigma_diag > 0 ? o->sigma_diag : 1.0);
+  k_init_sys<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, nsys, tol, maxit, d_omega);
+  setup_dd<T, NS, SEG>(c, w, precond, o->sigma_diag > 0 ? o->sigma_diag : 1.0);
   const int mode = precond;
-  tune_spmv<T, NS>(c, w);
+  tune_spmv<T, NS, SEG>(c, w);
   const bool learned = mode == AFEM_PRECOND_LEARNED;
   if (learned) {
     using V = typename I::V;
@@ -939,12 +1076,12 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   }
   if (stalled) *stalled = false;
   double watch = 1e300, win_min = 1e300;  // stagnation windows (see below)
-  const int sweep_blocks = coresident_blocks(k_fwd<T, NS>, c->num_sms);
-  const int sb2 = coresident_blocks(k_bwd<T, NS>, c->num_sms);
+  const int sweep_blocks = coresident_blocks(k_fwd<T, NS, SEG>, c->num_sms);
+  const int sb2 = coresident_blocks(k_bwd<T, NS, SEG>, c->num_sms);
   const int sblocks = std::min(std::min(sweep_blocks, sb2), w->nblocks);
   if (mode == AFEM_PRECOND_SSOR_MC)
-    w->mc_blocks = std::min(std::min(coresident_blocks(k_fwd_mc<T, NS>, c->num_sms),
-                                     coresident_blocks(k_bwd_mc<T, NS>, c->num_sms)), w->nblocks);
+    w->mc_blocks = std::min(std::min(coresident_blocks(k_fwd_mc<T, NS, SEG>, c->num_sms),
+                                     coresident_blocks(k_bwd_mc<T, NS, SEG>, c->num_sms)), w->nblocks);
   // every solve starts a fresh flag generation: a solve that stopped inside a
   // chunk left its last forward-sweep flags at the epoch it ended on
   w->epoch_host += 1;
@@ -967,7 +1104,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
     if (e == cudaSuccess) {
       bool ok = true;
       try {
-        for (int k = 0; k < chunk; ++k) enqueue_iteration<T, NS>(c, w, mode, sblocks, ev_of(k));
+        for (int k = 0; k < chunk; ++k) enqueue_iteration<T, NS, SEG>(c, w, mode, sblocks, ev_of(k));
       } catch (const Error&) {
         ok = false;
       }
@@ -989,7 +1126,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
     if (use_graph) {
       AFEM_CUDA(cudaGraphLaunch(gexec, s));
     } else {
-      for (int k = 0; k < chunk; ++k) enqueue_iteration<T, NS>(c, w, mode, sblocks, ev_of(k));
+      for (int k = 0; k < chunk; ++k) enqueue_iteration<T, NS, SEG>(c, w, mode, sblocks, ev_of(k));
     }
     AFEM_CUDA(cudaMemcpyAsync(w->h_ctrl, w->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
     AFEM_CUDA(cudaStreamSynchronize(s));
@@ -999,10 +1136,12 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
       const int executed = std::min(chunk, w->h_ctrl->iter - iter_before);
       const char* tag = sizeof(T) == 8 ? "fp64" : "fp32";
       char nf[48], nb[48], np_[48], ns_[48];
-      snprintf(nf, sizeof nf, "cocg_fwd_sweep_%s_ns%d", tag, NS);
-      snprintf(nb, sizeof nb, "cocg_bwd_sweep_%s_ns%d", tag, NS);
-      snprintf(np_, sizeof np_, "cocg_p_update_%s_ns%d", tag, NS);
-      snprintf(ns_, sizeof ns_, "cocg_spmv_%s_ns%d", tag, NS);
+      const char* kind = SEG ? "seg" : "ns";
+      const int cnt = SEG ? nsys : NS;
+      snprintf(nf, sizeof nf, "cocg_fwd_sweep_%s_%s%d", tag, kind, cnt);
+      snprintf(nb, sizeof nb, "cocg_bwd_sweep_%s_%s%d", tag, kind, cnt);
+      snprintf(np_, sizeof np_, "cocg_p_update_%s_%s%d", tag, kind, cnt);
+      snprintf(ns_, sizeof ns_, "cocg_spmv_%s_%s%d", tag, kind, cnt);
       for (int k = 0; k < executed; ++k) {
         float a = 0, b = 0, d = 0, e = 0;
         cudaEvent_t* E = &evs[7L * k];
@@ -1028,10 +1167,10 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
     // and a restart from the true residual resumes the descent
     const int win = learned ? 4 : (sizeof(T) == 4 ? 16 : 64);
     if (!w->no_window) {
-      AFEM_CUDA(cudaMemcpyAsync(w->h_sc, w->sc.p, sizeof(SysScal) * NS, cudaMemcpyDeviceToHost, s));
+      AFEM_CUDA(cudaMemcpyAsync(w->h_sc, w->sc.p, sizeof(SysScal) * nsys, cudaMemcpyDeviceToHost, s));
       AFEM_CUDA(cudaStreamSynchronize(s));
       double worst = 0.0;
-      for (int k = 0; k < NS; ++k)
+      for (int k = 0; k < nsys; ++k)
         if (w->h_sc[k].active) worst = std::max(worst, w->h_sc[k].resid);
       win_min = std::min(win_min, worst);
       if ((w->h_ctrl->iter / chunk) % win == 0) {
@@ -1050,44 +1189,47 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   if (gexec) cudaGraphExecDestroy(gexec);
   for (auto& e : evs) cudaEventDestroy(e);
   w->epoch_host = w->h_ctrl->epoch;
-  hs.resize(NS);
-  AFEM_CUDA(cudaMemcpyAsync(w->h_sc, w->sc.p, sizeof(SysScal) * NS, cudaMemcpyDeviceToHost, s));
+  hs.resize(nsys);
+  AFEM_CUDA(cudaMemcpyAsync(w->h_sc, w->sc.p, sizeof(SysScal) * nsys, cudaMemcpyDeviceToHost, s));
   AFEM_CUDA(cudaStreamSynchronize(s));
-  for (int k = 0; k < NS; ++k) hs[k] = w->h_sc[k];
+  for (int k = 0; k < nsys; ++k) hs[k] = w->h_sc[k];
   iters_done = 0;
-  for (int k = 0; k < NS; ++k) iters_done = std::max(iters_done, hs[k].iter);
+  for (int k = 0; k < nsys; ++k) iters_done = std::max(iters_done, hs[k].iter);
   return iters_done;
 }
 
-template <int NS>
+template <int NS, bool SEG>
 int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_opts* o, afem_solve_stats* st,
              const SolveExtra* ex) {
   SolverWork* w = c->work;
   cudaStream_t s = c->stream;
   const int n = c->nline;
   const long total = (long)n * NS;
+  const int nsys = SEG ? c->nseg : NS;
   const bool mixed = o->precision == AFEM_MIXED;
   // ---- workspace
   if (!w) {
     w = new SolverWork();
     c->work = w;
   }
-  if (w->n != n || w->ns != NS) {
+  if (w->n != n || w->ns != NS || w->seg != SEG) {
     w->n = n;
     w->ns = NS;
+    w->seg = SEG;
     w->x.alloc(total); w->b.alloc(total); w->r64.alloc(total);
     w->r.alloc(total); w->z.alloc(total); w->p.alloc(total); w->q.alloc(total); w->dd.alloc(total);
     w->rf.release(); w->zf.release(); w->pf.release(); w->qf.release(); w->ddf.release();
     w->flag_f.alloc(n); w->flag_b.alloc(n);
     w->rpw64 = w->rpw32 = 0;
     w->flag_f.zero(s); w->flag_b.zero(s);
-    w->sc.alloc(MAX_NS);
+    w->sc.alloc(MAX_SYS);
     w->ctrl.alloc(1);
     w->ctrl.zero(s);
     w->epoch_host = 1;
     if (!w->h_ctrl) AFEM_CUDA(cudaMallocHost(&w->h_ctrl, sizeof(Ctrl)));
-    if (!w->h_sc) AFEM_CUDA(cudaMallocHost(&w->h_sc, sizeof(SysScal) * MAX_NS));
+    if (!w->h_sc) AFEM_CUDA(cudaMallocHost(&w->h_sc, sizeof(SysScal) * MAX_SYS));
   }
+  w->nsys = nsys;
   if (mixed && w->rf.n != (size_t)total) {
     w->rf.alloc(total); w->zf.alloc(total); w->pf.alloc(total); w->qf.alloc(total); w->ddf.alloc(total);
   }
@@ -1098,23 +1240,23 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
   }
   {
     int b1 = 0;
-    AFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_spmv<double, NS>, 256, 0));
+    AFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_spmv<double, NS, 1, SEG>, 256, 0));
     w->nblocks = std::max(1, b1) * c->num_sms;
-    w->nblocks = std::max(w->nblocks, coresident_blocks(k_fwd_mc<double, NS>, c->num_sms));
-    int bf = coresident_blocks(k_fwd<double, NS>, c->num_sms);
-    int bb = coresident_blocks(k_bwd<double, NS>, c->num_sms);
+    w->nblocks = std::max(w->nblocks, coresident_blocks(k_fwd_mc<double, NS, SEG>, c->num_sms));
+    int bf = coresident_blocks(k_fwd<double, NS, SEG>, c->num_sms);
+    int bb = coresident_blocks(k_bwd<double, NS, SEG>, c->num_sms);
     w->nblocks = std::max(w->nblocks, std::max(bf, bb));
     if (mixed) {
-      w->nblocks = std::max(w->nblocks, coresident_blocks(k_fwd<float, NS>, c->num_sms));
-      w->nblocks = std::max(w->nblocks, coresident_blocks(k_bwd<float, NS>, c->num_sms));
+      w->nblocks = std::max(w->nblocks, coresident_blocks(k_fwd<float, NS, SEG>, c->num_sms));
+      w->nblocks = std::max(w->nblocks, coresident_blocks(k_bwd<float, NS, SEG>, c->num_sms));
     }
-    w->part.alloc((size_t)w->nblocks * MAX_NS * 4);
+    w->part.alloc((size_t)w->nblocks * MAX_SYS * 4);
   }
   // ---- right-hand sides and omegas
   {
     DBuf<int> dsrc;
-    std::vector<int> hsrc(NS);
-    for (int k = 0; k < NS; ++k) {
+    std::vector<int> hsrc(nsys);
+    for (int k = 0; k < nsys; ++k) {
       hsrc[k] = srcs ? srcs[k] : 0;
       AFEM_REQUIRE((ex && ex->rhs) || (hsrc[k] >= 0 && hsrc[k] < c->rhs_nsrc), AFEM_EINVAL,
                    "solve: source index out of range");
@@ -1122,21 +1264,21 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     if (ex && ex->rhs) {
       w->b.upload(reinterpret_cast<const double2*>(ex->rhs), total, s);
     } else {
-      dsrc.upload(hsrc.data(), NS, s);
-      k_gather_rhs<<<c->num_sms * 8, 256, 0, s>>>(c->rhs.p, n, NS, dsrc.p, w->b.p);
+      dsrc.upload(hsrc.data(), nsys, s);
+      k_gather_rhs<<<c->num_sms * 8, 256, 0, s>>>(c->rhs.p, n, NS, dsrc.p, w->b.p, SEG ? c->seg_of_row.p : nullptr);
     }
     AFEM_CUDA(cudaStreamSynchronize(s));
   }
-  std::vector<double> om(NS);
+  std::vector<double> om(nsys);
   const double pi = 4.0 * std::atan(1.0);
-  for (int k = 0; k < NS; ++k) om[k] = 2.0 * pi * freq[k];
+  for (int k = 0; k < nsys; ++k) om[k] = 2.0 * pi * freq[k];
   DBuf<double> d_om;
-  d_om.upload(om.data(), NS, s);
+  d_om.upload(om.data(), nsys, s);
   // SysScal.omega must be valid for the residual SpMV before k_init_sys runs
   {
-    std::vector<SysScal> tmp(MAX_NS);
-    for (int k = 0; k < NS; ++k) { memset(&tmp[k], 0, sizeof(SysScal)); tmp[k].omega = om[k]; }
-    AFEM_CUDA(cudaMemcpyAsync(w->sc.p, tmp.data(), sizeof(SysScal) * NS, cudaMemcpyHostToDevice, s));
+    std::vector<SysScal> tmp(MAX_SYS);
+    for (int k = 0; k < nsys; ++k) { memset(&tmp[k], 0, sizeof(SysScal)); tmp[k].omega = om[k]; }
+    AFEM_CUDA(cudaMemcpyAsync(w->sc.p, tmp.data(), sizeof(SysScal) * nsys, cudaMemcpyHostToDevice, s));
     AFEM_CUDA(cudaStreamSynchronize(s));
   }
   cudaEvent_t e0, e1;
@@ -1151,9 +1293,9 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
   if (ex && ex->x0) {
     xacc.upload(reinterpret_cast<const double2*>(ex->x0), total, s);
     AFEM_CUDA(cudaMemcpyAsync(w->x.p, xacc.p, sizeof(double2) * total, cudaMemcpyDeviceToDevice, s));
-    true_residual<NS>(c, w, rr, bb);  // r64 = b - A x0
+    true_residual<NS, SEG>(c, w, rr, bb);  // r64 = b - A x0
     double worst_r = 0.0;
-    for (int k = 0; k < NS; ++k)
+    for (int k = 0; k < nsys; ++k)
       if (bb[k] > 0) worst_r = std::max(worst_r, std::sqrt(rr[k] / bb[k]));
     if (worst_r > 0) tol_scale = 1.0 / worst_r;
   } else {
@@ -1167,7 +1309,7 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
   const int maxit = o->maxit > 0 ? o->maxit : 100000;
   int it_total = 0, refinements = 0;
   std::vector<SysScal> hs;
-  std::vector<int> status(NS, AFEM_EMAXITER);
+  std::vector<int> status(nsys, AFEM_EMAXITER);
   double worst = 0.0, rec = 0.0;
   double prev = 1.0;  // current ||b - A x|| / ||b|| (worst system)
   int precond_now = o->precond;
@@ -1186,10 +1328,12 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     if (left <= 0) break;
     int its;
     bool stalled = false;
-    if (mixed) its = inner_cocg<float, NS>(c, w, o, precond_now, inner_tol, left, o->check_every, d_om.p, hs, &stalled);
-    else its = inner_cocg<double, NS>(c, w, o, precond_now, inner_tol, left, o->check_every, d_om.p, hs, &stalled);
+    if (mixed)
+      its = inner_cocg<float, NS, SEG>(c, w, o, precond_now, inner_tol, left, o->check_every, d_om.p, hs, &stalled);
+    else
+      its = inner_cocg<double, NS, SEG>(c, w, o, precond_now, inner_tol, left, o->check_every, d_om.p, hs, &stalled);
     if (precond_now != AFEM_PRECOND_LEARNED && stalled) {
-      for (int k = 0; k < NS; ++k)
+      for (int k = 0; k < nsys; ++k)
         if (hs[k].active) hs[k].status = AFEM_ESTAGNATION;
     }
     if (precond_now == AFEM_PRECOND_LEARNED) {
@@ -1204,11 +1348,11 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     refinements += 1;
     k_add_x<<<c->num_sms * 8, 256, 0, s>>>(xacc.p, w->x.p, total);
     AFEM_CUDA(cudaMemcpyAsync(w->x.p, xacc.p, sizeof(double2) * total, cudaMemcpyDeviceToDevice, s));
-    true_residual<NS>(c, w, rr, bb);  // r64 = b - A x_acc
+    true_residual<NS, SEG>(c, w, rr, bb);  // r64 = b - A x_acc
     worst = 0.0;
     rec = 0.0;
     bool all_ok = true, any_fatal = false;
-    for (int k = 0; k < NS; ++k) {
+    for (int k = 0; k < nsys; ++k) {
       const double rel = bb[k] > 0 ? std::sqrt(rr[k] / bb[k]) : 0.0;
       worst = std::max(worst, rel);
       rec = std::max(rec, hs[k].resid);
@@ -1218,14 +1362,14 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     }
     if (recursive_only) {
       // COCG13_single semantics: one Krylov run judged on its recursive residual
-      for (int k = 0; k < NS; ++k) status[k] = hs[k].status;
+      for (int k = 0; k < nsys; ++k) status[k] = hs[k].status;
       rec = 0.0;
-      for (int k = 0; k < NS; ++k) rec = std::max(rec, hs[k].resid / tol_scale);
+      for (int k = 0; k < nsys; ++k) rec = std::max(rec, hs[k].resid / tol_scale);
       break;
     }
     if (all_ok || any_fatal || !std::isfinite(worst)) break;
     if (worst > 0.9 * prev && outer > 0 && !fell_back) {  // no progress from a restart
-      for (int k = 0; k < NS; ++k)
+      for (int k = 0; k < nsys; ++k)
         if (status[k] == AFEM_OK || status[k] == AFEM_EMAXITER) status[k] = status[k] == AFEM_OK ? AFEM_OK : AFEM_ESTAGNATION;
       break;
     }
@@ -1242,10 +1386,11 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
   c->X.alloc(total);
   AFEM_CUDA(cudaMemcpyAsync(c->X.p, xacc.p, sizeof(double2) * total, cudaMemcpyDeviceToDevice, s));
   AFEM_CUDA(cudaStreamSynchronize(s));
-  c->nsys = NS;
-  c->sol_freq.assign(freq, freq + NS);
+  c->nsys = nsys;
+  c->sol_packed = SEG;
+  c->sol_freq.assign(freq, freq + nsys);
   int stat = AFEM_OK;
-  for (int k = 0; k < NS; ++k)
+  for (int k = 0; k < nsys; ++k)
     if (status[k] != AFEM_OK) { stat = status[k]; break; }
   c->last_learned_its = learned_its;
   if (st) {
@@ -1265,12 +1410,19 @@ int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, cons
                  afem_solve_stats* st, const SolveExtra* ex) {
   AFEM_REQUIRE(c->assembled, AFEM_ESTATE, "solve: system not assembled");
   build_schedule(c);
+  if (c->nseg > 0) {
+    AFEM_REQUIRE(nsys == c->nseg, AFEM_EINVAL, "solve: a packed batch solves one system per mesh (nsys = nseg)");
+    AFEM_REQUIRE(o->precond != AFEM_PRECOND_LEARNED, AFEM_EINVAL,
+                 "solve: the learned preconditioner does not run on packed batches");
+    AFEM_REQUIRE(!ex || (!ex->x0 && !ex->rhs), AFEM_EINVAL, "solve: packed batches take the assembled sources");
+    return solve_ns<1, true>(c, freq, src, o, st, ex);
+  }
   switch (nsys) {
-    case 1: return solve_ns<1>(c, freq, src, o, st, ex);
-    case 2: return solve_ns<2>(c, freq, src, o, st, ex);
-    case 4: return solve_ns<4>(c, freq, src, o, st, ex);
-    case 8: return solve_ns<8>(c, freq, src, o, st, ex);
-    case 16: return solve_ns<16>(c, freq, src, o, st, ex);
+    case 1: return solve_ns<1, false>(c, freq, src, o, st, ex);
+    case 2: return solve_ns<2, false>(c, freq, src, o, st, ex);
+    case 4: return solve_ns<4, false>(c, freq, src, o, st, ex);
+    case 8: return solve_ns<8, false>(c, freq, src, o, st, ex);
+    case 16: return solve_ns<16, false>(c, freq, src, o, st, ex);
     default: throw Error{AFEM_EINVAL, "solve: nsys must be 1, 2, 4, 8 or 16"};
   }
 }
@@ -1278,6 +1430,12 @@ int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, cons
 void get_residual(afem_ctx* c, int k, double* r) {
   SolverWork* w = c->work;
   AFEM_REQUIRE(w && c->nsys > 0 && k >= 0 && k < c->nsys, AFEM_ESTATE, "get_residual: no such system");
+  if (w->seg) {  // packed batch: the rows of mesh k
+    const int r0 = c->seg_row_ptr[k], r1 = c->seg_row_ptr[k + 1];
+    AFEM_CUDA(cudaMemcpyAsync(r, w->r64.p + r0, sizeof(double2) * (r1 - r0), cudaMemcpyDeviceToHost, c->stream));
+    AFEM_CUDA(cudaStreamSynchronize(c->stream));
+    return;
+  }
   std::vector<double2> all((size_t)w->n * w->ns);
   w->r64.download(all.data(), all.size(), c->stream);
   AFEM_CUDA(cudaStreamSynchronize(c->stream));

@@ -46,6 +46,7 @@ class Forward:
         if not self.ctx:
             raise AfemError(-7, f"afem_create({device}) failed: no usable CUDA device")
         self.node = self.ntet = self.nline = 0
+        self.row_ptr = None
 
     def close(self):
         if self.ctx:
@@ -82,6 +83,37 @@ class Forward:
         n = C.c_int(0)
         self._check(self._L.afem_get_lines(self.ctx, C.byref(n), None, None))
         self.nline = n.value
+        self.row_ptr = None
+
+    def set_segments(self, node_ptr):
+        """Declare the mesh as a packed batch of independent meshes (0-based node-range prefix)."""
+        self.row_ptr = None
+        if node_ptr is None or len(node_ptr) <= 1:
+            self._check(self._L.afem_set_segments(self.ctx, 0, None))
+            return
+        npt = _c(node_ptr, np.int32)
+        self._check(self._L.afem_set_segments(self.ctx, len(npt) - 1, ptr(npt)))
+        self.row_ptr, self.tet_ptr = self.segment_info()
+
+    def segment_info(self):
+        """(row_ptr, tet_ptr) of the declared meshes."""
+        k = C.c_int(0)
+        self._check(self._L.afem_segment_info(self.ctx, C.byref(k), None, None))
+        rp = np.zeros(k.value + 1, np.int32); tp = np.zeros(k.value + 1, np.int32)
+        self._check(self._L.afem_segment_info(self.ctx, C.byref(k), ptr(rp), ptr(tp)))
+        return rp, tp
+
+    def load_packed(self, pk):
+        """Load a synth.PackedModels batch: union mesh, mesh declaration, conductivity, source, bounds."""
+        self.set_mesh(pk.xyz, pk.n4, pk.tag)
+        self.set_segments(pk.node_ptr)
+        self.set_sigma(pk.sigma_tet)
+        self.set_source(pk.F, pk.v, 0)
+        b = pk.bounds
+        self.set_bounds(b["zmin"], b["zmax"], b["xout"], b["yout"])
+
+    def _rows(self, k):
+        return self.nline if self.row_ptr is None else int(self.row_ptr[k + 1] - self.row_ptr[k])
 
     def lines(self):
         line = np.zeros((self.nline, 2), np.int32); n6 = np.zeros((self.ntet, 6), np.int32)
@@ -174,6 +206,7 @@ class Forward:
                                                ptr(AU), ptr(INU), ptr(IAU), ptr(B), ptr(X), precond.encode(),
                                                sigma_diag, sigma, C.byref(R), C.byref(IT), C.byref(ER), nset))
         self.nline = n
+        self.row_ptr = None
         return dict(x=X, resid=R.value, iter=IT.value, error=ER.value)
 
     def solve_rhs(self, freqs, rhs, precond="SSOR", precision="fp64", tol=1e-8, maxit=100000) -> SolveResult:
@@ -211,7 +244,7 @@ class Forward:
 
     def residual(self, k: int = 0):
         """FP64 b - A x of system k after the last solve."""
-        r = np.zeros(self.nline, np.complex128)
+        r = np.zeros(self._rows(k), np.complex128)
         self._check(self._L.afem_get_residual(self.ctx, k, ptr(r)))
         return r
 
@@ -247,7 +280,7 @@ class Forward:
         return hist
 
     def solution(self, k: int = 0):
-        x = np.zeros(self.nline, np.complex128)
+        x = np.zeros(self._rows(k), np.complex128)
         self._check(self._L.afem_get_solution(self.ctx, k, ptr(x)))
         return x
 
@@ -290,6 +323,7 @@ class Forward:
         n = C.c_int(0)
         self._check(self._L.afem_get_lines(self.ctx, C.byref(n), None, None))
         self.nline = n.value
+        self.row_ptr = None
 
     def ctl_info(self):
         nf = C.c_int(0); no = C.c_int(0)

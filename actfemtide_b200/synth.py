@@ -130,7 +130,7 @@ def gaussian_random_field(shape, spacing, corr_km: float, rng) -> np.ndarray:
     ks.append(np.fft.rfftfreq(shape[-1], d=spacing[-1]) * 2 * np.pi)
     K2 = sum(np.meshgrid(*[k ** 2 for k in ks], indexing="ij"))
     F *= np.exp(-K2 * corr_km ** 2 / 4.0)
-    f = np.fft.irfftn(F, s=shape)
+    f = np.fft.irfftn(F, s=shape, axes=tuple(range(len(shape))))
     f -= f.mean()
     f /= f.std()
     return f
@@ -244,6 +244,75 @@ def tiny_model(nx=2, ny=2, nz=4, seed: int = 0) -> TidalModel:
     """A few hexes over [-10,10]^3 km (5 km cells, so the sea layer holds whole cells)."""
     return tidal_box(nx, ny, nz, seed=seed, block=False, site_grid=(-5.0, 5.0), half_km=10.0,
                      name=f"box{nx}x{ny}x{nz}")
+
+
+# ----------------------------------------------------------------------------- packed batches
+@dataclasses.dataclass
+class PackedModels:
+    """Independent meshes packed into one union mesh (one system per mesh in one solve).
+
+    Mesh k owns nodes ``node_ptr[k] .. node_ptr[k+1]-1`` (0-based) and its
+    tetrahedra follow mesh k-1's; node ids, tetrahedra, tags and
+    conductivities are the parts' own, offset.  The source arrays cover every
+    union node (zero outside each part's ocean nodes), which gives each part
+    exactly its own right-hand side.
+    """
+
+    parts: list
+    xyz: np.ndarray
+    n4: np.ndarray
+    tag: np.ndarray
+    sigma_tet: np.ndarray
+    F: np.ndarray
+    v: np.ndarray
+    node_ptr: np.ndarray
+    tet_ptr: np.ndarray
+    bounds: dict
+
+    @property
+    def nseg(self) -> int:
+        return len(self.parts)
+
+
+def uneven_models(count: int = 24, seed: int = 0, nmin: int = 8, nmax: int = 32) -> list:
+    """``count`` meshes of n x n x round(3n/4) cells over [-50,50]^3 km, n uniform in [nmin, nmax].
+
+    Each mesh has its own seeded log-normal subsurface (``grf``), conductive
+    block and velocity pattern; all share the M2 frequency and the 5x5 site grid.
+    """
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(nmin, nmax + 1, size=count)
+    out = []
+    for k, n in enumerate(ns):
+        n = int(n)
+        out.append(tidal_box(n, n, max(2, int(round(0.75 * n))), seed=seed * 1000 + k, field_seed=seed * 1000 + k + 1,
+                             grf=True, name=f"uneven{k}_n{n}"))
+    return out
+
+
+def pack(models) -> PackedModels:
+    """Union of independent meshes with the same Dirichlet bounds (see :class:`PackedModels`)."""
+    b0 = models[0].bounds
+    for m in models:
+        if m.bounds != b0:
+            raise ValueError("packed meshes must share the Dirichlet bounds")
+    node_ptr = np.zeros(len(models) + 1, np.int32)
+    tet_ptr = np.zeros(len(models) + 1, np.int32)
+    for k, m in enumerate(models):
+        node_ptr[k + 1] = node_ptr[k] + m.node
+        tet_ptr[k + 1] = tet_ptr[k] + m.ntet
+    total = int(node_ptr[-1])
+    F = np.zeros((total, 3)); v = np.zeros((total, 3), np.complex128)
+    for k, m in enumerate(models):
+        F[node_ptr[k]:node_ptr[k] + m.nodes] = m.F
+        v[node_ptr[k]:node_ptr[k] + m.nodes] = m.v
+    return PackedModels(
+        parts=list(models),
+        xyz=np.ascontiguousarray(np.concatenate([m.xyz for m in models])),
+        n4=np.ascontiguousarray(np.concatenate([m.n4 + node_ptr[k] for k, m in enumerate(models)]).astype(np.int32)),
+        tag=np.ascontiguousarray(np.concatenate([m.tag for m in models]).astype(np.int32)),
+        sigma_tet=np.ascontiguousarray(np.concatenate([m.sigma_per_tet() for m in models])),
+        F=F, v=v, node_ptr=node_ptr, tet_ptr=tet_ptr, bounds=dict(b0))
 
 
 # ----------------------------------------------------------------------------- reference file formats

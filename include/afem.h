@@ -100,6 +100,23 @@ int afem_set_mesh(afem_ctx *ctx, int node, const double *xyz, int ntet, const in
 /* Number of edges and the numbering in use (line: 2*nline, n6line: 6*ntet; either may be NULL). */
 int afem_get_lines(afem_ctx *ctx, int *nline, int32_t *line, int32_t *n6line);
 
+/* Packed batch of independent meshes (no counterpart in the reference, which
+ * runs one mesh per process).  After afem_set_mesh of the union of nseg
+ * meshes, with mesh k owning the 1-based node ids node_ptr[k]+1 ..
+ * node_ptr[k+1] (node_ptr[0] = 0, node_ptr[nseg] = node) and the
+ * tetrahedra grouped mesh by mesh, this declares the meshes.  The edge
+ * numbering of the union then runs mesh by mesh as well.  A later
+ * afem_solve takes nsys = nseg: system k is mesh k at freq_hz[k] with
+ * source src[k], with its own COCG scalars and convergence test, all meshes
+ * in one launch sequence.  afem_get_solution / afem_get_residual return
+ * the rows of mesh k only, and afem_sites searches system k's sites in
+ * mesh k's tetrahedra.  nseg <= 32; nseg = 0 removes the declaration
+ * (so does afem_set_mesh). */
+int afem_set_segments(afem_ctx *ctx, int nseg, const int32_t *node_ptr);
+/* The declared meshes: *nseg, and the row (edge) and tetrahedron ranges, 0-based prefixes
+ * row_ptr[nseg+1], tet_ptr[nseg+1] (either may be NULL). */
+int afem_segment_info(afem_ctx *ctx, int *nseg, int32_t *row_ptr, int32_t *tet_ptr);
+
 /* Replaces param_cond + SETNPHYS1INDEX2COND + READCOND (m_param.f90:449-485,
  * n_ebfem_bxyz_mpi.f90:470-527) and GENMAT's selection (forward_bxyz_mpi.f90:196-208):
  * tag 1 -> sigma_air, tag 2 -> sigma_ocean (the reference hard-codes 3.33),
@@ -168,7 +185,7 @@ int afem_solve_rhs(afem_ctx *ctx, int nsys, const double *freq_hz, const double 
 int afem_jacobian(afem_ctx *ctx, double freq_hz, const double *x_complex, int nadj, double *J_complex);
 /* FP64 true residual b - A x of system k after the last afem_solve (n complex values). */
 int afem_get_residual(afem_ctx *ctx, int k, double *r_complex);
-/* Solution of system k (n complex values, [nT*km] like bs in forward_bxyz). */
+/* Solution of system k (n complex values, [nT*km] like bs in forward_bxyz; a packed batch: the rows of mesh k). */
 int afem_get_solution(afem_ctx *ctx, int k, double *x_complex);
 
 /* ---- sites ---------------------------------------------------------------- */
