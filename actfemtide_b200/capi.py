@@ -32,7 +32,7 @@ EXPORTS = (
     "afem_profile_entry", "afem_cocg13_single", "afem_set_system", "afem_get_residual", "afem_mpnn_nparam",
     "afem_mpnn_set_params", "afem_mpnn_get_params", "afem_mpnn_forward", "afem_mpnn_loss_grad", "afem_mpnn_train",
     "afem_solve_rhs", "afem_jacobian", "afem_sweep_schedule", "afem_coloring", "afem_set_segments",
-    "afem_segment_info",
+    "afem_segment_info", "afem_launch_count",
 )
 
 
@@ -76,6 +76,8 @@ def lib():
     L.afem_stream.argtypes = [_vp]
     L.afem_set_mesh.argtypes = [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp, _vp]
     L.afem_get_lines.argtypes = [_vp, C.POINTER(C.c_int), _vp, _vp]
+    L.afem_launch_count.argtypes = []
+    L.afem_launch_count.restype = C.c_long
     L.afem_set_segments.argtypes = [_vp, C.c_int, _vp]
     L.afem_segment_info.argtypes = [_vp, C.POINTER(C.c_int), _vp, _vp]
     L.afem_set_cond.argtypes = [_vp, C.c_double, C.c_double, C.c_int, C.c_int, _vp, C.c_int, _vp]
@@ -122,6 +124,11 @@ def lib():
         getattr(L, name).restype = C.c_int
     _LIB = L
     return L
+
+
+def launch_count() -> int:
+    """Kernels the library has launched in this process."""
+    return int(lib().afem_launch_count())
 
 
 def ptr(a):

@@ -112,6 +112,7 @@ void jacobian_device(afem_ctx* c, double freq, const double* x_host, int nadj, d
   const double omega = 2.0 * (4.0 * atan(1.0)) * freq;
   k_jacobian<<<(c->ntet + 127) / 128, 128, 0, s>>>(c->xyz.p, c->n4.p, c->n6line.p, c->sigma.p, c->bc.p, c->ntet, omega,
                                                   x.p, c->X.p, nadj, J.p, c->status.p);
+  count_launch();
   check_status(c, "jacobian");
   J.download(reinterpret_cast<double2*>(J_host), (size_t)nadj * c->ntet, s);
   AFEM_CUDA(cudaStreamSynchronize(s));

@@ -222,6 +222,7 @@ void assemble_device(afem_ctx* c) {
   c->bc.alloc(c->nline);
   k_bc_flags<<<(c->nline + 255) / 256, 256, 0, s>>>(c->line.p, c->xyz.p, c->nline, c->zmin, c->zmax, c->xout, c->yout,
                                                   c->bc.p);
+  count_launch();
   SrcArgs sa{};
   sa.nsrc = (int)c->src.size();
   for (int i = 0; i < sa.nsrc; ++i) {
@@ -242,6 +243,7 @@ void assemble_device(afem_ctx* c) {
   k_assemble_rows<<<(c->nline + 127) / 128, 128, 0, s>>>(c->xyz.p, c->n4.p, c->tag.p, c->n6line.p, c->sigma.p,
                                                          c->etp.p, c->etl.p, c->rowptr.p, c->col.p, c->bc.p, c->nline,
                                                          sa, c->km.p, c->rhs.p, c->status.p);
+  count_launch();
   if (c->prof.on) {
     AFEM_CUDA(cudaEventRecord(e1, s));
     AFEM_CUDA(cudaEventSynchronize(e1));

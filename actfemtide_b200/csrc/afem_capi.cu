@@ -33,6 +33,9 @@ void check_status(afem_ctx* c, const char* what) {
   throw Error{code, buf};
 }
 
+std::atomic<long> g_launches{0};
+thread_local int g_capturing = 0;
+
 }  // namespace afem
 
 using afem::Error;
@@ -157,6 +160,8 @@ void afem_destroy(afem_ctx* c) {
 }
 
 const char* afem_last_error(const afem_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+long afem_launch_count(void) { return afem::g_launches.load(); }
 
 void* afem_stream(afem_ctx* c) { return c ? (void*)c->stream : nullptr; }
 

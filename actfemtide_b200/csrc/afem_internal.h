@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -111,6 +112,15 @@ struct Profile {
     e.push_back(ProfEntry{name, ms, n});
   }
 };
+
+// Kernel launches of this library in this process (measurement).  Launches
+// enqueued while a stream is captured into a CUDA graph are not counted
+// there; each launch of the graph counts its kernel nodes instead.
+extern std::atomic<long> g_launches;
+extern thread_local int g_capturing;
+inline void count_launch(long n = 1) {
+  if (!g_capturing) g_launches.fetch_add(n, std::memory_order_relaxed);
+}
 
 struct SolverWork;  // afem_solver.cu
 struct MpnnState;   // afem_mpnn.cu

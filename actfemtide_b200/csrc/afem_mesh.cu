@@ -245,8 +245,11 @@ void exclusive_scan(const int32_t* in, int32_t* out, int n, cudaStream_t s, long
   sums.alloc(nb + 1);
   if (n > 0) {
     k_scan_block<<<nb, SCAN_T, 0, s>>>(in, out, n, sums.p);
+    count_launch();
     k_scan_sums<<<1, 1, 0, s>>>(sums.p, nb, sums.p + nb);
+    count_launch();
     k_scan_add<<<nblk(n, 256), 256, 0, s>>>(out, n, sums.p);
+    count_launch();
   } else {
     AFEM_CUDA(cudaMemsetAsync(sums.p, 0, sizeof(int64_t), s));
   }
@@ -268,15 +271,19 @@ void build_lines_device(afem_ctx* c) {
   cnt.zero(s);
   nptr.alloc(node + 1);
   k_count_node_tets<<<nblk(4L * ntet, 256), 256, 0, s>>>(c->n4.p, ntet, cnt.p);
+  count_launch();
   exclusive_scan(cnt.p, nptr.p, node, s, nullptr);
   cursor.alloc(node);
   cursor.zero(s);
   nlist.alloc(4L * ntet);
   k_fill_node_tets<<<nblk(4L * ntet, 256), 256, 0, s>>>(c->n4.p, ntet, nptr.p, cursor.p, nlist.p);
+  count_launch();
   k_sort_segments<<<nblk(node, 128), 128, 0, s>>>(nptr.p, node, nlist.p, NODE_DEG_MAX, c->status.p);
+  count_launch();
   check_status(c, "edge numbering: node adjacency (more than 100 tetrahedra share a node)");
   k_mkline_group<<<nblk(node, 128), 128, 0, s>>>(c->n4.p, nptr.p, nlist.p, node, cnt.p, nullptr, nullptr,
                                                  c->status.p);
+  count_launch();
   DBuf<int32_t> stack;
   stack.alloc(node + 1);
   long nline = 0;
@@ -286,8 +293,10 @@ void build_lines_device(afem_ctx* c) {
   c->line.alloc(2L * nline);
   k_mkline_group<<<nblk(node, 128), 128, 0, s>>>(c->n4.p, nptr.p, nlist.p, node, nullptr, stack.p, c->line.p,
                                                  c->status.p);
+  count_launch();
   c->n6line.alloc(6L * ntet);
   k_mkn6<<<nblk(6L * ntet, 256), 256, 0, s>>>(c->n4.p, ntet, stack.p, c->line.p, c->n6line.p, c->status.p);
+  count_launch();
   check_status(c, "edge numbering: MKN6");
   (void)KL0;
   (void)KL1;
@@ -300,6 +309,7 @@ void build_pattern_device(afem_ctx* c) {
   cnt.alloc(nline);
   cnt.zero(s);
   k_count_edge_tets<<<nblk(6L * ntet, 256), 256, 0, s>>>(c->n6line.p, ntet, nline, cnt.p, c->status.p);
+  count_launch();
   check_status(c, "pattern: n6line holds an edge id outside 1..nline");
   c->etp.alloc(nline + 1);
   exclusive_scan(cnt.p, c->etp.p, nline, s, nullptr);
@@ -307,10 +317,13 @@ void build_pattern_device(afem_ctx* c) {
   cursor.zero(s);
   c->etl.alloc(6L * ntet);
   k_fill_edge_tets<<<nblk(6L * ntet, 256), 256, 0, s>>>(c->n6line.p, ntet, nline, c->etp.p, cursor.p, c->etl.p);
+  count_launch();
   k_sort_segments<<<nblk(nline, 128), 128, 0, s>>>(c->etp.p, nline, c->etl.p, EDGE_DEG_MAX, c->status.p);
+  count_launch();
   check_status(c, "pattern: edge shared by too many tetrahedra");
   k_row_pattern<<<nblk(nline, PAT_WARPS), PAT_WARPS * 32, 0, s>>>(c->n6line.p, c->etp.p, c->etl.p, nline, cnt.p,
                                                                   nullptr, nullptr, nullptr, c->status.p);
+  count_launch();
   check_status(c, "pattern: row length");
   c->rowptr.alloc(nline + 1);
   long nnz = 0;
@@ -320,6 +333,7 @@ void build_pattern_device(afem_ctx* c) {
   c->diagpos.alloc(nline);
   k_row_pattern<<<nblk(nline, PAT_WARPS), PAT_WARPS * 32, 0, s>>>(c->n6line.p, c->etp.p, c->etl.p, nline, nullptr,
                                                                   c->rowptr.p, c->col.p, c->diagpos.p, c->status.p);
+  count_launch();
   check_status(c, "pattern: fill");
   c->pattern_ready = true;
   c->schedule_ready = false;

@@ -576,6 +576,7 @@ void ensure_cast(afem_ctx* c, MpnnState* S) {
   S->wt.alloc((size_t)L * XW * H);
   S->small.alloc(FIN * H + L * H + 2 * H);
   k_cast_weights<<<(L * XW * H + 255) / 256, 256, 0, c->stream>>>(S->p.p, S->wl.p, S->wt.p, S->small.p);
+  count_launch();
   S->cast_valid = true;
 }
 
@@ -609,6 +610,7 @@ void rowinfo(afem_ctx* c, MpnnState* S, int ns) {
   const long rows = (long)c->nline * ns;
   k_rowinfo<<<blocks(rows, 256), 256, 0, c->stream>>>(c->km.p, c->diagpos.p, c->bc.p, c->nline, S->omega.p, ns, S->s.p,
                                                        S->feat.p);
+  count_launch();
 }
 
 template <class V>
@@ -619,6 +621,7 @@ void forward(afem_ctx* c, MpnnState* S, int ns, const V* r, V* z, bool train, co
   const long rows = (long)n * ns;
   const double* R = rms ? rms : S->rms.p;
   k_encode<V><<<blocks(rows, 256), 256, 0, st>>>(r, n, ns, S->s.p, S->feat.p, R, S->small.p + 0, S->h[0].p, skip);
+  count_launch();
   dim3 grid(blocks(n, ROWS), ns);
   for (int l = 0; l < L; ++l) {
     const __nv_bfloat16* hin = train ? S->h[l].p : S->h[l & 1].p;
@@ -626,10 +629,12 @@ void forward(afem_ctx* c, MpnnState* S, int ns, const V* r, V* z, bool train, co
     k_layer<<<grid, 128, 0, st>>>(c->rowptr.p, c->col.p, c->km.p, S->s.p, S->omega.p, n, hin, hout,
                                   S->wt.p + (size_t)l * XW * H, S->small.p + FIN * H + l * H,
                                   train ? S->sx[l].p : nullptr, train ? S->sy[l].p : nullptr, skip);
+    count_launch();
   }
   const __nv_bfloat16* hl = train ? S->h[L].p : S->h[L & 1].p;
   k_decode<V><<<blocks(rows, 256), 256, 0, st>>>(hl, n, ns, S->s.p, R, S->small.p + FIN * H + L * H, r, z,
                                                  nullptr, skip);
+  count_launch();
   AFEM_CUDA(cudaGetLastError());
 }
 
@@ -652,22 +657,29 @@ double loss_backward(afem_ctx* c, MpnnState* S, int ns, const double2* r) {
   S->sums.alloc(2 * ns);
   k_loss_res<<<dim3(nb, ns), 256, 0, st>>>(c->rowptr.p, c->col.p, c->km.p, S->omega.p, n, ns, S->z64.p, r, S->res.p,
                                            S->part.p);
+  count_launch();
   k_loss_sum<<<1, 32, 0, st>>>(S->part.p, nb, ns, S->sums.p);
+  count_launch();
   k_loss_grad<<<dim3(nb, ns), 256, 0, st>>>(c->rowptr.p, c->col.p, c->km.p, S->omega.p, n, ns, S->res.p, S->sums.p,
                                             S->rms.p, S->s.p, S->dout.p);
+  count_launch();
   float* G = S->grad.p;
   k_decode_bwd<<<std::min(1024u, blocks(rows, 256)), 256, 0, st>>>(S->h[L].p, rows, S->dout.p,
                                                                   S->small.p + FIN * H + L * H, S->dh.p,
                                                                   G + off_wout());
+  count_launch();
   for (int l = L - 1; l >= 0; --l) {
     k_layer_bwd<<<blocks(rows, ROWS), 128, LAYER_BWD_SMEM, st>>>(rows, S->dh.p, S->sx[l].p, S->sy[l].p,
                                                                  S->wl.p + (size_t)l * XW * H, S->dx.p, G + off_w(l),
                                                                  G + off_c(l));
+    count_launch();
     k_agg_bwd<<<dim3(std::min(4096u, blocks(n, 8)), ns), 256, 0, st>>>(c->rowptr.p, c->col.p, c->km.p, S->s.p,
                                                                        S->omega.p, n, S->dx.p, S->dh.p);
+    count_launch();
   }
   k_encode_bwd<double2><<<std::min(1024u, blocks(rows, 256)), 256, 0, st>>>(r, n, ns, S->s.p, S->feat.p, S->rms.p,
                                                                             S->dh.p, G + off_win());
+  count_launch();
   AFEM_CUDA(cudaGetLastError());
   std::vector<double> h(2 * ns);
   AFEM_CUDA(cudaMemcpyAsync(h.data(), S->sums.p, sizeof(double) * 2 * ns, cudaMemcpyDeviceToHost, st));
@@ -809,6 +821,7 @@ double mpnn_train_host(afem_ctx* c, double freq, int nsamp, const double* r_host
     const float bc1 = 1.f - std::pow(b1, (float)S->adam_t), bc2 = 1.f - std::pow(b2, (float)S->adam_t);
     k_adam<<<(NPARAM + 255) / 256, 256, 0, c->stream>>>(S->p.p, S->grad.p, S->m1.p, S->m2.p, NPARAM, lr, b1, b2, 1e-8f,
                                                         bc1, bc2, 1.0f / nsamp);
+    count_launch();
     S->cast_valid = false;
     last = Lsum / nsamp;
     if (hist) hist[it] = last;

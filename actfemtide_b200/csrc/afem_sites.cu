@@ -184,6 +184,7 @@ void site_coeffs_range(afem_ctx* c, int nobs, const double* xyz_obs, long t0, lo
   AFEM_CUDA(cudaMemcpyAsync(best.p, init.data(), sizeof(int) * nobs, cudaMemcpyHostToDevice, s));
   dim3 grid(std::max(1, std::min(2 * c->num_sms, (int)((t1 - t0 + 255) / 256))), nobs);
   k_find<<<grid, 256, 0, s>>>(c->xyz.p, c->n4.p, t0, t1, obs.p, nobs, best.p);
+  count_launch();
   DBuf<int32_t> ditem;
   DBuf<double> dve, dvf;
   ditem.alloc(6L * nobs);
@@ -191,6 +192,7 @@ void site_coeffs_range(afem_ctx* c, int nobs, const double* xyz_obs, long t0, lo
   dvf.alloc(18L * nobs);
   k_coeffs<<<(nobs + 63) / 64, 64, 0, s>>>(c->xyz.p, c->n4.p, c->n6line.p, obs.p, nobs, best.p, ditem.p, dve.p, dvf.p,
                                           c->status.p);
+  count_launch();
   check_status(c, "sites: a site lies outside every tetrahedron");
   if (item) ditem.download(item, 6L * nobs, s);
   if (val_e) dve.download(val_e, 18L * nobs, s);
@@ -235,6 +237,7 @@ void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out) {
       const long tot = 5L * nobs;
       k_eval<<<(unsigned)((tot + 127) / 128), 128, 0, s>>>(c->X.p, c->nline, 1, dom.p, nobs, ditem.p, dve.p, dvf.p,
                                                            dout.p + (long)k * 5 * nobs);
+      count_launch();
       AFEM_CUDA(cudaStreamSynchronize(s));
     }
     dout.download(reinterpret_cast<double2*>(out), (long)c->nsys * 5 * nobs, s);
@@ -258,6 +261,7 @@ void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out) {
   dout.alloc(tot);
   k_eval<<<(unsigned)((tot + 127) / 128), 128, 0, s>>>(c->X.p, c->nline, c->nsys, dom.p, nobs, ditem.p, dve.p, dvf.p,
                                                        dout.p);
+  count_launch();
   dout.download(reinterpret_cast<double2*>(out), tot, s);
   AFEM_CUDA(cudaStreamSynchronize(s));
 }

@@ -868,6 +868,7 @@ void launch_coop(K kernel, int blocks, cudaStream_t s, Args... args) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   AFEM_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
+  count_launch();
 }
 
 template <class K>
@@ -922,6 +923,7 @@ void launch_spmv(afem_ctx* c, SolverWork* w, int rpw, const typename Cx<T>::V* k
                                                                            bvec, sg);
   else
     k_spmv<T, NS, 1, SEG><<<w->nblocks, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p, bvec, sg);
+  count_launch();
 }
 
 // Rows-per-warp autotuner: times each variant on this matrix (q = A p with the
@@ -980,6 +982,7 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
   if (ev) AFEM_CUDA(cudaEventRecord(ev[1], s));
   const int swb = mc ? w->mc_blocks : sweep_blocks;
   k_scal_r<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, swb, nsys, learned ? w->rms.p : nullptr, n);
+  count_launch();
   if (learned) mpnn_run<V>(c, NS, w->rms.p, (const V*)I::R(w), I::Z(w), &w->ctrl.p->done);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[2], s));
   if (mc)
@@ -994,13 +997,16 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
                 (const int32_t*)c->perm_b.p, sg);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[3], s));
   k_scal_rho<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, swb, nsys, learned ? 1 : 0);
+  count_launch();
   if (ev) AFEM_CUDA(cudaEventRecord(ev[4], s));
   k_pupd<T, NS, SEG><<<c->num_sms * 8, 256, 0, s>>>(n, I::Z(w), I::P(w), w->sc.p, w->ctrl.p, sg);
+  count_launch();
   if (ev) AFEM_CUDA(cudaEventRecord(ev[5], s));
   launch_spmv<T, NS, SEG>(c, w, sizeof(T) == 8 ? w->rpw64 : w->rpw32, I::KM(c, w), (const V*)I::P(w), I::Q(w),
                           w->ctrl.p, (const V*)nullptr);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[6], s));
   k_scal_pq<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, nsys);
+  count_launch();
 }
 
 // FP64 true residual r64 = b - A x; returns per-system ||r||^2 and ||b||^2 on the host.
@@ -1011,9 +1017,11 @@ void true_residual(afem_ctx* c, SolverWork* w, std::vector<double>& rr, std::vec
   k_spmv<double, NS, 1, SEG><<<w->nblocks, 256, 0, s>>>((const int32_t*)c->rowptr.p, (const int32_t*)c->col.p, c->km.p,
                                                         w->n, w->x.p, w->r64.p, w->sc.p, (const Ctrl*)nullptr,
                                                         w->part.p, w->b.p, SEG ? c->seg_of_row.p : nullptr);
+  count_launch();
   DBuf<double> out;
   out.alloc(2 * nsys);
   k_true_resid<<<1, 32 * MAX_SYS, 0, s>>>(w->part.p, w->nblocks, nsys, out.p);
+  count_launch();
   std::vector<double> h(2 * nsys);
   out.download(h.data(), 2 * nsys, s);
   AFEM_CUDA(cudaStreamSynchronize(s));
@@ -1040,6 +1048,7 @@ void setup_dd(afem_ctx* c, SolverWork* w, int precond, double sd) {
   } else if (precond == AFEM_PRECOND_SSOR || precond == AFEM_PRECOND_DIAG || precond == AFEM_PRECOND_SSOR_MC) {
     k_dd_diag<T, NS><<<c->num_sms * 8, 256, 0, s>>>(I::KM(c, w), (const int32_t*)c->diagpos.p, w->n, sd,
                                                     (const SysScal*)w->sc.p, I::DD(w), sg);
+    count_launch();
   }
 }
 
@@ -1055,6 +1064,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   const long total = (long)n * NS;
   // r = rhs (as T), x = 0, ||b||^2
   k_copy_r<typename I::V><<<c->num_sms * 8, 256, 0, s>>>(w->r64.p, I::R(w), total);
+  count_launch();
   // ||r64||^2 via partials of a dedicated pass
   {
     // reuse SpMV-with-b path on x = 0: part[0] = ||b||^2
@@ -1062,8 +1072,10 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
     k_spmv<double, NS, 1, SEG><<<w->nblocks, 256, 0, s>>>((const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
                                                           c->km.p, n, w->x.p, w->q.p, w->sc.p, (const Ctrl*)nullptr,
                                                           w->part.p, w->r64.p, SEG ? c->seg_of_row.p : nullptr);
+    count_launch();
   }
   k_init_sys<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, nsys, tol, maxit, d_omega);
+  count_launch();
   setup_dd<T, NS, SEG>(c, w, precond, o->sigma_diag > 0 ? o->sigma_diag : 1.0);
   const int mode = precond;
   tune_spmv<T, NS, SEG>(c, w);
@@ -1097,20 +1109,32 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   }
   auto ev_of = [&](int k) -> cudaEvent_t* { return prof ? &evs[7L * k] : nullptr; };
   cudaGraphExec_t gexec = nullptr;
+  long graph_kernels = 0;  // kernel nodes of the captured chunk (launch count per graph launch)
   bool use_graph = o->use_graph != 0 && !prof;
   if (use_graph) {
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
       bool ok = true;
+      g_capturing = 1;
       try {
         for (int k = 0; k < chunk; ++k) enqueue_iteration<T, NS, SEG>(c, w, mode, sblocks, ev_of(k));
       } catch (const Error&) {
         ok = false;
       }
+      g_capturing = 0;
       e = cudaStreamEndCapture(s, &graph);
       if (ok && e == cudaSuccess && graph) {
         if (cudaGraphInstantiate(&gexec, graph, 0) != cudaSuccess) gexec = nullptr;
+        size_t nn = 0;
+        if (gexec && cudaGraphGetNodes(graph, nullptr, &nn) == cudaSuccess && nn > 0) {
+          std::vector<cudaGraphNode_t> nodes(nn);
+          if (cudaGraphGetNodes(graph, nodes.data(), &nn) == cudaSuccess)
+            for (size_t k = 0; k < nn; ++k) {
+              cudaGraphNodeType t;
+              if (cudaGraphNodeGetType(nodes[k], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++graph_kernels;
+            }
+        }
       }
       if (graph) cudaGraphDestroy(graph);
     }
@@ -1125,6 +1149,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
     AFEM_REQUIRE(nchunk < chunk_budget, AFEM_ESTATE, "COCG: inner solve made no progress");
     if (use_graph) {
       AFEM_CUDA(cudaGraphLaunch(gexec, s));
+      count_launch(graph_kernels);
     } else {
       for (int k = 0; k < chunk; ++k) enqueue_iteration<T, NS, SEG>(c, w, mode, sblocks, ev_of(k));
     }
@@ -1236,6 +1261,7 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
   if (mixed && (!w->kmf_valid || w->kmf.n != (size_t)c->nnz)) {
     w->kmf.alloc(c->nnz);
     k_convert<float2, double2><<<c->num_sms * 8, 256, 0, s>>>(c->km.p, w->kmf.p, c->nnz);
+    count_launch();
     w->kmf_valid = true;
   }
   {
@@ -1266,6 +1292,7 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     } else {
       dsrc.upload(hsrc.data(), nsys, s);
       k_gather_rhs<<<c->num_sms * 8, 256, 0, s>>>(c->rhs.p, n, NS, dsrc.p, w->b.p, SEG ? c->seg_of_row.p : nullptr);
+      count_launch();
     }
     AFEM_CUDA(cudaStreamSynchronize(s));
   }
@@ -1347,6 +1374,7 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     it_total += its;
     refinements += 1;
     k_add_x<<<c->num_sms * 8, 256, 0, s>>>(xacc.p, w->x.p, total);
+    count_launch();
     AFEM_CUDA(cudaMemcpyAsync(w->x.p, xacc.p, sizeof(double2) * total, cudaMemcpyDeviceToDevice, s));
     true_residual<NS, SEG>(c, w, rr, bb);  // r64 = b - A x_acc
     worst = 0.0;

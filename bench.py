@@ -8,8 +8,15 @@ E at the sites.  The workload is the 96x96x64-hex model (3,538,944 tets,
 4,193,536 edges, log-normal subsurface, M2 source, 400 sites), synthetic
 and seeded (no dataset exists for it).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--method plain|mixed|batched]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--method METHOD]
   python bench.py --impl reference ...   # the CPU reference path (oracle restatement)
+
+Methods (preconditioner, precision, systems per step): plain = SSOR-COCG
+FP64, one system (the reference's solver on the device); plain-mc = the
+multicolour SSOR; mixed = multicolour SSOR with FP32 inner COCG under FP64
+refinement; batched / batched-mixed = 8 tidal periods x 2 source patterns =
+16 systems per solve; learned* = flexible COCG with the learned network;
+packed = 24 uneven meshes (n x n x 3n/4, n in 8..32) in one solve.
 
 Prints ONE JSON line on rank 0.  Under torchrun every rank solves its own
 independent systems (replicas; weak scaling), the time is the max over ranks.
@@ -115,6 +122,8 @@ def kernel_bytes(name: str, n: int, nnz: int, ns: int, real_bytes: int, ntet: in
     ent = 2 * real_bytes + 4          # (K, M) pair + column index per stored entry
     vec = 2 * real_bytes * ns         # one complex value per system per row
     off = (nnz - n) // 2              # strictly lower (= strictly upper) entries
+    if "_seg" in name:
+        ns = 1  # packed batch: one system per row
     if name.startswith("cocg_fwd_sweep"):
         # L entries, rowptr+diagpos, flag write; r r/w, q, p, x r/w (FP64), DD, y write, y gather
         return ent * off + 12 * n + n * (vec * 6 + 32 * ns)
@@ -134,11 +143,24 @@ def kernel_bytes(name: str, n: int, nnz: int, ns: int, real_bytes: int, ntet: in
 
 
 # ----------------------------------------------------------------------------- workloads
+METHODS = {
+    # method: (preconditioner, precision, batched)
+    "plain": ("SSOR", "fp64", False),
+    "plain-mc": ("SSOR_MC", "fp64", False),
+    "mixed": ("SSOR_MC", "mixed", False),
+    "batched": ("SSOR_MC", "fp64", True),
+    "batched-mixed": ("SSOR_MC", "mixed", True),
+    "learned": ("LEARNED", "fp64", False),
+    "learned-batched-mixed": ("LEARNED", "mixed", True),
+    "packed": ("SSOR_MC", "mixed", False),
+}
+
+
 def build_workload(method: str, rank: int, workload: str = "large"):
     from actfemtide_b200 import synth
     make = synth.large_model if workload == "large" else synth.small_model
     m = make(seed=rank)
-    if method.startswith("batched"):
+    if METHODS[method][2]:
         m2 = make(seed=1000 + rank)
         freqs = 1.0 / (3600.0 * np.array(synth.BATCH_PERIODS_H))
         f = np.concatenate([freqs, freqs])
@@ -151,17 +173,76 @@ def build_workload(method: str, rank: int, workload: str = "large"):
     return m, f, src, sources
 
 
-def solve_kwargs(method: str):
-    if method in ("mixed", "batched-mixed"):
-        return dict(precond="SSOR", precision="mixed")
-    if method == "learned":
-        return dict(precond="LEARNED", precision="fp64")
-    if method == "learned-batched-mixed":
-        return dict(precond="LEARNED", precision="mixed")
-    return dict(precond="SSOR", precision="fp64")
+def solve_kwargs(method: str, precond: str | None = None):
+    pc, prec, _ = METHODS[method]
+    return dict(precond=precond or pc, precision=prec)
 
 
 # ----------------------------------------------------------------------------- GPU arm
+class Job:
+    """The inputs of one step's problem as host arrays, and how to load them through the C ABI."""
+
+    def __init__(self, method: str, rank: int, workload: str):
+        from actfemtide_b200 import synth
+        self.method = method
+        if method == "packed":
+            self.pk = synth.pack(synth.uneven_models(24, seed=rank))
+            self.parts = self.pk.parts
+            self.freqs = np.array([m.freqs[0] for m in self.parts])
+            self.srcs = np.zeros(len(self.parts), np.int32)
+            self.sites = self.parts[0].sites
+            self.ntet = int(self.pk.n4.shape[0])
+            self.node = int(self.pk.xyz.shape[0])
+            self.nodes = int(sum(m.nodes for m in self.parts))
+            self.nsrc = 1
+            dims = sorted(m.dims[0] for m in self.parts)
+            self.desc = (f"24 packed uneven meshes n x n x round(3n/4), n in {dims[0]}..{dims[-1]}: "
+                         f"{self.ntet} tets, {{n}} edges, nnz {{nnz}}, {self.sites.shape[0]} sites per mesh")
+        else:
+            m, self.freqs, self.srcs, self.sources = build_workload(method, rank, workload)
+            self.m = m
+            self.sites = m.sites
+            self.ntet, self.node, self.nodes, self.nsrc = m.ntet, m.node, m.nodes, len(self.sources)
+            self.desc = (f"{m.dims[0]}x{m.dims[1]}x{m.dims[2]} hex box: {m.ntet} tets, {{n}} edges, nnz {{nnz}}, "
+                         f"{m.sites.shape[0]} sites")
+
+    @property
+    def ns(self):
+        return len(self.freqs)
+
+    def host_arrays(self, pin, line=None, n6=None):
+        if self.method == "packed":
+            pk = self.pk
+            return dict(xyz=pin(pk.xyz), n4=pin(pk.n4), tag=pin(pk.tag), sig=pin(pk.sigma_tet), F=[pin(pk.F)],
+                        v=[pin(pk.v)], sites=pin(self.sites), node_ptr=pin(pk.node_ptr))
+        m = self.m
+        return dict(xyz=pin(m.xyz), n4=pin(m.n4), tag=pin(m.tag), line=pin(line), n6=pin(n6), sig=pin(m.sigma_land),
+                    F=[pin(F) for F, _ in self.sources], v=[pin(v) for _, v in self.sources], sites=pin(m.sites))
+
+    def load(self, fw, h=None):
+        """Load the problem (from the job's arrays, or from the host buffers h)."""
+        if self.method == "packed":
+            if h is None:
+                fw.load_packed(self.pk)
+                return
+            fw.set_mesh(h["xyz"], h["n4"], h["tag"])
+            fw.set_segments(h["node_ptr"])
+            fw.set_sigma(h["sig"])
+            fw.set_source(h["F"][0], h["v"][0], 0)
+            b = self.pk.bounds
+        else:
+            m = self.m
+            if h is None:
+                fw.load_model(m, sources=self.sources)
+                return
+            fw.set_mesh(h["xyz"], h["n4"], h["tag"], h["line"], h["n6"])
+            fw.set_cond(m.sigma_air, m.sigma_ocean, 1, sigma_file=h["sig"])
+            for k in range(len(h["F"])):
+                fw.set_source(h["F"][k], h["v"][k], k)
+            b = m.bounds
+        fw.set_bounds(b["zmin"], b["zmax"], b["xout"], b["yout"])
+
+
 def run_gpu(args):
     import torch
     ws, rank, local = dist_info()
@@ -169,77 +250,78 @@ def run_gpu(args):
     if ws > 1:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    from actfemtide_b200 import capi
     from actfemtide_b200.forward import Forward
 
-    m, freqs, srcs, sources = build_workload(args.method, rank, args.workload)
+    job = Job(args.method, rank, args.workload)
     fw = Forward(local)
-    fw.load_model(m, sources=sources)
+    job.load(fw)
     if "learned" in args.method:
         from actfemtide_b200 import learned
         fw.mpnn_set_params(learned.load())
-    line, n6 = fw.lines()
-    n, nnz_half = fw.nline, None
+    n = fw.nline
     INU, IAU, INL, IAL = fw.export_pattern()
     nnz = n + 2 * len(IAU)
-    ns = len(freqs)
-    kw = solve_kwargs(args.method)
+    ns = job.ns
+    kw = solve_kwargs(args.method, args.precond)
     stream = torch.cuda.ExternalStream(fw.stream_ptr(), device=local)
 
-    def step():
+    def step(maxit=args.maxit):
         fw.assemble()
-        res = fw.solve(freqs, srcs=srcs, tol=TOL, maxit=args.maxit, **kw)
-        out = fw.sites(m.sites, nsys=ns)
+        res = fw.solve(job.freqs, srcs=job.srcs, tol=TOL, maxit=maxit, **kw)
+        out = fw.sites(job.sites, nsys=ns)
         return res, out
 
     for _ in range(args.warmup):
         res, _ = step()
         if not res.ok and not args.allow_unconverged:
             raise SystemExit(f"warm-up solve failed: {res}")
-    fw.set_profiling(True)
     clocks = ClockSampler(local)
     clocks.start()
     if ws > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
+    l0 = capi.launch_count()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    iters, resid = [], []
+    iters, resid, refs = [], [], []
     for _ in range(args.steps):
         res, out = step()
         iters.append(res.iterations)
         resid.append(res.resid_true)
+        refs.append(res.refinements)
         if not res.ok and not args.allow_unconverged:
             raise SystemExit(f"timed solve failed: {res}")
     e1.record(stream)
     torch.cuda.synchronize()
+    launches = capi.launch_count() - l0
     if ws > 1:
         torch.distributed.barrier()
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
+
+    # ---- per-kernel device times: a separate, bounded pass with CUDA events around every kernel
+    fw.set_profiling(True)
+    step(maxit=args.prof_iters)
     prof = fw.profile()
     fw.set_profiling(False)
 
     # ---- end to end through the C ABI with pinned host buffers, copies inside the timed region
-    pin = lambda a: _pinned(torch, a)  # noqa: E731
-    h = dict(xyz=pin(m.xyz), n4=pin(m.n4), tag=pin(m.tag), line=pin(line), n6=pin(n6), sig=pin(m.sigma_land),
-             F=[pin(F) for F, _ in sources], v=[pin(v) for _, v in sources], sites=pin(m.sites))
-    h2d = sum(int(a.nbytes) for a in (h["xyz"], h["n4"], h["tag"], h["line"], h["n6"], h["sig"])) + \
-        sum(int(a.nbytes) for a in h["F"]) + sum(int(a.nbytes) for a in h["v"]) + int(h["sites"].nbytes)
-    d2h = 16 * 5 * m.sites.shape[0] * ns
+    line, n6 = fw.lines()
+    h = job.host_arrays(lambda a: _pinned(torch, a), line, n6)
+    h2d = sum(int(a.nbytes) for k, a in h.items() if not isinstance(a, list)) + \
+        sum(int(a.nbytes) for a in h["F"]) + sum(int(a.nbytes) for a in h["v"])
+    d2h = 16 * 5 * job.sites.shape[0] * ns
     e2e_steps = max(1, args.e2e_steps)
     torch.cuda.synchronize()
     if ws > 1:
         torch.distributed.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        fw.set_mesh(h["xyz"], h["n4"], h["tag"], h["line"], h["n6"])
-        fw.set_cond(m.sigma_air, m.sigma_ocean, 1, sigma_file=h["sig"])
-        for k in range(len(sources)):
-            fw.set_source(h["F"][k], h["v"][k], k)
-        fw.set_bounds(m.bounds["zmin"], m.bounds["zmax"], m.bounds["xout"], m.bounds["yout"])
+        job.load(fw, h)
         fw.assemble()
-        r2 = fw.solve(freqs, srcs=srcs, tol=TOL, maxit=args.maxit, **kw)
+        r2 = fw.solve(job.freqs, srcs=job.srcs, tol=TOL, maxit=args.maxit, **kw)
         out = fw.sites(h["sites"], nsys=ns)
         if not r2.ok and not args.allow_unconverged:
             raise SystemExit(f"e2e solve failed: {r2}")
@@ -259,35 +341,39 @@ def run_gpu(args):
 
     # ---- roofline of the dominant kernel
     peak, peak_kind = peaks()
-    real_bytes = 4 if args.method == "mixed" else 8
     dom, dom_ms, dom_n = None, 0.0, 0
     for name, (kms, cnt) in prof.items():
         if kms > dom_ms:
             dom, dom_ms, dom_n = name, kms, cnt
-    rb = 4 if "fp32" in (dom or "") else real_bytes
-    per_launch = kernel_bytes(dom or "", n, nnz, ns, rb, m.ntet, len(sources), m.node, m.nodes)
+    rb = 4 if "fp32" in (dom or "") else 8
+    per_launch = kernel_bytes(dom or "", n, nnz, ns, rb, job.ntet, job.nsrc, job.node, job.nodes)
     achieved = per_launch / (dom_ms / max(1, dom_n) / 1e3) / 1e9 if dom_ms > 0 else 0.0
-    launches = sum(c for _, c in prof.values())
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(m, freqs[0], int(np.median(iters)), args.cpu_seconds)
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.method != "packed":
+        cpu = cpu_baseline(job.m, job.freqs[0], int(np.median(iters)), args.cpu_seconds)
+    total_ms = sum(x[0] for x in prof.values())
     line_out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "complex-f64" if args.method != "mixed" else "complex-f32 inner / f64 refinement",
-        "data": "synthetic (seeded Kuhn-split box, log-normal subsurface, M2 tidal source)",
-        "config": {"workload": f"96x96x64 hex box: {m.ntet} tets, {n} edges, nnz {nnz}, {m.sites.shape[0]} sites",
+        "dtype": "complex-f64" if kw["precision"] == "fp64" else "complex-f32 inner / f64 refinement",
+        "data": "synthetic (seeded Kuhn-split boxes, log-normal subsurface, M2 tidal source)",
+        "config": {"workload": job.desc.format(n=n, nnz=nnz),
                    "method": f"{args.method}: COCG-{kw['precond']} {kw['precision']}, {ns} system(s) per step",
                    "solves_per_step": ns, "tol_true_residual": TOL, "iterations_median": int(np.median(iters)),
-                   "true_residual_max": float(max(resid)), "parallelism": f"replicas x{ws}",
+                   "refinements_median": int(np.median(refs)), "true_residual_max": float(max(resid)),
+                   "parallelism": f"replicas x{ws}",
                    "l2": "working set > 126 MB L2 (matrix alone %.2f GB)" % (nnz * 20 / 1e9)},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps, "includes": "set_mesh (upload, pattern) + cond + source + assemble + solve + sites"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "peak_kind": peak_kind,
                      "bytes_per_launch": per_launch, "avg_launch_ms": dom_ms / max(1, dom_n), "traffic": None,
-                     "kernel_share": {k: round(v[0] / max(1e-9, sum(x[0] for x in prof.values())), 4)
-                                      for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}},
+                     "profile_pass": f"one step with the iteration cap at {args.prof_iters}, CUDA events around "
+                                     "every kernel (graphs off), outside the timed region",
+                     "kernel_share": {k: round(v[0] / max(1e-9, total_ms), 4)
+                                      for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+                     "kernel_avg_ms": {k: round(v[0] / max(1, v[1]), 5)
+                                       for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}},
         "gpu_launches": int(launches),
         "clocks": clk,
         "cpu_baseline": cpu,
@@ -384,8 +470,11 @@ def main():
     p.add_argument("--steps", type=int, default=2)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--method", default="plain",
-                   choices=["plain", "mixed", "batched", "batched-mixed", "learned", "learned-batched-mixed"])
+    p.add_argument("--method", default="batched-mixed", choices=sorted(METHODS))
+    p.add_argument("--precond", default=None, choices=["IC", "SSOR", "DIAG", "NONE", "LEARNED", "SSOR_MC"],
+                   help="override the method's preconditioner")
+    p.add_argument("--prof-iters", type=int, default=256,
+                   help="iteration cap of the per-kernel profiling pass (outside the timed region)")
     p.add_argument("--workload", default="large", choices=["large", "small"],
                    help="large: 96x96x64 hexes (the measured workload); small: 20x20x20 (quick checks)")
     p.add_argument("--allow-unconverged", action="store_true",

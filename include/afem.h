@@ -224,6 +224,10 @@ int afem_profile_count(afem_ctx *ctx);
 /* Entry i: kernel name, total milliseconds, launches. */
 int afem_profile_entry(afem_ctx *ctx, int i, char *name, int cap, double *ms, long *launches);
 
+/* Kernels this library has launched in this process (each kernel of a CUDA
+ * graph launch counts once per launch).  Host only. */
+long afem_launch_count(void);
+
 /* Host only: the triangular-sweep schedules of a CSR pattern (0-based columns
  * ascending, diagonal included): rows sorted by dependency level of the
  * forward (lower) and backward (upper) sweeps; the sweep kernels visit rows
