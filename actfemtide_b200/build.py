@@ -20,8 +20,8 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 # Files whose arithmetic must round like the serial reference (no FMA contraction).
 NOFMA = {"afem_assemble.cu", "afem_sites.cu", "afem_adjoint.cu"}
 SOURCES = ["afem_capi.cu", "afem_mesh.cu", "afem_assemble.cu", "afem_solver.cu", "afem_sites.cu", "afem_mpnn.cu",
-           "afem_adjoint.cu", "afem_io.cpp"]
-HEADERS = ["afem_internal.h", os.path.join("..", "..", "include", "afem.h")]
+           "afem_adjoint.cu", "afem_hybrid.cu", "afem_io.cpp"]
+HEADERS = ["afem_internal.h", "afem_hybrid.h", os.path.join("..", "..", "include", "afem.h")]
 
 
 def _stale(target, deps):

@@ -20,7 +20,7 @@ STATUS = {
     -5: "AFEM_EBREAKDOWN", -6: "AFEM_ENONFINITE", -7: "AFEM_ECUDA", -8: "AFEM_ESTATE", -9: "AFEM_ETIMEOUT",
     -10: "AFEM_EIO", -11: "AFEM_ENOPRECOND", -12: "AFEM_ESITE", -13: "AFEM_ESTAGNATION",
 }
-PRECOND = {"IC": 0, "SSOR": 1, "DIAG": 2, "NONE": 3, "LEARNED": 4, "SSOR_MC": 5}
+PRECOND = {"IC": 0, "SSOR": 1, "DIAG": 2, "NONE": 3, "LEARNED": 4, "SSOR_MC": 5, "HYBRID": 6}
 PRECISION = {"fp64": 0, "mixed": 1}
 
 # Every entry point declared in include/afem.h.
@@ -32,7 +32,7 @@ EXPORTS = (
     "afem_profile_entry", "afem_cocg13_single", "afem_set_system", "afem_get_residual", "afem_mpnn_nparam",
     "afem_mpnn_set_params", "afem_mpnn_get_params", "afem_mpnn_forward", "afem_mpnn_loss_grad", "afem_mpnn_train",
     "afem_solve_rhs", "afem_jacobian", "afem_sweep_schedule", "afem_coloring", "afem_set_segments",
-    "afem_segment_info", "afem_launch_count",
+    "afem_segment_info", "afem_launch_count", "afem_hybrid_matrix",
 )
 
 
@@ -76,6 +76,8 @@ def lib():
     L.afem_stream.argtypes = [_vp]
     L.afem_set_mesh.argtypes = [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp, _vp]
     L.afem_get_lines.argtypes = [_vp, C.POINTER(C.c_int), _vp, _vp]
+    L.afem_hybrid_matrix.argtypes = [_vp, C.POINTER(C.c_int), C.POINTER(C.c_long), _vp, _vp, _vp]
+    L.afem_hybrid_matrix.restype = C.c_int
     L.afem_launch_count.argtypes = []
     L.afem_launch_count.restype = C.c_long
     L.afem_set_segments.argtypes = [_vp, C.c_int, _vp]

@@ -255,6 +255,7 @@ void assemble_device(afem_ctx* c) {
   }
   check_status(c, "assemble");
   c->assembled = true;
+  c->assemble_gen += 1;
 }
 
 }  // namespace afem

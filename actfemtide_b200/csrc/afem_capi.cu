@@ -4,6 +4,7 @@
 #include <cstring>
 #include <exception>
 
+#include "afem_hybrid.h"
 #include "afem_internal.h"
 
 namespace afem {
@@ -96,6 +97,8 @@ void load_split_system(afem_ctx* c, int n, const int32_t* INU, const int32_t* IA
   c->pattern_ready = true;
   c->schedule_ready = false;
   c->assembled = true;
+  c->assemble_gen += 1;
+  afem::hybrid_invalidate(c);
   invalidate_work(c);
 }
 
@@ -150,6 +153,7 @@ void afem_destroy(afem_ctx* c) {
   afem::destroy_work(c);
   afem::destroy_ctl(c);
   afem::mpnn_destroy(c);
+  afem::hybrid_destroy(c);
   for (auto* s : c->src) delete s;
   c->src.clear();
     if (c->stream) {
@@ -162,6 +166,13 @@ void afem_destroy(afem_ctx* c) {
 const char* afem_last_error(const afem_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
 long afem_launch_count(void) { return afem::g_launches.load(); }
+
+int afem_hybrid_matrix(afem_ctx* c, int* node, long* nnz, int32_t* rowptr, int32_t* col, double* km) {
+  return guarded(c, [&]() {
+    afem::hybrid_export(c, node, nnz, rowptr, col, km);
+    return (int)AFEM_OK;
+  });
+}
 
 void* afem_stream(afem_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
@@ -191,6 +202,7 @@ int afem_set_mesh(afem_ctx* c, int node, const double* xyz, int ntet, const int3
     c->assembled = false;
     c->sigma_set = false;
     afem::clear_segments(c);
+    afem::hybrid_invalidate(c);
     afem::reset_status(c);
     if (nline > 0) {
       c->nline = nline;
@@ -433,7 +445,7 @@ int afem_solve(afem_ctx* c, int nsys, const double* freq, const int* src, const 
                afem_solve_stats* stats) {
   return guarded(c, [&]() {
     AFEM_REQUIRE(freq && opts, AFEM_EINVAL, "solve: null freq or opts");
-    AFEM_REQUIRE(opts->precond >= 0 && opts->precond <= 5, AFEM_EINVAL, "solve: unknown preconditioner");
+    AFEM_REQUIRE(opts->precond >= 0 && opts->precond <= 6, AFEM_EINVAL, "solve: unknown preconditioner");
     afem::reset_status(c);
     return afem::solve_device(c, nsys, freq, src, opts, stats);
   });

@@ -122,8 +122,9 @@ inline void count_launch(long n = 1) {
   if (!g_capturing) g_launches.fetch_add(n, std::memory_order_relaxed);
 }
 
-struct SolverWork;  // afem_solver.cu
-struct MpnnState;   // afem_mpnn.cu
+struct SolverWork;   // afem_solver.cu
+struct MpnnState;    // afem_mpnn.cu
+struct HybridState;  // afem_hybrid.cu
 
 }  // namespace afem
 
@@ -178,6 +179,7 @@ struct afem_ctx {
   afem::DBuf<double2> rhs;      // nline * nsrc
   int rhs_nsrc = 0;
   bool assembled = false;
+  long assemble_gen = 0;        // increases with every new set of matrix values
 
   // packed batch of independent meshes (segments): mesh k owns nodes
   // [seg_node_ptr[k], seg_node_ptr[k+1]), tetrahedra [seg_tet_ptr[k], ..) and
@@ -194,6 +196,7 @@ struct afem_ctx {
 
   afem::SolverWork* work = nullptr;
   afem::MpnnState* mpnn = nullptr;
+  afem::HybridState* hyb = nullptr;
   int last_learned_its = 0;  // iterations the last solve ran with the learned preconditioner
   afem::CtlInfo* ctl = nullptr;
 
@@ -208,6 +211,8 @@ void build_lines_device(afem_ctx* c);     // MKLINE_V2 + MKN6 on the device
 void build_pattern_device(afem_ctx* c);   // adjacency + full CSR pattern
 void build_schedule(afem_ctx* c);         // sweep level schedules from the pattern
 void exclusive_scan(const int32_t* in, int32_t* out, int n, cudaStream_t s, long* total_host);
+int compute_coloring(int n, const int32_t* rp, const int32_t* cl, uint8_t* color, int32_t* perm, int32_t* cptr,
+                     int max_colors);  // greedy distance-1 colouring, rows sorted by colour
 
 // afem_assemble.cu
 void assemble_device(afem_ctx* c);        // K, M, rhs, bc (GENMAT + COPY_UL + GENBCCSEM + SET_BC)

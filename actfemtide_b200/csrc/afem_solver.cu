@@ -31,6 +31,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "afem_hybrid.h"
 #include "afem_internal.h"
 
 namespace afem {
@@ -83,6 +84,9 @@ struct SolverWork {
   DBuf<double2> rprev;              // flexible COCG: previous residual (FP64 inner)
   DBuf<float2> rprevf;              // flexible COCG: previous residual (FP32 inner)
   DBuf<double> rms;                 // per-system rms(r) for the learned preconditioner
+  DBuf<double2> ht, hy, hdd;        // gradient-space correction: nodal rhs, solution, 1/diag (FP64 inner)
+  DBuf<float2> htf, hyf, hddf;      // the same for the FP32 inner solve
+  int nmc_blocks = 0;               // co-resident grid of the nodal multicolour sweeps
   int rpw64 = 0, rpw32 = 0;         // SpMV rows per warp chosen by tune_spmv (0 = not tuned)
   int mc_blocks = 0;                // co-resident grid of the multicolour sweeps
   bool no_window = false;           // COCG13_single semantics: no stagnation window, run to the cap
@@ -506,6 +510,173 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ------------------------------------------------------------------ gradient-space correction
+// z += G SSOR_node(G^T r) (Hiptmair's hybrid smoother in additive form): the
+// nodal right-hand side t = G^T r, two multicolour sweeps on A_G = K_G + i omega M_G,
+// then z += G u and the rho = r^T z partial sums of the corrected z.
+
+// t_a = sum over the non-Dirichlet edges e at node a of g_ea r_e (g = +1 at the head, -1 at the tail)
+template <class T, int NS>
+__global__ void k_grad_t(int node, const int32_t* __restrict__ nptr, const int32_t* __restrict__ nlist,
+                         const uint8_t* __restrict__ bc, const typename Cx<T>::V* __restrict__ r,
+                         typename Cx<T>::V* __restrict__ t, const Ctrl* __restrict__ ctrl) {
+  if (ctrl->done) return;
+  const long total = (long)node * NS;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int a = (int)(i / NS), s = (int)(i % NS);
+    T ax = 0, ay = 0;
+    for (int q = __ldg(nptr + a); q < __ldg(nptr + a + 1); ++q) {
+      const int v = __ldg(nlist + q), e = v >> 1;
+      if (__ldg(bc + e)) continue;
+      const typename Cx<T>::V re = r[(long)e * NS + s];
+      if (v & 1) { ax -= re.x; ay -= re.y; }
+      else { ax += re.x; ay += re.y; }
+    }
+    t[i] = Cx<T>::make(ax, ay);
+  }
+}
+
+// One multicolour SSOR sweep on the nodal matrix: forward y_a = (t_a - sum_{col(b)<col(a)} A_ab y_b) dd_a,
+// backward (in place) y_a -= dd_a sum_{col(b)>col(a)} A_ab y_b.  Grid barrier between colours.
+template <class T, int NS, bool SEG>
+__global__ void __launch_bounds__(256)
+    k_nsweep_mc(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                const typename Cx<T>::V* __restrict__ km, const typename Cx<T>::V* __restrict__ t,
+                typename Cx<T>::V* __restrict__ y, const typename Cx<T>::V* __restrict__ dd,
+                const uint8_t* __restrict__ color, const int32_t* __restrict__ perm, const int32_t* __restrict__ cptr,
+                int ncolors, const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl,
+                const uint8_t* __restrict__ seg, int backward) {
+  using V = typename Cx<T>::V;
+  static_assert(!SEG || NS == 1, "packed batches hold one system per row");
+  if (ctrl->done) return;
+  cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+  constexpr int G = 32 / NS;
+  const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double om = sc[s].omega;
+  for (int cc = 0; cc < ncolors; ++cc) {
+    const int c = backward ? ncolors - 1 - cc : cc;
+    const int p0 = cptr[c], p1 = cptr[c + 1];
+    for (int pos = p0 + warp; pos < p1; pos += nwarps) {
+      const int row = __ldg(perm + pos);
+      if constexpr (SEG) om = sc[__ldg(seg + row)].omega;
+      T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
+      for (int k = __ldg(rowptr + row) + g; k < __ldg(rowptr + row + 1); k += G) {
+        const int j = __ldg(col + k);
+        const int cj = __ldg(color + j);
+        if (backward ? cj <= c : cj >= c) continue;
+        const V a = km[k];
+        const V yj = ldcg(y + (long)j * NS + s);
+        t1x += a.x * yj.x; t1y += a.x * yj.y;
+        t2x += a.y * yj.x; t2y += a.y * yj.y;
+      }
+      group_reduce<T, NS>(t1x, t1y, t2x, t2y);
+      if (g == 0) {
+        const T o = (T)om;
+        const T sx = t1x - o * t2y, sy = t1y + o * t2x;
+        const V d = dd[(long)row * NS + s];
+        if (!backward) {
+          const V ti = t[(long)row * NS + s];
+          const T wx = ti.x - sx, wy = ti.y - sy;
+          y[(long)row * NS + s] = Cx<T>::make(wx * d.x - wy * d.y, wx * d.y + wy * d.x);
+        } else {
+          const V yi = y[(long)row * NS + s];
+          y[(long)row * NS + s] = Cx<T>::make(yi.x - (d.x * sx - d.y * sy), yi.y - (d.x * sy + d.y * sx));
+        }
+      }
+    }
+    grid.sync();
+  }
+}
+
+// Packed batches: the lanes of a warp hold rows of possibly different meshes;
+// lane 0 adds them to the warp's per-mesh slots in lane order (deterministic).
+template <int NVAL>
+__device__ __forceinline__ void seg_warp_add(double (*red)[MAX_SYS][NVAL], int slot, int sid, const double (&v)[NVAL]) {
+  const int lane = threadIdx.x & 31;
+  for (int l = 0; l < 32; ++l) {
+    const int sl = __shfl_sync(0xffffffffu, sid, l);
+    double vl[NVAL];
+#pragma unroll
+    for (int k = 0; k < NVAL; ++k) vl[k] = __shfl_sync(0xffffffffu, v[k], l);
+    if (lane == 0 && sl >= 0) {
+#pragma unroll
+      for (int k = 0; k < NVAL; ++k) red[slot][sl][k] += vl[k];
+    }
+  }
+}
+
+// z_e += u_head(e) - u_tail(e) on the non-Dirichlet edges, then rho = r^T z partial sums (slots 0, 1)
+template <class T, int NS, bool SEG>
+__global__ void __launch_bounds__(256)
+    k_grad_add(int n, const int32_t* __restrict__ line, const uint8_t* __restrict__ bc,
+               const typename Cx<T>::V* __restrict__ u, typename Cx<T>::V* __restrict__ z,
+               const typename Cx<T>::V* __restrict__ r, const Ctrl* __restrict__ ctrl, double* __restrict__ part,
+               const uint8_t* __restrict__ seg) {
+  using V = typename Cx<T>::V;
+  static_assert(!SEG || NS == 1, "packed batches hold one system per row");
+  if (ctrl->done) return;
+  const long total = (long)n * NS;
+  const long stride = (long)gridDim.x * blockDim.x;  // a multiple of NS: lane % NS is the system
+  double rx = 0.0, ry = 0.0;
+  double (*red)[MAX_SYS][4] = nullptr;
+  if constexpr (SEG) red = seg_sums<8, 4>();
+  const long span = (total + stride - 1) / stride * stride;  // every lane runs the same trip count
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < span; i += stride) {
+    double ex = 0.0, ey = 0.0;
+    int sid = -1;
+    if (i < total) {
+      const int e = (int)(i / NS), s = (int)(i % NS);
+      V zi = z[i];
+      if (!__ldg(bc + e)) {
+        const V uh = u[(long)(__ldg(line + 2 * e + 1) - 1) * NS + s];
+        const V ut = u[(long)(__ldg(line + 2 * e) - 1) * NS + s];
+        zi = Cx<T>::make(zi.x + (uh.x - ut.x), zi.y + (uh.y - ut.y));
+        z[i] = zi;
+      }
+      const V ri = r[i];
+      ex = (double)ri.x * (double)zi.x - (double)ri.y * (double)zi.y;
+      ey = (double)ri.x * (double)zi.y + (double)ri.y * (double)zi.x;
+      sid = SEG ? (int)__ldg(seg + e) : s;
+    }
+    if constexpr (SEG) {
+      const double v[4] = {ex, ey, 0.0, 0.0};
+      seg_warp_add<4>(red, threadIdx.x >> 5, sid, v);
+    } else {
+      rx += ex;
+      ry += ey;
+    }
+  }
+  if constexpr (SEG) {
+    seg_partials<8, 4>(red, part);
+  } else {
+#pragma unroll
+    for (int m = NS; m < 32; m <<= 1) {
+      rx += __shfl_xor_sync(0xffffffffu, rx, m);
+      ry += __shfl_xor_sync(0xffffffffu, ry, m);
+    }
+    double v[4] = {rx, ry, 0.0, 0.0};
+    block_partials<NS, 4>(v, part);
+  }
+}
+
+// dd_a = 1 / A_G(omega)_aa for nodes with a non-Dirichlet edge, 0 for the others
+template <class T, int NS>
+__global__ void k_dd_node(const double2* __restrict__ km, const int32_t* __restrict__ diagpos,
+                          const uint8_t* __restrict__ live, int node, const SysScal* __restrict__ sc,
+                          typename Cx<T>::V* __restrict__ dd, const uint8_t* __restrict__ seg) {
+  const long total = (long)node * NS;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int a = (int)(i / NS), s = seg ? (int)__ldg(seg + a) : (int)(i % NS);
+    const double2 v = km[diagpos[a]];
+    const double2 D = make_double2(v.x, sc[s].omega * v.y);
+    double2 w = make_double2(0.0, 0.0);
+    if (live[a] && (D.x != 0.0 || D.y != 0.0)) w = cdiv(make_double2(1.0, 0.0), D);
+    dd[i] = Cx<T>::make((T)w.x, (T)w.y);
+  }
+}
+
 // ------------------------------------------------------------------ p update, SpMV
 template <class T, int NS, bool SEG = false>
 __global__ void k_pupd(int n, const typename Cx<T>::V* __restrict__ z, typename Cx<T>::V* __restrict__ p,
@@ -894,6 +1065,10 @@ struct Inner<double, NS> {
   static V* DD(SolverWork* w) { return w->dd.p; }
   static V* RP(SolverWork* w) { return w->rprev.p; }
   static const V* KM(afem_ctx* c, SolverWork*) { return c->km.p; }
+  static V* HT(SolverWork* w) { return w->ht.p; }
+  static V* HY(SolverWork* w) { return w->hy.p; }
+  static V* HDD(SolverWork* w) { return w->hdd.p; }
+  static const V* HKM(afem_ctx* c) { return c->hyb->km.p; }
 };
 template <int NS>
 struct Inner<float, NS> {
@@ -905,6 +1080,10 @@ struct Inner<float, NS> {
   static V* DD(SolverWork* w) { return w->ddf.p; }
   static V* RP(SolverWork* w) { return w->rprevf.p; }
   static const V* KM(afem_ctx*, SolverWork* w) { return w->kmf.p; }
+  static V* HT(SolverWork* w) { return w->htf.p; }
+  static V* HY(SolverWork* w) { return w->hyf.p; }
+  static V* HDD(SolverWork* w) { return w->hddf.p; }
+  static const V* HKM(afem_ctx* c) { return c->hyb->kmf.p; }
 };
 
 template <class T, int NS, bool SEG>
@@ -967,7 +1146,8 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
   const uint8_t* sg = SEG ? c->seg_of_row.p : nullptr;
   const bool learned = mode == AFEM_PRECOND_LEARNED;
   V* rp = learned ? I::RP(w) : nullptr;
-  const bool mc = mode == AFEM_PRECOND_SSOR_MC;
+  const bool hyb = mode == AFEM_PRECOND_HYBRID;
+  const bool mc = mode == AFEM_PRECOND_SSOR_MC || hyb;  // the hybrid's edge part is the multicolour SSOR
   if (ev) AFEM_CUDA(cudaEventRecord(ev[0], s));
   if (mc)
     launch_coop(k_fwd_mc<T, NS, SEG>, w->mc_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
@@ -996,15 +1176,35 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
                 w->flag_b.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, (const V*)rp,
                 (const int32_t*)c->perm_b.p, sg);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[3], s));
-  k_scal_rho<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, swb, nsys, learned ? 1 : 0);
-  count_launch();
+  int rho_blocks = swb;
+  if (hyb) {
+    // z += G SSOR_node(G^T r); the rho partials are taken again from the corrected z
+    HybridState* h = c->hyb;
+    const int node = h->node;
+    const uint8_t* hs = SEG ? h->seg.p : nullptr;
+    k_grad_t<T, NS><<<c->num_sms * 8, 256, 0, s>>>(node, h->nptr.p, h->nlist.p, c->bc.p, (const V*)I::R(w), I::HT(w),
+                                                    w->ctrl.p);
+    count_launch();
+    for (int bwd = 0; bwd < 2; ++bwd)
+      launch_coop(k_nsweep_mc<T, NS, SEG>, w->nmc_blocks, s, (const int32_t*)h->rowptr.p, (const int32_t*)h->col.p,
+                  I::HKM(c), (const V*)I::HT(w), I::HY(w), (const V*)I::HDD(w), (const uint8_t*)h->color.p,
+                  (const int32_t*)h->perm.p, (const int32_t*)h->cptr.p, h->ncolors, (const SysScal*)w->sc.p,
+                  (const Ctrl*)w->ctrl.p, hs, bwd);
+    k_grad_add<T, NS, SEG><<<w->nblocks, 256, 0, s>>>(n, c->line.p, c->bc.p, (const V*)I::HY(w), I::Z(w),
+                                                        (const V*)I::R(w), w->ctrl.p, w->part.p, sg);
+    count_launch();
+    rho_blocks = w->nblocks;
+  }
   if (ev) AFEM_CUDA(cudaEventRecord(ev[4], s));
-  k_pupd<T, NS, SEG><<<c->num_sms * 8, 256, 0, s>>>(n, I::Z(w), I::P(w), w->sc.p, w->ctrl.p, sg);
+  k_scal_rho<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, rho_blocks, nsys, learned ? 1 : 0);
   count_launch();
   if (ev) AFEM_CUDA(cudaEventRecord(ev[5], s));
+  k_pupd<T, NS, SEG><<<c->num_sms * 8, 256, 0, s>>>(n, I::Z(w), I::P(w), w->sc.p, w->ctrl.p, sg);
+  count_launch();
+  if (ev) AFEM_CUDA(cudaEventRecord(ev[6], s));
   launch_spmv<T, NS, SEG>(c, w, sizeof(T) == 8 ? w->rpw64 : w->rpw32, I::KM(c, w), (const V*)I::P(w), I::Q(w),
                           w->ctrl.p, (const V*)nullptr);
-  if (ev) AFEM_CUDA(cudaEventRecord(ev[6], s));
+  if (ev) AFEM_CUDA(cudaEventRecord(ev[7], s));
   k_scal_pq<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, nsys);
   count_launch();
 }
@@ -1045,9 +1245,16 @@ void setup_dd(afem_ctx* c, SolverWork* w, int precond, double sd) {
                 (const Ctrl*)w->ctrl.p, c->status.p, (const int32_t*)c->perm_f.p, sg);
     w->epoch_host += 1;
     AFEM_CUDA(cudaMemcpyAsync(&w->ctrl.p->epoch, &w->epoch_host, sizeof(unsigned), cudaMemcpyHostToDevice, s));
-  } else if (precond == AFEM_PRECOND_SSOR || precond == AFEM_PRECOND_DIAG || precond == AFEM_PRECOND_SSOR_MC) {
+  } else if (precond == AFEM_PRECOND_SSOR || precond == AFEM_PRECOND_DIAG || precond == AFEM_PRECOND_SSOR_MC ||
+             precond == AFEM_PRECOND_HYBRID) {
     k_dd_diag<T, NS><<<c->num_sms * 8, 256, 0, s>>>(I::KM(c, w), (const int32_t*)c->diagpos.p, w->n, sd,
                                                     (const SysScal*)w->sc.p, I::DD(w), sg);
+    count_launch();
+  }
+  if (precond == AFEM_PRECOND_HYBRID) {
+    HybridState* h = c->hyb;
+    k_dd_node<T, NS><<<c->num_sms * 8, 256, 0, s>>>(h->km.p, h->diagpos.p, h->live.p, h->node,
+                                                    (const SysScal*)w->sc.p, I::HDD(w), SEG ? h->seg.p : nullptr);
     count_launch();
   }
 }
@@ -1076,6 +1283,21 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   }
   k_init_sys<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, nsys, tol, maxit, d_omega);
   count_launch();
+  if (precond == AFEM_PRECOND_HYBRID) {
+    HybridState* h = c->hyb;
+    const long nt = (long)h->node * NS;
+    if (sizeof(T) == 8) {
+      w->ht.alloc(nt); w->hy.alloc(nt); w->hdd.alloc(nt);
+    } else {
+      w->htf.alloc(nt); w->hyf.alloc(nt); w->hddf.alloc(nt);
+      if (!h->kmf_valid || h->kmf.n != (size_t)h->nnz) {
+        h->kmf.alloc(h->nnz);
+        k_convert<float2, double2><<<c->num_sms * 8, 256, 0, s>>>(h->km.p, h->kmf.p, h->nnz);
+        count_launch();
+        h->kmf_valid = true;
+      }
+    }
+  }
   setup_dd<T, NS, SEG>(c, w, precond, o->sigma_diag > 0 ? o->sigma_diag : 1.0);
   const int mode = precond;
   tune_spmv<T, NS, SEG>(c, w);
@@ -1091,23 +1313,25 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   const int sweep_blocks = coresident_blocks(k_fwd<T, NS, SEG>, c->num_sms);
   const int sb2 = coresident_blocks(k_bwd<T, NS, SEG>, c->num_sms);
   const int sblocks = std::min(std::min(sweep_blocks, sb2), w->nblocks);
-  if (mode == AFEM_PRECOND_SSOR_MC)
+  if (mode == AFEM_PRECOND_SSOR_MC || mode == AFEM_PRECOND_HYBRID)
     w->mc_blocks = std::min(std::min(coresident_blocks(k_fwd_mc<T, NS, SEG>, c->num_sms),
                                      coresident_blocks(k_bwd_mc<T, NS, SEG>, c->num_sms)), w->nblocks);
+  if (mode == AFEM_PRECOND_HYBRID)
+    w->nmc_blocks = std::min(coresident_blocks(k_nsweep_mc<T, NS, SEG>, c->num_sms), w->nblocks);
   // every solve starts a fresh flag generation: a solve that stopped inside a
   // chunk left its last forward-sweep flags at the epoch it ended on
   w->epoch_host += 1;
   AFEM_CUDA(cudaMemcpyAsync(&w->ctrl.p->epoch, &w->epoch_host, sizeof(unsigned), cudaMemcpyHostToDevice, s));
   int iters_done = 0;
   const int chunk = check_every > 0 ? check_every : 32;
-  // profiling: 7 events per iteration of a chunk (fwd | scal | bwd | scal | pupd | spmv)
+  // profiling: 8 events per iteration of a chunk (fwd | scal | bwd | nodal correction | scal | pupd | spmv)
   const bool prof = c->prof.on;
   std::vector<cudaEvent_t> evs;
   if (prof) {
-    evs.resize(7L * chunk);
+    evs.resize(8L * chunk);
     for (auto& e : evs) AFEM_CUDA(cudaEventCreate(&e));
   }
-  auto ev_of = [&](int k) -> cudaEvent_t* { return prof ? &evs[7L * k] : nullptr; };
+  auto ev_of = [&](int k) -> cudaEvent_t* { return prof ? &evs[8L * k] : nullptr; };
   cudaGraphExec_t gexec = nullptr;
   long graph_kernels = 0;  // kernel nodes of the captured chunk (launch count per graph launch)
   bool use_graph = o->use_graph != 0 && !prof;
@@ -1160,23 +1384,27 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
       // count only iterations that ran to their last kernel
       const int executed = std::min(chunk, w->h_ctrl->iter - iter_before);
       const char* tag = sizeof(T) == 8 ? "fp64" : "fp32";
-      char nf[48], nb[48], np_[48], ns_[48];
+      char nf[64], nb[64], nh[64], np_[64], ns_[64];
       const char* kind = SEG ? "seg" : "ns";
       const int cnt = SEG ? nsys : NS;
-      snprintf(nf, sizeof nf, "cocg_fwd_sweep_%s_%s%d", tag, kind, cnt);
-      snprintf(nb, sizeof nb, "cocg_bwd_sweep_%s_%s%d", tag, kind, cnt);
+      const bool mcs = mode == AFEM_PRECOND_SSOR_MC || mode == AFEM_PRECOND_HYBRID;
+      snprintf(nf, sizeof nf, "cocg_fwd_sweep%s_%s_%s%d", mcs ? "_mc" : "", tag, kind, cnt);
+      snprintf(nb, sizeof nb, "cocg_bwd_sweep%s_%s_%s%d", mcs ? "_mc" : "", tag, kind, cnt);
+      snprintf(nh, sizeof nh, "cocg_nodal_correction_%s_%s%d", tag, kind, cnt);
       snprintf(np_, sizeof np_, "cocg_p_update_%s_%s%d", tag, kind, cnt);
       snprintf(ns_, sizeof ns_, "cocg_spmv_%s_%s%d", tag, kind, cnt);
       for (int k = 0; k < executed; ++k) {
-        float a = 0, b = 0, d = 0, e = 0;
-        cudaEvent_t* E = &evs[7L * k];
+        float a = 0, b = 0, h = 0, d = 0, e = 0;
+        cudaEvent_t* E = &evs[8L * k];
         if (cudaEventElapsedTime(&a, E[0], E[1]) != cudaSuccess || cudaEventElapsedTime(&b, E[2], E[3]) != cudaSuccess ||
-            cudaEventElapsedTime(&d, E[4], E[5]) != cudaSuccess || cudaEventElapsedTime(&e, E[5], E[6]) != cudaSuccess) {
+            cudaEventElapsedTime(&h, E[3], E[4]) != cudaSuccess || cudaEventElapsedTime(&d, E[5], E[6]) != cudaSuccess ||
+            cudaEventElapsedTime(&e, E[6], E[7]) != cudaSuccess) {
           cudaGetLastError();
           continue;
         }
         c->prof.add(nf, a);
         c->prof.add(nb, b);
+        if (mode == AFEM_PRECOND_HYBRID) c->prof.add(nh, h);
         c->prof.add(np_, d);
         c->prof.add(ns_, e);
       }
@@ -1438,6 +1666,7 @@ int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, cons
                  afem_solve_stats* st, const SolveExtra* ex) {
   AFEM_REQUIRE(c->assembled, AFEM_ESTATE, "solve: system not assembled");
   build_schedule(c);
+  if (o->precond == AFEM_PRECOND_HYBRID) hybrid_prepare(c);
   if (c->nseg > 0) {
     AFEM_REQUIRE(nsys == c->nseg, AFEM_EINVAL, "solve: a packed batch solves one system per mesh (nsys = nseg)");
     AFEM_REQUIRE(o->precond != AFEM_PRECOND_LEARNED, AFEM_EINVAL,

@@ -314,6 +314,14 @@ class Forward:
             out[buf.value.decode()] = (ms.value, n.value)
         return out
 
+    def hybrid_matrix(self):
+        """(rowptr, col, K_G, M_G) of the gradient-space correction's nodal matrix."""
+        node = C.c_int(0); nnz = C.c_long(0)
+        self._check(self._L.afem_hybrid_matrix(self.ctx, C.byref(node), C.byref(nnz), None, None, None))
+        rp = np.zeros(node.value + 1, np.int32); col = np.zeros(nnz.value, np.int32); km = np.zeros((nnz.value, 2))
+        self._check(self._L.afem_hybrid_matrix(self.ctx, None, None, ptr(rp), ptr(col), ptr(km)))
+        return rp, col, km[:, 0].copy(), km[:, 1].copy()
+
     def stream_ptr(self) -> int:
         return int(self._L.afem_stream(self.ctx) or 0)
 

@@ -158,8 +158,14 @@ METHODS = {
 
 def build_workload(method: str, rank: int, workload: str = "large"):
     from actfemtide_b200 import synth
-    make = synth.large_model if workload == "large" else synth.small_model
-    m = make(seed=rank)
+
+    def make(seed):
+        if workload == "large":
+            return synth.large_model(seed=seed)
+        if workload == "medium":  # matrix ~0.17 GB: larger than L2, small enough for ncu captures
+            return synth.tidal_box(48, 48, 32, seed=seed, grf=True, block=False, name="box48x48x32")
+        return synth.small_model(seed=seed)
+    m = make(rank)
     if METHODS[method][2]:
         m2 = make(seed=1000 + rank)
         freqs = 1.0 / (3600.0 * np.array(synth.BATCH_PERIODS_H))
@@ -475,8 +481,9 @@ def main():
                    help="override the method's preconditioner")
     p.add_argument("--prof-iters", type=int, default=256,
                    help="iteration cap of the per-kernel profiling pass (outside the timed region)")
-    p.add_argument("--workload", default="large", choices=["large", "small"],
-                   help="large: 96x96x64 hexes (the measured workload); small: 20x20x20 (quick checks)")
+    p.add_argument("--workload", default="large", choices=["large", "medium", "small"],
+                   help="large: 96x96x64 hexes (the measured workload); medium: 48x48x32 (profiler captures); "
+                        "small: 20x20x20 (quick checks)")
     p.add_argument("--allow-unconverged", action="store_true",
                    help="profiling runs with a small --maxit: accept solves stopped by the cap (not a bench number)")
     p.add_argument("--maxit", type=int, default=200000)

@@ -54,7 +54,9 @@ typedef enum afem_precond {
   AFEM_PRECOND_DIAG = 2,  /* z = DD * r */
   AFEM_PRECOND_NONE = 3,
   AFEM_PRECOND_LEARNED = 4,  /* flexible COCG with the learned network; SSOR-COCG restart when it stalls */
-  AFEM_PRECOND_SSOR_MC = 5   /* SSOR of the colour-permuted matrix: every sweep is ~20 parallel passes */
+  AFEM_PRECOND_SSOR_MC = 5,  /* SSOR of the colour-permuted matrix: every sweep is ~10 parallel passes */
+  AFEM_PRECOND_HYBRID = 6    /* multicolour SSOR plus a gradient-space correction G SSOR_node(G^T r)
+                                (Hiptmair's hybrid smoother, additive); needs the mesh */
 } afem_precond;
 
 typedef enum afem_precision {
@@ -223,6 +225,14 @@ int afem_set_profiling(afem_ctx *ctx, int enable);
 int afem_profile_count(afem_ctx *ctx);
 /* Entry i: kernel name, total milliseconds, launches. */
 int afem_profile_entry(afem_ctx *ctx, int i, char *name, int cap, double *ms, long *launches);
+
+/* The nodal matrix of the gradient-space correction (AFEM_PRECOND_HYBRID) for the
+ * assembled system: A_G = G^T P A P G with G the edge-node incidence (+1 at
+ * line(2,e), -1 at line(1,e)) and P dropping the Dirichlet edges, split as
+ * (K_G, M_G) pairs per entry like A (km: 2*nnz doubles); rowptr[node+1] and
+ * 0-based ascending col[nnz] over the node graph.  Any pointer may be NULL.
+ * No counterpart in the reference. */
+int afem_hybrid_matrix(afem_ctx *ctx, int *node, long *nnz, int32_t *rowptr, int32_t *col, double *km);
 
 /* Kernels this library has launched in this process (each kernel of a CUDA
  * graph launch counts once per launch).  Host only. */

@@ -9,8 +9,19 @@ from actfemtide_b200 import synth
 pytestmark = pytest.mark.gpu
 
 
-def test_ctl_driver_matches_oracle(gpulib, oracle, tmp_path):
+@pytest.fixture
+def short_dir():
+    """The reference reads file names into character(70) fields (m_param.f90:29-47): keep paths short."""
+    import shutil
+    import tempfile
+    d = tempfile.mkdtemp(prefix="afem", dir="/tmp")
+    yield d
+    shutil.rmtree(d, ignore_errors=True)
+
+
+def test_ctl_driver_matches_oracle(gpulib, oracle, short_dir):
     from actfemtide_b200.forward import Forward, amp_phase
+    tmp_path = short_dir
     m = synth.tidal_box(4, 4, 6, seed=3, site_grid=(-6.0, 0.0, 6.0), half_km=12.0)
     m.freqs = np.array([1.0 / 44714.0, 1.0 / 43200.0])
     of = oracle.OracleForward(m)
