@@ -32,7 +32,8 @@ EXPORTS = (
     "afem_profile_entry", "afem_cocg13_single", "afem_set_system", "afem_get_residual", "afem_mpnn_nparam",
     "afem_mpnn_set_params", "afem_mpnn_get_params", "afem_mpnn_forward", "afem_mpnn_loss_grad", "afem_mpnn_train",
     "afem_solve_rhs", "afem_jacobian", "afem_sweep_schedule", "afem_coloring", "afem_set_segments",
-    "afem_segment_info", "afem_launch_count", "afem_hybrid_matrix",
+    "afem_segment_info", "afem_launch_count", "afem_hybrid_matrix", "afem_sites_grid", "afem_site_coeffs_grid",
+    "afem_xy_points", "afem_sort_index", "afem_mesh_info", "afem_solution_count",
 )
 
 
@@ -76,10 +77,22 @@ def lib():
     L.afem_stream.argtypes = [_vp]
     L.afem_set_mesh.argtypes = [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp, _vp]
     L.afem_get_lines.argtypes = [_vp, C.POINTER(C.c_int), _vp, _vp]
+    L.afem_sites_grid.argtypes = [_vp, C.c_int, _vp, _vp]
+    L.afem_sites_grid.restype = C.c_int
+    L.afem_site_coeffs_grid.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp]
+    L.afem_site_coeffs_grid.restype = C.c_int
+    L.afem_xy_points.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, _vp]
+    L.afem_xy_points.restype = C.c_int
+    L.afem_sort_index.argtypes = [C.c_int, _vp, _vp]
+    L.afem_sort_index.restype = C.c_int
     L.afem_hybrid_matrix.argtypes = [_vp, C.POINTER(C.c_int), C.POINTER(C.c_long), _vp, _vp, _vp]
     L.afem_hybrid_matrix.restype = C.c_int
     L.afem_launch_count.argtypes = []
     L.afem_launch_count.restype = C.c_long
+    L.afem_mesh_info.argtypes = [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.afem_mesh_info.restype = C.c_int
+    L.afem_solution_count.argtypes = [_vp, C.POINTER(C.c_int)]
+    L.afem_solution_count.restype = C.c_int
     L.afem_set_segments.argtypes = [_vp, C.c_int, _vp]
     L.afem_segment_info.argtypes = [_vp, C.POINTER(C.c_int), _vp, _vp]
     L.afem_set_cond.argtypes = [_vp, C.c_double, C.c_double, C.c_int, C.c_int, _vp, C.c_int, _vp]
@@ -126,6 +139,14 @@ def lib():
         getattr(L, name).restype = C.c_int
     _LIB = L
     return L
+
+
+def xy_points(xmin, xmax, ymin, ymax, nx, ny, z):
+    """PREPOBSCOEFF_XY's plan-view points (nx*ny, 3), point (j-1)*ny + i for x cell j and y cell i."""
+    out = np.zeros((nx * ny, 3))
+    if lib().afem_xy_points(xmin, xmax, ymin, ymax, nx, ny, z, out.ctypes.data_as(_vp)) != 0:
+        raise ValueError("xy_points: bad grid")
+    return out
 
 
 def launch_count() -> int:

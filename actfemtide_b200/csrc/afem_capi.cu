@@ -154,6 +154,7 @@ void afem_destroy(afem_ctx* c) {
   afem::destroy_ctl(c);
   afem::mpnn_destroy(c);
   afem::hybrid_destroy(c);
+  afem::grid_destroy(c);
   for (auto* s : c->src) delete s;
   c->src.clear();
     if (c->stream) {
@@ -203,6 +204,7 @@ int afem_set_mesh(afem_ctx* c, int node, const double* xyz, int ntet, const int3
     c->sigma_set = false;
     afem::clear_segments(c);
     afem::hybrid_invalidate(c);
+    if (c->grid) c->grid->ready = false;
     afem::reset_status(c);
     if (nline > 0) {
       c->nline = nline;
@@ -213,6 +215,23 @@ int afem_set_mesh(afem_ctx* c, int node, const double* xyz, int ntet, const int3
     }
     AFEM_CUDA(cudaStreamSynchronize(s));
     afem::build_pattern_device(c);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_mesh_info(afem_ctx* c, int* node, int* ntet, int* nline) {
+  return guarded(c, [&]() {
+    if (node) *node = c->node;
+    if (ntet) *ntet = c->ntet;
+    if (nline) *nline = c->nline;
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_solution_count(afem_ctx* c, int* nsys) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(nsys, AFEM_EINVAL, "solution_count: null output");
+    *nsys = c->nsys;
     return (int)AFEM_OK;
   });
 }
@@ -518,6 +537,48 @@ int afem_site_coeffs(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item
     afem::site_coeffs_device(c, nobs, xyz_obs, item, val_e, val_f, iele);
     return (int)AFEM_OK;
   });
+}
+
+int afem_sites_grid(afem_ctx* c, int nobs, const double* xyz_obs, double* out) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(nobs > 0 && xyz_obs && out, AFEM_EINVAL, "sites_grid: empty or null");
+    AFEM_REQUIRE(c->ntet > 0 && c->nline > 0, AFEM_ESTATE, "sites_grid: no mesh");
+    afem::reset_status(c);
+    afem::sites_device(c, nobs, xyz_obs, out, true);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_site_coeffs_grid(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item, double* val_e, double* val_f,
+                          int32_t* iele) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(nobs > 0 && xyz_obs, AFEM_EINVAL, "site_coeffs_grid: empty or null");
+    AFEM_REQUIRE(c->ntet > 0 && c->nline > 0, AFEM_ESTATE, "site_coeffs_grid: no mesh");
+    afem::reset_status(c);
+    afem::site_coeffs_grid_device(c, nobs, xyz_obs, item, val_e, val_f, iele);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_sort_index(int n, int32_t* na, double* ra) {
+  if (n < 0 || (n > 0 && (!na || !ra))) return AFEM_EINVAL;
+  afem::sort_index_heap(n, na, ra);
+  return AFEM_OK;
+}
+
+int afem_xy_points(double xmin, double xmax, double ymin, double ymax, int nx, int ny, double z, double* xyz) {
+  if (nx <= 0 || ny <= 0 || !xyz) return AFEM_EINVAL;
+  // PREPOBSCOEFF_XY (n_ebfem_bxyz_mpi.f90:769-784): cell centres, ii = (j-1)*ny + i;
+  // dx = (xmax - xmin)/float(nx) divides by a default-real count
+  const double dx = (xmax - xmin) / (double)(float)nx, dy = (ymax - ymin) / (double)(float)ny;
+  for (int j = 1; j <= nx; ++j)
+    for (int i = 1; i <= ny; ++i) {
+      const long ii = (long)(j - 1) * ny + i - 1;
+      xyz[3 * ii] = (j - 1) * dx + xmin + dx / 2.0;
+      xyz[3 * ii + 1] = (i - 1) * dy + ymin + dy / 2.0;
+      xyz[3 * ii + 2] = z;
+    }
+  return AFEM_OK;
 }
 
 int afem_set_system(afem_ctx* c, int n, const int32_t* INU, const int32_t* IAU, const int32_t* INL,

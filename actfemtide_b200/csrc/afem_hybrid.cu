@@ -161,17 +161,30 @@ void hybrid_prepare(afem_ctx* c) {
     exclusive_scan(len.p, h->rowptr.p, node, s, &nnz);
     h->nnz = nnz;
     h->col.alloc(nnz);
+    AFEM_CUDA(cudaMemsetAsync(h->col.p, 0xff, sizeof(int32_t) * nnz, s));  // -1: a row left unwritten shows
     h->diagpos.alloc(node);
     k_node_rows<<<nblk(node, 128), 128, 0, s>>>(c->line.p, node, h->nptr.p, h->nlist.p, h->rowptr.p, h->col.p,
                                                  h->diagpos.p, c->status.p);
     count_launch();
     check_status(c, "hybrid preconditioner: more than 128 edges meet at one node");
-    // multicolour order of the node graph (host greedy colouring, as for the edges)
-    std::vector<int32_t> rp(node + 1), cl(nnz), pm(node), cptr(256);
+    std::vector<int32_t> rp(node + 1), cl(nnz), pm(node), cptr(256), dp(node);
     std::vector<uint8_t> color(node);
     h->rowptr.download(rp.data(), node + 1, s);
     h->col.download(cl.data(), nnz, s);
     AFEM_CUDA(cudaStreamSynchronize(s));
+    // every row: ascending node ids within 0..node-1, holding its own node once
+    for (int a = 0; a < node; ++a) {
+      int d = -1;
+      for (int k = rp[a]; k < rp[a + 1]; ++k) {
+        AFEM_REQUIRE(cl[k] >= 0 && cl[k] < node && (k == rp[a] || cl[k] > cl[k - 1]), AFEM_EPATTERN,
+                     "hybrid preconditioner: the node graph row of node " + std::to_string(a) + " is malformed");
+        if (cl[k] == a) d = k;
+      }
+      AFEM_REQUIRE(d >= 0, AFEM_EPATTERN, "hybrid preconditioner: node " + std::to_string(a) + " misses its diagonal");
+      dp[a] = d;
+    }
+    h->diagpos.upload(dp.data(), node, s);
+    // multicolour order of the node graph (host greedy colouring, as for the edges)
     const int nc = compute_coloring(node, rp.data(), cl.data(), color.data(), pm.data(), cptr.data(), 255);
     AFEM_REQUIRE(nc > 0, AFEM_EPATTERN, "hybrid preconditioner: more than 255 colours in the node graph");
     h->ncolors = nc;

@@ -97,6 +97,17 @@ struct SourceSet {
 
 struct CtlInfo;  // drop-in driver state (afem_io.cpp)
 
+// Gridded element list of gengridforlist / classifyelement2grd
+// (m_mesh_type.f90:56-202): nx*ny*nz boxes over the node extent +-1 km,
+// tetrahedra sorted by the box of their centroid (SORT_INDEX heap order).
+struct GridList {
+  int nx = 300, ny = 300, nz = 50;
+  DBuf<double> xg, yg, zg;       // box boundaries, nx+1 / ny+1 / nz+1 values
+  DBuf<int32_t> stack;           // 0..nx*ny*nz: tetrahedra with box <= b
+  DBuf<int32_t> ordered;         // ntet, 0-based tetrahedra in list order
+  bool ready = false;
+};
+
 // Per-kernel device time accumulated with CUDA events while profiling is on.
 struct ProfEntry {
   std::string name;
@@ -118,7 +129,12 @@ struct Profile {
 // there; each launch of the graph counts its kernel nodes instead.
 extern std::atomic<long> g_launches;
 extern thread_local int g_capturing;
+// Every launch site calls this right after the launch, so a launch that the
+// runtime refused (bad configuration, too many resources) is reported at once
+// instead of leaving its outputs unwritten.
 inline void count_launch(long n = 1) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw Error{AFEM_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e)};
   if (!g_capturing) g_launches.fetch_add(n, std::memory_order_relaxed);
 }
 
@@ -171,6 +187,11 @@ struct afem_ctx {
   afem::DBuf<int32_t> perm_mc;  // nline
   afem::DBuf<int32_t> color_ptr;// ncolors + 1
   int ncolors = 0;
+  // the same rows in colour order, split: entries of earlier colours (mc_l*) and of
+  // later colours (mc_u*); *src = index of the entry in the CSR, *km the values
+  afem::DBuf<int32_t> mc_lptr, mc_lcol, mc_lsrc, mc_uptr, mc_ucol, mc_usrc;
+  afem::DBuf<double2> mc_lkm, mc_ukm;
+  long mc_vals_gen = -1;        // assembly generation of mc_lkm / mc_ukm
   bool schedule_ready = false;
 
   // values: A(omega) = K + i*omega*M, stored interleaved (K_k, M_k)
@@ -197,6 +218,7 @@ struct afem_ctx {
   afem::SolverWork* work = nullptr;
   afem::MpnnState* mpnn = nullptr;
   afem::HybridState* hyb = nullptr;
+  afem::GridList* grid = nullptr;   // element locator of the plan-view sites
   int last_learned_its = 0;  // iterations the last solve ran with the learned preconditioner
   afem::CtlInfo* ctl = nullptr;
 
@@ -260,7 +282,11 @@ void jacobian_device(afem_ctx* c, double freq, const double* x_host, int nadj, d
 // afem_sites.cu
 void site_coeffs_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item, double* val_e, double* val_f,
                         int32_t* iele);
-void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out);
+void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out, bool grid = false);
+void site_coeffs_grid_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item, double* val_e,
+                             double* val_f, int32_t* iele);
+void sort_index_heap(int n, int32_t* na, double* ra);  // SORT_INDEX (sort_index.f90:13-56)
+void grid_destroy(afem_ctx* c);
 
 // status helpers
 void reset_status(afem_ctx* c);

@@ -425,6 +425,41 @@ void build_schedule(afem_ctx* c) {
   c->color.upload(color.data(), n, s);
   c->perm_mc.upload(pm.data(), n, s);
   c->color_ptr.upload(cptr.data(), nc + 1, s);
+  // colour-ordered split rows for the multicolour sweeps: position p holds row
+  // perm[p]; its entries of earlier colours (the forward sweep's) and of later
+  // colours (the backward sweep's), each with the index of the entry in the CSR
+  {
+    std::vector<int32_t> lptr(n + 1), uptr(n + 1);
+    lptr[0] = uptr[0] = 0;
+    for (int p = 0; p < n; ++p) {
+      const int i = pm[p];
+      int nl = 0, nu = 0;
+      for (int k = rp[i]; k < rp[i + 1]; ++k) {
+        const int j = cl[k];
+        if (color[j] < color[i]) ++nl;
+        else if (color[j] > color[i]) ++nu;
+      }
+      lptr[p + 1] = lptr[p] + nl;
+      uptr[p + 1] = uptr[p] + nu;
+    }
+    std::vector<int32_t> lcol(lptr[n]), lsrc(lptr[n]), ucol(uptr[n]), usrc(uptr[n]);
+    for (int p = 0; p < n; ++p) {
+      const int i = pm[p];
+      int a = lptr[p], b = uptr[p];
+      for (int k = rp[i]; k < rp[i + 1]; ++k) {
+        const int j = cl[k];
+        if (color[j] < color[i]) { lcol[a] = j; lsrc[a++] = k; }
+        else if (color[j] > color[i]) { ucol[b] = j; usrc[b++] = k; }
+      }
+    }
+    c->mc_lptr.upload(lptr.data(), n + 1, s);
+    c->mc_lcol.upload(lcol.data(), lcol.size(), s);
+    c->mc_lsrc.upload(lsrc.data(), lsrc.size(), s);
+    c->mc_uptr.upload(uptr.data(), n + 1, s);
+    c->mc_ucol.upload(ucol.data(), ucol.size(), s);
+    c->mc_usrc.upload(usrc.data(), usrc.size(), s);
+    c->mc_vals_gen = -1;
+  }
   AFEM_CUDA(cudaStreamSynchronize(s));
   c->schedule_ready = true;
 }

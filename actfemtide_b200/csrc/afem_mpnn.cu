@@ -380,7 +380,8 @@ __global__ void __launch_bounds__(128)
   __syncthreads();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   // dc
-  for (int k = threadIdx.x; k < ROWS * H; k += blockDim.x) atomicAdd(&csum[k % H], __bfloat162float(dys[k]));
+  for (int k = threadIdx.x; k < ROWS * H; k += blockDim.x)
+    atomicAdd(&csum[k % H], __bfloat162float(dys[(k / H) * DS + (k % H)]));  // the tile's rows are padded to DS
   // ---- dX (rows 16w.. x XW) = dY (16 x H) * W^T: B[k=j][n=m] = W[m][j] -> [n][k] = wsm rows
   {
     const unsigned* A = reinterpret_cast<const unsigned*>(dys);

@@ -10,6 +10,8 @@
 // coordinates are all >= 0; on the device every tetrahedron is tested in
 // parallel and the smallest qualifying id wins (atomicMin).  Compiled with
 // -fmad=false so the >= 0 decisions round exactly like the serial code.
+#include <algorithm>
+
 #include "afem_internal.h"
 
 namespace afem {
@@ -70,6 +72,72 @@ __global__ void k_find(const double* __restrict__ xyz, const int32_t* __restrict
       atomicMin(best + s, (int)t);
       break;
     }
+  }
+}
+
+// FINDELEWITHGRID (m_mesh_type.f90:204-277): the site's box, then growing
+// shells of boxes (iside = 0, 1, ...; z outer, y, x inner; the boxes of the
+// previous shells skipped), each box's tetrahedra in list order; the first
+// tetrahedron with all barycentrics >= 0 wins (FINDELEMENT, :739-790).  One
+// warp per site: boxes are visited in order, a box's tetrahedra 32 at a time,
+// and the lowest lane that holds the site wins, which is the list order.
+constexpr int GRID_SIDE_MAX = 64;  // shells searched before a site is declared outside the mesh
+
+__device__ __forceinline__ int grid_box(const double* g, int n, double v) {
+  // the box i (1-based) with g(i) < v <= g(i+1): the number of boundaries below v
+  int lo = 0, hi = n + 1;  // count of g[0..n] that are < v
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (g[mid] < v) lo = mid + 1;
+    else hi = mid;
+  }
+  return (lo >= 1 && lo <= n) ? lo : 0;
+}
+
+__global__ void k_find_grid(const double* __restrict__ xyz, const int32_t* __restrict__ n4,
+                            const double* __restrict__ xg, const double* __restrict__ yg,
+                            const double* __restrict__ zg, int nx, int ny, int nz, const int32_t* __restrict__ stack,
+                            const int32_t* __restrict__ ordered, const double* __restrict__ obs, int nobs,
+                            int* __restrict__ best) {
+  const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (s >= nobs) return;
+  const V3 x3{obs[3 * s], obs[3 * s + 1], obs[3 * s + 2]};
+  const int ix = grid_box(xg, nx, x3.x), iy = grid_box(yg, ny, x3.y), iz = grid_box(zg, nz, x3.z);
+  if (!ix || !iy || !iz) return;  // outside the grid: left not found
+  for (int iside = 0; iside <= GRID_SIDE_MAX; ++iside) {
+    for (int l = max(iz - iside, 1); l <= min(iz + iside, nz); ++l)
+      for (int k = max(iy - iside, 1); k <= min(iy + iside, ny); ++k)
+        for (int j = max(ix - iside, 1); j <= min(ix + iside, nx); ++j) {
+          if (iz - (iside - 1) <= l && l <= iz + (iside - 1) && iy - (iside - 1) <= k && k <= iy + (iside - 1) &&
+              ix - (iside - 1) <= j && j <= ix + (iside - 1))
+            continue;  // searched in an inner shell
+          const long b = (long)nx * ny * (l - 1) + (long)nx * (k - 1) + j;
+          const int e0 = stack[b - 1], e1 = stack[b];
+          for (int base = e0; base < e1; base += 32) {
+            const int e = base + lane;
+            bool ok = false;
+            int t = 0;
+            if (e < e1) {
+              t = ordered[e];
+              V3 el[4];
+              load_tet(xyz, n4, t, el);
+              double a[4];
+              nodebasis(el, x3, a);
+              ok = a[0] >= 0.0 && a[1] >= 0.0 && a[2] >= 0.0 && a[3] >= 0.0;
+            }
+            const unsigned hit = __ballot_sync(0xffffffffu, ok);
+            if (hit) {
+              const int w = __ffs(hit) - 1;
+              const int tw = __shfl_sync(0xffffffffu, t, w);
+              if (lane == 0) best[s] = tw;
+              return;
+            }
+          }
+        }
+    if (iz - iside <= 1 && iz + iside >= nz && iy - iside <= 1 && iy + iside >= ny && ix - iside <= 1 &&
+        ix + iside >= nx)
+      return;  // every box searched
   }
 }
 
@@ -171,10 +239,116 @@ __global__ void k_eval(const double2* __restrict__ X, int nline, int nsys, const
 
 }  // namespace
 
+// SORT_INDEX (src/solver/sort_index.f90:13-56): heapsort of ra (ascending)
+// carrying na along, after Numerical Recipes' SORT.  Equal keys leave in the
+// order this heapsort produces, which the grid list inherits; hence the same
+// hire / retire steps.
+void sort_index_heap(int n, int32_t* na, double* ra) {
+  if (n < 2) return;
+  // 1-based views
+  int32_t* NA = na - 1;
+  double* RA = ra - 1;
+  int l = n / 2 + 1, ir = n;
+  for (;;) {
+    double rra;
+    int32_t iia;
+    if (l > 1) {
+      --l;
+      rra = RA[l];
+      iia = NA[l];
+    } else {
+      rra = RA[ir];
+      iia = NA[ir];
+      RA[ir] = RA[1];
+      NA[ir] = NA[1];
+      if (--ir == 1) {
+        RA[1] = rra;
+        NA[1] = iia;
+        return;
+      }
+    }
+    int i = l, j = l + l;
+    while (j <= ir) {
+      if (j < ir && RA[j] < RA[j + 1]) ++j;
+      if (rra < RA[j]) {
+        RA[i] = RA[j];
+        NA[i] = NA[j];
+        i = j;
+        j += j;
+      } else {
+        j = ir + 1;
+      }
+    }
+    RA[i] = rra;
+    NA[i] = iia;
+  }
+}
+
 namespace {
 
+// gengridforlist + classifyelement2grd (m_mesh_type.f90:73-202) on the host:
+// the grid over the node extent (GENXYZMINMAX) widened by 1 km, each
+// tetrahedron's box by its centroid, the list sorted by box with SORT_INDEX.
+void build_grid(afem_ctx* c) {
+  if (!c->grid) c->grid = new GridList();
+  GridList* g = c->grid;
+  if (g->ready) return;
+  cudaStream_t s = c->stream;
+  const int node = c->node, ntet = c->ntet;
+  std::vector<double> xyz(3L * node);
+  std::vector<int32_t> n4(4L * ntet);
+  c->xyz.download(xyz.data(), xyz.size(), s);
+  c->n4.download(n4.data(), n4.size(), s);
+  AFEM_CUDA(cudaStreamSynchronize(s));
+  double mn[3] = {xyz[0], xyz[1], xyz[2]}, mx[3] = {xyz[0], xyz[1], xyz[2]};
+  for (int i = 0; i < node; ++i)
+    for (int k = 0; k < 3; ++k) {
+      mn[k] = std::min(mn[k], xyz[3L * i + k]);
+      mx[k] = std::max(mx[k], xyz[3L * i + k]);
+    }
+  const int nn[3] = {g->nx, g->ny, g->nz};
+  std::vector<double> grd[3];
+  for (int k = 0; k < 3; ++k) {
+    const double lo = mn[k] - 1.0, hi = mx[k] + 1.0;
+    grd[k].resize(nn[k] + 1);
+    for (int i = 0; i <= nn[k]; ++i) grd[k][i] = ((double)i * (hi - lo)) / (double)nn[k] + lo;
+  }
+  auto box = [&](int k, double v) {
+    const std::vector<double>& gr = grd[k];
+    const int pos = (int)(std::lower_bound(gr.begin(), gr.end(), v) - gr.begin());  // count of gr < v
+    return (pos >= 1 && pos <= nn[k]) ? pos : 0;
+  };
+  std::vector<double> order(ntet);
+  std::vector<int32_t> index(ntet);
+  const long nxy = (long)g->nx * g->ny;
+  for (int t = 0; t < ntet; ++t) {
+    double cen[3] = {0.0, 0.0, 0.0};
+    for (int j = 0; j < 4; ++j) {
+      const double* P = &xyz[3L * (n4[4L * t + j] - 1)];
+      for (int k = 0; k < 3; ++k) cen[k] = cen[k] + P[k] / 4.0;
+    }
+    const int ix = box(0, cen[0]), iy = box(1, cen[1]), iz = box(2, cen[2]);
+    AFEM_REQUIRE(ix && iy && iz, AFEM_EINVAL, "grid list: a centroid lies outside the node extent");
+    order[t] = (double)(nxy * (iz - 1) + (long)g->nx * (iy - 1) + ix);
+    index[t] = t + 1;
+  }
+  sort_index_heap(ntet, index.data(), order.data());
+  const long nbox = nxy * g->nz;
+  std::vector<int32_t> stack(nbox + 1, 0);
+  for (int t = 0; t < ntet; ++t) stack[(long)order[t]] += 1;
+  for (long b = 1; b <= nbox; ++b) stack[b] += stack[b - 1];
+  for (int t = 0; t < ntet; ++t) index[t] -= 1;
+  g->xg.upload(grd[0].data(), grd[0].size(), s);
+  g->yg.upload(grd[1].data(), grd[1].size(), s);
+  g->zg.upload(grd[2].data(), grd[2].size(), s);
+  g->stack.upload(stack.data(), stack.size(), s);
+  g->ordered.upload(index.data(), index.size(), s);
+  AFEM_CUDA(cudaStreamSynchronize(s));
+  g->ready = true;
+}
+
 void site_coeffs_range(afem_ctx* c, int nobs, const double* xyz_obs, long t0, long t1, int32_t* item, double* val_e,
-                       double* val_f, int32_t* iele) {
+                       double* val_f, int32_t* iele, bool grid_search = false) {
   cudaStream_t s = c->stream;
   DBuf<double> obs;
   obs.upload(xyz_obs, 3L * nobs, s);
@@ -182,9 +356,17 @@ void site_coeffs_range(afem_ctx* c, int nobs, const double* xyz_obs, long t0, lo
   best.alloc(nobs);
   std::vector<int> init(nobs, 0x7fffffff);
   AFEM_CUDA(cudaMemcpyAsync(best.p, init.data(), sizeof(int) * nobs, cudaMemcpyHostToDevice, s));
-  dim3 grid(std::max(1, std::min(2 * c->num_sms, (int)((t1 - t0 + 255) / 256))), nobs);
-  k_find<<<grid, 256, 0, s>>>(c->xyz.p, c->n4.p, t0, t1, obs.p, nobs, best.p);
-  count_launch();
+  if (grid_search) {
+    build_grid(c);
+    GridList* g = c->grid;
+    k_find_grid<<<(nobs * 32 + 127) / 128, 128, 0, s>>>(c->xyz.p, c->n4.p, g->xg.p, g->yg.p, g->zg.p, g->nx, g->ny,
+                                                         g->nz, g->stack.p, g->ordered.p, obs.p, nobs, best.p);
+    count_launch();
+  } else {
+    dim3 grid(std::max(1, std::min(2 * c->num_sms, (int)((t1 - t0 + 255) / 256))), nobs);
+    k_find<<<grid, 256, 0, s>>>(c->xyz.p, c->n4.p, t0, t1, obs.p, nobs, best.p);
+    count_launch();
+  }
   DBuf<int32_t> ditem;
   DBuf<double> dve, dvf;
   ditem.alloc(6L * nobs);
@@ -213,10 +395,21 @@ void site_coeffs_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* i
   site_coeffs_range(c, nobs, xyz_obs, 0, c->ntet, item, val_e, val_f, iele);
 }
 
-void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out) {
+void site_coeffs_grid_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item, double* val_e,
+                             double* val_f, int32_t* iele) {
+  site_coeffs_range(c, nobs, xyz_obs, 0, c->ntet, item, val_e, val_f, iele, true);
+}
+
+void grid_destroy(afem_ctx* c) {
+  delete c->grid;
+  c->grid = nullptr;
+}
+
+void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out, bool grid) {
   AFEM_REQUIRE(c->nsys > 0 && c->X.p, AFEM_ESTATE, "sites: no solution");
   cudaStream_t s = c->stream;
   if (c->sol_packed) {
+    AFEM_REQUIRE(!grid, AFEM_EINVAL, "sites: the grid search covers one mesh, not a packed batch");
     // packed batch: system k is mesh k; its sites are searched in its own tetrahedra
     AFEM_REQUIRE((int)c->seg_tet_ptr.size() == c->nsys + 1, AFEM_ESTATE, "sites: the packed meshes changed");
     const double pi = 4.0 * std::atan(1.0);
@@ -246,7 +439,7 @@ void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out) {
   }
   std::vector<int32_t> item(6L * nobs);
   std::vector<double> ve(18L * nobs), vf(18L * nobs);
-  site_coeffs_device(c, nobs, xyz_obs, item.data(), ve.data(), vf.data(), nullptr);
+  site_coeffs_range(c, nobs, xyz_obs, 0, c->ntet, item.data(), ve.data(), vf.data(), nullptr, grid);
   DBuf<int32_t> ditem;
   DBuf<double> dve, dvf, dom;
   ditem.upload(item.data(), item.size(), s);

@@ -81,6 +81,7 @@ struct SolverWork {
   DBuf<double2> r, z, p, q, dd;     // FP64 inner vectors
   DBuf<float2> rf, zf, pf, qf, ddf; // FP32 inner vectors
   DBuf<float2> kmf;                 // FP32 copy of (K, M)
+  DBuf<float2> mc_lkmf, mc_ukmf;    // FP32 copies of the colour-ordered split rows
   DBuf<double2> rprev;              // flexible COCG: previous residual (FP64 inner)
   DBuf<float2> rprevf;              // flexible COCG: previous residual (FP32 inner)
   DBuf<double> rms;                 // per-system rms(r) for the learned preconditioner
@@ -364,44 +365,59 @@ __global__ void __launch_bounds__(256)
 // SSOR of the colour-permuted matrix: rows of one colour share no nonzero, so
 // the forward sweep updates colour 0, 1, ... in turn (each a parallel pass over
 // its rows, summing only entries of earlier colours) and the backward sweep
-// goes through the colours in reverse.  One persistent cooperative kernel per
-// sweep with a grid barrier between colours; no flags, no waits.
+// goes through the colours in reverse.  The rows are stored a second time in
+// colour order and split into their earlier-colour part (forward) and their
+// later-colour part (backward), so a sweep reads half the entries, row data is
+// contiguous by position and no entry needs a colour test.  RPW rows share a
+// warp (lane = sub * 32/RPW + g * NS + s), which keeps several rows' loads in
+// flight per warp.  One persistent cooperative kernel per sweep with a grid
+// barrier between colours; no flags, no waits.
+template <int NS>
+struct McShape {
+  static constexpr int RPW = NS <= 8 ? 4 : 2;  // rows per warp
+  static constexpr int LPR = 32 / RPW;         // lanes per row
+  static constexpr int G = LPR / NS;           // entry groups per row
+};
+
 template <class T, int NS, bool SEG = false>
 __global__ void __launch_bounds__(256)
-    k_fwd_mc(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const typename Cx<T>::V* __restrict__ km,
+    k_fwd_mc(const int32_t* __restrict__ lptr, const int32_t* __restrict__ lcol, const typename Cx<T>::V* __restrict__ lkm,
              int n, typename Cx<T>::V* __restrict__ r, typename Cx<T>::V* __restrict__ y,
              const typename Cx<T>::V* __restrict__ p, const typename Cx<T>::V* __restrict__ q, double2* __restrict__ x,
-             const typename Cx<T>::V* __restrict__ dd, const uint8_t* __restrict__ color,
-             const int32_t* __restrict__ perm, const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc,
-             Ctrl* __restrict__ ctrl, double* __restrict__ part, const uint8_t* __restrict__ seg) {
+             const typename Cx<T>::V* __restrict__ dd, const int32_t* __restrict__ perm,
+             const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl,
+             double* __restrict__ part, const uint8_t* __restrict__ seg) {
   using V = typename Cx<T>::V;
+  using S = McShape<NS>;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;  // uniform over the grid
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
-  constexpr int G = 32 / NS;
   const bool update = ctrl->iter > 0;
-  const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
+  const int lane = threadIdx.x & 31, sub = lane / S::LPR, s = lane % NS, g = (lane % S::LPR) / NS;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int slot = (threadIdx.x >> 5) * S::RPW + sub;
   double om = sc[s].omega;
   double2 al = sc[s].alpha;
   bool act = sc[s].active;
   double rr = 0.0;
   double (*red)[MAX_SYS][1] = nullptr;
-  if constexpr (SEG) red = seg_sums<8, 1>();
+  if constexpr (SEG) red = seg_sums<8 * S::RPW, 1>();
   for (int c = 0; c < ncolors; ++c) {
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    for (int pos = p0 + warp; pos < p1; pos += nwarps) {
-      const int row = __ldg(perm + pos);
+    for (int pos0 = p0 + warp * S::RPW; pos0 < p1; pos0 += nwarps * S::RPW) {
+      const int pos = pos0 + sub;
+      const bool live = pos < p1;
+      const int row = live ? __ldg(perm + pos) : 0;
       int sid = s;
       if constexpr (SEG) {
-        sid = __ldg(seg + row);
+        sid = live ? (int)__ldg(seg + row) : 0;
         om = sc[sid].omega;
         al = sc[sid].alpha;
         act = sc[sid].active;
       }
-      V ri = r[(long)row * NS + s];
-      if (update && act && g == 0) {
+      V ri = live ? r[(long)row * NS + s] : Cx<T>::make(0, 0);
+      if (live && update && act && g == 0) {
         const V qi = q[(long)row * NS + s], pi = p[(long)row * NS + s];
         ri = Cx<T>::make((T)((double)ri.x - (al.x * (double)qi.x - al.y * (double)qi.y)),
                          (T)((double)ri.y - (al.x * (double)qi.y + al.y * (double)qi.x)));
@@ -411,22 +427,27 @@ __global__ void __launch_bounds__(256)
         xi.y += al.x * (double)pi.y + al.y * (double)pi.x;
         x[(long)row * NS + s] = xi;
       }
-      if (g == 0) {
+      if (live && g == 0) {
         const double v = (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
-        if constexpr (SEG) red[threadIdx.x >> 5][sid][0] += v;
+        if constexpr (SEG) red[slot][sid][0] += v;
         else rr += v;
       }
       T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
-      for (int k = rowptr[row] + g; k < rowptr[row + 1]; k += G) {
-        const int j = __ldg(col + k);
-        if (__ldg(color + j) >= c) continue;
-        const V a = km[k];
-        const V yj = ldcg(y + (long)j * NS + s);
-        t1x += a.x * yj.x; t1y += a.x * yj.y;
-        t2x += a.y * yj.x; t2y += a.y * yj.y;
+      if (live) {
+        for (int k = __ldg(lptr + pos) + g; k < __ldg(lptr + pos + 1); k += S::G) {
+          const int j = __ldg(lcol + k);
+          const V a = lkm[k];
+          const V yj = ldcg(y + (long)j * NS + s);
+          t1x += a.x * yj.x; t1y += a.x * yj.y;
+          t2x += a.y * yj.x; t2y += a.y * yj.y;
+        }
       }
-      group_reduce<T, NS>(t1x, t1y, t2x, t2y);
-      if (g == 0) {
+#pragma unroll
+      for (int m = NS; m < S::LPR; m <<= 1) {
+        t1x += shfl_xor(t1x, m); t1y += shfl_xor(t1y, m);
+        t2x += shfl_xor(t2x, m); t2y += shfl_xor(t2y, m);
+      }
+      if (live && g == 0) {
         const T o = (T)om;
         const T wx = ri.x - (t1x - o * t2y), wy = ri.y - (t1y + o * t2x);
         const V d = dd[(long)row * NS + s];
@@ -436,8 +457,10 @@ __global__ void __launch_bounds__(256)
     grid.sync();
   }
   if constexpr (SEG) {
-    seg_partials<8, 1>(red, part);
+    seg_partials<8 * S::RPW, 1>(red, part);
   } else {
+#pragma unroll
+    for (int m = S::LPR; m < 32; m <<= 1) rr += __shfl_xor_sync(0xffffffffu, rr, m);
     double v[1] = {rr};
     block_partials<NS, 1>(v, part);
   }
@@ -445,43 +468,51 @@ __global__ void __launch_bounds__(256)
 
 template <class T, int NS, bool SEG = false>
 __global__ void __launch_bounds__(256)
-    k_bwd_mc(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const typename Cx<T>::V* __restrict__ km,
+    k_bwd_mc(const int32_t* __restrict__ uptr, const int32_t* __restrict__ ucol, const typename Cx<T>::V* __restrict__ ukm,
              int n, const typename Cx<T>::V* __restrict__ r, typename Cx<T>::V* __restrict__ z,
-             const typename Cx<T>::V* __restrict__ dd, const uint8_t* __restrict__ color,
-             const int32_t* __restrict__ perm, const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc,
-             Ctrl* __restrict__ ctrl, double* __restrict__ part, const uint8_t* __restrict__ seg) {
+             const typename Cx<T>::V* __restrict__ dd, const int32_t* __restrict__ perm,
+             const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl,
+             double* __restrict__ part, const uint8_t* __restrict__ seg) {
   using V = typename Cx<T>::V;
+  using S = McShape<NS>;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
-  constexpr int G = 32 / NS;
-  const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
+  const int lane = threadIdx.x & 31, sub = lane / S::LPR, s = lane % NS, g = (lane % S::LPR) / NS;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int slot = (threadIdx.x >> 5) * S::RPW + sub;
   double om = sc[s].omega;
   double rx = 0.0, ry = 0.0;
   double (*red)[MAX_SYS][4] = nullptr;
-  if constexpr (SEG) red = seg_sums<8, 4>();
+  if constexpr (SEG) red = seg_sums<8 * S::RPW, 4>();
   for (int c = ncolors - 1; c >= 0; --c) {
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    for (int pos = p0 + warp; pos < p1; pos += nwarps) {
-      const int row = __ldg(perm + pos);
+    for (int pos0 = p0 + warp * S::RPW; pos0 < p1; pos0 += nwarps * S::RPW) {
+      const int pos = pos0 + sub;
+      const bool live = pos < p1;
+      const int row = live ? __ldg(perm + pos) : 0;
       int sid = s;
       if constexpr (SEG) {
-        sid = __ldg(seg + row);
+        sid = live ? (int)__ldg(seg + row) : 0;
         om = sc[sid].omega;
       }
       T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
-      for (int k = rowptr[row] + g; k < rowptr[row + 1]; k += G) {
-        const int j = __ldg(col + k);
-        if (__ldg(color + j) <= c) continue;
-        const V a = km[k];
-        const V zj = ldcg(z + (long)j * NS + s);
-        t1x += a.x * zj.x; t1y += a.x * zj.y;
-        t2x += a.y * zj.x; t2y += a.y * zj.y;
+      if (live) {
+        for (int k = __ldg(uptr + pos) + g; k < __ldg(uptr + pos + 1); k += S::G) {
+          const int j = __ldg(ucol + k);
+          const V a = ukm[k];
+          const V zj = ldcg(z + (long)j * NS + s);
+          t1x += a.x * zj.x; t1y += a.x * zj.y;
+          t2x += a.y * zj.x; t2y += a.y * zj.y;
+        }
       }
-      group_reduce<T, NS>(t1x, t1y, t2x, t2y);
-      if (g == 0) {
+#pragma unroll
+      for (int m = NS; m < S::LPR; m <<= 1) {
+        t1x += shfl_xor(t1x, m); t1y += shfl_xor(t1y, m);
+        t2x += shfl_xor(t2x, m); t2y += shfl_xor(t2y, m);
+      }
+      if (live && g == 0) {
         V zi = z[(long)row * NS + s];
         const T o = (T)om;
         const T swx = t1x - o * t2y, swy = t1y + o * t2x;
@@ -492,8 +523,8 @@ __global__ void __launch_bounds__(256)
         const double ex = (double)ri.x * (double)zi.x - (double)ri.y * (double)zi.y;
         const double ey = (double)ri.x * (double)zi.y + (double)ri.y * (double)zi.x;
         if constexpr (SEG) {
-          red[threadIdx.x >> 5][sid][0] += ex;
-          red[threadIdx.x >> 5][sid][1] += ey;
+          red[slot][sid][0] += ex;
+          red[slot][sid][1] += ey;
         } else {
           rx += ex;
           ry += ey;
@@ -503,10 +534,26 @@ __global__ void __launch_bounds__(256)
     grid.sync();
   }
   if constexpr (SEG) {
-    seg_partials<8, 4>(red, part);
+    seg_partials<8 * S::RPW, 4>(red, part);
   } else {
+#pragma unroll
+    for (int m = S::LPR; m < 32; m <<= 1) {
+      rx += __shfl_xor_sync(0xffffffffu, rx, m);
+      ry += __shfl_xor_sync(0xffffffffu, ry, m);
+    }
     double v[4] = {rx, ry, 0.0, 0.0};
     block_partials<NS, 4>(v, part);
+  }
+}
+
+// values of the colour-ordered split rows: out[k] = km[src[k]]
+template <class Vd>
+__global__ void k_gather_entries(const double2* __restrict__ km, const int32_t* __restrict__ src, long cnt,
+                                 Vd* __restrict__ out) {
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < cnt; k += (long)gridDim.x * blockDim.x) {
+    const double2 v = km[__ldg(src + k)];
+    if constexpr (sizeof(Vd) == 16) out[k] = v;
+    else out[k] = make_float2((float)v.x, (float)v.y);
   }
 }
 
@@ -1069,6 +1116,8 @@ struct Inner<double, NS> {
   static V* HY(SolverWork* w) { return w->hy.p; }
   static V* HDD(SolverWork* w) { return w->hdd.p; }
   static const V* HKM(afem_ctx* c) { return c->hyb->km.p; }
+  static const V* LKM(afem_ctx* c, SolverWork*) { return c->mc_lkm.p; }
+  static const V* UKM(afem_ctx* c, SolverWork*) { return c->mc_ukm.p; }
 };
 template <int NS>
 struct Inner<float, NS> {
@@ -1084,6 +1133,8 @@ struct Inner<float, NS> {
   static V* HY(SolverWork* w) { return w->hyf.p; }
   static V* HDD(SolverWork* w) { return w->hddf.p; }
   static const V* HKM(afem_ctx* c) { return c->hyb->kmf.p; }
+  static const V* LKM(afem_ctx*, SolverWork* w) { return w->mc_lkmf.p; }
+  static const V* UKM(afem_ctx*, SolverWork* w) { return w->mc_ukmf.p; }
 };
 
 template <class T, int NS, bool SEG>
@@ -1150,10 +1201,10 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
   const bool mc = mode == AFEM_PRECOND_SSOR_MC || hyb;  // the hybrid's edge part is the multicolour SSOR
   if (ev) AFEM_CUDA(cudaEventRecord(ev[0], s));
   if (mc)
-    launch_coop(k_fwd_mc<T, NS, SEG>, w->mc_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
-                I::KM(c, w), n, I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w), w->x.p, (const V*)I::DD(w),
-                (const uint8_t*)c->color.p, (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors,
-                w->sc.p, w->ctrl.p, w->part.p, sg);
+    launch_coop(k_fwd_mc<T, NS, SEG>, w->mc_blocks, s, (const int32_t*)c->mc_lptr.p, (const int32_t*)c->mc_lcol.p,
+                I::LKM(c, w), n, I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w), w->x.p, (const V*)I::DD(w),
+                (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p,
+                w->part.p, sg);
   else
     launch_coop(k_fwd<T, NS, SEG>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
                 (const int32_t*)c->diagpos.p, I::KM(c, w), n, I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w),
@@ -1166,10 +1217,9 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
   if (learned) mpnn_run<V>(c, NS, w->rms.p, (const V*)I::R(w), I::Z(w), &w->ctrl.p->done);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[2], s));
   if (mc)
-    launch_coop(k_bwd_mc<T, NS, SEG>, w->mc_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
-                I::KM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w), (const uint8_t*)c->color.p,
-                (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p,
-                sg);
+    launch_coop(k_bwd_mc<T, NS, SEG>, w->mc_blocks, s, (const int32_t*)c->mc_uptr.p, (const int32_t*)c->mc_ucol.p,
+                I::UKM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w), (const int32_t*)c->perm_mc.p,
+                (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p, sg);
   else
     launch_coop(k_bwd<T, NS, SEG>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
                 (const int32_t*)c->diagpos.p, I::KM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w),
@@ -1490,6 +1540,17 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     w->kmf.alloc(c->nnz);
     k_convert<float2, double2><<<c->num_sms * 8, 256, 0, s>>>(c->km.p, w->kmf.p, c->nnz);
     count_launch();
+    const long nl = (long)c->mc_lcol.n, nu = (long)c->mc_ucol.n;
+    w->mc_lkmf.alloc(nl);
+    w->mc_ukmf.alloc(nu);
+    if (nl) {
+      k_gather_entries<float2><<<c->num_sms * 8, 256, 0, s>>>(c->km.p, c->mc_lsrc.p, nl, w->mc_lkmf.p);
+      count_launch();
+    }
+    if (nu) {
+      k_gather_entries<float2><<<c->num_sms * 8, 256, 0, s>>>(c->km.p, c->mc_usrc.p, nu, w->mc_ukmf.p);
+      count_launch();
+    }
     w->kmf_valid = true;
   }
   {
@@ -1666,6 +1727,22 @@ int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, cons
                  afem_solve_stats* st, const SolveExtra* ex) {
   AFEM_REQUIRE(c->assembled, AFEM_ESTATE, "solve: system not assembled");
   build_schedule(c);
+  if (c->mc_vals_gen != c->assemble_gen) {
+    // values of the colour-ordered split rows (FP64; the FP32 copies follow with the workspace)
+    const long nl = (long)c->mc_lcol.n, nu = (long)c->mc_ucol.n;
+    c->mc_lkm.alloc(nl);
+    c->mc_ukm.alloc(nu);
+    if (nl) {
+      k_gather_entries<double2><<<c->num_sms * 8, 256, 0, c->stream>>>(c->km.p, c->mc_lsrc.p, nl, c->mc_lkm.p);
+      count_launch();
+    }
+    if (nu) {
+      k_gather_entries<double2><<<c->num_sms * 8, 256, 0, c->stream>>>(c->km.p, c->mc_usrc.p, nu, c->mc_ukm.p);
+      count_launch();
+    }
+    c->mc_vals_gen = c->assemble_gen;
+    invalidate_work(c);
+  }
   if (o->precond == AFEM_PRECOND_HYBRID) hybrid_prepare(c);
   if (c->nseg > 0) {
     AFEM_REQUIRE(nsys == c->nseg, AFEM_EINVAL, "solve: a packed batch solves one system per mesh (nsys = nseg)");

@@ -80,10 +80,14 @@ class Forward:
             line = _c(line, np.int32); n6line = _c(n6line, np.int32)
             self._check(self._L.afem_set_mesh(self.ctx, self.node, ptr(xyz), self.ntet, ptr(n4), ptr(tag), line.shape[0],
                                               ptr(line), ptr(n6line)))
-        n = C.c_int(0)
-        self._check(self._L.afem_get_lines(self.ctx, C.byref(n), None, None))
-        self.nline = n.value
+        self._sizes()
         self.row_ptr = None
+
+    def _sizes(self):
+        """Mesh sizes as the library holds them (host buffers are always sized from these)."""
+        node = C.c_int(0); ntet = C.c_int(0); nline = C.c_int(0)
+        self._check(self._L.afem_mesh_info(self.ctx, C.byref(node), C.byref(ntet), C.byref(nline)))
+        self.node, self.ntet, self.nline = node.value, ntet.value, nline.value
 
     def set_segments(self, node_ptr):
         """Declare the mesh as a packed batch of independent meshes (0-based node-range prefix)."""
@@ -116,6 +120,7 @@ class Forward:
         return self.nline if self.row_ptr is None else int(self.row_ptr[k + 1] - self.row_ptr[k])
 
     def lines(self):
+        self._sizes()
         line = np.zeros((self.nline, 2), np.int32); n6 = np.zeros((self.ntet, 6), np.int32)
         self._check(self._L.afem_get_lines(self.ctx, None, ptr(line), ptr(n6)))
         return line, n6
@@ -205,7 +210,7 @@ class Forward:
         self._check(self._L.afem_cocg13_single(self.ctx, n, len(AL), len(AU), ptr(D), ptr(AL), ptr(INL), ptr(IAL),
                                                ptr(AU), ptr(INU), ptr(IAU), ptr(B), ptr(X), precond.encode(),
                                                sigma_diag, sigma, C.byref(R), C.byref(IT), C.byref(ER), nset))
-        self.nline = n
+        self._sizes()
         self.row_ptr = None
         return dict(x=X, resid=R.value, iter=IT.value, error=ER.value)
 
@@ -285,12 +290,34 @@ class Forward:
         return x
 
     # ------------------------------------------------------------ sites
-    def sites(self, xyz_obs, nsys: int = 1):
-        """Complex (nsys, 5, nobs): bx, by, bz (B = curl A), ex, ey (E = -i omega A)."""
+    def _nsys(self, nsys):
+        k = C.c_int(0)
+        self._check(self._L.afem_solution_count(self.ctx, C.byref(k)))
+        if nsys is not None and nsys != k.value:
+            raise ValueError(f"the last solve holds {k.value} system(s), not {nsys}")
+        return k.value
+
+    def sites(self, xyz_obs, nsys=None):
+        """Complex (nsys, 5, nobs): bx, by, bz (B = curl A), ex, ey (E = -i omega A) for every solved system."""
         o = _c(xyz_obs, np.float64)
-        out = np.zeros((nsys, 5, o.shape[0]), np.complex128)
+        out = np.zeros((self._nsys(nsys), 5, o.shape[0]), np.complex128)
         self._check(self._L.afem_sites(self.ctx, o.shape[0], ptr(o), ptr(out)))
         return out
+
+    def sites_grid(self, xyz_obs, nsys=None):
+        """As sites(), with PREPOBSCOEFF_XY's grid-list element search (FINDELEWITHGRID)."""
+        o = _c(xyz_obs, np.float64)
+        out = np.zeros((self._nsys(nsys), 5, o.shape[0]), np.complex128)
+        self._check(self._L.afem_sites_grid(self.ctx, o.shape[0], ptr(o), ptr(out)))
+        return out
+
+    def site_coeffs_grid(self, xyz_obs):
+        o = _c(xyz_obs, np.float64)
+        nobs = o.shape[0]
+        item = np.zeros((nobs, 6), np.int32); ve = np.zeros((3, nobs, 6)); vf = np.zeros((3, nobs, 6))
+        iele = np.zeros(nobs, np.int32)
+        self._check(self._L.afem_site_coeffs_grid(self.ctx, nobs, ptr(o), ptr(item), ptr(ve), ptr(vf), ptr(iele)))
+        return item, ve, vf, iele
 
     def site_coeffs(self, xyz_obs):
         o = _c(xyz_obs, np.float64)
@@ -328,9 +355,7 @@ class Forward:
     # ------------------------------------------------------------ drop-in driver
     def load_ctl(self, path: str):
         self._check(self._L.afem_load_ctl(self.ctx, path.encode()))
-        n = C.c_int(0)
-        self._check(self._L.afem_get_lines(self.ctx, C.byref(n), None, None))
-        self.nline = n.value
+        self._sizes()
         self.row_ptr = None
 
     def ctl_info(self):

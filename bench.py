@@ -12,11 +12,12 @@ and seeded (no dataset exists for it).
   python bench.py --impl reference ...   # the CPU reference path (oracle restatement)
 
 Methods (preconditioner, precision, systems per step): plain = SSOR-COCG
-FP64, one system (the reference's solver on the device); plain-mc = the
-multicolour SSOR; mixed = multicolour SSOR with FP32 inner COCG under FP64
-refinement; batched / batched-mixed = 8 tidal periods x 2 source patterns =
-16 systems per solve; learned* = flexible COCG with the learned network;
-packed = 24 uneven meshes (n x n x 3n/4, n in 8..32) in one solve.
+FP64, one system (the reference's solver on the device, natural row order);
+plain-mc = the multicolour SSOR; hybrid = multicolour SSOR plus the
+gradient-space (nodal) correction; mixed = hybrid with FP32 inner COCG
+under FP64 refinement; batched / batched-mixed = 8 tidal periods x 2 source
+patterns = 16 systems per solve; learned* = flexible COCG with the learned
+network; packed = 24 uneven meshes (n x n x 3n/4, n in 8..32) in one solve.
 
 Prints ONE JSON line on rank 0.  Under torchrun every rank solves its own
 independent systems (replicas; weak scaling), the time is the max over ranks.
@@ -119,11 +120,23 @@ def dist_info():
 def kernel_bytes(name: str, n: int, nnz: int, ns: int, real_bytes: int, ntet: int = 0, nsrc: int = 1,
                  node: int = 0, nodes: int = 0) -> float:
     """Algorithmic bytes of one launch of the named kernel (values read/written once)."""
+    if "_seg" in name:
+        ns = 1  # packed batch: one system per row
     ent = 2 * real_bytes + 4          # (K, M) pair + column index per stored entry
     vec = 2 * real_bytes * ns         # one complex value per system per row
     off = (nnz - n) // 2              # strictly lower (= strictly upper) entries
-    if "_seg" in name:
-        ns = 1  # packed batch: one system per row
+    if name.startswith("cocg_fwd_sweep_mc"):
+        # colour-ordered split rows: the earlier-colour half, position pointers, row ids; vectors as below
+        return ent * off + 8 * n + n * (vec * 6 + 32 * ns)
+    if name.startswith("cocg_bwd_sweep_mc"):
+        return ent * off + 8 * n + n * vec * 5
+    if name.startswith("cocg_nodal_correction"):
+        nnz_n = node + 2 * n          # node graph: the node and its edge neighbours
+        vn = vec                      # nodal vectors have the edge vectors' width
+        gt = 4 * (node + 1) + 8 * n + n + 2 * n * vec + node * vn
+        sweeps = 2 * (2 * real_bytes * n + 5 * nnz_n + 4 * (node + 1) + 4 * node + 3 * node * vn)
+        gadd = 8 * n + n + 2 * n * vec + 3 * n * vec
+        return gt + sweeps + gadd
     if name.startswith("cocg_fwd_sweep"):
         # L entries, rowptr+diagpos, flag write; r r/w, q, p, x r/w (FP64), DD, y write, y gather
         return ent * off + 12 * n + n * (vec * 6 + 32 * ns)
@@ -145,14 +158,15 @@ def kernel_bytes(name: str, n: int, nnz: int, ns: int, real_bytes: int, ntet: in
 # ----------------------------------------------------------------------------- workloads
 METHODS = {
     # method: (preconditioner, precision, batched)
-    "plain": ("SSOR", "fp64", False),
+    "plain": ("SSOR", "fp64", False),          # the reference's COCG13_single with SSOR, natural row order
     "plain-mc": ("SSOR_MC", "fp64", False),
-    "mixed": ("SSOR_MC", "mixed", False),
-    "batched": ("SSOR_MC", "fp64", True),
-    "batched-mixed": ("SSOR_MC", "mixed", True),
+    "hybrid": ("HYBRID", "fp64", False),
+    "mixed": ("HYBRID", "mixed", False),
+    "batched": ("HYBRID", "fp64", True),
+    "batched-mixed": ("HYBRID", "mixed", True),
     "learned": ("LEARNED", "fp64", False),
     "learned-batched-mixed": ("LEARNED", "mixed", True),
-    "packed": ("SSOR_MC", "mixed", False),
+    "packed": ("HYBRID", "mixed", False),
 }
 
 
@@ -477,7 +491,7 @@ def main():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--method", default="batched-mixed", choices=sorted(METHODS))
-    p.add_argument("--precond", default=None, choices=["IC", "SSOR", "DIAG", "NONE", "LEARNED", "SSOR_MC"],
+    p.add_argument("--precond", default=None, choices=["IC", "SSOR", "DIAG", "NONE", "LEARNED", "SSOR_MC", "HYBRID"],
                    help="override the method's preconditioner")
     p.add_argument("--prof-iters", type=int, default=256,
                    help="iteration cap of the per-kernel profiling pass (outside the timed region)")

@@ -99,6 +99,10 @@ void *afem_stream(afem_ctx *ctx);
  * m_line_type.f90:120-277) is then built on the device. */
 int afem_set_mesh(afem_ctx *ctx, int node, const double *xyz, int ntet, const int32_t *n4, const int32_t *tag,
                   int nline, const int32_t *line, const int32_t *n6line);
+/* Sizes of the loaded mesh (any pointer may be NULL). */
+int afem_mesh_info(afem_ctx *ctx, int *node, int *ntet, int *nline);
+/* Systems held by the last solve (afem_sites writes 5*nobs values for each). */
+int afem_solution_count(afem_ctx *ctx, int *nsys);
 /* Number of edges and the numbering in use (line: 2*nline, n6line: 6*ntet; either may be NULL). */
 int afem_get_lines(afem_ctx *ctx, int *nline, int32_t *line, int32_t *n6line);
 
@@ -201,6 +205,23 @@ int afem_sites(afem_ctx *ctx, int nobs, const double *xyz_obs, double *out_compl
  * [(c*nobs + s)*6 + j]; iele: containing tetrahedron) for parity checks. */
 int afem_site_coeffs(afem_ctx *ctx, int nobs, const double *xyz_obs, int32_t *item, double *val_e, double *val_f,
                      int32_t *iele);
+
+/* The same with the element search of PREPOBSCOEFF_XY / CALCOEFF_LINE: FINDELEWITHGRID
+ * (m_mesh_type.f90:204-277) over the grid list of gengridforlist / classifyelement2grd
+ * (300 x 300 x 50 boxes over the node extent +-1 km, tetrahedra sorted by the box of
+ * their centroid with SORT_INDEX): the first tetrahedron holding the site in the
+ * list's search order.  Sites whose tetrahedron lies more than 64 box shells away
+ * are reported as outside the mesh (AFEM_ESITE). */
+int afem_sites_grid(afem_ctx *ctx, int nobs, const double *xyz_obs, double *out_complex);
+int afem_site_coeffs_grid(afem_ctx *ctx, int nobs, const double *xyz_obs, int32_t *item, double *val_e,
+                          double *val_f, int32_t *iele);
+/* Host only: SORT_INDEX (src/solver/sort_index.f90:13-56), the heapsort that orders the
+ * grid list: ra ascending, na carried along (equal keys in the heapsort's own order). */
+int afem_sort_index(int n, int32_t *na, double *ra);
+/* Host only: the plan-view points of PREPOBSCOEFF_XY (n_ebfem_bxyz_mpi.f90:769-784),
+ * nx*ny cell centres over [xmin,xmax]x[ymin,ymax] at depth z, point (j-1)*ny + i
+ * for x cell j and y cell i; xyz holds 3*nx*ny values. */
+int afem_xy_points(double xmin, double xmax, double ymin, double ymax, int nx, int ny, double z, double *xyz);
 
 /* ---- learned preconditioner (no counterpart in the reference) ---------------- */
 /* A message-passing network over the matrix graph (6 layers, width 48, BF16

@@ -621,6 +621,172 @@ long orc_findelement0(const double* x3, const double* xyz, long ntet, const int*
   return 0;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The coefficient rows of one site in tetrahedron t (0-based): PREPOBSCOEFF
+// :681-721 / CALCOEFF_LINE (n_ebfem_bxyz_mpi.f90:880-929) with EDGEBASISFUN /
+// FACEBASISFUN (m_fem_edge_util.f90:27-82), entries sorted by edge id.
+void coeff_rows(const double* xyz, const int* n4, const int* n6line, int nobs, int s, long t, const double* x3,
+                int* item, double* val_e, double* val_f) {
+  double e[4][3];
+  load_tet(xyz, n4, t, e);
+  V3 gn[4];
+  double vol, lam[4];
+  gradnodebasisfun(e, gn, &vol);
+  nodebasisfun(e, x3, lam);
+  double w[6][3], wf[4][3], wfe[6][3];
+  for (int i = 0; i < 6; ++i) {
+    int k = KL[i][0], l = KL[i][1];
+    for (int c = 0; c < 3; ++c) w[i][c] = lam[k - 1] * gn[l - 1].x[c] - lam[l - 1] * gn[k - 1].x[c];
+  }
+  for (int i = 0; i < 4; ++i) {
+    int l = LMN[i][0], m = LMN[i][1], n = LMN[i][2];
+    V3 o1 = outer(gn[m - 1], gn[n - 1]), o2 = outer(gn[l - 1], gn[m - 1]), o3 = outer(gn[n - 1], gn[l - 1]);
+    for (int c = 0; c < 3; ++c)
+      wf[i][c] = 2.0 * (lam[l - 1] * o1.x[c] + lam[n - 1] * o2.x[c] + lam[m - 1] * o3.x[c]);
+  }
+  for (int c = 0; c < 3; ++c)  // mul_ab (m_matrix.f90:1106-1126)
+    for (int j = 0; j < 6; ++j) {
+      double acc = 0.0;
+      for (int k = 0; k < 4; ++k) acc = acc + wf[k][c] * (CROT[k][j] * 1.0);
+      wfe[j][c] = acc;
+    }
+  double r6[6];
+  int n6[6];
+  double ce[6][3], cf[6][3];
+  for (int j = 0; j < 6; ++j) {
+    int sg = (n6line[t * 6 + j] < 0) ? -1 : 1;
+    for (int c = 0; c < 3; ++c) { ce[j][c] = w[j][c] * sg; cf[j][c] = wfe[j][c] * sg; }
+    r6[j] = std::abs(n6line[t * 6 + j]) * 1.0;
+    n6[j] = j + 1;
+  }
+  sort_index(6, n6, r6);
+  for (int j = 0; j < 6; ++j) {
+    int jj = std::abs(n6line[t * 6 + n6[j] - 1]);
+    item[s * 6 + j] = jj;
+    for (int c = 0; c < 3; ++c) {
+      val_e[((long)c * nobs + s) * 6 + j] = ce[n6[j] - 1][c];
+      val_f[((long)c * nobs + s) * 6 + j] = cf[n6[j] - 1][c];
+    }
+  }
+}
+
+// Grid list of gengridforlist + classifyelement2grd (m_mesh_type.f90:56-202).
+struct GridList {
+  int nx, ny, nz;
+  std::vector<double> xg, yg, zg;   // 1-based: xg[1..nx+1]
+  std::vector<int> stack;           // 0..nx*ny*nz
+  std::vector<int> ordered;         // 1-based tetrahedron ids, ordered[1..ntet]
+};
+
+GridList make_grid_list(const double* xyz, long node, long ntet, const int* n4) {
+  GridList g;
+  g.nx = 300; g.ny = 300; g.nz = 50;  // PREPOBSCOEFF_XY (n_ebfem_bxyz_mpi.f90:793)
+  // GENXYZMINMAX (src/src_inv_ap/n_inv_ap.f90:1175-1205)
+  double xmin = xyz[0], xmax = xyz[0], ymin = xyz[1], ymax = xyz[1], zmin = xyz[2], zmax = xyz[2];
+  for (long i = 0; i < node; ++i) {
+    xmin = std::min(xmin, xyz[3 * i]); xmax = std::max(xmax, xyz[3 * i]);
+    ymin = std::min(ymin, xyz[3 * i + 1]); ymax = std::max(ymax, xyz[3 * i + 1]);
+    zmin = std::min(zmin, xyz[3 * i + 2]); zmax = std::max(zmax, xyz[3 * i + 2]);
+  }
+  // gengridforlist (:73-107): the extent widened by the default-real literal 1.
+  xmin = xmin - 1.0; xmax = xmax + 1.0; ymin = ymin - 1.0; ymax = ymax + 1.0; zmin = zmin - 1.0; zmax = zmax + 1.0;
+  g.zg.assign(g.nz + 2, 0.0); g.yg.assign(g.ny + 2, 0.0); g.xg.assign(g.nx + 2, 0.0);
+  for (int i = 1; i <= g.nz + 1; ++i) g.zg[i] = (i - 1) * (zmax - zmin) / (double)(float)g.nz + zmin;
+  for (int i = 1; i <= g.ny + 1; ++i) g.yg[i] = (i - 1) * (ymax - ymin) / (double)(float)g.ny + ymin;
+  for (int i = 1; i <= g.nx + 1; ++i) g.xg[i] = (i - 1) * (xmax - xmin) / (double)(float)g.nx + xmin;
+  // classifyelement2grd (:110-202)
+  std::vector<double> order(ntet + 1, 0.0);  // order(0) stays 0
+  std::vector<int> index(ntet);
+  for (long ii = 1; ii <= ntet; ++ii) {
+    double x3[3] = {0.0, 0.0, 0.0};
+    for (int j = 0; j < 4; ++j)
+      for (int c = 0; c < 3; ++c) x3[c] = x3[c] + xyz[3L * (n4[(ii - 1) * 4 + j] - 1) + c] / 4.0;
+    int ix = 0, iy = 0, iz = 0;
+    for (int k = 1; k <= g.nz && !ix; ++k) {
+      if (g.zg[k] < x3[2] && x3[2] <= g.zg[k + 1]) {
+        iz = k;
+        for (int j = 1; j <= g.ny && !ix; ++j) {
+          if (g.yg[j] < x3[1] && x3[1] <= g.yg[j + 1]) {
+            iy = j;
+            for (int i = 1; i <= g.nx; ++i)
+              if (g.xg[i] < x3[0] && x3[0] <= g.xg[i + 1]) { ix = i; break; }
+          }
+        }
+      }
+    }
+    order[ii] = ((g.nx * g.ny) * (iz - 1) + g.nx * (iy - 1) + ix) * 1.0;
+    index[ii - 1] = (int)ii;
+  }
+  sort_index((int)ntet, index.data(), order.data() + 1);
+  g.ordered.assign(ntet + 1, 0);
+  for (long i = 1; i <= ntet; ++i) g.ordered[i] = index[i - 1];
+  // the stack loop as written (:170-190)
+  const long nxyz = (long)g.nx * g.ny * g.nz;
+  g.stack.assign(nxyz + 1, 0);
+  long ipre = 0, ii = 0;
+  for (ii = 0; ii <= nxyz - 1; ++ii) {
+    for (;;) {
+      if (ipre == ntet) goto done;
+      if (order[ipre] < order[ipre + 1]) {
+        g.stack[ii] = (int)ipre;
+        if (ii + 1 == (long)order[ipre + 1]) ipre = ipre + 1;
+        break;
+      } else {
+        ipre = ipre + 1;
+      }
+    }
+  }
+done:
+  for (long k = ii; k <= nxyz; ++k) g.stack[k] = (int)ntet;
+  return g;
+}
+
+// findelewithgrid (m_mesh_type.f90:204-277) + FINDELEMENT (:739-790); 1-based id or 0
+long findelewithgrid(const GridList& g, const double* xyz, const int* n4, const double* x3) {
+  int ix = 0, iy = 0, iz = 0;
+  for (int l = 1; l <= g.nz && !ix; ++l) {
+    if (g.zg[l] < x3[2] && x3[2] <= g.zg[l + 1]) {
+      iz = l;
+      for (int k = 1; k <= g.ny && !ix; ++k) {
+        if (g.yg[k] < x3[1] && x3[1] <= g.yg[k + 1]) {
+          iy = k;
+          for (int j = 1; j <= g.nx; ++j)
+            if (g.xg[j] < x3[0] && x3[0] <= g.xg[j + 1]) { ix = j; break; }
+        }
+      }
+    }
+  }
+  if (!ix) return 0;
+  std::vector<int> elist;
+  for (int iside = 0; iside <= 64; ++iside) {  // the reference grows iside without bound
+    elist.clear();
+    for (int l = std::max(iz - iside, 1); l <= std::min(iz + iside, g.nz); ++l)
+      for (int k = std::max(iy - iside, 1); k <= std::min(iy + iside, g.ny); ++k)
+        for (int j = std::max(ix - iside, 1); j <= std::min(ix + iside, g.nx); ++j) {
+          if (iz - (iside - 1) <= l && l <= iz + (iside - 1) && iy - (iside - 1) <= k && k <= iy + (iside - 1) &&
+              ix - (iside - 1) <= j && j <= ix + (iside - 1))
+            continue;
+          const long index = (long)(g.nx * g.ny) * (l - 1) + g.nx * (k - 1) + j;
+          const int num = g.stack[index] - g.stack[index - 1];
+          for (int i = 1; i <= num; ++i) elist.push_back(g.ordered[g.stack[index - 1] + i]);
+        }
+    for (int ii : elist) {
+      double e[4][3], a[4];
+      load_tet(xyz, n4, ii - 1, e);
+      nodebasisfun(e, x3, a);
+      if (a[0] >= 0.0 && a[1] >= 0.0 && a[2] >= 0.0 && a[3] >= 0.0) return ii;
+    }
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
 // PREPOBSCOEFF (n_ebfem_bxyz_mpi.f90:653-726) with EDGEBASISFUN/FACEBASISFUN
 // (m_fem_edge_util.f90:27-82): per site, 6 entries sorted by edge id (item,
 // 1-based) with edge-basis values val_e (3 comps) and face-basis*C values val_f.
@@ -634,48 +800,22 @@ long orc_prepobscoeff(const double* xyz, long ntet, const int* n4, const int* n6
     long iele = orc_findelement0(x3, xyz, ntet, n4, a4);
     if (iele == 0) return -(s + 1);
     if (iele_out) iele_out[s] = (int)iele;
-    long t = iele - 1;
-    double e[4][3];
-    load_tet(xyz, n4, t, e);
-    V3 gn[4];
-    double vol, lam[4];
-    gradnodebasisfun(e, gn, &vol);
-    nodebasisfun(e, x3, lam);
-    double w[6][3], wf[4][3], wfe[6][3];
-    for (int i = 0; i < 6; ++i) {
-      int k = KL[i][0], l = KL[i][1];
-      for (int c = 0; c < 3; ++c) w[i][c] = lam[k - 1] * gn[l - 1].x[c] - lam[l - 1] * gn[k - 1].x[c];
-    }
-    for (int i = 0; i < 4; ++i) {
-      int l = LMN[i][0], m = LMN[i][1], n = LMN[i][2];
-      V3 o1 = outer(gn[m - 1], gn[n - 1]), o2 = outer(gn[l - 1], gn[m - 1]), o3 = outer(gn[n - 1], gn[l - 1]);
-      for (int c = 0; c < 3; ++c)
-        wf[i][c] = 2.0 * (lam[l - 1] * o1.x[c] + lam[n - 1] * o2.x[c] + lam[m - 1] * o3.x[c]);
-    }
-    for (int c = 0; c < 3; ++c)  // mul_ab (m_matrix.f90:1106-1126)
-      for (int j = 0; j < 6; ++j) {
-        double acc = 0.0;
-        for (int k = 0; k < 4; ++k) acc = acc + wf[k][c] * (CROT[k][j] * 1.0);
-        wfe[j][c] = acc;
-      }
-    double r6[6];
-    int n6[6];
-    double ce[6][3], cf[6][3];
-    for (int j = 0; j < 6; ++j) {
-      int sg = (n6line[t * 6 + j] < 0) ? -1 : 1;
-      for (int c = 0; c < 3; ++c) { ce[j][c] = w[j][c] * sg; cf[j][c] = wfe[j][c] * sg; }
-      r6[j] = std::abs(n6line[t * 6 + j]) * 1.0;
-      n6[j] = j + 1;
-    }
-    sort_index(6, n6, r6);
-    for (int j = 0; j < 6; ++j) {
-      int jj = std::abs(n6line[t * 6 + n6[j] - 1]);
-      item[s * 6 + j] = jj;
-      for (int c = 0; c < 3; ++c) {
-        val_e[((long)c * nobs + s) * 6 + j] = ce[n6[j] - 1][c];
-        val_f[((long)c * nobs + s) * 6 + j] = cf[n6[j] - 1][c];
-      }
-    }
+    coeff_rows(xyz, n4, n6line, nobs, s, iele - 1, x3, item, val_e, val_f);
+  }
+  return 0;
+}
+
+// PREPOBSCOEFF_XY's element search and CALCOEFF_LINE (n_ebfem_bxyz_mpi.f90:792-929):
+// the grid list over the node extent, FINDELEWITHGRID per site, the same rows.
+long orc_prepobscoeff_grid(const double* xyz, long node, long ntet, const int* n4, const int* n6line, int nobs,
+                           const double* xyzobs, int* item, double* val_e, double* val_f, int* iele_out) {
+  GridList g = make_grid_list(xyz, node, ntet, n4);
+  for (int s = 0; s < nobs; ++s) {
+    const double* x3 = xyzobs + 3 * s;
+    long iele = findelewithgrid(g, xyz, n4, x3);
+    if (iele == 0) return -(s + 1);
+    if (iele_out) iele_out[s] = (int)iele;
+    coeff_rows(xyz, n4, n6line, nobs, s, iele - 1, x3, item, val_e, val_f);
   }
   return 0;
 }

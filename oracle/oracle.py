@@ -66,6 +66,9 @@ def lib():
         L.orc_findelement0.argtypes = [_f64p, _f64p, C.c_long, _i32p, _f64p]
         L.orc_prepobscoeff.restype = C.c_long
         L.orc_prepobscoeff.argtypes = [_f64p, C.c_long, _i32p, _i32p, C.c_int, _f64p, _i32p, _f64p, _f64p, _i32p]
+        L.orc_prepobscoeff_grid.restype = C.c_long
+        L.orc_prepobscoeff_grid.argtypes = [_f64p, C.c_long, C.c_long, _i32p, _i32p, C.c_int, _f64p, _i32p, _f64p,
+                                            _f64p, _i32p]
         L.orc_calobsebcomp.restype = None
         L.orc_calobsebcomp.argtypes = [C.c_int, C.c_int, C.c_double, _c128p, C.c_int, _i32p, _f64p, _f64p, _c128p,
                                        _f64p, _f64p]
@@ -217,6 +220,19 @@ def prepobscoeff(m, n6line, sites):
     ve = np.zeros((3, nobs, 6)); vf = np.zeros((3, nobs, 6)); iele = np.zeros(nobs, np.int32)
     rc = lib().orc_prepobscoeff(_c(m.xyz, np.float64).reshape(-1), m.ntet, _c(m.n4, np.int32), _c(n6line, np.int32), nobs,
                                 sites.reshape(-1), item, ve, vf, iele)
+    if rc != 0:
+        raise RuntimeError(f"site {-rc} is outside the mesh")
+    return item, ve, vf, iele
+
+
+def prepobscoeff_grid(m, n6line, sites):
+    """PREPOBSCOEFF_XY's search: FINDELEWITHGRID over the grid list (m_mesh_type.f90:56-277), same rows."""
+    sites = _c(sites, np.float64)
+    nobs = sites.shape[0]
+    item = np.zeros((nobs, 6), np.int32)
+    ve = np.zeros((3, nobs, 6)); vf = np.zeros((3, nobs, 6)); iele = np.zeros(nobs, np.int32)
+    rc = lib().orc_prepobscoeff_grid(_c(m.xyz, np.float64).reshape(-1), m.node, m.ntet, _c(m.n4, np.int32),
+                                     _c(n6line, np.int32), nobs, sites.reshape(-1), item, ve, vf, iele)
     if rc != 0:
         raise RuntimeError(f"site {-rc} is outside the mesh")
     return item, ve, vf, iele
