@@ -24,69 +24,6 @@ namespace {
 
 constexpr int NODE_EDGE_MAX = 128;  // edges meeting at one node
 
-// node -> incident edges; entry = edge << 1 | 1 when the node is the tail
-// line(1,e) (coefficient -1 in G), edge << 1 when it is the head (+1)
-__global__ void k_count_node_edges(const int32_t* __restrict__ line, int nline, int* __restrict__ cnt) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= nline) return;
-  atomicAdd(cnt + line[2 * e] - 1, 1);
-  atomicAdd(cnt + line[2 * e + 1] - 1, 1);
-}
-
-__global__ void k_fill_node_edges(const int32_t* __restrict__ line, int nline, const int32_t* __restrict__ nptr,
-                                  int* __restrict__ cursor, int32_t* __restrict__ nlist) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= nline) return;
-  const int a = line[2 * e] - 1, b = line[2 * e + 1] - 1;
-  nlist[nptr[a] + atomicAdd(cursor + a, 1)] = (e << 1) | 1;
-  nlist[nptr[b] + atomicAdd(cursor + b, 1)] = e << 1;
-}
-
-// per node: sort the incident edges (the fill order is not deterministic), then
-// write the nodal pattern row: the node and the far ends of its edges, ascending
-__global__ void k_node_rows(const int32_t* __restrict__ line, int node, const int32_t* __restrict__ nptr,
-                            int32_t* __restrict__ nlist, const int32_t* __restrict__ rowptr, int32_t* __restrict__ col,
-                            int32_t* __restrict__ diagpos, DevStatus* st) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= node) return;
-  const int p0 = nptr[a], p1 = nptr[a + 1];
-  if (p1 - p0 > NODE_EDGE_MAX) {
-    raise_status(st, DEV_DEGREE, a);
-    return;
-  }
-  for (int i = p0 + 1; i < p1; ++i) {
-    const int32_t v = nlist[i];
-    int j = i - 1;
-    while (j >= p0 && nlist[j] > v) {
-      nlist[j + 1] = nlist[j];
-      --j;
-    }
-    nlist[j + 1] = v;
-  }
-  const int r0 = rowptr[a];
-  int len = 0;
-  col[r0 + len++] = a;
-  for (int i = p0; i < p1; ++i) {
-    const int e = nlist[i] >> 1;
-    const int far = (nlist[i] & 1) ? line[2 * e + 1] - 1 : line[2 * e] - 1;
-    // insertion keeps the row ascending (a mesh has no repeated edge)
-    int j = len - 1;
-    while (j >= 0 && col[r0 + j] > far) {
-      col[r0 + j + 1] = col[r0 + j];
-      --j;
-    }
-    col[r0 + j + 1] = far;
-    ++len;
-  }
-  for (int k = 0; k < len; ++k)
-    if (col[r0 + k] == a) diagpos[a] = r0 + k;
-}
-
-__global__ void k_node_row_len(const int32_t* __restrict__ nptr, int node, int32_t* __restrict__ len) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a < node) len[a] = 1 + nptr[a + 1] - nptr[a];
-}
-
 // A_G = G^T P (K, M) P G, thread per nodal row (a fixed summation order)
 __global__ void k_node_values(const int32_t* __restrict__ line, const uint8_t* __restrict__ bc, int node,
                               const int32_t* __restrict__ nptr, const int32_t* __restrict__ nlist,
@@ -141,49 +78,58 @@ void hybrid_prepare(afem_ctx* c) {
   if (h->node != node || h->nline != c->nline || !h->pattern_ready) {
     h->node = node;
     h->nline = c->nline;
-    DBuf<int32_t> cnt, cursor, len;
-    cnt.alloc(node);
-    cnt.zero(s);
-    k_count_node_edges<<<nblk(c->nline, 256), 256, 0, s>>>(c->line.p, c->nline, cnt.p);
-    count_launch();
-    h->nptr.alloc(node + 1);
-    exclusive_scan(cnt.p, h->nptr.p, node, s, nullptr);
-    h->nlist.alloc(2L * c->nline);
-    cursor.alloc(node);
-    cursor.zero(s);
-    k_fill_node_edges<<<nblk(c->nline, 256), 256, 0, s>>>(c->line.p, c->nline, h->nptr.p, cursor.p, h->nlist.p);
-    count_launch();
-    len.alloc(node);
-    k_node_row_len<<<nblk(node, 256), 256, 0, s>>>(h->nptr.p, node, len.p);
-    count_launch();
-    h->rowptr.alloc(node + 1);
-    long nnz = 0;
-    exclusive_scan(len.p, h->rowptr.p, node, s, &nnz);
-    h->nnz = nnz;
-    h->col.alloc(nnz);
-    AFEM_CUDA(cudaMemsetAsync(h->col.p, 0xff, sizeof(int32_t) * nnz, s));  // -1: a row left unwritten shows
-    h->diagpos.alloc(node);
-    k_node_rows<<<nblk(node, 128), 128, 0, s>>>(c->line.p, node, h->nptr.p, h->nlist.p, h->rowptr.p, h->col.p,
-                                                 h->diagpos.p, c->status.p);
-    count_launch();
-    check_status(c, "hybrid preconditioner: more than 128 edges meet at one node");
-    std::vector<int32_t> rp(node + 1), cl(nnz), pm(node), cptr(256), dp(node);
-    std::vector<uint8_t> color(node);
-    h->rowptr.download(rp.data(), node + 1, s);
-    h->col.download(cl.data(), nnz, s);
+    // The node graph, once per mesh, on the host: incident edges per node in
+    // ascending edge order (edge << 1 | 1 at the tail line(1,e), edge << 1 at
+    // the head), rows = the node and the far ends of its edges, ascending.
+    const int nline = c->nline;
+    std::vector<int32_t> ln(2L * nline);
+    c->line.download(ln.data(), ln.size(), s);
     AFEM_CUDA(cudaStreamSynchronize(s));
-    // every row: ascending node ids within 0..node-1, holding its own node once
-    for (int a = 0; a < node; ++a) {
-      int d = -1;
-      for (int k = rp[a]; k < rp[a + 1]; ++k) {
-        AFEM_REQUIRE(cl[k] >= 0 && cl[k] < node && (k == rp[a] || cl[k] > cl[k - 1]), AFEM_EPATTERN,
-                     "hybrid preconditioner: the node graph row of node " + std::to_string(a) + " is malformed");
-        if (cl[k] == a) d = k;
-      }
-      AFEM_REQUIRE(d >= 0, AFEM_EPATTERN, "hybrid preconditioner: node " + std::to_string(a) + " misses its diagonal");
-      dp[a] = d;
+    std::vector<int32_t> np(node + 1, 0);
+    for (int e = 0; e < nline; ++e) {
+      const int a = ln[2L * e] - 1, b = ln[2L * e + 1] - 1;
+      AFEM_REQUIRE(a >= 0 && a < node && b >= 0 && b < node && a != b, AFEM_EINVAL,
+                   "hybrid preconditioner: edge " + std::to_string(e + 1) + " has a bad node id");
+      np[a + 1] += 1;
+      np[b + 1] += 1;
     }
-    h->diagpos.upload(dp.data(), node, s);
+    for (int a = 0; a < node; ++a) {
+      AFEM_REQUIRE(np[a + 1] <= NODE_EDGE_MAX, AFEM_EPATTERN,
+                   "hybrid preconditioner: more than 128 edges meet at node " + std::to_string(a + 1));
+      np[a + 1] += np[a];
+    }
+    std::vector<int32_t> nl(2L * nline), cur(np.begin(), np.end() - 1);
+    for (int e = 0; e < nline; ++e) {
+      nl[cur[ln[2L * e] - 1]++] = (e << 1) | 1;
+      nl[cur[ln[2L * e + 1] - 1]++] = e << 1;
+    }
+    std::vector<int32_t> rp(node + 1, 0), dp(node);
+    for (int a = 0; a < node; ++a) rp[a + 1] = rp[a] + 1 + (np[a + 1] - np[a]);
+    const long nnz = rp[node];
+    std::vector<int32_t> cl(nnz);
+    for (int a = 0; a < node; ++a) {
+      int32_t* row = cl.data() + rp[a];
+      int len = 0;
+      row[len++] = a;
+      for (int q = np[a]; q < np[a + 1]; ++q) {
+        const int e = nl[q] >> 1;
+        row[len++] = (nl[q] & 1) ? ln[2L * e + 1] - 1 : ln[2L * e] - 1;
+      }
+      std::sort(row, row + len);
+      for (int k = 0; k < len; ++k) {
+        AFEM_REQUIRE(k == 0 || row[k] > row[k - 1], AFEM_EPATTERN,
+                     "hybrid preconditioner: repeated edge at node " + std::to_string(a + 1));
+        if (row[k] == a) dp[a] = rp[a] + k;
+      }
+    }
+    h->nnz = nnz;
+    h->nptr.upload(np.data(), np.size(), s);
+    h->nlist.upload(nl.data(), nl.size(), s);
+    h->rowptr.upload(rp.data(), rp.size(), s);
+    h->col.upload(cl.data(), cl.size(), s);
+    h->diagpos.upload(dp.data(), dp.size(), s);
+    std::vector<int32_t> pm(node), cptr(256);
+    std::vector<uint8_t> color(node);
     // multicolour order of the node graph (host greedy colouring, as for the edges)
     const int nc = compute_coloring(node, rp.data(), cl.data(), color.data(), pm.data(), cptr.data(), 255);
     AFEM_REQUIRE(nc > 0, AFEM_EPATTERN, "hybrid preconditioner: more than 255 colours in the node graph");

@@ -34,6 +34,10 @@ struct CtlInfo {
   double sigma_air = 1e-8;
   std::vector<double> sigma_land;
   int nodes = 0;
+  // plan view (ixyflag = 1): OUTFREQFILES2 files <outputfolder><xyfilehead><freq>_S<k>.dat
+  std::string xyfilehead;
+  int xy_nx = 0, xy_ny = 0, ixydepth = 0;
+  double depth_xy = 0.0;
 };
 
 namespace {
@@ -389,10 +393,12 @@ int load_ctl(afem_ctx* c, const char* path) {
   }
   ci->ixyflag = (int)r.num("ixyflag");
   if (ci->ixyflag == 1) {
-    r.skip("xyfilehead");
-    r.skip("nx ny");
-    const int ixydepth = (int)r.num("ixydepth");
-    if (ixydepth == 1) r.skip("depth_xy");
+    ci->xyfilehead = r.word("xyfilehead");
+    auto nxy = r.nums("nx ny", 2);
+    ci->xy_nx = (int)nxy[0];
+    ci->xy_ny = (int)nxy[1];
+    ci->ixydepth = (int)r.num("ixydepth");
+    if (ci->ixydepth == 1) ci->depth_xy = r.num("depth_xy");
     r.skip("pokimsh");
     r.skip("ki23dfile");
   } else if (ci->ixyflag == 2) {
@@ -458,6 +464,39 @@ int ctl_info(afem_ctx* c, int* nfreq, double* freq, int* nobs, double* xyz) {
   return AFEM_OK;
 }
 
+// Fortran Ew.d as write(num,'(e9.2)') prints a frequency for the plan-view file names
+// (OUTFREQFILES2, m_outresp.f90:192): [sign]0.ddE+ee, mantissa in [0.1, 1).
+std::string fortran_e(double x, int w, int d) {
+  char buf[64];
+  const double ax = std::fabs(x);
+  int e = 0;
+  double m = 0.0;
+  if (ax > 0.0) {
+    e = (int)std::floor(std::log10(ax)) + 1;
+    m = ax / std::pow(10.0, e);
+    if (m < 0.1) { m *= 10.0; e -= 1; }
+    if (m >= 1.0) { m /= 10.0; e += 1; }
+    const double scale = std::pow(10.0, d);
+    double r = std::nearbyint(m * scale) / scale;
+    if (r >= 1.0) { r /= 10.0; e += 1; }
+    m = r;
+  }
+  std::snprintf(buf, sizeof(buf), "%s0.%0*lldE%c%02d", x < 0 ? "-" : "", d, (long long)std::llround(m * std::pow(10.0, d)),
+                e < 0 ? '-' : '+', std::abs(e));
+  std::string s(buf);
+  if ((int)s.size() < w) s = std::string(w - s.size(), ' ') + s;
+  return s;
+}
+
+// Fortran Fw.d: right-justified fixed point, asterisks when it does not fit.
+std::string fortran_f(double x, int w, int d) {
+  char buf[96];
+  std::snprintf(buf, sizeof(buf), "%*.*f", w, d, x);
+  std::string s(buf);
+  if ((int)s.size() > w) s = std::string(w, '*');
+  return s;
+}
+
 // Frequency loop of n_ebfem_bxyz (n_ebfem_bxyz_mpi.f90:144-183): one forward
 // solve per frequency, CALOBSEBCOMP, then OUTOBSFILESFWD.  GENMAT fills
 // right-hand-side column 1 only, so sources 2..nsr have zero fields.
@@ -465,9 +504,21 @@ int run_ctl(afem_ctx* c, const afem_solve_opts* o) {
   AFEM_REQUIRE(c->ctl, AFEM_ESTATE, "run_ctl: no ctl loaded");
   AFEM_REQUIRE(o, AFEM_EINVAL, "run_ctl: null options");
   CtlInfo* ci = c->ctl;
+  AFEM_REQUIRE(ci->ixyflag == 0 || (ci->ixyflag == 1 && ci->ixydepth == 1), AFEM_EIO,
+               "run_ctl: plan views on the seafloor (ixyflag 2, or ixydepth 2) need the polygon_ki mesh (PREPZOBS); "
+               "only the constant-depth plan view (ixyflag 1, ixydepth 1) is supported");
   int rc = afem_assemble(c);
   if (rc) throw Error{rc, c->err};
   const int nf = (int)ci->freq.size(), nobs = ci->nobs;
+  // plan-view points of PREPOBSCOEFF_XY: the cells of [xbound(2), xbound(3)] x [ybound(2), ybound(3)]
+  std::vector<double> xy;
+  const int nxy = ci->ixyflag == 1 ? ci->xy_nx * ci->xy_ny : 0;
+  if (nxy > 0) {
+    xy.resize(3L * nxy);
+    rc = afem_xy_points(ci->xbound[1], ci->xbound[2], ci->ybound[1], ci->ybound[2], ci->xy_nx, ci->xy_ny, ci->depth_xy,
+                        xy.data());
+    if (rc) throw Error{rc, "run_ctl: plan-view grid"};
+  }
   std::vector<double> amp((size_t)nf * 5 * nobs), ph((size_t)nf * 5 * nobs);
   const double pi = 4.0 * std::atan(1.0), r2d = 180.0 / pi;
   for (int i = 0; i < nf; ++i) {
@@ -478,6 +529,35 @@ int run_ctl(afem_ctx* c, const afem_solve_opts* o) {
     std::vector<double> out(2L * 5 * nobs);
     rc = afem_sites(c, nobs, ci->xyzobs.data(), out.data());
     if (rc) throw Error{rc, c->err};
+    if (nxy > 0) {
+      // OUTFREQFILES2 (m_outresp.f90:181-217): x, y, z and (amp, phase) of bx..ey per plan-view point
+      std::vector<double> o2(2L * 5 * nxy);
+      rc = afem_sites_grid(c, nxy, xy.data(), o2.data());
+      if (rc) throw Error{rc, c->err};
+      const std::string num = fortran_e(ci->freq[i], 9, 2);
+      for (int k = 0; k < ci->nsource; ++k) {
+        // the reference assembles the name in a character(50) variable
+        const std::string fn = (rtrim(ci->outputfolder) + rtrim(ci->xyfilehead) + num.substr(1, 8) + "_S" +
+                                std::to_string((k + 1) % 10) + ".dat").substr(0, 50);
+        FILE* f = std::fopen(fn.c_str(), "w");
+        if (!f) throw Error{AFEM_EIO, "cannot write " + fn};
+        for (int sidx = 0; sidx < nxy; ++sidx) {
+          std::string row;
+          for (int j = 0; j < 3; ++j) row += fortran_f(xy[3L * sidx + j], 15, 7);
+          for (int comp = 0; comp < 5; ++comp) {
+            double a = 0.0, p = 0.0;
+            if (k == 0) {
+              const double re = o2[2 * ((long)comp * nxy + sidx)], im = o2[2 * ((long)comp * nxy + sidx) + 1];
+              a = std::sqrt(std::pow(re, 2.0) + std::pow(im, 2.0));
+              p = std::atan2(im, re) * r2d;
+            }
+            row += fortran_f(a, 15, 7) + fortran_f(p, 15, 7);
+          }
+          std::fprintf(f, "%s\n", row.c_str());
+        }
+        std::fclose(f);
+      }
+    }
     for (int comp = 0; comp < 5; ++comp)
       for (int s = 0; s < nobs; ++s) {
         const double re = out[2 * ((long)comp * nobs + s)], im = out[2 * ((long)comp * nobs + s) + 1];
@@ -487,7 +567,9 @@ int run_ctl(afem_ctx* c, const afem_solve_opts* o) {
   }
   for (int l = 0; l < nobs; ++l)
     for (int k = 0; k < ci->nsource; ++k) {
-      const std::string fn = rtrim(ci->outputfolder) + rtrim(ci->obsname[l]) + "_" + rtrim(ci->sourcename[k]) + ".dat";
+      // OUTOBSFILESFWD (m_outresp.f90:228-247): head, site and source names are character(50), the name (70)
+      const std::string fn = (rtrim(ci->outputfolder.substr(0, 50)) + rtrim(ci->obsname[l].substr(0, 50)) + "_" +
+                              rtrim(ci->sourcename[k].substr(0, 50)) + ".dat").substr(0, 70);
       FILE* f = std::fopen(fn.c_str(), "w");
       if (!f) throw Error{AFEM_EIO, "cannot write " + fn};
       for (int i = 0; i < nf; ++i) {

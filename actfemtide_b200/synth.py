@@ -330,7 +330,8 @@ def _write_msh(path, xyz, elems, etype):
         f.write("$EndElements\n")
 
 
-def write_reference_inputs(m: TidalModel, outdir: str, line=None, n6line=None, site_names=None) -> str:
+def write_reference_inputs(m: TidalModel, outdir: str, line=None, n6line=None, site_names=None,
+                           plan_view=None) -> str:
     """Write model m as the files the reference's tide forward reads; returns the ctl path.
 
     em3d.msh (tetrahedra, tags = elementary volume), polygonz.msh (top-of-earth
@@ -404,7 +405,14 @@ def write_reference_inputs(m: TidalModel, outdir: str, line=None, n6line=None, s
              lab("UTM ZONE") + "none", lab("lonlatorigin") + "0.0 0.0"]
     for nm, s in zip(names, m.sites):
         rows += [lab("Name") + nm, lab("xyz") + f"{float(s[0])!r} {float(s[1])!r} {-SITE_DEPTH_KM!r}"]
-    rows += [lab("0:no,1:nxny,2:ntrik") + "0", lab("# of sources") + "1", lab("Source Name") + "S1",
+    if plan_view is None:
+        rows += [lab("0:no,1:nxny,2:ntrik") + "0"]
+    else:  # (xyfilehead, nx, ny, depth_xy): a constant-depth plan view (ixyflag 1, ixydepth 1)
+        head, pnx, pny, depth = plan_view
+        rows += [lab("0:no,1:nxny,2:ntrik") + "1", lab("xyfilehead") + head, lab("nx ny") + f"{pnx} {pny}",
+                 lab("ixydepth") + "1", lab("depth_xy [km]") + repr(float(depth)), lab("pokimsh") + p("polygon_ki.msh"),
+                 lab("ki23dfile") + p("ki23dptr.dat")]
+    rows += [lab("# of sources") + "1", lab("Source Name") + "S1",
              lab("source start point") + "0.0 0.0 -0.001", lab("source end   point") + "0.1 0.0 -0.001",
              lab("Elcetric current[A]") + "0.0", lab("sigma_air    [S/m]") + repr(float(m.sigma_air)),
              lab("condflag 0:home,1:") + "1", lab("condfile") + p("cond_test.msh")]

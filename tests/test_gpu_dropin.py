@@ -52,3 +52,35 @@ def test_ctl_driver_matches_oracle(gpulib, oracle, short_dir):
             big = amp[0, :, s] > 1e-3 * amp[0].max()
             dphi = (vals[big, 1] - ph[0, big, s] + 180.0) % 360.0 - 180.0
             assert np.all(np.abs(dphi) <= 1e-3)
+
+
+def test_ctl_plan_view_matches_oracle(gpulib, oracle, short_dir):
+    """ixyflag 1, ixydepth 1: PREPOBSCOEFF_XY points, FINDELEWITHGRID elements, OUTFREQFILES2 files."""
+    from actfemtide_b200 import capi
+    from actfemtide_b200.forward import Forward
+    m = synth.tidal_box(4, 4, 6, seed=3, site_grid=(-6.0, 0.0, 6.0), half_km=12.0)
+    m.freqs = np.array([1.0 / 44714.0])
+    of = oracle.OracleForward(m)
+    pnx, pny, depth = 5, 4, -5.5
+    ctl = synth.write_reference_inputs(m, short_dir, of.line, of.n6line, plan_view=("xy", pnx, pny, depth))
+    with Forward(0) as fw:
+        fw.load_ctl(ctl)
+        fw.run_ctl(precond="SSOR", tol=1e-10)
+    xb = 12.0 - 10.0
+    pts = capi.xy_points(-xb, xb, -xb, xb, pnx, pny, depth)
+    m33 = synth.TidalModel(**{**m.__dict__, "sigma_ocean": float(np.float32(3.33))})
+    of33 = oracle.OracleForward(m33, of.line, of.n6line)
+    fr = m.freqs[0]
+    A = of33.assemble(fr)
+    r = oracle.cocg13_single(A, precond="SSOR", resid=1e-11, maxit=100000)
+    item, ve, vf, _ = oracle.prepobscoeff_grid(m33, of.n6line, pts)
+    _, amp, ph = oracle.calobsebcomp(r["x"][None, :], 2 * np.pi * fr, item, ve, vf)
+    name = os.path.join(short_dir, "xy" + "0.22E-04" + "_S1.dat")
+    rows = np.array([list(map(float, ln.split())) for ln in open(name).read().splitlines()])
+    assert rows.shape == (pnx * pny, 13)
+    np.testing.assert_allclose(rows[:, :3], pts, atol=5e-8)
+    vals = rows[:, 3:].reshape(-1, 5, 2)
+    np.testing.assert_allclose(vals[:, :, 0], amp[0].T, rtol=2e-6, atol=1e-6 * amp[0].max() + 5e-8)
+    big = amp[0].T > 1e-3 * amp[0].max()
+    dphi = (vals[:, :, 1][big] - ph[0].T[big] + 180.0) % 360.0 - 180.0
+    assert np.all(np.abs(dphi) <= 1e-3)
