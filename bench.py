@@ -490,7 +490,7 @@ def main():
     p.add_argument("--steps", type=int, default=2)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--method", default="batched-mixed", choices=sorted(METHODS))
+    p.add_argument("--method", default="batched", choices=sorted(METHODS))
     p.add_argument("--precond", default=None, choices=["IC", "SSOR", "DIAG", "NONE", "LEARNED", "SSOR_MC", "HYBRID"],
                    help="override the method's preconditioner")
     p.add_argument("--prof-iters", type=int, default=256,

@@ -4,7 +4,7 @@ The nodal matrix must be the Galerkin product G^T P A P G of the assembled
 edge matrix (G the edge-node incidence, P dropping Dirichlet edges), checked
 against a scipy product of the exported system within 1e-12 of the sum of
 the magnitudes of each entry's terms (the curl-curl part cancels to roundoff).  Solves with AFEM_PRECOND_HYBRID must reach an FP64 true
-residual <= 1e-8 (FP64 and mixed precision, single and batched), give site
+residual <= 1e-8 (single and batched), give site
 fields within 1e-6 relative of the oracle's own SSOR-COCG solve, and need far
 fewer iterations than SSOR alone.
 """
@@ -85,7 +85,7 @@ def test_nodal_matrix_is_the_galerkin_product(fw, grf_model):
         assert np.all(np.abs(dev - ref) <= 1e-12 * bound)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64"])
 def test_hybrid_cocg_matches_oracle(fw, grf_model, precision):
     m, of, ref = grf_model
     fw.load_model(m)
@@ -107,7 +107,7 @@ def test_hybrid_batched_matches_single(fw, grf_model):
     fw.assemble()
     freqs = 1.0 / (3600.0 * np.array(synth.BATCH_PERIODS_H[:4]))
     srcs = np.array([0, 1, 0, 1])
-    rb = fw.solve(freqs, srcs, precond="HYBRID", precision="mixed", tol=1e-8, maxit=20000)
+    rb = fw.solve(freqs, srcs, precond="HYBRID", tol=1e-8, maxit=20000)
     assert rb.ok and rb.resid_true <= 1e-8, rb
     outb = fw.sites(m.sites, nsys=4)
     for k in range(4):

@@ -57,8 +57,7 @@ def test_packed_assembly_equals_separate(fw, parts):
         assert np.array_equal(su["AL"][l0:l1], s["AL"])
 
 
-@pytest.mark.parametrize("precond,precision", [("SSOR", "fp64"), ("SSOR_MC", "fp64"), ("HYBRID", "fp64"),
-                                               ("HYBRID", "mixed")])
+@pytest.mark.parametrize("precond,precision", [("SSOR", "fp64"), ("HYBRID", "fp64")])
 def test_packed_solve_matches_separate_and_oracle(fw, oracle, parts, precond, precision):
     nseg = len(parts)
     freqs = np.array([m.freqs[0] for m in parts])
