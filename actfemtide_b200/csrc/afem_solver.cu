@@ -372,11 +372,15 @@ __global__ void __launch_bounds__(256)
 // warp (lane = sub * 32/RPW + g * NS + s), which keeps several rows' loads in
 // flight per warp.  One persistent cooperative kernel per sweep with a grid
 // barrier between colours; no flags, no waits.
-template <int NS>
+// A lane per (row, system): the earlier- or later-colour part of a row holds ~8
+// entries, so a row per lane keeps 32/NS rows' dependent loads in flight per
+// warp (the sweeps are latency-bound, not bandwidth-bound).  Packed batches
+// keep 4 rows per warp so that each row's per-mesh sums have their own slot.
+template <int NS, bool SEG = false>
 struct McShape {
-  static constexpr int RPW = NS <= 8 ? 4 : 2;  // rows per warp
-  static constexpr int LPR = 32 / RPW;         // lanes per row
-  static constexpr int G = LPR / NS;           // entry groups per row
+  static constexpr int RPW = SEG ? 4 : 32 / NS;  // rows per warp
+  static constexpr int LPR = 32 / RPW;           // lanes per row
+  static constexpr int G = LPR / NS;             // entry groups per row
 };
 
 template <class T, int NS, bool SEG = false>
@@ -388,7 +392,7 @@ __global__ void __launch_bounds__(256)
              const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl,
              double* __restrict__ part, const uint8_t* __restrict__ seg) {
   using V = typename Cx<T>::V;
-  using S = McShape<NS>;
+  using S = McShape<NS, SEG>;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;  // uniform over the grid
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
@@ -474,7 +478,7 @@ __global__ void __launch_bounds__(256)
              const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl,
              double* __restrict__ part, const uint8_t* __restrict__ seg) {
   using V = typename Cx<T>::V;
-  using S = McShape<NS>;
+  using S = McShape<NS, SEG>;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();

@@ -370,7 +370,7 @@ def run_gpu(args):
     achieved = per_launch / (dom_ms / max(1, dom_n) / 1e3) / 1e9 if dom_ms > 0 else 0.0
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.method != "packed":
-        cpu = cpu_baseline(job.m, job.freqs[0], int(np.median(iters)), args.cpu_seconds)
+        cpu = cpu_baseline(job.m, job.freqs[0], args.ref_iters, args.cpu_seconds)
     total_ms = sum(x[0] for x in prof.values())
     line_out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -406,22 +406,26 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+_PINNED = []  # pinned host tensors behind the numpy views handed out by _pinned
+
+
 def _pinned(torch, a):
     a = np.ascontiguousarray(a)
     t = torch.empty(a.shape, dtype=getattr(torch, {"float64": "float64", "int32": "int32", "complex128": "complex128"}[
         str(a.dtype)]), pin_memory=True)
     out = t.numpy()
     out[...] = a
-    out._keep = t  # keep the pinned tensor alive with the view
+    _PINNED.append(t)
     return out
 
 
 # ----------------------------------------------------------------------------- CPU baseline
-def cpu_baseline(m, freq, gpu_iters, seconds, threads=1):
-    """The oracle's serial assembly + SSOR-COCG on the same model, on a bounded sample of iterations.
+def cpu_baseline(m, freq, plain_iters, seconds, threads=1):
+    """The oracle's serial assembly + SSOR-COCG (the reference's solver) on the same model, on a bounded sample.
 
-    s/solve = assembly time + (time per COCG iteration) x (iterations the
-    solve needs, taken from the GPU run of the same system)."""
+    s/solve = assembly time + (time per SSOR-COCG iteration) x (iterations the
+    reference's SSOR-COCG runs on this model: --ref-iters, measured with the
+    COCG13_single seam on the GPU)."""
     from oracle import oracle as O
     of = O.OracleForward(m)
     t0 = time.perf_counter()
@@ -448,11 +452,11 @@ def cpu_baseline(m, freq, gpu_iters, seconds, threads=1):
         dt = time.perf_counter() - t0
         per_it = dt / k / threads  # throughput: `threads` independent solves in parallel
         eff = threads
-    value = t_asm / eff + per_it * gpu_iters
+    value = t_asm / eff + per_it * plain_iters
     return {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"oracle GENMAT+COPY_UL+BC once ({t_asm:.2f} s) + {k} SSOR-COCG iterations "
-                      f"x {threads} thread(s) ({per_it * 1e3:.1f} ms/iteration/solve), extrapolated to "
-                      f"{gpu_iters} iterations"}
+                      f"x {threads} thread(s) ({per_it * 1e3:.1f} ms/iteration/solve), extrapolated to the "
+                      f"{plain_iters} iterations of the reference's SSOR-COCG on this model"}
 
 
 # ----------------------------------------------------------------------------- reference arm
