@@ -55,6 +55,12 @@ __global__ void k_node_values(const int32_t* __restrict__ line, const uint8_t* _
   live[a] = any ? 1 : 0;
 }
 
+__global__ void k_gather_km(const double2* __restrict__ km, const int32_t* __restrict__ src, long cnt,
+                            double2* __restrict__ out) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k < cnt) out[k] = km[src[k]];
+}
+
 __global__ void k_node_seg(const int32_t* __restrict__ ptr, int nseg, int node, uint8_t* __restrict__ seg) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= node) return;
@@ -137,6 +143,28 @@ void hybrid_prepare(afem_ctx* c) {
     h->color.upload(color.data(), node, s);
     h->perm.upload(pm.data(), node, s);
     h->cptr.upload(cptr.data(), nc + 1, s);
+    {
+      std::vector<int32_t> lp(node + 1, 0), up(node + 1, 0), lc, ls, uc, us;
+      lc.reserve(nnz / 2); ls.reserve(nnz / 2); uc.reserve(nnz / 2); us.reserve(nnz / 2);
+      for (int p = 0; p < node; ++p) {
+        const int a = pm[p];
+        for (int k = rp[a]; k < rp[a + 1]; ++k) {
+          const int b = cl[k];
+          if (color[b] < color[a]) { lc.push_back(b); ls.push_back(k); }
+          else if (color[b] > color[a]) { uc.push_back(b); us.push_back(k); }
+        }
+        lp[p + 1] = (int32_t)lc.size();
+        up[p + 1] = (int32_t)uc.size();
+      }
+      h->lptr.upload(lp.data(), lp.size(), s);
+      h->lcol.upload(lc.data(), lc.size(), s);
+      h->lsrc.upload(ls.data(), ls.size(), s);
+      h->uptr.upload(up.data(), up.size(), s);
+      h->ucol.upload(uc.data(), uc.size(), s);
+      h->usrc.upload(us.data(), us.size(), s);
+      h->lkm.alloc(lc.size());
+      h->ukm.alloc(uc.size());
+    }
     h->km.alloc(nnz);
     h->live.alloc(node);
     h->pattern_ready = true;
@@ -146,6 +174,14 @@ void hybrid_prepare(afem_ctx* c) {
     k_node_values<<<nblk(node, 128), 128, 0, s>>>(c->line.p, c->bc.p, node, h->nptr.p, h->nlist.p, c->rowptr.p,
                                                    c->col.p, c->km.p, h->rowptr.p, h->col.p, h->km.p, h->live.p);
     count_launch();
+    if (h->lcol.n) {
+      k_gather_km<<<nblk((long)h->lcol.n, 256), 256, 0, s>>>(h->km.p, h->lsrc.p, (long)h->lcol.n, h->lkm.p);
+      count_launch();
+    }
+    if (h->ucol.n) {
+      k_gather_km<<<nblk((long)h->ucol.n, 256), 256, 0, s>>>(h->km.p, h->usrc.p, (long)h->ucol.n, h->ukm.p);
+      count_launch();
+    }
     h->values_gen = c->assemble_gen;
     h->kmf_valid = false;
   }

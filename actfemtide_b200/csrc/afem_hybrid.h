@@ -20,6 +20,11 @@ struct HybridState {
   DBuf<uint8_t> color;          // nodal multicolour order
   DBuf<int32_t> perm, cptr;
   int ncolors = 0;
+  // rows in colour order, split into earlier-colour (l*) and later-colour (u*) parts;
+  // *src = index of the entry in the nodal CSR, *km the values (FP64, FP32 copies)
+  DBuf<int32_t> lptr, lcol, lsrc, uptr, ucol, usrc;
+  DBuf<double2> lkm, ukm;
+  DBuf<float2> lkmf, ukmf;
   DBuf<uint8_t> seg;            // packed batches: mesh of each node
   int seg_nseg = 0;
 };

@@ -587,43 +587,50 @@ __global__ void k_grad_t(int node, const int32_t* __restrict__ nptr, const int32
   }
 }
 
-// One multicolour SSOR sweep on the nodal matrix: forward y_a = (t_a - sum_{col(b)<col(a)} A_ab y_b) dd_a,
+// One multicolour SSOR sweep on the nodal matrix, over its colour-ordered split
+// rows (as the edge sweeps): forward y_a = (t_a - sum_{col(b)<col(a)} A_ab y_b) dd_a,
 // backward (in place) y_a -= dd_a sum_{col(b)>col(a)} A_ab y_b.  Grid barrier between colours.
 template <class T, int NS, bool SEG>
 __global__ void __launch_bounds__(256)
-    k_nsweep_mc(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
-                const typename Cx<T>::V* __restrict__ km, const typename Cx<T>::V* __restrict__ t,
+    k_nsweep_mc(const int32_t* __restrict__ xptr, const int32_t* __restrict__ xcol,
+                const typename Cx<T>::V* __restrict__ xkm, const typename Cx<T>::V* __restrict__ t,
                 typename Cx<T>::V* __restrict__ y, const typename Cx<T>::V* __restrict__ dd,
-                const uint8_t* __restrict__ color, const int32_t* __restrict__ perm, const int32_t* __restrict__ cptr,
-                int ncolors, const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl,
-                const uint8_t* __restrict__ seg, int backward) {
+                const int32_t* __restrict__ perm, const int32_t* __restrict__ cptr, int ncolors,
+                const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl, const uint8_t* __restrict__ seg,
+                int backward) {
   using V = typename Cx<T>::V;
+  using S = McShape<NS, SEG>;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
-  constexpr int G = 32 / NS;
-  const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
+  const int lane = threadIdx.x & 31, sub = lane / S::LPR, s = lane % NS, g = (lane % S::LPR) / NS;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double om = sc[s].omega;
   for (int cc = 0; cc < ncolors; ++cc) {
     const int c = backward ? ncolors - 1 - cc : cc;
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    for (int pos = p0 + warp; pos < p1; pos += nwarps) {
-      const int row = __ldg(perm + pos);
-      if constexpr (SEG) om = sc[__ldg(seg + row)].omega;
+    for (int pos0 = p0 + warp * S::RPW; pos0 < p1; pos0 += nwarps * S::RPW) {
+      const int pos = pos0 + sub;
+      const bool live = pos < p1;
+      const int row = live ? __ldg(perm + pos) : 0;
+      if constexpr (SEG) om = sc[live ? (int)__ldg(seg + row) : 0].omega;
       T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
-      for (int k = __ldg(rowptr + row) + g; k < __ldg(rowptr + row + 1); k += G) {
-        const int j = __ldg(col + k);
-        const int cj = __ldg(color + j);
-        if (backward ? cj <= c : cj >= c) continue;
-        const V a = km[k];
-        const V yj = ldcg(y + (long)j * NS + s);
-        t1x += a.x * yj.x; t1y += a.x * yj.y;
-        t2x += a.y * yj.x; t2y += a.y * yj.y;
+      if (live) {
+        for (int k = __ldg(xptr + pos) + g; k < __ldg(xptr + pos + 1); k += S::G) {
+          const int j = __ldg(xcol + k);
+          const V a = xkm[k];
+          const V yj = ldcg(y + (long)j * NS + s);
+          t1x += a.x * yj.x; t1y += a.x * yj.y;
+          t2x += a.y * yj.x; t2y += a.y * yj.y;
+        }
       }
-      group_reduce<T, NS>(t1x, t1y, t2x, t2y);
-      if (g == 0) {
+#pragma unroll
+      for (int m = NS; m < S::LPR; m <<= 1) {
+        t1x += shfl_xor(t1x, m); t1y += shfl_xor(t1y, m);
+        t2x += shfl_xor(t2x, m); t2y += shfl_xor(t2y, m);
+      }
+      if (live && g == 0) {
         const T o = (T)om;
         const T sx = t1x - o * t2y, sy = t1y + o * t2x;
         const V d = dd[(long)row * NS + s];
@@ -1120,6 +1127,8 @@ struct Inner<double, NS> {
   static V* HY(SolverWork* w) { return w->hy.p; }
   static V* HDD(SolverWork* w) { return w->hdd.p; }
   static const V* HKM(afem_ctx* c) { return c->hyb->km.p; }
+  static const V* HLKM(afem_ctx* c) { return c->hyb->lkm.p; }
+  static const V* HUKM(afem_ctx* c) { return c->hyb->ukm.p; }
   static const V* LKM(afem_ctx* c, SolverWork*) { return c->mc_lkm.p; }
   static const V* UKM(afem_ctx* c, SolverWork*) { return c->mc_ukm.p; }
 };
@@ -1137,6 +1146,8 @@ struct Inner<float, NS> {
   static V* HY(SolverWork* w) { return w->hyf.p; }
   static V* HDD(SolverWork* w) { return w->hddf.p; }
   static const V* HKM(afem_ctx* c) { return c->hyb->kmf.p; }
+  static const V* HLKM(afem_ctx* c) { return c->hyb->lkmf.p; }
+  static const V* HUKM(afem_ctx* c) { return c->hyb->ukmf.p; }
   static const V* LKM(afem_ctx*, SolverWork* w) { return w->mc_lkmf.p; }
   static const V* UKM(afem_ctx*, SolverWork* w) { return w->mc_ukmf.p; }
 };
@@ -1240,10 +1251,10 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
                                                     w->ctrl.p);
     count_launch();
     for (int bwd = 0; bwd < 2; ++bwd)
-      launch_coop(k_nsweep_mc<T, NS, SEG>, w->nmc_blocks, s, (const int32_t*)h->rowptr.p, (const int32_t*)h->col.p,
-                  I::HKM(c), (const V*)I::HT(w), I::HY(w), (const V*)I::HDD(w), (const uint8_t*)h->color.p,
-                  (const int32_t*)h->perm.p, (const int32_t*)h->cptr.p, h->ncolors, (const SysScal*)w->sc.p,
-                  (const Ctrl*)w->ctrl.p, hs, bwd);
+      launch_coop(k_nsweep_mc<T, NS, SEG>, w->nmc_blocks, s, (const int32_t*)(bwd ? h->uptr.p : h->lptr.p),
+                  (const int32_t*)(bwd ? h->ucol.p : h->lcol.p), bwd ? I::HUKM(c) : I::HLKM(c),
+                  (const V*)I::HT(w), I::HY(w), (const V*)I::HDD(w), (const int32_t*)h->perm.p,
+                  (const int32_t*)h->cptr.p, h->ncolors, (const SysScal*)w->sc.p, (const Ctrl*)w->ctrl.p, hs, bwd);
     k_grad_add<T, NS, SEG><<<w->nblocks, 256, 0, s>>>(n, c->line.p, c->bc.p, (const V*)I::HY(w), I::Z(w),
                                                         (const V*)I::R(w), w->ctrl.p, w->part.p, sg);
     count_launch();
@@ -1348,6 +1359,16 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
         h->kmf.alloc(h->nnz);
         k_convert<float2, double2><<<c->num_sms * 8, 256, 0, s>>>(h->km.p, h->kmf.p, h->nnz);
         count_launch();
+        h->lkmf.alloc(h->lkm.n);
+        h->ukmf.alloc(h->ukm.n);
+        if (h->lkm.n) {
+          k_convert<float2, double2><<<c->num_sms * 8, 256, 0, s>>>(h->lkm.p, h->lkmf.p, (long)h->lkm.n);
+          count_launch();
+        }
+        if (h->ukm.n) {
+          k_convert<float2, double2><<<c->num_sms * 8, 256, 0, s>>>(h->ukm.p, h->ukmf.p, (long)h->ukm.n);
+          count_launch();
+        }
         h->kmf_valid = true;
       }
     }
