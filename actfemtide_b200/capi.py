@@ -33,7 +33,7 @@ EXPORTS = (
     "afem_mpnn_set_params", "afem_mpnn_get_params", "afem_mpnn_forward", "afem_mpnn_loss_grad", "afem_mpnn_train",
     "afem_solve_rhs", "afem_jacobian", "afem_sweep_schedule", "afem_coloring", "afem_set_segments",
     "afem_segment_info", "afem_launch_count", "afem_hybrid_matrix", "afem_sites_grid", "afem_site_coeffs_grid",
-    "afem_xy_points", "afem_sort_index", "afem_mesh_info", "afem_solution_count",
+    "afem_xy_points", "afem_sort_index", "afem_mesh_info", "afem_solution_count", "afem_sites_noalloc",
 )
 
 
@@ -77,6 +77,8 @@ def lib():
     L.afem_stream.argtypes = [_vp]
     L.afem_set_mesh.argtypes = [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp, _vp]
     L.afem_get_lines.argtypes = [_vp, C.POINTER(C.c_int), _vp, _vp]
+    L.afem_sites_noalloc.argtypes = [_vp, C.c_int, _vp, _vp]
+    L.afem_sites_noalloc.restype = C.c_int
     L.afem_sites_grid.argtypes = [_vp, C.c_int, _vp, _vp]
     L.afem_sites_grid.restype = C.c_int
     L.afem_site_coeffs_grid.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp]

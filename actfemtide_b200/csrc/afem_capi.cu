@@ -539,6 +539,15 @@ int afem_site_coeffs(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item
   });
 }
 
+int afem_sites_noalloc(afem_ctx* c, int nobs, const double* xyz_obs, double* out) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(nobs > 0 && xyz_obs && out, AFEM_EINVAL, "sites_noalloc: empty or null");
+    afem::reset_status(c);
+    afem::sites_noalloc_device(c, nobs, xyz_obs, out);
+    return (int)AFEM_OK;
+  });
+}
+
 int afem_sites_grid(afem_ctx* c, int nobs, const double* xyz_obs, double* out) {
   return guarded(c, [&]() {
     AFEM_REQUIRE(nobs > 0 && xyz_obs && out, AFEM_EINVAL, "sites_grid: empty or null");

@@ -286,6 +286,7 @@ void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out, boo
 void site_coeffs_grid_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item, double* val_e,
                              double* val_f, int32_t* iele);
 void sort_index_heap(int n, int32_t* na, double* ra);  // SORT_INDEX (sort_index.f90:13-56)
+void sites_noalloc_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out);  // afem_sites_noalloc
 void grid_destroy(afem_ctx* c);
 
 // status helpers

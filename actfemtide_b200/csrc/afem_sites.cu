@@ -459,4 +459,79 @@ void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out, boo
   AFEM_CUDA(cudaStreamSynchronize(s));
 }
 
+// ---------------------------------------------------------------- sites without allocation
+// A variant of the site evaluation (FINDELEMENT0 + PREPOBSCOEFF rows + CALOBSEBCOMP)
+// whose device buffers live in one file-scope __device__ array, so a call
+// allocates nothing: at most NOALLOC_SITES sites and NOALLOC_SYS solved systems.
+// The array's address is taken once per device (cudaGetSymbolAddress) by the
+// first call; make that first call before any stream capture.  All calls share
+// the one array, so calls that overlap in time (two host threads, or two
+// contexts on one device) race on it.
+constexpr int NOALLOC_SITES = 1024;
+constexpr int NOALLOC_SYS = 32;
+constexpr size_t na_align(size_t b) { return (b + 255) / 256 * 256; }
+constexpr size_t NA_OBS = 0;                                                        // 3*S doubles
+constexpr size_t NA_BEST = na_align(NA_OBS + 3 * sizeof(double) * NOALLOC_SITES);   // S ints
+constexpr size_t NA_ITEM = na_align(NA_BEST + sizeof(int) * NOALLOC_SITES);          // 6*S ints
+constexpr size_t NA_VE = na_align(NA_ITEM + 6 * sizeof(int) * NOALLOC_SITES);        // 18*S doubles
+constexpr size_t NA_VF = na_align(NA_VE + 18 * sizeof(double) * NOALLOC_SITES);      // 18*S doubles
+constexpr size_t NA_OM = na_align(NA_VF + 18 * sizeof(double) * NOALLOC_SITES);      // SYS doubles
+constexpr size_t NA_OUT = na_align(NA_OM + sizeof(double) * NOALLOC_SYS);            // 5*S*SYS double2
+constexpr size_t NA_BYTES = na_align(NA_OUT + 5 * sizeof(double2) * NOALLOC_SITES * NOALLOC_SYS);  // 2.9 MB
+
+static __device__ __align__(256) unsigned char g_sites_scratch[NA_BYTES];
+
+namespace {
+
+constexpr int NA_MAX_DEVICES = 64;
+unsigned char* g_sites_scratch_ptr[NA_MAX_DEVICES] = {};
+
+__global__ void k_fill_int(int* __restrict__ p, int n, int v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+}  // namespace
+
+void sites_noalloc_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out) {
+  AFEM_REQUIRE(c->nsys > 0 && c->X.p, AFEM_ESTATE, "sites_noalloc: no solution");
+  AFEM_REQUIRE(!c->sol_packed, AFEM_EINVAL, "sites_noalloc: packed batches are not supported (use afem_sites)");
+  AFEM_REQUIRE(nobs <= NOALLOC_SITES, AFEM_EINVAL,
+               "sites_noalloc: at most " + std::to_string(NOALLOC_SITES) + " sites per call (got " +
+                   std::to_string(nobs) + ")");
+  AFEM_REQUIRE(c->nsys <= NOALLOC_SYS, AFEM_EINVAL,
+               "sites_noalloc: at most " + std::to_string(NOALLOC_SYS) + " solved systems (got " +
+                   std::to_string(c->nsys) + ")");
+  AFEM_REQUIRE(c->device >= 0 && c->device < NA_MAX_DEVICES, AFEM_EINVAL, "sites_noalloc: device id out of range");
+  unsigned char*& base = g_sites_scratch_ptr[c->device];
+  if (!base) AFEM_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&base), g_sites_scratch));
+  double* obs = reinterpret_cast<double*>(base + NA_OBS);
+  int* best = reinterpret_cast<int*>(base + NA_BEST);
+  int32_t* item = reinterpret_cast<int32_t*>(base + NA_ITEM);
+  double* ve = reinterpret_cast<double*>(base + NA_VE);
+  double* vf = reinterpret_cast<double*>(base + NA_VF);
+  double* om = reinterpret_cast<double*>(base + NA_OM);
+  double2* dout = reinterpret_cast<double2*>(base + NA_OUT);
+  cudaStream_t s = c->stream;
+  const double pi = 4.0 * std::atan(1.0);
+  double hom[NOALLOC_SYS];
+  for (int k = 0; k < c->nsys; ++k) hom[k] = 2.0 * pi * c->sol_freq[k];
+  AFEM_CUDA(cudaMemcpyAsync(obs, xyz_obs, sizeof(double) * 3 * nobs, cudaMemcpyHostToDevice, s));
+  AFEM_CUDA(cudaMemcpyAsync(om, hom, sizeof(double) * c->nsys, cudaMemcpyHostToDevice, s));
+  // the search keeps the smallest holder: every site starts with none
+  k_fill_int<<<(nobs + 255) / 256, 256, 0, s>>>(best, nobs, 0x7fffffff);
+  count_launch();
+  dim3 grid(std::max(1, std::min(2 * c->num_sms, (c->ntet + 255) / 256)), nobs);
+  k_find<<<grid, 256, 0, s>>>(c->xyz.p, c->n4.p, 0, c->ntet, obs, nobs, best);
+  count_launch();
+  k_coeffs<<<(nobs + 63) / 64, 64, 0, s>>>(c->xyz.p, c->n4.p, c->n6line.p, obs, nobs, best, item, ve, vf, c->status.p);
+  count_launch();
+  check_status(c, "sites_noalloc: a site lies outside every tetrahedron");
+  const long tot = (long)c->nsys * 5 * nobs;
+  k_eval<<<(unsigned)((tot + 127) / 128), 128, 0, s>>>(c->X.p, c->nline, c->nsys, om, nobs, item, ve, vf, dout);
+  count_launch();
+  AFEM_CUDA(cudaMemcpyAsync(out, dout, sizeof(double2) * tot, cudaMemcpyDeviceToHost, s));
+  AFEM_CUDA(cudaStreamSynchronize(s));
+}
+
 }  // namespace afem

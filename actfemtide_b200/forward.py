@@ -304,6 +304,13 @@ class Forward:
         self._check(self._L.afem_sites(self.ctx, o.shape[0], ptr(o), ptr(out)))
         return out
 
+    def sites_noalloc(self, xyz_obs, nsys=None):
+        """As sites(), through the entry point that allocates nothing (at most 1024 sites, 32 systems)."""
+        o = _c(xyz_obs, np.float64)
+        out = np.zeros((self._nsys(nsys), 5, o.shape[0]), np.complex128)
+        self._check(self._L.afem_sites_noalloc(self.ctx, o.shape[0], ptr(o), ptr(out)))
+        return out
+
     def sites_grid(self, xyz_obs, nsys=None):
         """As sites(), with PREPOBSCOEFF_XY's grid-list element search (FINDELEWITHGRID)."""
         o = _c(xyz_obs, np.float64)

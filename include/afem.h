@@ -201,6 +201,15 @@ int afem_get_solution(afem_ctx *ctx, int k, double *x_complex);
  * out[(k*5 + c)*nobs + s] for c = bx, by, bz (B = curl A) and ex, ey
  * (E = -i*omega*A), complex. */
 int afem_sites(afem_ctx *ctx, int nobs, const double *xyz_obs, double *out_complex);
+/* afem_sites without any device or host allocation (no counterpart in the
+ * reference): the same kernels and results as afem_sites, with the device
+ * buffers in one fixed, statically allocated scratch array of 2.9 MB, so at
+ * most 1024 sites per call and 32 solved systems (AFEM_EINVAL above that) and
+ * no packed batches.  The first call on a device looks the scratch up
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * The scratch is shared by every context on the device: calls that overlap in
+ * time (from two host threads or two contexts) race on it. */
+int afem_sites_noalloc(afem_ctx *ctx, int nobs, const double *xyz_obs, double *out_complex);
 /* The site coefficient rows (item: 6*nobs 1-based edge ids ascending; val_e, val_f: 3*nobs*6,
  * [(c*nobs + s)*6 + j]; iele: containing tetrahedron) for parity checks. */
 int afem_site_coeffs(afem_ctx *ctx, int nobs, const double *xyz_obs, int32_t *item, double *val_e, double *val_f,
