@@ -34,6 +34,7 @@ EXPORTS = (
     "afem_solve_rhs", "afem_jacobian", "afem_sweep_schedule", "afem_coloring", "afem_set_segments",
     "afem_segment_info", "afem_launch_count", "afem_hybrid_matrix", "afem_sites_grid", "afem_site_coeffs_grid",
     "afem_xy_points", "afem_sort_index", "afem_mesh_info", "afem_solution_count", "afem_sites_noalloc",
+    "afem_mpnn_set_base", "afem_precond_apply",
 )
 
 
@@ -77,6 +78,10 @@ def lib():
     L.afem_stream.argtypes = [_vp]
     L.afem_set_mesh.argtypes = [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp, _vp]
     L.afem_get_lines.argtypes = [_vp, C.POINTER(C.c_int), _vp, _vp]
+    L.afem_mpnn_set_base.argtypes = [_vp, C.c_int]
+    L.afem_mpnn_set_base.restype = C.c_int
+    L.afem_precond_apply.argtypes = [_vp, C.c_double, _vp, _vp]
+    L.afem_precond_apply.restype = C.c_int
     L.afem_sites_noalloc.argtypes = [_vp, C.c_int, _vp, _vp]
     L.afem_sites_noalloc.restype = C.c_int
     L.afem_sites_grid.argtypes = [_vp, C.c_int, _vp, _vp]

@@ -539,6 +539,28 @@ int afem_site_coeffs(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item
   });
 }
 
+int afem_mpnn_set_base(afem_ctx* c, int base) {
+  return guarded(c, [&]() {
+    afem::mpnn_set_base(c, base);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_precond_apply(afem_ctx* c, double freq, const double* r, double* z) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(r && z && freq > 0, AFEM_EINVAL, "precond_apply: null vector or bad frequency");
+    AFEM_REQUIRE(c->assembled && c->nline > 0, AFEM_ESTATE, "precond_apply: assemble first");
+    afem::reset_status(c);
+    afem::DBuf<double2> dr, dz;
+    dr.upload(reinterpret_cast<const double2*>(r), c->nline, c->stream);
+    dz.alloc(c->nline);
+    afem::precond_apply_device(c, 2.0 * (4.0 * std::atan(1.0)) * freq, dr.p, dz.p);
+    dz.download(reinterpret_cast<double2*>(z), c->nline, c->stream);
+    AFEM_CUDA(cudaStreamSynchronize(c->stream));
+    return (int)AFEM_OK;
+  });
+}
+
 int afem_sites_noalloc(afem_ctx* c, int nobs, const double* xyz_obs, double* out) {
   return guarded(c, [&]() {
     AFEM_REQUIRE(nobs > 0 && xyz_obs && out, AFEM_EINVAL, "sites_noalloc: empty or null");

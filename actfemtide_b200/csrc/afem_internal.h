@@ -268,6 +268,11 @@ int mpnn_nparam();
 void mpnn_set_params(afem_ctx* c, const float* p, int np);
 void mpnn_get_params(afem_ctx* c, float* p);
 bool mpnn_ready(afem_ctx* c);
+int mpnn_base(afem_ctx* c);                 // 0: Jacobi base, 1: gradient-corrected SSOR base
+void mpnn_set_base(afem_ctx* c, int base);
+// z = H(r) for one system at angular frequency omega: the gradient-corrected multicolour
+// SSOR of the assembled system (the learned preconditioner's base), device vectors of n values
+void precond_apply_device(afem_ctx* c, double omega, const double2* r, double2* z);
 void mpnn_prepare(afem_ctx* c, int ns, const double* d_omega);
 template <class V>
 void mpnn_run(afem_ctx* c, int ns, const double* d_rms, const V* r, V* z, const int* skip);

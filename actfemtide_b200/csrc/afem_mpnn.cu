@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(128)
 template <class V>
 __global__ void k_decode(const __nv_bfloat16* __restrict__ h, int n, int ns, const float* __restrict__ s,
                          const double* __restrict__ rms, const float* __restrict__ wout, const V* __restrict__ r,
-                         V* __restrict__ z, float* __restrict__ o_save, const int* skip) {
+                         V* __restrict__ z, float* __restrict__ o_save, const int* skip, int add) {
   if (skip && *skip) return;
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= (long)n * ns) return;
@@ -232,10 +232,16 @@ __global__ void k_decode(const __nv_bfloat16* __restrict__ h, int n, int ns, con
   }
   const float si = s[i];
   const float f = (float)rms[sy] / si, jac = 1.0f / (si * si);
-  const V ri = r[(long)row * ns + sy];
   V out;
-  out.x = o0 * f + (float)ri.x * jac;
-  out.y = o1 * f + (float)ri.y * jac;
+  if (add) {  // the correction on top of a base preconditioner's output already in z
+    const V zi = z[(long)row * ns + sy];
+    out.x = zi.x + o0 * f;
+    out.y = zi.y + o1 * f;
+  } else {
+    const V ri = r[(long)row * ns + sy];
+    out.x = o0 * f + (float)ri.x * jac;
+    out.y = o1 * f + (float)ri.y * jac;
+  }
   z[(long)row * ns + sy] = out;
 }
 
@@ -550,6 +556,7 @@ struct MpnnState {
   DBuf<float> small;                     // W_in, biases, W_out (FP32, W_in/W_out BF16-rounded)
   bool cast_valid = false;
   int adam_t = 0;
+  int base = 0;  // 0: z = r/|A_ii| + correction (Jacobi base); 1: z = H(r) + correction, H the gradient-corrected SSOR
   // workspace for n x ns rows
   long rows = 0;
   int ns = 0;
@@ -616,7 +623,7 @@ void rowinfo(afem_ctx* c, MpnnState* S, int ns) {
 
 template <class V>
 void forward(afem_ctx* c, MpnnState* S, int ns, const V* r, V* z, bool train, const double* rms = nullptr,
-             const int* skip = nullptr) {
+             const int* skip = nullptr, int add = 0) {
   cudaStream_t st = c->stream;
   const int n = c->nline;
   const long rows = (long)n * ns;
@@ -634,7 +641,7 @@ void forward(afem_ctx* c, MpnnState* S, int ns, const V* r, V* z, bool train, co
   }
   const __nv_bfloat16* hl = train ? S->h[L].p : S->h[L & 1].p;
   k_decode<V><<<blocks(rows, 256), 256, 0, st>>>(hl, n, ns, S->s.p, R, S->small.p + FIN * H + L * H, r, z,
-                                                 nullptr, skip);
+                                                 nullptr, skip, add);
   count_launch();
   AFEM_CUDA(cudaGetLastError());
 }
@@ -652,7 +659,15 @@ double loss_backward(afem_ctx* c, MpnnState* S, int ns, const double2* r) {
     attr_set = true;
   }
   rowinfo(c, S, ns);
-  forward<double2>(c, S, ns, r, S->z64.p, true);
+  if (S->base) {
+    // z = H(r) + correction: the base preconditioner's output first, the network adds to it
+    AFEM_REQUIRE(ns == 1, AFEM_EINVAL, "learned preconditioner: training over a base takes one system per sample");
+    double om = 0.0;
+    AFEM_CUDA(cudaMemcpyAsync(&om, S->omega.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    AFEM_CUDA(cudaStreamSynchronize(st));
+    precond_apply_device(c, om, r, S->z64.p);
+  }
+  forward<double2>(c, S, ns, r, S->z64.p, true, nullptr, nullptr, S->base);
   const int nb = std::min(1024, (int)blocks(n, 256));
   S->part.alloc((size_t)2 * nb * ns);
   S->sums.alloc(2 * ns);
@@ -735,6 +750,11 @@ void mpnn_get_params(afem_ctx* c, float* p) {
 }
 
 bool mpnn_ready(afem_ctx* c) { return c->mpnn && c->mpnn->p.p; }
+int mpnn_base(afem_ctx* c) { return c->mpnn ? c->mpnn->base : 0; }
+void mpnn_set_base(afem_ctx* c, int base) {
+  AFEM_REQUIRE(base == 0 || base == 1, AFEM_EINVAL, "learned preconditioner: base must be 0 (Jacobi) or 1 (hybrid)");
+  state(c)->base = base;
+}
 
 // Inside COCG: mpnn_prepare once per solve (omega per system known), then
 // mpnn_run per iteration (capturable: kernel launches only; skip = the
@@ -749,7 +769,8 @@ void mpnn_prepare(afem_ctx* c, int ns, const double* d_omega) {
 
 template <class V>
 void mpnn_run(afem_ctx* c, int ns, const double* d_rms, const V* r, V* z, const int* skip) {
-  forward<V>(c, state(c), ns, r, z, false, d_rms, skip);
+  MpnnState* S = state(c);
+  forward<V>(c, S, ns, r, z, false, d_rms, skip, S->base);
 }
 template void mpnn_run<double2>(afem_ctx*, int, const double*, const double2*, double2*, const int*);
 template void mpnn_run<float2>(afem_ctx*, int, const double*, const float2*, float2*, const int*);
@@ -763,7 +784,11 @@ void mpnn_forward_host(afem_ctx* c, int ns, const double* freq, const double* r_
   S->r64.upload(reinterpret_cast<const double2*>(r_host), rows, c->stream);
   S->z64.alloc(rows);
   rowinfo(c, S, ns);
-  forward<double2>(c, S, ns, S->r64.p, S->z64.p, false);
+  if (S->base) {
+    AFEM_REQUIRE(ns == 1, AFEM_EINVAL, "learned preconditioner: the hybrid base applies to one system at a time");
+    precond_apply_device(c, 2.0 * (4.0 * std::atan(1.0)) * freq[0], S->r64.p, S->z64.p);
+  }
+  forward<double2>(c, S, ns, S->r64.p, S->z64.p, false, nullptr, nullptr, S->base);
   S->z64.download(reinterpret_cast<double2*>(z_host), rows, c->stream);
   AFEM_CUDA(cudaStreamSynchronize(c->stream));
 }

@@ -146,6 +146,35 @@ __device__ __forceinline__ void group_reduce(T& a, T& b, T& c, T& d) {
   }
 }
 
+// Sum over a row's entries k0, k0+G, ... < k1 of A_k * v_col(k) for system s, split
+// as t1 = sum K*v and t2 = sum M*v.  Four entries at a time: their columns,
+// then their values and gathers, so four independent gathers are in flight
+// per lane; the additions keep the entries' order (the sums do not change).
+template <class T, int NS, int G>
+__device__ __forceinline__ void row_gather(const int32_t* __restrict__ cols, const typename Cx<T>::V* __restrict__ vals,
+                                           const typename Cx<T>::V* vec, int k0, int k1, int s, T& t1x, T& t1y,
+                                           T& t2x, T& t2y) {
+  using V = typename Cx<T>::V;
+  int k = k0;
+  for (; k + 3 * G < k1; k += 4 * G) {
+    const int j0 = __ldg(cols + k), j1 = __ldg(cols + k + G), j2 = __ldg(cols + k + 2 * G), j3 = __ldg(cols + k + 3 * G);
+    const V a0 = vals[k], a1 = vals[k + G], a2 = vals[k + 2 * G], a3 = vals[k + 3 * G];
+    const V v0 = ldcg(vec + (long)j0 * NS + s), v1 = ldcg(vec + (long)j1 * NS + s);
+    const V v2 = ldcg(vec + (long)j2 * NS + s), v3 = ldcg(vec + (long)j3 * NS + s);
+    t1x += a0.x * v0.x; t1y += a0.x * v0.y; t2x += a0.y * v0.x; t2y += a0.y * v0.y;
+    t1x += a1.x * v1.x; t1y += a1.x * v1.y; t2x += a1.y * v1.x; t2y += a1.y * v1.y;
+    t1x += a2.x * v2.x; t1y += a2.x * v2.y; t2x += a2.y * v2.x; t2y += a2.y * v2.y;
+    t1x += a3.x * v3.x; t1y += a3.x * v3.y; t2x += a3.y * v3.x; t2y += a3.y * v3.y;
+  }
+  for (; k < k1; k += G) {
+    const int j = __ldg(cols + k);
+    const V a = vals[k];
+    const V v = ldcg(vec + (long)j * NS + s);
+    t1x += a.x * v.x; t1y += a.x * v.y;
+    t2x += a.y * v.x; t2y += a.y * v.y;
+  }
+}
+
 // Block-reduce NS-per-lane doubles into part[blockIdx][s*4 + slot]; lanes with g == 0 hold system s values.
 template <int NS, int NVAL>
 __device__ __forceinline__ void block_partials(const double (&v)[NVAL], double* part) {
@@ -390,7 +419,7 @@ __global__ void __launch_bounds__(256)
              const typename Cx<T>::V* __restrict__ p, const typename Cx<T>::V* __restrict__ q, double2* __restrict__ x,
              const typename Cx<T>::V* __restrict__ dd, const int32_t* __restrict__ perm,
              const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl,
-             double* __restrict__ part, const uint8_t* __restrict__ seg) {
+             double* __restrict__ part, const uint8_t* __restrict__ seg, typename Cx<T>::V* __restrict__ rprev) {
   using V = typename Cx<T>::V;
   using S = McShape<NS, SEG>;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
@@ -421,6 +450,7 @@ __global__ void __launch_bounds__(256)
         act = sc[sid].active;
       }
       V ri = live ? r[(long)row * NS + s] : Cx<T>::make(0, 0);
+      if (rprev && live && g == 0) rprev[(long)row * NS + s] = ri;  // flexible COCG keeps r_k
       if (live && update && act && g == 0) {
         const V qi = q[(long)row * NS + s], pi = p[(long)row * NS + s];
         ri = Cx<T>::make((T)((double)ri.x - (al.x * (double)qi.x - al.y * (double)qi.y)),
@@ -437,15 +467,8 @@ __global__ void __launch_bounds__(256)
         else rr += v;
       }
       T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
-      if (live) {
-        for (int k = __ldg(lptr + pos) + g; k < __ldg(lptr + pos + 1); k += S::G) {
-          const int j = __ldg(lcol + k);
-          const V a = lkm[k];
-          const V yj = ldcg(y + (long)j * NS + s);
-          t1x += a.x * yj.x; t1y += a.x * yj.y;
-          t2x += a.y * yj.x; t2y += a.y * yj.y;
-        }
-      }
+      if (live)
+        row_gather<T, NS, S::G>(lcol, lkm, y, __ldg(lptr + pos) + g, __ldg(lptr + pos + 1), s, t1x, t1y, t2x, t2y);
 #pragma unroll
       for (int m = NS; m < S::LPR; m <<= 1) {
         t1x += shfl_xor(t1x, m); t1y += shfl_xor(t1y, m);
@@ -502,15 +525,8 @@ __global__ void __launch_bounds__(256)
         om = sc[sid].omega;
       }
       T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
-      if (live) {
-        for (int k = __ldg(uptr + pos) + g; k < __ldg(uptr + pos + 1); k += S::G) {
-          const int j = __ldg(ucol + k);
-          const V a = ukm[k];
-          const V zj = ldcg(z + (long)j * NS + s);
-          t1x += a.x * zj.x; t1y += a.x * zj.y;
-          t2x += a.y * zj.x; t2y += a.y * zj.y;
-        }
-      }
+      if (live)
+        row_gather<T, NS, S::G>(ucol, ukm, z, __ldg(uptr + pos) + g, __ldg(uptr + pos + 1), s, t1x, t1y, t2x, t2y);
 #pragma unroll
       for (int m = NS; m < S::LPR; m <<= 1) {
         t1x += shfl_xor(t1x, m); t1y += shfl_xor(t1y, m);
@@ -616,15 +632,8 @@ __global__ void __launch_bounds__(256)
       const int row = live ? __ldg(perm + pos) : 0;
       if constexpr (SEG) om = sc[live ? (int)__ldg(seg + row) : 0].omega;
       T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
-      if (live) {
-        for (int k = __ldg(xptr + pos) + g; k < __ldg(xptr + pos + 1); k += S::G) {
-          const int j = __ldg(xcol + k);
-          const V a = xkm[k];
-          const V yj = ldcg(y + (long)j * NS + s);
-          t1x += a.x * yj.x; t1y += a.x * yj.y;
-          t2x += a.y * yj.x; t2y += a.y * yj.y;
-        }
-      }
+      if (live)
+        row_gather<T, NS, S::G>(xcol, xkm, y, __ldg(xptr + pos) + g, __ldg(xptr + pos + 1), s, t1x, t1y, t2x, t2y);
 #pragma unroll
       for (int m = NS; m < S::LPR; m <<= 1) {
         t1x += shfl_xor(t1x, m); t1y += shfl_xor(t1y, m);
@@ -719,6 +728,29 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// rho = r^T z and rprev^T z partial sums (slots 0..3) after the learned correction
+// changed z (flexible COCG's beta needs both); NS systems per row, no packed batches
+template <class T, int NS>
+__global__ void __launch_bounds__(256)
+    k_dots(int n, const typename Cx<T>::V* __restrict__ r, const typename Cx<T>::V* __restrict__ z,
+           const typename Cx<T>::V* __restrict__ rprev, const Ctrl* __restrict__ ctrl, double* __restrict__ part) {
+  if (ctrl->done) return;
+  const long total = (long)n * NS;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const typename Cx<T>::V ri = r[i], zi = z[i], pi = rprev[i];
+    v[0] += (double)ri.x * (double)zi.x - (double)ri.y * (double)zi.y;
+    v[1] += (double)ri.x * (double)zi.y + (double)ri.y * (double)zi.x;
+    v[2] += (double)pi.x * (double)zi.x - (double)pi.y * (double)zi.y;
+    v[3] += (double)pi.x * (double)zi.y + (double)pi.y * (double)zi.x;
+  }
+#pragma unroll
+  for (int m = NS; m < 32; m <<= 1)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], m);
+  block_partials<NS, 4>(v, part);
+}
+
 // dd_a = 1 / A_G(omega)_aa for nodes with a non-Dirichlet edge, 0 for the others
 template <class T, int NS>
 __global__ void k_dd_node(const double2* __restrict__ km, const int32_t* __restrict__ diagpos,
@@ -791,13 +823,7 @@ __global__ void __launch_bounds__(256)
     }
     const int k0 = live ? rowptr[row] : 0, k1 = live ? rowptr[row + 1] : 0;
     T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
-    for (int k = k0 + g; k < k1; k += G) {
-      const int j = __ldg(col + k);
-      const V a = km[k];
-      const V pj = p[(long)j * NS + s];
-      t1x += a.x * pj.x; t1y += a.x * pj.y;
-      t2x += a.y * pj.x; t2y += a.y * pj.y;
-    }
+    row_gather<T, NS, G>(col, km, p, k0 + g, k1, s, t1x, t1y, t2x, t2y);
 #pragma unroll
     for (int m = NS; m < LPR; m <<= 1) {
       t1x += shfl_xor(t1x, m); t1y += shfl_xor(t1y, m);
@@ -1212,14 +1238,17 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
   const uint8_t* sg = SEG ? c->seg_of_row.p : nullptr;
   const bool learned = mode == AFEM_PRECOND_LEARNED;
   V* rp = learned ? I::RP(w) : nullptr;
-  const bool hyb = mode == AFEM_PRECOND_HYBRID;
+  // the learned network either replaces the preconditioner (Jacobi base) or adds its
+  // correction to the gradient-corrected SSOR (hybrid base): z = H(r) + N(r)
+  const bool lbase = learned && mpnn_base(c) == 1;
+  const bool hyb = mode == AFEM_PRECOND_HYBRID || lbase;
   const bool mc = mode == AFEM_PRECOND_SSOR_MC || hyb;  // the hybrid's edge part is the multicolour SSOR
   if (ev) AFEM_CUDA(cudaEventRecord(ev[0], s));
   if (mc)
     launch_coop(k_fwd_mc<T, NS, SEG>, w->mc_blocks, s, (const int32_t*)c->mc_lptr.p, (const int32_t*)c->mc_lcol.p,
                 I::LKM(c, w), n, I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w), w->x.p, (const V*)I::DD(w),
                 (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p,
-                w->part.p, sg);
+                w->part.p, sg, rp);
   else
     launch_coop(k_fwd<T, NS, SEG>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
                 (const int32_t*)c->diagpos.p, I::KM(c, w), n, I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w),
@@ -1229,7 +1258,7 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
   const int swb = mc ? w->mc_blocks : sweep_blocks;
   k_scal_r<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, swb, nsys, learned ? w->rms.p : nullptr, n);
   count_launch();
-  if (learned) mpnn_run<V>(c, NS, w->rms.p, (const V*)I::R(w), I::Z(w), &w->ctrl.p->done);
+  if (learned && !lbase) mpnn_run<V>(c, NS, w->rms.p, (const V*)I::R(w), I::Z(w), &w->ctrl.p->done);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[2], s));
   if (mc)
     launch_coop(k_bwd_mc<T, NS, SEG>, w->mc_blocks, s, (const int32_t*)c->mc_uptr.p, (const int32_t*)c->mc_ucol.p,
@@ -1257,6 +1286,14 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
                   (const int32_t*)h->cptr.p, h->ncolors, (const SysScal*)w->sc.p, (const Ctrl*)w->ctrl.p, hs, bwd);
     k_grad_add<T, NS, SEG><<<w->nblocks, 256, 0, s>>>(n, c->line.p, c->bc.p, (const V*)I::HY(w), I::Z(w),
                                                         (const V*)I::R(w), w->ctrl.p, w->part.p, sg);
+    count_launch();
+    rho_blocks = w->nblocks;
+  }
+  if (lbase) {
+    // z += N(r), then rho = r^T z and rprev^T z of the final z for the flexible beta
+    mpnn_run<V>(c, NS, w->rms.p, (const V*)I::R(w), I::Z(w), &w->ctrl.p->done);
+    k_dots<T, NS><<<w->nblocks, 256, 0, s>>>(n, (const V*)I::R(w), (const V*)I::Z(w), (const V*)rp, w->ctrl.p,
+                                             w->part.p);
     count_launch();
     rho_blocks = w->nblocks;
   }
@@ -1348,7 +1385,8 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   }
   k_init_sys<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, nsys, tol, maxit, d_omega);
   count_launch();
-  if (precond == AFEM_PRECOND_HYBRID) {
+  const bool use_hyb = precond == AFEM_PRECOND_HYBRID || (precond == AFEM_PRECOND_LEARNED && mpnn_base(c) == 1);
+  if (use_hyb) {
     HybridState* h = c->hyb;
     const long nt = (long)h->node * NS;
     if (sizeof(T) == 8) {
@@ -1373,7 +1411,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
       }
     }
   }
-  setup_dd<T, NS, SEG>(c, w, precond, o->sigma_diag > 0 ? o->sigma_diag : 1.0);
+  setup_dd<T, NS, SEG>(c, w, use_hyb ? AFEM_PRECOND_HYBRID : precond, o->sigma_diag > 0 ? o->sigma_diag : 1.0);
   const int mode = precond;
   tune_spmv<T, NS, SEG>(c, w);
   const bool learned = mode == AFEM_PRECOND_LEARNED;
@@ -1388,10 +1426,10 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   const int sweep_blocks = coresident_blocks(k_fwd<T, NS, SEG>, c->num_sms);
   const int sb2 = coresident_blocks(k_bwd<T, NS, SEG>, c->num_sms);
   const int sblocks = std::min(std::min(sweep_blocks, sb2), w->nblocks);
-  if (mode == AFEM_PRECOND_SSOR_MC || mode == AFEM_PRECOND_HYBRID)
+  if (mode == AFEM_PRECOND_SSOR_MC || use_hyb)
     w->mc_blocks = std::min(std::min(coresident_blocks(k_fwd_mc<T, NS, SEG>, c->num_sms),
                                      coresident_blocks(k_bwd_mc<T, NS, SEG>, c->num_sms)), w->nblocks);
-  if (mode == AFEM_PRECOND_HYBRID)
+  if (use_hyb)
     w->nmc_blocks = std::min(coresident_blocks(k_nsweep_mc<T, NS, SEG>, c->num_sms), w->nblocks);
   // every solve starts a fresh flag generation: a solve that stopped inside a
   // chunk left its last forward-sweep flags at the epoch it ended on
@@ -1462,7 +1500,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
       char nf[64], nb[64], nh[64], np_[64], ns_[64];
       const char* kind = SEG ? "seg" : "ns";
       const int cnt = SEG ? nsys : NS;
-      const bool mcs = mode == AFEM_PRECOND_SSOR_MC || mode == AFEM_PRECOND_HYBRID;
+      const bool mcs = mode == AFEM_PRECOND_SSOR_MC || use_hyb;
       snprintf(nf, sizeof nf, "cocg_fwd_sweep%s_%s_%s%d", mcs ? "_mc" : "", tag, kind, cnt);
       snprintf(nb, sizeof nb, "cocg_bwd_sweep%s_%s_%s%d", mcs ? "_mc" : "", tag, kind, cnt);
       snprintf(nh, sizeof nh, "cocg_nodal_correction_%s_%s%d", tag, kind, cnt);
@@ -1479,7 +1517,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
         }
         c->prof.add(nf, a);
         c->prof.add(nb, b);
-        if (mode == AFEM_PRECOND_HYBRID) c->prof.add(nh, h);
+        if (use_hyb) c->prof.add(nh, h);
         c->prof.add(np_, d);
         c->prof.add(ns_, e);
       }
@@ -1526,16 +1564,13 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   return iters_done;
 }
 
+// The solve workspace for NS systems per row (SEG: a packed batch), FP32 copies when mixed.
 template <int NS, bool SEG>
-int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_opts* o, afem_solve_stats* st,
-             const SolveExtra* ex) {
+SolverWork* ensure_work(afem_ctx* c, int nsys, bool mixed) {
   SolverWork* w = c->work;
   cudaStream_t s = c->stream;
   const int n = c->nline;
   const long total = (long)n * NS;
-  const int nsys = SEG ? c->nseg : NS;
-  const bool mixed = o->precision == AFEM_MIXED;
-  // ---- workspace
   if (!w) {
     w = new SolverWork();
     c->work = w;
@@ -1592,6 +1627,18 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     }
     w->part.alloc((size_t)w->nblocks * MAX_SYS * 4);
   }
+  return w;
+}
+
+template <int NS, bool SEG>
+int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_opts* o, afem_solve_stats* st,
+             const SolveExtra* ex) {
+  cudaStream_t s = c->stream;
+  const int n = c->nline;
+  const long total = (long)n * NS;
+  const int nsys = SEG ? c->nseg : NS;
+  const bool mixed = o->precision == AFEM_MIXED;
+  SolverWork* w = ensure_work<NS, SEG>(c, nsys, mixed);
   // ---- right-hand sides and omegas
   {
     DBuf<int> dsrc;
@@ -1680,8 +1727,9 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     if (precond_now == AFEM_PRECOND_LEARNED) {
       learned_its += its;
       if (stalled) {
-        // fallback: continue from the current iterate with SSOR-COCG
-        precond_now = AFEM_PRECOND_SSOR;
+        // fallback: continue from the current iterate without the network (its base: the
+        // gradient-corrected SSOR, or the reference's SSOR)
+        precond_now = mpnn_base(c) == 1 ? AFEM_PRECOND_HYBRID : AFEM_PRECOND_SSOR;
         fell_back = true;
       }
     }
@@ -1748,12 +1796,12 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
 
 }  // namespace
 
-int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, const afem_solve_opts* o,
-                 afem_solve_stats* st, const SolveExtra* ex) {
-  AFEM_REQUIRE(c->assembled, AFEM_ESTATE, "solve: system not assembled");
-  build_schedule(c);
+namespace {
+
+// values of the colour-ordered split rows for the current assembly (FP64; the
+// FP32 copies follow with the workspace)
+void ensure_mc_values(afem_ctx* c) {
   if (c->mc_vals_gen != c->assemble_gen) {
-    // values of the colour-ordered split rows (FP64; the FP32 copies follow with the workspace)
     const long nl = (long)c->mc_lcol.n, nu = (long)c->mc_ucol.n;
     c->mc_lkm.alloc(nl);
     c->mc_ukm.alloc(nu);
@@ -1768,7 +1816,17 @@ int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, cons
     c->mc_vals_gen = c->assemble_gen;
     invalidate_work(c);
   }
-  if (o->precond == AFEM_PRECOND_HYBRID) hybrid_prepare(c);
+}
+
+}  // namespace
+
+int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, const afem_solve_opts* o,
+                 afem_solve_stats* st, const SolveExtra* ex) {
+  AFEM_REQUIRE(c->assembled, AFEM_ESTATE, "solve: system not assembled");
+  build_schedule(c);
+  ensure_mc_values(c);
+  if (o->precond == AFEM_PRECOND_HYBRID || (o->precond == AFEM_PRECOND_LEARNED && mpnn_base(c) == 1))
+    hybrid_prepare(c);
   if (c->nseg > 0) {
     AFEM_REQUIRE(nsys == c->nseg, AFEM_EINVAL, "solve: a packed batch solves one system per mesh (nsys = nseg)");
     AFEM_REQUIRE(o->precond != AFEM_PRECOND_LEARNED, AFEM_EINVAL,
@@ -1784,6 +1842,60 @@ int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, cons
     case 16: return solve_ns<16, false>(c, freq, src, o, st, ex);
     default: throw Error{AFEM_EINVAL, "solve: nsys must be 1, 2, 4, 8 or 16"};
   }
+}
+
+void precond_apply_device(afem_ctx* c, double omega, const double2* r, double2* z) {
+  AFEM_REQUIRE(c->assembled, AFEM_ESTATE, "preconditioner: system not assembled");
+  AFEM_REQUIRE(c->nseg == 0, AFEM_EINVAL, "preconditioner: packed batches are not supported here");
+  build_schedule(c);
+  ensure_mc_values(c);
+  hybrid_prepare(c);
+  SolverWork* w = ensure_work<1, false>(c, 1, false);
+  cudaStream_t s = c->stream;
+  const int n = c->nline;
+  HybridState* h = c->hyb;
+  // one system at omega, iteration 0: the sweeps leave x, p and q alone
+  SysScal sc0;
+  std::memset(&sc0, 0, sizeof sc0);
+  sc0.omega = omega;
+  sc0.active = 1;
+  Ctrl ct;
+  std::memset(&ct, 0, sizeof ct);
+  ct.epoch = w->epoch_host;
+  ct.maxit = 1;
+  AFEM_CUDA(cudaMemcpyAsync(w->sc.p, &sc0, sizeof(SysScal), cudaMemcpyHostToDevice, s));
+  AFEM_CUDA(cudaMemcpyAsync(w->ctrl.p, &ct, sizeof(Ctrl), cudaMemcpyHostToDevice, s));
+  AFEM_CUDA(cudaMemcpyAsync(w->r.p, r, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
+  w->ht.alloc(h->node);
+  w->hy.alloc(h->node);
+  w->hdd.alloc(h->node);
+  setup_dd<double, 1, false>(c, w, AFEM_PRECOND_HYBRID, 1.0);
+  w->mc_blocks = std::min(std::min(coresident_blocks(k_fwd_mc<double, 1, false>, c->num_sms),
+                                   coresident_blocks(k_bwd_mc<double, 1, false>, c->num_sms)), w->nblocks);
+  w->nmc_blocks = std::min(coresident_blocks(k_nsweep_mc<double, 1, false>, c->num_sms), w->nblocks);
+  launch_coop(k_fwd_mc<double, 1, false>, w->mc_blocks, s, (const int32_t*)c->mc_lptr.p, (const int32_t*)c->mc_lcol.p,
+              (const double2*)c->mc_lkm.p, n, w->r.p, w->z.p, (const double2*)w->p.p, (const double2*)w->q.p, w->x.p,
+              (const double2*)w->dd.p, (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors,
+              w->sc.p, w->ctrl.p, w->part.p, (const uint8_t*)nullptr, (double2*)nullptr);
+  launch_coop(k_bwd_mc<double, 1, false>, w->mc_blocks, s, (const int32_t*)c->mc_uptr.p, (const int32_t*)c->mc_ucol.p,
+              (const double2*)c->mc_ukm.p, n, (const double2*)w->r.p, w->z.p, (const double2*)w->dd.p,
+              (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p,
+              (const uint8_t*)nullptr);
+  k_grad_t<double, 1><<<c->num_sms * 8, 256, 0, s>>>(h->node, h->nptr.p, h->nlist.p, c->bc.p, (const double2*)w->r.p,
+                                                      w->ht.p, w->ctrl.p);
+  count_launch();
+  for (int bwd = 0; bwd < 2; ++bwd)
+    launch_coop(k_nsweep_mc<double, 1, false>, w->nmc_blocks, s, (const int32_t*)(bwd ? h->uptr.p : h->lptr.p),
+                (const int32_t*)(bwd ? h->ucol.p : h->lcol.p), (const double2*)(bwd ? h->ukm.p : h->lkm.p),
+                (const double2*)w->ht.p, w->hy.p, (const double2*)w->hdd.p, (const int32_t*)h->perm.p,
+                (const int32_t*)h->cptr.p, h->ncolors, (const SysScal*)w->sc.p, (const Ctrl*)w->ctrl.p,
+                (const uint8_t*)nullptr, bwd);
+  k_grad_add<double, 1, false><<<w->nblocks, 256, 0, s>>>(n, c->line.p, c->bc.p, (const double2*)w->hy.p, w->z.p,
+                                                          (const double2*)w->r.p, w->ctrl.p, w->part.p,
+                                                          (const uint8_t*)nullptr);
+  count_launch();
+  AFEM_CUDA(cudaMemcpyAsync(z, w->z.p, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
+  AFEM_CUDA(cudaStreamSynchronize(s));
 }
 
 void get_residual(afem_ctx* c, int k, double* r) {

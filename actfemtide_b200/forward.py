@@ -254,6 +254,17 @@ class Forward:
         return r
 
     # ------------------------------------------------------------ learned preconditioner
+    def mpnn_set_base(self, hybrid: bool):
+        """The network's base: False -> Jacobi (a preconditioner on its own), True -> z = H(r) + N(r)."""
+        self._check(self._L.afem_mpnn_set_base(self.ctx, 1 if hybrid else 0))
+
+    def precond_apply(self, freq, r):
+        """z = H(r): one application of the gradient-corrected multicolour SSOR."""
+        r = _c(np.asarray(r).reshape(self.nline), np.complex128)
+        z = np.zeros_like(r)
+        self._check(self._L.afem_precond_apply(self.ctx, float(freq), ptr(r), ptr(z)))
+        return z
+
     def mpnn_set_params(self, p):
         p = _c(p, np.float32)
         self._check(self._L.afem_mpnn_set_params(self.ctx, ptr(p), len(p)))

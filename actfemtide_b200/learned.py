@@ -23,6 +23,7 @@ SHAPES = [("W_in", (FIN, H))] + [x for l in range(L) for x in ((f"W{l}", (3 * H,
 NPARAM = sum(int(np.prod(s)) for _, s in SHAPES)
 WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
 DEFAULT_CKPT = os.path.join(WEIGHTS_DIR, "mpnn_tidal_32x32x24")
+HYBRID_CKPT = os.path.join(WEIGHTS_DIR, "mpnn_tidal_32x32x24_hybrid")  # correction over the gradient-corrected SSOR
 
 
 def flatten(P: dict) -> np.ndarray:
@@ -69,6 +70,12 @@ def save(path: str, p: np.ndarray, meta: dict):
         json.dump(hdr, f, indent=1)
 
 
+def load_base(path: str = DEFAULT_CKPT) -> int:
+    """The base the checkpoint was trained over: 0 Jacobi, 1 the gradient-corrected SSOR."""
+    with open(path + ".json") as f:
+        return int(json.load(f).get("base", 0))
+
+
 def load(path: str = DEFAULT_CKPT) -> np.ndarray:
     with open(path + ".json") as f:
         hdr = json.load(f)
@@ -83,21 +90,26 @@ def training_model(k: int, nx=32, ny=32, nz=24):
     return synth.tidal_box(nx, ny, nz, seed=k, field_seed=10_000 + k, grf=True, block=False, name=f"train{k}")
 
 
-def collect_residuals(fw, freq, iters=(1, 4, 16, 64)):
-    """True residuals b - A x_k of plain FP64 SSOR-COCG after k iterations on the loaded system."""
+def collect_residuals(fw, freq, iters=(1, 4, 16, 64), precond="SSOR"):
+    """True residuals b - A x_k of FP64 COCG (SSOR, or the network's base) after k iterations on the loaded system."""
     out = []
     for k in iters:
-        fw.solve(freq, precond="SSOR", tol=1e-30, maxit=k)
+        fw.solve(freq, precond=precond, tol=1e-30, maxit=k)
         out.append(fw.residual(0))
     return np.stack(out)
 
 
 def train(fw, n_models: int = 512, steps_per_model: int = 2, lr: float = 1e-3, seed: int = 0, epochs: int = 1,
-          params=None, log=print, nx=32, ny=32, nz=24):
-    """Train on n_models seeded models of the training mesh; returns (params, record)."""
+          params=None, log=print, nx=32, ny=32, nz=24, base: int = 0):
+    """Train on n_models seeded models of the training mesh; returns (params, record).
+
+    base 0: the network is the preconditioner (Jacobi term plus its output),
+    trained on residuals of SSOR-COCG; base 1: it corrects the gradient-corrected
+    SSOR H (z = H(r) + N(r)), trained on residuals of H-preconditioned COCG."""
     freq = 1.0 / synth.M2_PERIOD_S
     p = init_params(seed) if params is None else np.asarray(params, np.float32)
     fw.mpnn_set_params(p)
+    fw.mpnn_set_base(base == 1)
     m0 = training_model(0, nx, ny, nz)
     fw.load_model(m0)
     hist = []
@@ -107,13 +119,14 @@ def train(fw, n_models: int = 512, steps_per_model: int = 2, lr: float = 1e-3, s
             m = training_model(k, nx, ny, nz)
             fw.set_cond(m.sigma_air, m.sigma_ocean, 1, sigma_file=m.sigma_land)
             fw.assemble()
-            R = collect_residuals(fw, freq)
+            R = collect_residuals(fw, freq, precond="HYBRID" if base == 1 else "SSOR")
             h = fw.mpnn_train(freq, R, steps_per_model, lr)
             hist.append(float(h[-1]))
             if log and (k % 64 == 0 or k == n_models - 1):
                 log(f"epoch {ep} model {k}: loss {h[-1]:.4f} ({time.time() - t0:.1f} s)")
     p = fw.mpnn_get_params()
     rec = {"models": n_models, "epochs": epochs, "steps_per_model": steps_per_model, "lr": lr, "seed": seed,
+           "base": base,
            "mesh": f"{nx}x{ny}x{nz}", "loss_first": hist[0] if hist else None,
            "loss_last_64": float(np.mean(hist[-64:])) if hist else None, "seconds": time.time() - t0}
     return p, rec

@@ -1,12 +1,13 @@
 """Train the learned preconditioner on the GPU and write its checkpoint.
 
-  python -m actfemtide_b200.train_learned [--models 512] [--steps 2] [--lr 1e-3] [--out PATH]
+  python -m actfemtide_b200.train_learned [--models 512] [--steps 2] [--lr 1e-3] [--base hybrid|jacobi] [--out PATH]
 
 Training models: seeded log-normal conductivity on the 32x32x24 mesh (air and
-sea layers, M2 source); residuals from plain FP64 SSOR-COCG; the network's
-own forward/backward kernels and Adam on the device.  After training, the
-held-out evaluation compares flexible COCG with the network against COCG
-without a preconditioner and against SSOR-COCG on fresh models.
+sea layers, M2 source); residuals from FP64 COCG with the network's base
+preconditioner (the gradient-corrected SSOR, or SSOR for the Jacobi base);
+the network's own forward/backward kernels and Adam on the device.  After
+training, the held-out evaluation compares flexible COCG with the network
+against its base alone and against the reference's SSOR-COCG on fresh models.
 """
 from __future__ import annotations
 
@@ -20,14 +21,18 @@ from . import learned, synth
 from .forward import Forward
 
 
-def evaluate(fw, params, models, freq, tol=1e-8, maxit=20000):
+def evaluate(fw, params, models, freq, tol=1e-8, maxit=20000, base=0):
+    """Iterations and time of flexible COCG with the network against its base and the reference's SSOR."""
     rows = []
     fw.mpnn_set_params(params)
+    fw.mpnn_set_base(base == 1)
+    runs = (("learned", "LEARNED"), ("hybrid", "HYBRID"), ("ssor", "SSOR")) if base == 1 else \
+        (("learned", "LEARNED"), ("none", "NONE"), ("ssor", "SSOR"))
     for m in models:
         fw.set_cond(m.sigma_air, m.sigma_ocean, 1, sigma_file=m.sigma_land)
         fw.assemble()
         rec = {}
-        for name, pc in (("learned", "LEARNED"), ("none", "NONE"), ("ssor", "SSOR")):
+        for name, pc in runs:
             r = fw.solve(freq, precond=pc, tol=tol, maxit=maxit)
             rec[name] = {"iterations": r.iterations, "seconds": r.seconds, "resid_true": r.resid_true,
                          "status": r.status}
@@ -43,19 +48,23 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--eval", type=int, default=4, help="held-out training-mesh models to evaluate")
-    ap.add_argument("--out", default=learned.DEFAULT_CKPT)
+    ap.add_argument("--base", choices=["jacobi", "hybrid"], default="hybrid",
+                    help="jacobi: the network is the preconditioner; hybrid: it corrects the gradient-corrected SSOR")
+    ap.add_argument("--out", default=None)
     a = ap.parse_args()
+    base = 1 if a.base == "hybrid" else 0
+    out = a.out or (learned.HYBRID_CKPT if base else learned.DEFAULT_CKPT)
     freq = 1.0 / synth.M2_PERIOD_S
     t0 = time.time()
     with Forward(0) as fw:
-        p, rec = learned.train(fw, a.models, a.steps, a.lr, a.seed, a.epochs)
+        p, rec = learned.train(fw, a.models, a.steps, a.lr, a.seed, a.epochs, base=base)
         held = [learned.training_model(100_000 + k) for k in range(a.eval)]
-        ev = evaluate(fw, p, held, freq)
-        ev0 = evaluate(fw, learned.init_params(a.seed), held[:1], freq)
+        ev = evaluate(fw, p, held, freq, base=base)
+        ev0 = evaluate(fw, learned.init_params(a.seed), held[:1], freq, base=base)
     rec["held_out"] = ev
     rec["untrained_held_out"] = ev0
     rec["wall_s"] = time.time() - t0
-    learned.save(a.out, p, rec)
+    learned.save(out, p, rec)
     print(json.dumps(rec))
 
 

@@ -241,6 +241,14 @@ int afem_xy_points(double xmin, double xmax, double ymin, double ymax, int nx, i
 int afem_mpnn_nparam(void);
 int afem_mpnn_set_params(afem_ctx *ctx, const float *params, int nparam);
 int afem_mpnn_get_params(afem_ctx *ctx, float *params);
+/* The network's base: 0 (default) z = r/|A_ii| + correction, a preconditioner on its
+ * own; 1: z = H(r) + correction with H the gradient-corrected multicolour SSOR
+ * (AFEM_PRECOND_HYBRID), so the network learns what H leaves; inside afem_solve the
+ * fallback on a stall is then H.  Training and afem_mpnn_forward follow the base. */
+int afem_mpnn_set_base(afem_ctx *ctx, int base);
+/* z = H(r), one application of the gradient-corrected multicolour SSOR to n complex values
+ * of the assembled system at freq_hz (the learned base; also for tests). */
+int afem_precond_apply(afem_ctx *ctx, double freq_hz, const double *r, double *z);
 /* z = P(r) for nsys systems at freq[k]; r, z: [row][system] interleaved complex. */
 int afem_mpnn_forward(afem_ctx *ctx, int nsys, const double *freq, const double *r, double *z);
 /* Sum over nsamp residuals (each n complex values) of ||A P(r) - r||^2/||r||^2 and its gradient. */

@@ -97,3 +97,57 @@ def test_flexible_cocg_learned_reaches_tolerance(fw):
     assert res_l.ok and res_l.resid_true <= 1e-8
     res_n = fw.solve(f, precond="NONE", tol=1e-8, maxit=20000)
     assert res_l.iterations < res_n.iterations
+
+
+def test_hybrid_base_adds_the_same_correction(fw):
+    """With the hybrid base the network's output is H(r) plus the correction it gives over the Jacobi base."""
+    m = synth.tidal_box(4, 4, 6, seed=3, site_grid=(-6.0, 0.0, 6.0), half_km=12.0)
+    fw.load_model(m)
+    fw.assemble()
+    f = m.freqs[0]
+    rng = np.random.default_rng(4)
+    p = learned.init_params(2)
+    p[-2 * learned.H:] = rng.standard_normal(2 * learned.H) * 0.1
+    p0 = p.copy()
+    p0[-2 * learned.H:] = 0.0  # no correction: the base alone
+    r = rng.standard_normal(fw.nline) + 1j * rng.standard_normal(fw.nline)
+    out = {}
+    for base in (False, True):
+        fw.mpnn_set_base(base)
+        fw.mpnn_set_params(p)
+        z = fw.mpnn_forward(f, r)
+        fw.mpnn_set_params(p0)
+        z0 = fw.mpnn_forward(f, r)
+        out[base] = (z, z0)
+    fw.mpnn_set_base(False)
+    h = fw.precond_apply(f, r)
+    assert np.array_equal(out[True][1], h)
+    corr_j = out[False][0] - out[False][1]
+    corr_h = out[True][0] - out[True][1]
+    # the Jacobi base adds r/|A_ii| and the correction in FP32; the hybrid base adds the correction to H(r)
+    assert np.abs(corr_h - corr_j).max() <= 1e-6 * np.abs(out[False][0]).max()
+    assert np.abs(corr_j).max() > 0
+
+
+def test_learned_over_hybrid_reaches_tolerance(fw):
+    """Flexible COCG with z = H(r) + N(r), trained briefly, reaches 1e-8 with no more than a few extra iterations."""
+    m = learned.training_model(7, 8, 8, 6)
+    fw.load_model(m)
+    fw.assemble()
+    f = m.freqs[0]
+    fw.mpnn_set_params(learned.init_params(0))
+    fw.mpnn_set_base(True)
+    for k in range(4):
+        mk = learned.training_model(k, 8, 8, 6)
+        fw.set_cond(mk.sigma_air, mk.sigma_ocean, 1, sigma_file=mk.sigma_land)
+        fw.assemble()
+        hist = fw.mpnn_train(f, learned.collect_residuals(fw, f, precond="HYBRID"), steps=20, lr=1e-3)
+        assert np.all(np.isfinite(hist))
+    fw.set_cond(m.sigma_air, m.sigma_ocean, 1, sigma_file=m.sigma_land)
+    fw.assemble()
+    r_l = fw.solve(f, precond="LEARNED", tol=1e-8, maxit=5000)
+    r_h = fw.solve(f, precond="HYBRID", tol=1e-8, maxit=5000)
+    fw.mpnn_set_base(False)
+    assert r_l.ok and r_l.resid_true <= 1e-8, r_l
+    assert r_h.ok
+    assert r_l.iterations <= 2 * r_h.iterations + 16, (r_l.iterations, r_h.iterations)
