@@ -17,7 +17,9 @@ plain-mc = the multicolour SSOR; hybrid = multicolour SSOR plus the
 gradient-space (nodal) correction; mixed = hybrid with FP32 inner COCG
 under FP64 refinement; batched / batched-mixed = 8 tidal periods x 2 source
 patterns = 16 systems per solve; learned* = flexible COCG with the learned
-network; packed = 24 uneven meshes (n x n x 3n/4, n in 8..32) in one solve.
+network (flexible COCG, z = H(r) + N(r) over the gradient-corrected SSOR H when
+that checkpoint exists); packed = 24 uneven meshes (n x n x 3n/4, n in 8..32)
+in one solve.
 
 Prints ONE JSON line on rank 0.  Under torchrun every rank solves its own
 independent systems (replicas; weak scaling), the time is the max over ranks.
@@ -171,6 +173,7 @@ METHODS = {
     "batched": ("HYBRID", "fp64", True),
     "batched-mixed": ("HYBRID", "mixed", True),
     "learned": ("LEARNED", "fp64", False),
+    "learned-batched": ("LEARNED", "fp64", True),
     "learned-batched-mixed": ("LEARNED", "mixed", True),
     "packed": ("HYBRID", "mixed", False),
 }
@@ -283,8 +286,11 @@ def run_gpu(args):
     fw = Forward(local)
     job.load(fw)
     if "learned" in args.method:
+        # the network over the gradient-corrected SSOR when that checkpoint exists, else the Jacobi-base one
         from actfemtide_b200 import learned
-        fw.mpnn_set_params(learned.load())
+        ckpt = learned.HYBRID_CKPT if os.path.exists(learned.HYBRID_CKPT + ".json") else learned.DEFAULT_CKPT
+        fw.mpnn_set_params(learned.load(ckpt))
+        fw.mpnn_set_base(learned.load_base(ckpt) == 1)
     n = fw.nline
     INU, IAU, INL, IAL = fw.export_pattern()
     nnz = n + 2 * len(IAU)
