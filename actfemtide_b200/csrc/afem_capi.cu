@@ -99,7 +99,7 @@ void load_split_system(afem_ctx* c, int n, const int32_t* INU, const int32_t* IA
   c->assembled = true;
   c->assemble_gen += 1;
   afem::hybrid_invalidate(c);
-  invalidate_work(c);
+  invalidate_pattern_work(c);
 }
 
 }  // namespace afem
@@ -204,6 +204,7 @@ int afem_set_mesh(afem_ctx* c, int node, const double* xyz, int ntet, const int3
     c->sigma_set = false;
     afem::clear_segments(c);
     afem::hybrid_invalidate(c);
+    afem::invalidate_pattern_work(c);
     if (c->grid) c->grid->ready = false;
     afem::reset_status(c);
     if (nline > 0) {
@@ -300,7 +301,7 @@ int afem_set_segments(afem_ctx* c, int nseg, const int32_t* node_ptr) {
     c->seg_of_row.upload(seg.data(), seg.size(), s);
     AFEM_CUDA(cudaStreamSynchronize(s));
     c->nseg = nseg;
-    afem::invalidate_work(c);
+    afem::invalidate_pattern_work(c);
     c->nsys = 0;
     return (int)AFEM_OK;
   });

@@ -259,8 +259,9 @@ int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, cons
 void load_split_system(afem_ctx* c, int n, const int32_t* INU, const int32_t* IAU, const int32_t* INL,
                        const int32_t* IAL, const double* D, const double* AU, const double* AL, const double* b);
 void destroy_work(afem_ctx* c);
-void invalidate_work(afem_ctx* c);
-void get_residual(afem_ctx* c, int k, double* r);  // b - A x of system k after the last solve      // values changed: drop derived copies (FP32 matrix)
+void invalidate_work(afem_ctx* c);          // new matrix values
+void invalidate_pattern_work(afem_ctx* c);  // new pattern
+void get_residual(afem_ctx* c, int k, double* r);  // b - A x of system k after the last solve
 
 // afem_mpnn.cu (learned preconditioner)
 void mpnn_destroy(afem_ctx* c);

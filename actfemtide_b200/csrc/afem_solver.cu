@@ -156,16 +156,19 @@ __device__ __forceinline__ void row_gather(const int32_t* __restrict__ cols, con
                                            T& t2x, T& t2y) {
   using V = typename Cx<T>::V;
   int k = k0;
-  for (; k + 3 * G < k1; k += 4 * G) {
-    const int j0 = __ldg(cols + k), j1 = __ldg(cols + k + G), j2 = __ldg(cols + k + 2 * G), j3 = __ldg(cols + k + 3 * G);
-    const V a0 = vals[k], a1 = vals[k + G], a2 = vals[k + 2 * G], a3 = vals[k + 3 * G];
-    const V v0 = ldcg(vec + (long)j0 * NS + s), v1 = ldcg(vec + (long)j1 * NS + s);
-    const V v2 = ldcg(vec + (long)j2 * NS + s), v3 = ldcg(vec + (long)j3 * NS + s);
-    t1x += a0.x * v0.x; t1y += a0.x * v0.y; t2x += a0.y * v0.x; t2y += a0.y * v0.y;
-    t1x += a1.x * v1.x; t1y += a1.x * v1.y; t2x += a1.y * v1.x; t2y += a1.y * v1.y;
-    t1x += a2.x * v2.x; t1y += a2.x * v2.y; t2x += a2.y * v2.x; t2y += a2.y * v2.y;
-    t1x += a3.x * v3.x; t1y += a3.x * v3.y; t2x += a3.y * v3.x; t2y += a3.y * v3.y;
-  }
+  // four loads in flight only where one lane owns the row: with G > 1 lanes per row each
+  // holds few entries and the unrolled registers cost occupancy
+  if constexpr (G == 1)
+    for (; k + 3 < k1; k += 4) {
+      const int j0 = __ldg(cols + k), j1 = __ldg(cols + k + 1), j2 = __ldg(cols + k + 2), j3 = __ldg(cols + k + 3);
+      const V a0 = vals[k], a1 = vals[k + 1], a2 = vals[k + 2], a3 = vals[k + 3];
+      const V v0 = ldcg(vec + (long)j0 * NS + s), v1 = ldcg(vec + (long)j1 * NS + s);
+      const V v2 = ldcg(vec + (long)j2 * NS + s), v3 = ldcg(vec + (long)j3 * NS + s);
+      t1x += a0.x * v0.x; t1y += a0.x * v0.y; t2x += a0.y * v0.x; t2y += a0.y * v0.y;
+      t1x += a1.x * v1.x; t1y += a1.x * v1.y; t2x += a1.y * v1.x; t2y += a1.y * v1.y;
+      t1x += a2.x * v2.x; t1y += a2.x * v2.y; t2x += a2.y * v2.x; t2y += a2.y * v2.y;
+      t1x += a3.x * v3.x; t1y += a3.x * v3.y; t2x += a3.y * v3.x; t2y += a3.y * v3.y;
+    }
   for (; k < k1; k += G) {
     const int j = __ldg(cols + k);
     const V a = vals[k];
@@ -1916,11 +1919,21 @@ void get_residual(afem_ctx* c, int k, double* r) {
   }
 }
 
+// New matrix values: the FP32 copies are stale.  The SpMV tuning stays (it
+// depends on the pattern only), so repeated solves take the same reduction
+// order and give the same bits.
 void invalidate_work(afem_ctx* c) {
+  if (c->work) c->work->kmf_valid = false;
+}
+
+// A new pattern: also tune the SpMV again.
+void invalidate_pattern_work(afem_ctx* c) {
   if (c->work) {
     c->work->kmf_valid = false;
     c->work->rpw64 = c->work->rpw32 = 0;
+    c->work->n = -1;  // re-allocate for the new size
   }
+  c->nsys = 0;  // the old solutions belong to the old pattern
 }
 
 void destroy_work(afem_ctx* c) {

@@ -124,8 +124,11 @@ def test_hybrid_base_adds_the_same_correction(fw):
     assert np.array_equal(out[True][1], h)
     corr_j = out[False][0] - out[False][1]
     corr_h = out[True][0] - out[True][1]
-    # the Jacobi base adds r/|A_ii| and the correction in FP32; the hybrid base adds the correction to H(r)
-    assert np.abs(corr_h - corr_j).max() <= 1e-6 * np.abs(out[False][0]).max()
+    # the Jacobi base adds r/|A_ii| and the correction in one FP32 sum, the hybrid base adds the
+    # correction to H(r) in FP64: where the two FP32 terms nearly cancel (rows with a small |A_ii|)
+    # the rounding scales with the terms, so bound each element by FP32 rounding of its terms
+    terms = np.abs(out[False][0]) + np.abs(out[False][1]) + np.abs(corr_j)
+    assert np.all(np.abs(corr_h - corr_j) <= 4 * 2.0 ** -24 * terms + 1e-12)
     assert np.abs(corr_j).max() > 0
 
 
