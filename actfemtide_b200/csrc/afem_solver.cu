@@ -60,7 +60,7 @@ struct SysScal {
   int active;     // 1 while iterating
   int status;     // afem_status of this system
   int iter;       // iterations done
-  int pad;
+  int xpend;      // multicolour path: this iteration's x += alpha p waits for the p update
 };
 
 struct Ctrl {
@@ -89,11 +89,13 @@ struct SolverWork {
   DBuf<float2> htf, hyf, hddf;      // the same for the FP32 inner solve
   int nmc_blocks = 0;               // co-resident grid of the nodal multicolour sweeps
   int rpw64 = 0, rpw32 = 0;         // SpMV rows per warp chosen by tune_spmv (0 = not tuned)
-  int mc_blocks = 0;                // co-resident grid of the multicolour sweeps
+  int mc_blocks = 0;                // co-resident grid of the forward multicolour sweep
+  int mcb_blocks = 0;               // and of the backward one (fewer registers: more blocks)
   bool no_window = false;           // COCG13_single semantics: no stagnation window, run to the cap
   bool kmf_valid = false;
   DBuf<unsigned> flag_f, flag_b;
   DBuf<double> part;                // partial sums [block][sys][4]
+  DBuf<double> part2;               // nodal share of rho (hybrid), same layout
   DBuf<SysScal> sc;
   DBuf<Ctrl> ctrl;
   Ctrl* h_ctrl = nullptr;           // pinned mirror
@@ -419,8 +421,8 @@ template <class T, int NS, bool SEG = false>
 __global__ void __launch_bounds__(256)
     k_fwd_mc(const int32_t* __restrict__ lptr, const int32_t* __restrict__ lcol, const typename Cx<T>::V* __restrict__ lkm,
              int n, typename Cx<T>::V* __restrict__ r, typename Cx<T>::V* __restrict__ y,
-             const typename Cx<T>::V* __restrict__ p, const typename Cx<T>::V* __restrict__ q, double2* __restrict__ x,
-             const typename Cx<T>::V* __restrict__ dd, const int32_t* __restrict__ perm,
+             const typename Cx<T>::V* __restrict__ q, const typename Cx<T>::V* __restrict__ dd,
+             const int32_t* __restrict__ perm,
              const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl,
              double* __restrict__ part, const uint8_t* __restrict__ seg, typename Cx<T>::V* __restrict__ rprev) {
   using V = typename Cx<T>::V;
@@ -454,15 +456,11 @@ __global__ void __launch_bounds__(256)
       }
       V ri = live ? r[(long)row * NS + s] : Cx<T>::make(0, 0);
       if (rprev && live && g == 0) rprev[(long)row * NS + s] = ri;  // flexible COCG keeps r_k
-      if (live && update && act && g == 0) {
-        const V qi = q[(long)row * NS + s], pi = p[(long)row * NS + s];
+      if (live && update && act && g == 0) {  // x += alpha p follows in the p update
+        const V qi = q[(long)row * NS + s];
         ri = Cx<T>::make((T)((double)ri.x - (al.x * (double)qi.x - al.y * (double)qi.y)),
                          (T)((double)ri.y - (al.x * (double)qi.y + al.y * (double)qi.x)));
         r[(long)row * NS + s] = ri;
-        double2 xi = x[(long)row * NS + s];
-        xi.x += al.x * (double)pi.x - al.y * (double)pi.y;
-        xi.y += al.x * (double)pi.y + al.y * (double)pi.x;
-        x[(long)row * NS + s] = xi;
       }
       if (live && g == 0) {
         const double v = (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
@@ -609,6 +607,8 @@ __global__ void k_grad_t(int node, const int32_t* __restrict__ nptr, const int32
 // One multicolour SSOR sweep on the nodal matrix, over its colour-ordered split
 // rows (as the edge sweeps): forward y_a = (t_a - sum_{col(b)<col(a)} A_ab y_b) dd_a,
 // backward (in place) y_a -= dd_a sum_{col(b)>col(a)} A_ab y_b.  Grid barrier between colours.
+// part (backward, nullable): partial sums of t^T y over the final y, the share
+// r^T G u of rho = r^T (z + G u) (since t = G^T r), slots 0, 1.
 template <class T, int NS, bool SEG>
 __global__ void __launch_bounds__(256)
     k_nsweep_mc(const int32_t* __restrict__ xptr, const int32_t* __restrict__ xcol,
@@ -616,7 +616,7 @@ __global__ void __launch_bounds__(256)
                 typename Cx<T>::V* __restrict__ y, const typename Cx<T>::V* __restrict__ dd,
                 const int32_t* __restrict__ perm, const int32_t* __restrict__ cptr, int ncolors,
                 const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl, const uint8_t* __restrict__ seg,
-                int backward) {
+                int backward, double* __restrict__ part) {
   using V = typename Cx<T>::V;
   using S = McShape<NS, SEG>;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
@@ -626,6 +626,7 @@ __global__ void __launch_bounds__(256)
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double om = sc[s].omega;
+  double tx = 0.0, ty = 0.0;
   for (int cc = 0; cc < ncolors; ++cc) {
     const int c = backward ? ncolors - 1 - cc : cc;
     const int p0 = cptr[c], p1 = cptr[c + 1];
@@ -652,11 +653,26 @@ __global__ void __launch_bounds__(256)
           y[(long)row * NS + s] = Cx<T>::make(wx * d.x - wy * d.y, wx * d.y + wy * d.x);
         } else {
           const V yi = y[(long)row * NS + s];
-          y[(long)row * NS + s] = Cx<T>::make(yi.x - (d.x * sx - d.y * sy), yi.y - (d.x * sy + d.y * sx));
+          const V yn = Cx<T>::make(yi.x - (d.x * sx - d.y * sy), yi.y - (d.x * sy + d.y * sx));
+          y[(long)row * NS + s] = yn;
+          if (part) {
+            const V ti = t[(long)row * NS + s];
+            tx += (double)ti.x * (double)yn.x - (double)ti.y * (double)yn.y;
+            ty += (double)ti.x * (double)yn.y + (double)ti.y * (double)yn.x;
+          }
         }
       }
     }
     grid.sync();
+  }
+  if (part) {  // uniform over the grid
+#pragma unroll
+    for (int m = S::LPR; m < 32; m <<= 1) {
+      tx += __shfl_xor_sync(0xffffffffu, tx, m);
+      ty += __shfl_xor_sync(0xffffffffu, ty, m);
+    }
+    double v[4] = {tx, ty, 0.0, 0.0};
+    block_partials<NS, 4>(v, part);
   }
 }
 
@@ -771,21 +787,54 @@ __global__ void k_dd_node(const double2* __restrict__ km, const int32_t* __restr
 }
 
 // ------------------------------------------------------------------ p update, SpMV
+// Multicolour path (x != nullptr): first x += alpha p with the old p for the
+// systems whose update is pending (also after the residual check ended the
+// solve).  Hybrid preconditioner with the gradient add folded in (u != nullptr):
+// z_e + u_head(e) - u_tail(e) on the non-Dirichlet edges stands for z.
 template <class T, int NS, bool SEG = false>
 __global__ void k_pupd(int n, const typename Cx<T>::V* __restrict__ z, typename Cx<T>::V* __restrict__ p,
-                       const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl, const uint8_t* __restrict__ seg) {
+                       const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl, const uint8_t* __restrict__ seg,
+                       double2* __restrict__ x, int nsys, const int32_t* __restrict__ line,
+                       const uint8_t* __restrict__ bc, const typename Cx<T>::V* __restrict__ u) {
   using V = typename Cx<T>::V;
-  if (ctrl->done) return;
+  const bool done = ctrl->done;
+  if (done) {
+    if (!x) return;
+    bool any = false;
+    for (int k = 0; k < nsys; ++k) any |= sc[k].xpend != 0;
+    if (!any) return;
+  }
   const bool first = ctrl->iter == 0;
   const long total = (long)n * NS;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
     const int s = SEG ? (int)__ldg(seg + i) : (int)(i % NS);
-    const V zi = z[i];
+    V pi = Cx<T>::make(0, 0);
+    bool have_p = false;
+    if (x && sc[s].xpend) {
+      pi = p[i];
+      have_p = true;
+      const double2 al = sc[s].alpha;
+      double2 xi = x[i];
+      xi.x += al.x * (double)pi.x - al.y * (double)pi.y;
+      xi.y += al.x * (double)pi.y + al.y * (double)pi.x;
+      x[i] = xi;
+    }
+    if (done) continue;
+    V zi = z[i];
+    if (u) {
+      const int e = (int)(i / NS);
+      if (!__ldg(bc + e)) {
+        const int sn = SEG ? 0 : s;
+        const V uh = u[(long)(__ldg(line + 2 * e + 1) - 1) * NS + sn];
+        const V ut = u[(long)(__ldg(line + 2 * e) - 1) * NS + sn];
+        zi = Cx<T>::make(zi.x + (uh.x - ut.x), zi.y + (uh.y - ut.y));
+      }
+    }
     if (first) {
       p[i] = zi;
     } else {
       const double2 be = sc[s].beta;
-      const V pi = p[i];
+      if (!have_p) pi = p[i];
       p[i] = Cx<T>::make((T)((double)zi.x + (be.x * (double)pi.x - be.y * (double)pi.y)),
                          (T)((double)zi.y + (be.x * (double)pi.y + be.y * (double)pi.x)));
     }
@@ -890,8 +939,16 @@ __device__ __forceinline__ void sum_partials(const double* part, int nblocks, in
   for (int v = 0; v < nvals; ++v) out[v] = sh[threadIdx.x >> 5][v];
 }
 
-__global__ void k_scal_r(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns, double* rms, int n) {
-  if (ctrl->done) return;
+// defer_x (multicolour path): the sweep updated r only; x += alpha p of an active
+// system is marked pending and applied by the p update of the same iteration,
+// which also runs when this kernel ends the solve.
+__global__ void k_scal_r(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns, double* rms, int n,
+                         int defer_x) {
+  if (ctrl->done) {
+    // the update pending when the solve ended was applied by that iteration's p update
+    if (defer_x && threadIdx.x < ns) sc[threadIdx.x].xpend = 0;
+    return;
+  }
   const int s = threadIdx.x >> 5;
   bool finished = true;
   if (s < ns) {
@@ -899,6 +956,7 @@ __global__ void k_scal_r(SysScal* sc, Ctrl* ctrl, const double* part, int nblock
     sum_partials(part, nblocks, s, 0, &rr, 1);
     if ((threadIdx.x & 31) == 0) {
       SysScal& S = sc[s];
+      S.xpend = defer_x && S.active && ctrl->iter > 0;
       if (S.active) {
         S.rr = rr;
         if (rms) rms[s] = sqrt(rr / n) > 0.0 ? sqrt(rr / n) : 1.0;
@@ -922,12 +980,22 @@ __global__ void k_scal_r(SysScal* sc, Ctrl* ctrl, const double* part, int nblock
 
 __device__ __forceinline__ double2 d_cdiv(double2 a, double2 b) { return cdiv(a, b); }
 
-__global__ void k_scal_rho(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns, int flexible) {
+// part2 (nullable): the nodal correction's share r^T G u = t^T u of rho, summed by
+// the backward nodal sweep when the gradient add is folded into the p update
+__global__ void k_scal_rho(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns, int flexible,
+                           const double* part2, int nblocks2) {
   if (ctrl->done) return;
   const int s = threadIdx.x >> 5;
   if (s >= ns) return;
   double v[4];
   sum_partials(part, nblocks, s, 0, v, 4);
+  if (part2) {
+    double v2[2];
+    __syncwarp();
+    sum_partials(part2, nblocks2, s, 0, v2, 2);
+    v[0] += v2[0];
+    v[1] += v2[1];
+  }
   if ((threadIdx.x & 31) == 0) {
     SysScal& S = sc[s];
     S.rho = make_double2(v[0], v[1]);
@@ -1079,6 +1147,7 @@ __global__ void k_init_sys(SysScal* sc, Ctrl* ctrl, const double* part, int nblo
       S.resid = 1.0;
       S.rho = S.rho1 = S.alpha = S.beta = S.pq = make_double2(0.0, 0.0);
       S.iter = 0;
+      S.xpend = 0;
       S.active = v[0] > 0.0;
       S.status = AFEM_OK;
     }
@@ -1246,10 +1315,13 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
   const bool lbase = learned && mpnn_base(c) == 1;
   const bool hyb = mode == AFEM_PRECOND_HYBRID || lbase;
   const bool mc = mode == AFEM_PRECOND_SSOR_MC || hyb;  // the hybrid's edge part is the multicolour SSOR
+  // hybrid alone (one matrix): z + G u is formed inside the p update, and the
+  // backward nodal sweep sums t^T u, the nodal share of rho
+  const bool fold_grad = hyb && !lbase && !SEG;
   if (ev) AFEM_CUDA(cudaEventRecord(ev[0], s));
-  if (mc)
+  if (mc)  // the multicolour sweep updates r only: x += alpha p moves to the p update
     launch_coop(k_fwd_mc<T, NS, SEG>, w->mc_blocks, s, (const int32_t*)c->mc_lptr.p, (const int32_t*)c->mc_lcol.p,
-                I::LKM(c, w), n, I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w), w->x.p, (const V*)I::DD(w),
+                I::LKM(c, w), n, I::R(w), I::Z(w), (const V*)I::Q(w), (const V*)I::DD(w),
                 (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p,
                 w->part.p, sg, rp);
   else
@@ -1259,12 +1331,13 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
                 (const int32_t*)c->perm_f.p, sg);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[1], s));
   const int swb = mc ? w->mc_blocks : sweep_blocks;
-  k_scal_r<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, swb, nsys, learned ? w->rms.p : nullptr, n);
+  k_scal_r<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, swb, nsys, learned ? w->rms.p : nullptr, n,
+                                      mc ? 1 : 0);
   count_launch();
   if (learned && !lbase) mpnn_run<V>(c, NS, w->rms.p, (const V*)I::R(w), I::Z(w), &w->ctrl.p->done);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[2], s));
   if (mc)
-    launch_coop(k_bwd_mc<T, NS, SEG>, w->mc_blocks, s, (const int32_t*)c->mc_uptr.p, (const int32_t*)c->mc_ucol.p,
+    launch_coop(k_bwd_mc<T, NS, SEG>, w->mcb_blocks, s, (const int32_t*)c->mc_uptr.p, (const int32_t*)c->mc_ucol.p,
                 I::UKM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w), (const int32_t*)c->perm_mc.p,
                 (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p, sg);
   else
@@ -1273,9 +1346,10 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
                 w->flag_b.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, (const V*)rp,
                 (const int32_t*)c->perm_b.p, sg);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[3], s));
-  int rho_blocks = swb;
+  int rho_blocks = mc ? w->mcb_blocks : sweep_blocks;
   if (hyb) {
-    // z += G SSOR_node(G^T r); the rho partials are taken again from the corrected z
+    // z += G SSOR_node(G^T r): folded into the p update, or (packed batches, learned
+    // base) a pass of its own that takes the rho partials again from the corrected z
     HybridState* h = c->hyb;
     const int node = h->node;
     const uint8_t* hs = SEG ? h->seg.p : nullptr;
@@ -1286,11 +1360,14 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
       launch_coop(k_nsweep_mc<T, NS, SEG>, w->nmc_blocks, s, (const int32_t*)(bwd ? h->uptr.p : h->lptr.p),
                   (const int32_t*)(bwd ? h->ucol.p : h->lcol.p), bwd ? I::HUKM(c) : I::HLKM(c),
                   (const V*)I::HT(w), I::HY(w), (const V*)I::HDD(w), (const int32_t*)h->perm.p,
-                  (const int32_t*)h->cptr.p, h->ncolors, (const SysScal*)w->sc.p, (const Ctrl*)w->ctrl.p, hs, bwd);
-    k_grad_add<T, NS, SEG><<<w->nblocks, 256, 0, s>>>(n, c->line.p, c->bc.p, (const V*)I::HY(w), I::Z(w),
-                                                        (const V*)I::R(w), w->ctrl.p, w->part.p, sg);
-    count_launch();
-    rho_blocks = w->nblocks;
+                  (const int32_t*)h->cptr.p, h->ncolors, (const SysScal*)w->sc.p, (const Ctrl*)w->ctrl.p, hs, bwd,
+                  (fold_grad && bwd) ? w->part2.p : (double*)nullptr);
+    if (!fold_grad) {
+      k_grad_add<T, NS, SEG><<<w->nblocks, 256, 0, s>>>(n, c->line.p, c->bc.p, (const V*)I::HY(w), I::Z(w),
+                                                          (const V*)I::R(w), w->ctrl.p, w->part.p, sg);
+      count_launch();
+      rho_blocks = w->nblocks;
+    }
   }
   if (lbase) {
     // z += N(r), then rho = r^T z and rprev^T z of the final z for the flexible beta
@@ -1301,10 +1378,14 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
     rho_blocks = w->nblocks;
   }
   if (ev) AFEM_CUDA(cudaEventRecord(ev[4], s));
-  k_scal_rho<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, rho_blocks, nsys, learned ? 1 : 0);
+  k_scal_rho<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, rho_blocks, nsys, learned ? 1 : 0,
+                                        fold_grad ? w->part2.p : (const double*)nullptr, w->nmc_blocks);
   count_launch();
   if (ev) AFEM_CUDA(cudaEventRecord(ev[5], s));
-  k_pupd<T, NS, SEG><<<c->num_sms * 8, 256, 0, s>>>(n, I::Z(w), I::P(w), w->sc.p, w->ctrl.p, sg);
+  k_pupd<T, NS, SEG><<<c->num_sms * 8, 256, 0, s>>>(
+      n, I::Z(w), I::P(w), w->sc.p, w->ctrl.p, sg, mc ? w->x.p : (double2*)nullptr, nsys,
+      fold_grad ? (const int32_t*)c->line.p : (const int32_t*)nullptr, fold_grad ? c->bc.p : (const uint8_t*)nullptr,
+      fold_grad ? (const V*)I::HY(w) : (const V*)nullptr);
   count_launch();
   if (ev) AFEM_CUDA(cudaEventRecord(ev[6], s));
   launch_spmv<T, NS, SEG>(c, w, sizeof(T) == 8 ? w->rpw64 : w->rpw32, I::KM(c, w), (const V*)I::P(w), I::Q(w),
@@ -1429,9 +1510,10 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   const int sweep_blocks = coresident_blocks(k_fwd<T, NS, SEG>, c->num_sms);
   const int sb2 = coresident_blocks(k_bwd<T, NS, SEG>, c->num_sms);
   const int sblocks = std::min(std::min(sweep_blocks, sb2), w->nblocks);
-  if (mode == AFEM_PRECOND_SSOR_MC || use_hyb)
-    w->mc_blocks = std::min(std::min(coresident_blocks(k_fwd_mc<T, NS, SEG>, c->num_sms),
-                                     coresident_blocks(k_bwd_mc<T, NS, SEG>, c->num_sms)), w->nblocks);
+  if (mode == AFEM_PRECOND_SSOR_MC || use_hyb) {
+    w->mc_blocks = std::min(coresident_blocks(k_fwd_mc<T, NS, SEG>, c->num_sms), w->nblocks);
+    w->mcb_blocks = std::min(coresident_blocks(k_bwd_mc<T, NS, SEG>, c->num_sms), w->nblocks);
+  }
   if (use_hyb)
     w->nmc_blocks = std::min(coresident_blocks(k_nsweep_mc<T, NS, SEG>, c->num_sms), w->nblocks);
   // every solve starts a fresh flag generation: a solve that stopped inside a
@@ -1621,6 +1703,7 @@ SolverWork* ensure_work(afem_ctx* c, int nsys, bool mixed) {
     AFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_spmv<double, NS, 1, SEG>, 256, 0));
     w->nblocks = std::max(1, b1) * c->num_sms;
     w->nblocks = std::max(w->nblocks, coresident_blocks(k_fwd_mc<double, NS, SEG>, c->num_sms));
+    w->nblocks = std::max(w->nblocks, coresident_blocks(k_bwd_mc<double, NS, SEG>, c->num_sms));
     int bf = coresident_blocks(k_fwd<double, NS, SEG>, c->num_sms);
     int bb = coresident_blocks(k_bwd<double, NS, SEG>, c->num_sms);
     w->nblocks = std::max(w->nblocks, std::max(bf, bb));
@@ -1629,6 +1712,7 @@ SolverWork* ensure_work(afem_ctx* c, int nsys, bool mixed) {
       w->nblocks = std::max(w->nblocks, coresident_blocks(k_bwd<float, NS, SEG>, c->num_sms));
     }
     w->part.alloc((size_t)w->nblocks * MAX_SYS * 4);
+    w->part2.alloc((size_t)w->nblocks * MAX_SYS * 4);
   }
   return w;
 }
@@ -1877,7 +1961,7 @@ void precond_apply_device(afem_ctx* c, double omega, const double2* r, double2* 
                                    coresident_blocks(k_bwd_mc<double, 1, false>, c->num_sms)), w->nblocks);
   w->nmc_blocks = std::min(coresident_blocks(k_nsweep_mc<double, 1, false>, c->num_sms), w->nblocks);
   launch_coop(k_fwd_mc<double, 1, false>, w->mc_blocks, s, (const int32_t*)c->mc_lptr.p, (const int32_t*)c->mc_lcol.p,
-              (const double2*)c->mc_lkm.p, n, w->r.p, w->z.p, (const double2*)w->p.p, (const double2*)w->q.p, w->x.p,
+              (const double2*)c->mc_lkm.p, n, w->r.p, w->z.p, (const double2*)w->q.p,
               (const double2*)w->dd.p, (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors,
               w->sc.p, w->ctrl.p, w->part.p, (const uint8_t*)nullptr, (double2*)nullptr);
   launch_coop(k_bwd_mc<double, 1, false>, w->mc_blocks, s, (const int32_t*)c->mc_uptr.p, (const int32_t*)c->mc_ucol.p,
@@ -1892,7 +1976,7 @@ void precond_apply_device(afem_ctx* c, double omega, const double2* r, double2* 
                 (const int32_t*)(bwd ? h->ucol.p : h->lcol.p), (const double2*)(bwd ? h->ukm.p : h->lkm.p),
                 (const double2*)w->ht.p, w->hy.p, (const double2*)w->hdd.p, (const int32_t*)h->perm.p,
                 (const int32_t*)h->cptr.p, h->ncolors, (const SysScal*)w->sc.p, (const Ctrl*)w->ctrl.p,
-                (const uint8_t*)nullptr, bwd);
+                (const uint8_t*)nullptr, bwd, (double*)nullptr);
   k_grad_add<double, 1, false><<<w->nblocks, 256, 0, s>>>(n, c->line.p, c->bc.p, (const double2*)w->hy.p, w->z.p,
                                                           (const double2*)w->r.p, w->ctrl.p, w->part.p,
                                                           (const uint8_t*)nullptr);

@@ -48,6 +48,10 @@ METRIC = "s per complex edge-FEM solve to 1e-8 residual: learned+batched vs plai
 PLAIN_96 = {"iterations": 30000, "converged": False, "resid_true_at_cap": 6.843e-05, "ms_per_iteration": 15.862,
             "seconds_at_cap": 475.9}
 UNIT = "s/solve"
+# DRAM traffic of one forward multicolour sweep (FP64, 16 systems) from an ncu capture of the
+# 48x48x32 model (532,352 edges: dram__bytes_read.sum + dram__bytes_write.sum = 1.628 GB per
+# launch), per edge row; scaled to the bench's model by its rows
+FWD_MC_NS16_TRAFFIC = {"kernel": "cocg_fwd_sweep_mc_fp64_ns16", "bytes": 1.628e9, "rows": 532352}
 TOL = 1e-8
 FALLBACK_HBM_GBS = 6650.0
 
@@ -126,16 +130,20 @@ def dist_info():
 
 
 def kernel_bytes(name: str, n: int, nnz: int, ns: int, real_bytes: int, ntet: int = 0, nsrc: int = 1,
-                 node: int = 0, nodes: int = 0) -> float:
-    """Algorithmic bytes of one launch of the named kernel (values read/written once)."""
+                 node: int = 0, nodes: int = 0, mc: bool = False, fold: bool = False) -> float:
+    """Algorithmic bytes of one launch of the named kernel (values read/written once).
+
+    mc: multicolour iteration (x += alpha p moves from the forward sweep to the p
+    update); fold: the hybrid's z += G u is formed inside the p update."""
     if "_seg" in name:
         ns = 1  # packed batch: one system per row
     ent = 2 * real_bytes + 4          # (K, M) pair + column index per stored entry
     vec = 2 * real_bytes * ns         # one complex value per system per row
     off = (nnz - n) // 2              # strictly lower (= strictly upper) entries
     if name.startswith("cocg_fwd_sweep_mc"):
-        # colour-ordered split rows: the earlier-colour half, position pointers, row ids; vectors as below
-        return ent * off + 8 * n + n * (vec * 6 + 32 * ns)
+        # colour-ordered split rows: the earlier-colour half, position pointers, row ids;
+        # r r/w, q, DD, y write (x is updated in the p update)
+        return ent * off + 8 * n + n * vec * 5
     if name.startswith("cocg_bwd_sweep_mc"):
         return ent * off + 8 * n + n * vec * 5
     if name.startswith("cocg_nodal_correction"):
@@ -143,6 +151,8 @@ def kernel_bytes(name: str, n: int, nnz: int, ns: int, real_bytes: int, ntet: in
         vn = vec                      # nodal vectors have the edge vectors' width
         gt = 4 * (node + 1) + 8 * n + n + 2 * n * vec + node * vn
         sweeps = 2 * (2 * real_bytes * n + 5 * nnz_n + 4 * (node + 1) + 4 * node + 3 * node * vn)
+        if fold:  # the backward nodal sweep also reads t for t^T u
+            return gt + sweeps + node * vn
         gadd = 8 * n + n + 2 * n * vec + 3 * n * vec
         return gt + sweeps + gadd
     if name.startswith("cocg_fwd_sweep"):
@@ -155,7 +165,12 @@ def kernel_bytes(name: str, n: int, nnz: int, ns: int, real_bytes: int, ntet: in
         # all entries, rowptr; p gather, p own read (p^T q), q write
         return ent * nnz + 4 * (n + 1) + n * vec * 3
     if name.startswith("cocg_p_update"):
-        return n * vec * 3
+        b = n * vec * 3                     # z read, p read and write
+        if mc:
+            b += n * 32 * ns                # x read and write (FP64)
+        if fold:
+            b += 8 * n + n + node * vec     # line, bc, u (each node once)
+        return b
     if name.startswith("assemble_rows"):
         # tetrahedron data (n4, n6line, tag, sigma), node coordinates, adjacency, pattern, values, rhs
         return ntet * (16 + 24 + 4 + 8) + 24 * node + 24 * ntet + 4 * (n + 1) + 4 * nnz + 16 * nnz + 16 * n * nsrc \
@@ -378,8 +393,16 @@ def run_gpu(args):
         if kms > dom_ms:
             dom, dom_ms, dom_n = name, kms, cnt
     rb = 4 if "fp32" in (dom or "") else 8
-    per_launch = kernel_bytes(dom or "", n, nnz, ns, rb, job.ntet, job.nsrc, job.node, job.nodes)
+    pc = kw["precond"]
+    mc = pc in ("SSOR_MC", "HYBRID") or "learned" in args.method
+    fold = pc == "HYBRID" and args.method != "packed"
+    per_launch = kernel_bytes(dom or "", n, nnz, ns, rb, job.ntet, job.nsrc, job.node, job.nodes, mc=mc, fold=fold)
     achieved = per_launch / (dom_ms / max(1, dom_n) / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    traffic, traffic_src = None, None
+    if dom == FWD_MC_NS16_TRAFFIC["kernel"]:
+        traffic = FWD_MC_NS16_TRAFFIC["bytes"] * n / FWD_MC_NS16_TRAFFIC["rows"]
+        traffic_src = ("ncu dram bytes of one launch on the 48x48x32 model (1.628 GB, 532,352 rows) scaled by "
+                       "the rows; a lower estimate, since the L2 hit rate falls as the working set grows")
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.method != "packed":
         cpu = cpu_baseline(job.m, job.freqs[0], args.ref_iters, args.cpu_seconds)
@@ -402,7 +425,8 @@ def run_gpu(args):
                 "steps": e2e_steps, "includes": "set_mesh (upload, pattern) + cond + source + assemble + solve + sites"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "peak_kind": peak_kind,
-                     "bytes_per_launch": per_launch, "avg_launch_ms": dom_ms / max(1, dom_n), "traffic": None,
+                     "bytes_per_launch": per_launch, "avg_launch_ms": dom_ms / max(1, dom_n), "traffic": traffic,
+                     "traffic_source": traffic_src,
                      "profile_pass": f"one step with the iteration cap at {args.prof_iters}, CUDA events around "
                                      "every kernel (graphs off), outside the timed region",
                      "kernel_share": {k: round(v[0] / max(1e-9, total_ms), 4)
