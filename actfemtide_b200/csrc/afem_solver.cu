@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(256)
   double om = sc[s].omega;
   double2 al = sc[s].alpha;
   bool act = sc[s].active;
-  double rr = 0.0;
+  double rr = 0.0, rhx = 0.0, rhy = 0.0;
   double (*red)[MAX_SYS][1] = nullptr;
   if constexpr (SEG) red = seg_sums<8 * S::RPW, 1>();
   for (int c = 0; c < ncolors; ++c) {
@@ -480,6 +480,11 @@ __global__ void __launch_bounds__(256)
         const T wx = ri.x - (t1x - o * t2y), wy = ri.y - (t1y + o * t2x);
         const V d = dd[(long)row * NS + s];
         y[(long)row * NS + s] = Cx<T>::make(wx * d.x - wy * d.y, wx * d.y + wy * d.x);
+        if constexpr (!SEG) {  // rho = r^T z = y^T D y = sum dd_i w_i^2 (U = L^T)
+          const double w2x = (double)wx * (double)wx - (double)wy * (double)wy, w2y = 2.0 * (double)wx * (double)wy;
+          rhx += (double)d.x * w2x - (double)d.y * w2y;
+          rhy += (double)d.x * w2y + (double)d.y * w2x;
+        }
       }
     }
     grid.sync();
@@ -488,9 +493,13 @@ __global__ void __launch_bounds__(256)
     seg_partials<8 * S::RPW, 1>(red, part);
   } else {
 #pragma unroll
-    for (int m = S::LPR; m < 32; m <<= 1) rr += __shfl_xor_sync(0xffffffffu, rr, m);
-    double v[1] = {rr};
-    block_partials<NS, 1>(v, part);
+    for (int m = S::LPR; m < 32; m <<= 1) {
+      rr += __shfl_xor_sync(0xffffffffu, rr, m);
+      rhx += __shfl_xor_sync(0xffffffffu, rhx, m);
+      rhy += __shfl_xor_sync(0xffffffffu, rhy, m);
+    }
+    double v[3] = {rr, rhx, rhy};  // slot 0: ||r||^2, slots 1, 2: rho
+    block_partials<NS, 3>(v, part);
   }
 }
 
@@ -511,7 +520,6 @@ __global__ void __launch_bounds__(256)
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int slot = (threadIdx.x >> 5) * S::RPW + sub;
   double om = sc[s].omega;
-  double rx = 0.0, ry = 0.0;
   double (*red)[MAX_SYS][4] = nullptr;
   if constexpr (SEG) red = seg_sums<8 * S::RPW, 4>();
   for (int c = ncolors - 1; c >= 0; --c) {
@@ -540,31 +548,16 @@ __global__ void __launch_bounds__(256)
         const V d = dd[(long)row * NS + s];
         zi = Cx<T>::make(zi.x - (d.x * swx - d.y * swy), zi.y - (d.x * swy + d.y * swx));
         z[(long)row * NS + s] = zi;
-        const V ri = r[(long)row * NS + s];
-        const double ex = (double)ri.x * (double)zi.x - (double)ri.y * (double)zi.y;
-        const double ey = (double)ri.x * (double)zi.y + (double)ri.y * (double)zi.x;
-        if constexpr (SEG) {
-          red[slot][sid][0] += ex;
-          red[slot][sid][1] += ey;
-        } else {
-          rx += ex;
-          ry += ey;
+        if constexpr (SEG) {  // per-mesh rho = r^T z (one matrix: the forward sweep sums it)
+          const V ri = r[(long)row * NS + s];
+          red[slot][sid][0] += (double)ri.x * (double)zi.x - (double)ri.y * (double)zi.y;
+          red[slot][sid][1] += (double)ri.x * (double)zi.y + (double)ri.y * (double)zi.x;
         }
       }
     }
     grid.sync();
   }
-  if constexpr (SEG) {
-    seg_partials<8 * S::RPW, 4>(red, part);
-  } else {
-#pragma unroll
-    for (int m = S::LPR; m < 32; m <<= 1) {
-      rx += __shfl_xor_sync(0xffffffffu, rx, m);
-      ry += __shfl_xor_sync(0xffffffffu, ry, m);
-    }
-    double v[4] = {rx, ry, 0.0, 0.0};
-    block_partials<NS, 4>(v, part);
-  }
+  if constexpr (SEG) seg_partials<8 * S::RPW, 4>(red, part);
 }
 
 // values of the colour-ordered split rows: out[k] = km[src[k]]
@@ -982,13 +975,14 @@ __device__ __forceinline__ double2 d_cdiv(double2 a, double2 b) { return cdiv(a,
 
 // part2 (nullable): the nodal correction's share r^T G u = t^T u of rho, summed by
 // the backward nodal sweep when the gradient add is folded into the p update
+// slot0: where rho sits in part (1: the multicolour forward sweep's slots 1, 2)
 __global__ void k_scal_rho(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns, int flexible,
-                           const double* part2, int nblocks2) {
+                           const double* part2, int nblocks2, int slot0) {
   if (ctrl->done) return;
   const int s = threadIdx.x >> 5;
   if (s >= ns) return;
-  double v[4];
-  sum_partials(part, nblocks, s, 0, v, 4);
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  sum_partials(part, nblocks, s, slot0, v, slot0 ? 2 : 4);
   if (part2) {
     double v2[2];
     __syncwarp();
@@ -1346,7 +1340,10 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
                 w->flag_b.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, (const V*)rp,
                 (const int32_t*)c->perm_b.p, sg);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[3], s));
-  int rho_blocks = mc ? w->mcb_blocks : sweep_blocks;
+  // rho's partial sums: the multicolour forward sweep (one matrix, slots 1, 2), the
+  // backward sweep (packed batches, natural-order SSOR), or a later pass below
+  int rho_blocks = mc ? (SEG ? w->mcb_blocks : w->mc_blocks) : sweep_blocks;
+  int rho_slot = (mc && !SEG) ? 1 : 0;
   if (hyb) {
     // z += G SSOR_node(G^T r): folded into the p update, or (packed batches, learned
     // base) a pass of its own that takes the rho partials again from the corrected z
@@ -1367,6 +1364,7 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
                                                           (const V*)I::R(w), w->ctrl.p, w->part.p, sg);
       count_launch();
       rho_blocks = w->nblocks;
+      rho_slot = 0;
     }
   }
   if (lbase) {
@@ -1376,10 +1374,11 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
                                              w->part.p);
     count_launch();
     rho_blocks = w->nblocks;
+    rho_slot = 0;
   }
   if (ev) AFEM_CUDA(cudaEventRecord(ev[4], s));
   k_scal_rho<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, rho_blocks, nsys, learned ? 1 : 0,
-                                        fold_grad ? w->part2.p : (const double*)nullptr, w->nmc_blocks);
+                                        fold_grad ? w->part2.p : (const double*)nullptr, w->nmc_blocks, rho_slot);
   count_launch();
   if (ev) AFEM_CUDA(cudaEventRecord(ev[5], s));
   k_pupd<T, NS, SEG><<<c->num_sms * 8, 256, 0, s>>>(

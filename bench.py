@@ -145,7 +145,8 @@ def kernel_bytes(name: str, n: int, nnz: int, ns: int, real_bytes: int, ntet: in
         # r r/w, q, DD, y write (x is updated in the p update)
         return ent * off + 8 * n + n * vec * 5
     if name.startswith("cocg_bwd_sweep_mc"):
-        return ent * off + 8 * n + n * vec * 5
+        # y read, z write, DD, z gather; packed batches also read r for their per-mesh rho
+        return ent * off + 8 * n + n * vec * (5 if "_seg" in name else 4)
     if name.startswith("cocg_nodal_correction"):
         nnz_n = node + 2 * n          # node graph: the node and its edge neighbours
         vn = vec                      # nodal vectors have the edge vectors' width
