@@ -3,10 +3,12 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/afem.h"
@@ -235,6 +237,26 @@ void build_schedule(afem_ctx* c);         // sweep level schedules from the patt
 void exclusive_scan(const int32_t* in, int32_t* out, int n, cudaStream_t s, long* total_host);
 int compute_coloring(int n, const int32_t* rp, const int32_t* cl, uint8_t* color, int32_t* perm, int32_t* cptr,
                      int max_colors);  // greedy distance-1 colouring, rows sorted by colour
+
+// Host loop over [0, n) in contiguous chunks on up to 32 threads: f(begin, end).
+// Each index's work must be independent (and not throw); small n runs inline.
+template <class F>
+void host_parallel_for(long n, F f) {
+  const unsigned hw = std::thread::hardware_concurrency();
+  const long nt = std::min<long>(std::max(1u, hw), 32);
+  if (n < 200000 || nt == 1) {
+    f(0L, n);
+    return;
+  }
+  const long chunk = (n + nt - 1) / nt;
+  std::vector<std::thread> th;
+  for (long t = 0; t < nt; ++t) {
+    const long a = t * chunk, b = std::min(n, a + chunk);
+    if (a >= b) break;
+    th.emplace_back(f, a, b);
+  }
+  for (auto& x : th) x.join();
+}
 
 // afem_assemble.cu
 void assemble_device(afem_ctx* c);        // K, M, rhs, bc (GENMAT + COPY_UL + GENBCCSEM + SET_BC)

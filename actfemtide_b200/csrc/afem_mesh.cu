@@ -429,29 +429,39 @@ void build_schedule(afem_ctx* c) {
   // perm[p]; its entries of earlier colours (the forward sweep's) and of later
   // colours (the backward sweep's), each with the index of the entry in the CSR
   {
+    // two passes over the rows in parallel chunks (counts, then entries at the
+    // positions the prefix sums give), so the layout does not depend on the threads
     std::vector<int32_t> lptr(n + 1), uptr(n + 1);
     lptr[0] = uptr[0] = 0;
-    for (int p = 0; p < n; ++p) {
-      const int i = pm[p];
-      int nl = 0, nu = 0;
-      for (int k = rp[i]; k < rp[i + 1]; ++k) {
-        const int j = cl[k];
-        if (color[j] < color[i]) ++nl;
-        else if (color[j] > color[i]) ++nu;
+    host_parallel_for(n, [&](long p0, long p1) {
+      for (long p = p0; p < p1; ++p) {
+        const int i = pm[p];
+        int nl = 0, nu = 0;
+        for (int k = rp[i]; k < rp[i + 1]; ++k) {
+          const int j = cl[k];
+          if (color[j] < color[i]) ++nl;
+          else if (color[j] > color[i]) ++nu;
+        }
+        lptr[p + 1] = nl;
+        uptr[p + 1] = nu;
       }
-      lptr[p + 1] = lptr[p] + nl;
-      uptr[p + 1] = uptr[p] + nu;
+    });
+    for (int p = 0; p < n; ++p) {
+      lptr[p + 1] += lptr[p];
+      uptr[p + 1] += uptr[p];
     }
     std::vector<int32_t> lcol(lptr[n]), lsrc(lptr[n]), ucol(uptr[n]), usrc(uptr[n]);
-    for (int p = 0; p < n; ++p) {
-      const int i = pm[p];
-      int a = lptr[p], b = uptr[p];
-      for (int k = rp[i]; k < rp[i + 1]; ++k) {
-        const int j = cl[k];
-        if (color[j] < color[i]) { lcol[a] = j; lsrc[a++] = k; }
-        else if (color[j] > color[i]) { ucol[b] = j; usrc[b++] = k; }
+    host_parallel_for(n, [&](long p0, long p1) {
+      for (long p = p0; p < p1; ++p) {
+        const int i = pm[p];
+        int a = lptr[p], b = uptr[p];
+        for (int k = rp[i]; k < rp[i + 1]; ++k) {
+          const int j = cl[k];
+          if (color[j] < color[i]) { lcol[a] = j; lsrc[a++] = k; }
+          else if (color[j] > color[i]) { ucol[b] = j; usrc[b++] = k; }
+        }
       }
-    }
+    });
     c->mc_lptr.upload(lptr.data(), n + 1, s);
     c->mc_lcol.upload(lcol.data(), lcol.size(), s);
     c->mc_lsrc.upload(lsrc.data(), lsrc.size(), s);

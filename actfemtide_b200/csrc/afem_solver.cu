@@ -91,6 +91,7 @@ struct SolverWork {
   int rpw64 = 0, rpw32 = 0;         // SpMV rows per warp chosen by tune_spmv (0 = not tuned)
   int mc_blocks = 0;                // co-resident grid of the forward multicolour sweep
   int mcb_blocks = 0;               // and of the backward one (fewer registers: more blocks)
+  double sd = 1.0;                  // SSOR diagonal scale of the current solve (DD = 1 / (sd D))
   bool no_window = false;           // COCG13_single semantics: no stagnation window, run to the cap
   bool kmf_valid = false;
   DBuf<unsigned> flag_f, flag_b;
@@ -438,7 +439,7 @@ __global__ void __launch_bounds__(256)
   double om = sc[s].omega;
   double2 al = sc[s].alpha;
   bool act = sc[s].active;
-  double rr = 0.0, rhx = 0.0, rhy = 0.0;
+  double rr = 0.0;
   double (*red)[MAX_SYS][1] = nullptr;
   if constexpr (SEG) red = seg_sums<8 * S::RPW, 1>();
   for (int c = 0; c < ncolors; ++c) {
@@ -480,11 +481,6 @@ __global__ void __launch_bounds__(256)
         const T wx = ri.x - (t1x - o * t2y), wy = ri.y - (t1y + o * t2x);
         const V d = dd[(long)row * NS + s];
         y[(long)row * NS + s] = Cx<T>::make(wx * d.x - wy * d.y, wx * d.y + wy * d.x);
-        if constexpr (!SEG) {  // rho = r^T z = y^T D y = sum dd_i w_i^2 (U = L^T)
-          const double w2x = (double)wx * (double)wx - (double)wy * (double)wy, w2y = 2.0 * (double)wx * (double)wy;
-          rhx += (double)d.x * w2x - (double)d.y * w2y;
-          rhy += (double)d.x * w2y + (double)d.y * w2x;
-        }
       }
     }
     grid.sync();
@@ -493,13 +489,9 @@ __global__ void __launch_bounds__(256)
     seg_partials<8 * S::RPW, 1>(red, part);
   } else {
 #pragma unroll
-    for (int m = S::LPR; m < 32; m <<= 1) {
-      rr += __shfl_xor_sync(0xffffffffu, rr, m);
-      rhx += __shfl_xor_sync(0xffffffffu, rhx, m);
-      rhy += __shfl_xor_sync(0xffffffffu, rhy, m);
-    }
-    double v[3] = {rr, rhx, rhy};  // slot 0: ||r||^2, slots 1, 2: rho
-    block_partials<NS, 3>(v, part);
+    for (int m = S::LPR; m < 32; m <<= 1) rr += __shfl_xor_sync(0xffffffffu, rr, m);
+    double v[1] = {rr};
+    block_partials<NS, 1>(v, part);
   }
 }
 
@@ -509,7 +501,8 @@ __global__ void __launch_bounds__(256)
              int n, const typename Cx<T>::V* __restrict__ r, typename Cx<T>::V* __restrict__ z,
              const typename Cx<T>::V* __restrict__ dd, const int32_t* __restrict__ perm,
              const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl,
-             double* __restrict__ part, const uint8_t* __restrict__ seg) {
+             double* __restrict__ part, const uint8_t* __restrict__ seg, const typename Cx<T>::V* __restrict__ km,
+             const int32_t* __restrict__ diagpos, double sd) {
   using V = typename Cx<T>::V;
   using S = McShape<NS, SEG>;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
@@ -520,6 +513,7 @@ __global__ void __launch_bounds__(256)
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int slot = (threadIdx.x >> 5) * S::RPW + sub;
   double om = sc[s].omega;
+  double rx = 0.0, ry = 0.0;
   double (*red)[MAX_SYS][4] = nullptr;
   if constexpr (SEG) red = seg_sums<8 * S::RPW, 4>();
   for (int c = ncolors - 1; c >= 0; --c) {
@@ -543,12 +537,21 @@ __global__ void __launch_bounds__(256)
       }
       if (live && g == 0) {
         V zi = z[(long)row * NS + s];
+        if constexpr (!SEG) {
+          // rho = r^T z = y^T D' y (U = L^T, D' = sd diag(A), y = the forward sweep's output in z)
+          const V a = km[__ldg(diagpos + row)];
+          const double dx = sd * (double)a.x, dy = sd * om * (double)a.y;
+          const double y2x = (double)zi.x * (double)zi.x - (double)zi.y * (double)zi.y;
+          const double y2y = 2.0 * (double)zi.x * (double)zi.y;
+          rx += dx * y2x - dy * y2y;
+          ry += dx * y2y + dy * y2x;
+        }
         const T o = (T)om;
         const T swx = t1x - o * t2y, swy = t1y + o * t2x;
         const V d = dd[(long)row * NS + s];
         zi = Cx<T>::make(zi.x - (d.x * swx - d.y * swy), zi.y - (d.x * swy + d.y * swx));
         z[(long)row * NS + s] = zi;
-        if constexpr (SEG) {  // per-mesh rho = r^T z (one matrix: the forward sweep sums it)
+        if constexpr (SEG) {  // packed batches: per-mesh rho = r^T z
           const V ri = r[(long)row * NS + s];
           red[slot][sid][0] += (double)ri.x * (double)zi.x - (double)ri.y * (double)zi.y;
           red[slot][sid][1] += (double)ri.x * (double)zi.y + (double)ri.y * (double)zi.x;
@@ -557,7 +560,17 @@ __global__ void __launch_bounds__(256)
     }
     grid.sync();
   }
-  if constexpr (SEG) seg_partials<8 * S::RPW, 4>(red, part);
+  if constexpr (SEG) {
+    seg_partials<8 * S::RPW, 4>(red, part);
+  } else {
+#pragma unroll
+    for (int m = S::LPR; m < 32; m <<= 1) {
+      rx += __shfl_xor_sync(0xffffffffu, rx, m);
+      ry += __shfl_xor_sync(0xffffffffu, ry, m);
+    }
+    double v[4] = {rx, ry, 0.0, 0.0};
+    block_partials<NS, 4>(v, part);
+  }
 }
 
 // values of the colour-ordered split rows: out[k] = km[src[k]]
@@ -975,14 +988,13 @@ __device__ __forceinline__ double2 d_cdiv(double2 a, double2 b) { return cdiv(a,
 
 // part2 (nullable): the nodal correction's share r^T G u = t^T u of rho, summed by
 // the backward nodal sweep when the gradient add is folded into the p update
-// slot0: where rho sits in part (1: the multicolour forward sweep's slots 1, 2)
 __global__ void k_scal_rho(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns, int flexible,
-                           const double* part2, int nblocks2, int slot0) {
+                           const double* part2, int nblocks2) {
   if (ctrl->done) return;
   const int s = threadIdx.x >> 5;
   if (s >= ns) return;
-  double v[4] = {0.0, 0.0, 0.0, 0.0};
-  sum_partials(part, nblocks, s, slot0, v, slot0 ? 2 : 4);
+  double v[4];
+  sum_partials(part, nblocks, s, 0, v, 4);
   if (part2) {
     double v2[2];
     __syncwarp();
@@ -1333,17 +1345,15 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
   if (mc)
     launch_coop(k_bwd_mc<T, NS, SEG>, w->mcb_blocks, s, (const int32_t*)c->mc_uptr.p, (const int32_t*)c->mc_ucol.p,
                 I::UKM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w), (const int32_t*)c->perm_mc.p,
-                (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p, sg);
+                (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p, sg, I::KM(c, w),
+                (const int32_t*)c->diagpos.p, w->sd);
   else
     launch_coop(k_bwd<T, NS, SEG>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
                 (const int32_t*)c->diagpos.p, I::KM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w),
                 w->flag_b.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, (const V*)rp,
                 (const int32_t*)c->perm_b.p, sg);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[3], s));
-  // rho's partial sums: the multicolour forward sweep (one matrix, slots 1, 2), the
-  // backward sweep (packed batches, natural-order SSOR), or a later pass below
-  int rho_blocks = mc ? (SEG ? w->mcb_blocks : w->mc_blocks) : sweep_blocks;
-  int rho_slot = (mc && !SEG) ? 1 : 0;
+  int rho_blocks = mc ? w->mcb_blocks : sweep_blocks;
   if (hyb) {
     // z += G SSOR_node(G^T r): folded into the p update, or (packed batches, learned
     // base) a pass of its own that takes the rho partials again from the corrected z
@@ -1364,7 +1374,6 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
                                                           (const V*)I::R(w), w->ctrl.p, w->part.p, sg);
       count_launch();
       rho_blocks = w->nblocks;
-      rho_slot = 0;
     }
   }
   if (lbase) {
@@ -1374,11 +1383,10 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
                                              w->part.p);
     count_launch();
     rho_blocks = w->nblocks;
-    rho_slot = 0;
   }
   if (ev) AFEM_CUDA(cudaEventRecord(ev[4], s));
   k_scal_rho<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, rho_blocks, nsys, learned ? 1 : 0,
-                                        fold_grad ? w->part2.p : (const double*)nullptr, w->nmc_blocks, rho_slot);
+                                        fold_grad ? w->part2.p : (const double*)nullptr, w->nmc_blocks);
   count_launch();
   if (ev) AFEM_CUDA(cudaEventRecord(ev[5], s));
   k_pupd<T, NS, SEG><<<c->num_sms * 8, 256, 0, s>>>(
@@ -1494,7 +1502,8 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
       }
     }
   }
-  setup_dd<T, NS, SEG>(c, w, use_hyb ? AFEM_PRECOND_HYBRID : precond, o->sigma_diag > 0 ? o->sigma_diag : 1.0);
+  w->sd = o->sigma_diag > 0 ? o->sigma_diag : 1.0;
+  setup_dd<T, NS, SEG>(c, w, use_hyb ? AFEM_PRECOND_HYBRID : precond, w->sd);
   const int mode = precond;
   tune_spmv<T, NS, SEG>(c, w);
   const bool learned = mode == AFEM_PRECOND_LEARNED;
@@ -1966,7 +1975,7 @@ void precond_apply_device(afem_ctx* c, double omega, const double2* r, double2* 
   launch_coop(k_bwd_mc<double, 1, false>, w->mc_blocks, s, (const int32_t*)c->mc_uptr.p, (const int32_t*)c->mc_ucol.p,
               (const double2*)c->mc_ukm.p, n, (const double2*)w->r.p, w->z.p, (const double2*)w->dd.p,
               (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p,
-              (const uint8_t*)nullptr);
+              (const uint8_t*)nullptr, (const double2*)c->km.p, (const int32_t*)c->diagpos.p, 1.0);
   k_grad_t<double, 1><<<c->num_sms * 8, 256, 0, s>>>(h->node, h->nptr.p, h->nlist.p, c->bc.p, (const double2*)w->r.p,
                                                       w->ht.p, w->ctrl.p);
   count_launch();
@@ -2009,12 +2018,12 @@ void invalidate_work(afem_ctx* c) {
   if (c->work) c->work->kmf_valid = false;
 }
 
-// A new pattern: also tune the SpMV again.
+// A new pattern: also tune the SpMV again (ensure_work re-allocates when the
+// size changes; buffers of the same size are kept).
 void invalidate_pattern_work(afem_ctx* c) {
   if (c->work) {
     c->work->kmf_valid = false;
     c->work->rpw64 = c->work->rpw32 = 0;
-    c->work->n = -1;  // re-allocate for the new size
   }
   c->nsys = 0;  // the old solutions belong to the old pattern
 }

@@ -49,9 +49,9 @@ PLAIN_96 = {"iterations": 30000, "converged": False, "resid_true_at_cap": 6.843e
             "seconds_at_cap": 475.9}
 UNIT = "s/solve"
 # DRAM traffic of one forward multicolour sweep (FP64, 16 systems) from an ncu capture of the
-# 48x48x32 model (532,352 edges: dram__bytes_read.sum + dram__bytes_write.sum = 1.628 GB per
-# launch), per edge row; scaled to the bench's model by its rows
-FWD_MC_NS16_TRAFFIC = {"kernel": "cocg_fwd_sweep_mc_fp64_ns16", "bytes": 1.628e9, "rows": 532352}
+# 48x48x32 model (532,352 edges: dram__bytes_read.sum + dram__bytes_write.sum = 0.910 + 0.264 GB
+# per launch), per edge row; scaled to the bench's model by its rows
+FWD_MC_NS16_TRAFFIC = {"kernel": "cocg_fwd_sweep_mc_fp64_ns16", "bytes": 1.1745e9, "rows": 532352}
 TOL = 1e-8
 FALLBACK_HBM_GBS = 6650.0
 
@@ -145,8 +145,11 @@ def kernel_bytes(name: str, n: int, nnz: int, ns: int, real_bytes: int, ntet: in
         # r r/w, q, DD, y write (x is updated in the p update)
         return ent * off + 8 * n + n * vec * 5
     if name.startswith("cocg_bwd_sweep_mc"):
-        # y read, z write, DD, z gather; packed batches also read r for their per-mesh rho
-        return ent * off + 8 * n + n * vec * (5 if "_seg" in name else 4)
+        # y read, z write, DD, z gather; rho from the diagonal (diagpos + one (K, M) pair per row),
+        # packed batches read r instead for their per-mesh rho
+        if "_seg" in name:
+            return ent * off + 8 * n + n * vec * 5
+        return ent * off + 8 * n + n * (vec * 4 + 4 + 2 * real_bytes)
     if name.startswith("cocg_nodal_correction"):
         nnz_n = node + 2 * n          # node graph: the node and its edge neighbours
         vn = vec                      # nodal vectors have the edge vectors' width
@@ -402,7 +405,7 @@ def run_gpu(args):
     traffic, traffic_src = None, None
     if dom == FWD_MC_NS16_TRAFFIC["kernel"]:
         traffic = FWD_MC_NS16_TRAFFIC["bytes"] * n / FWD_MC_NS16_TRAFFIC["rows"]
-        traffic_src = ("ncu dram bytes of one launch on the 48x48x32 model (1.628 GB, 532,352 rows) scaled by "
+        traffic_src = ("ncu dram bytes of one launch on the 48x48x32 model (1.1745 GB, 532,352 rows) scaled by "
                        "the rows; a lower estimate, since the L2 hit rate falls as the working set grows")
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.method != "packed":
