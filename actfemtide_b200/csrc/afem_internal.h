@@ -192,8 +192,9 @@ struct afem_ctx {
   // the same rows in colour order, split: entries of earlier colours (mc_l*) and of
   // later colours (mc_u*); *src = index of the entry in the CSR, *km the values
   afem::DBuf<int32_t> mc_lptr, mc_lcol, mc_lsrc, mc_uptr, mc_ucol, mc_usrc;
-  afem::DBuf<double2> mc_lkm, mc_ukm;
-  long mc_vals_gen = -1;        // assembly generation of mc_lkm / mc_ukm
+  afem::DBuf<int32_t> mc_dsrc;  // CSR index of the diagonal of the row at each colour position
+  afem::DBuf<double2> mc_lkm, mc_ukm, mc_dkm;
+  long mc_vals_gen = -1;        // assembly generation of mc_lkm / mc_ukm / mc_dkm
   bool schedule_ready = false;
 
   // values: A(omega) = K + i*omega*M, stored interleaved (K_k, M_k)

@@ -468,6 +468,9 @@ void build_schedule(afem_ctx* c) {
     c->mc_uptr.upload(uptr.data(), n + 1, s);
     c->mc_ucol.upload(ucol.data(), ucol.size(), s);
     c->mc_usrc.upload(usrc.data(), usrc.size(), s);
+    std::vector<int32_t> dsrc(n);
+    for (int p = 0; p < n; ++p) dsrc[p] = dp[pm[p]];
+    c->mc_dsrc.upload(dsrc.data(), n, s);
     c->mc_vals_gen = -1;
   }
   AFEM_CUDA(cudaStreamSynchronize(s));

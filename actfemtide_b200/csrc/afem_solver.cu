@@ -501,8 +501,8 @@ __global__ void __launch_bounds__(256)
              int n, const typename Cx<T>::V* __restrict__ r, typename Cx<T>::V* __restrict__ z,
              const typename Cx<T>::V* __restrict__ dd, const int32_t* __restrict__ perm,
              const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl,
-             double* __restrict__ part, const uint8_t* __restrict__ seg, const typename Cx<T>::V* __restrict__ km,
-             const int32_t* __restrict__ diagpos, double sd) {
+             double* __restrict__ part, const uint8_t* __restrict__ seg, const double2* __restrict__ dkm,
+             double sd) {
   using V = typename Cx<T>::V;
   using S = McShape<NS, SEG>;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
@@ -538,9 +538,10 @@ __global__ void __launch_bounds__(256)
       if (live && g == 0) {
         V zi = z[(long)row * NS + s];
         if constexpr (!SEG) {
-          // rho = r^T z = y^T D' y (U = L^T, D' = sd diag(A), y = the forward sweep's output in z)
-          const V a = km[__ldg(diagpos + row)];
-          const double dx = sd * (double)a.x, dy = sd * om * (double)a.y;
+          // rho = r^T z = y^T D' y (U = L^T, D' = sd diag(A), y = the forward sweep's output in z);
+          // the diagonal sits in colour-position order, so its load does not wait for the row id
+          const double2 a = dkm[pos];
+          const double dx = sd * a.x, dy = sd * om * a.y;
           const double y2x = (double)zi.x * (double)zi.x - (double)zi.y * (double)zi.y;
           const double y2y = 2.0 * (double)zi.x * (double)zi.y;
           rx += dx * y2x - dy * y2y;
@@ -1345,8 +1346,8 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
   if (mc)
     launch_coop(k_bwd_mc<T, NS, SEG>, w->mcb_blocks, s, (const int32_t*)c->mc_uptr.p, (const int32_t*)c->mc_ucol.p,
                 I::UKM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w), (const int32_t*)c->perm_mc.p,
-                (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p, sg, I::KM(c, w),
-                (const int32_t*)c->diagpos.p, w->sd);
+                (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p, sg,
+                (const double2*)c->mc_dkm.p, w->sd);
   else
     launch_coop(k_bwd<T, NS, SEG>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
                 (const int32_t*)c->diagpos.p, I::KM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w),
@@ -1900,6 +1901,10 @@ void ensure_mc_values(afem_ctx* c) {
     const long nl = (long)c->mc_lcol.n, nu = (long)c->mc_ucol.n;
     c->mc_lkm.alloc(nl);
     c->mc_ukm.alloc(nu);
+    c->mc_dkm.alloc(c->nline);
+    k_gather_entries<double2><<<c->num_sms * 8, 256, 0, c->stream>>>(c->km.p, c->mc_dsrc.p, (long)c->nline,
+                                                                     c->mc_dkm.p);
+    count_launch();
     if (nl) {
       k_gather_entries<double2><<<c->num_sms * 8, 256, 0, c->stream>>>(c->km.p, c->mc_lsrc.p, nl, c->mc_lkm.p);
       count_launch();
@@ -1975,7 +1980,7 @@ void precond_apply_device(afem_ctx* c, double omega, const double2* r, double2* 
   launch_coop(k_bwd_mc<double, 1, false>, w->mc_blocks, s, (const int32_t*)c->mc_uptr.p, (const int32_t*)c->mc_ucol.p,
               (const double2*)c->mc_ukm.p, n, (const double2*)w->r.p, w->z.p, (const double2*)w->dd.p,
               (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p,
-              (const uint8_t*)nullptr, (const double2*)c->km.p, (const int32_t*)c->diagpos.p, 1.0);
+              (const uint8_t*)nullptr, (const double2*)c->mc_dkm.p, 1.0);
   k_grad_t<double, 1><<<c->num_sms * 8, 256, 0, s>>>(h->node, h->nptr.p, h->nlist.p, c->bc.p, (const double2*)w->r.p,
                                                       w->ht.p, w->ctrl.p);
   count_launch();

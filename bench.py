@@ -145,11 +145,11 @@ def kernel_bytes(name: str, n: int, nnz: int, ns: int, real_bytes: int, ntet: in
         # r r/w, q, DD, y write (x is updated in the p update)
         return ent * off + 8 * n + n * vec * 5
     if name.startswith("cocg_bwd_sweep_mc"):
-        # y read, z write, DD, z gather; rho from the diagonal (diagpos + one (K, M) pair per row),
-        # packed batches read r instead for their per-mesh rho
+        # y read, z write, DD, z gather; rho from the diagonal (one FP64 (K, M) pair per row in
+        # colour-position order), packed batches read r instead for their per-mesh rho
         if "_seg" in name:
             return ent * off + 8 * n + n * vec * 5
-        return ent * off + 8 * n + n * (vec * 4 + 4 + 2 * real_bytes)
+        return ent * off + 8 * n + n * (vec * 4 + 16)
     if name.startswith("cocg_nodal_correction"):
         nnz_n = node + 2 * n          # node graph: the node and its edge neighbours
         vn = vec                      # nodal vectors have the edge vectors' width
