@@ -1277,7 +1277,9 @@ void launch_spmv(afem_ctx* c, SolverWork* w, int rpw, const typename Cx<T>::V* k
 }
 
 // Rows-per-warp autotuner: times each variant on this matrix (q = A p with the
-// current p) and keeps the fastest; cached per workspace and precision.
+// current p) in three interleaved rounds and keeps the fastest by its best
+// round (one round alone flipped between close variants from run to run);
+// cached per workspace and precision.
 template <class T, int NS, bool SEG>
 int tune_spmv(afem_ctx* c, SolverWork* w) {
   using I = Inner<T, NS>;
@@ -1287,19 +1289,25 @@ int tune_spmv(afem_ctx* c, SolverWork* w) {
   cudaEvent_t a, b;
   AFEM_CUDA(cudaEventCreate(&a));
   AFEM_CUDA(cudaEventCreate(&b));
+  const int cand[3] = {1, 2, 4};
+  float tbest[3] = {1e30f, 1e30f, 1e30f};
+  for (int round = 0; round < 3; ++round)
+    for (int ci = 0; ci < 3; ++ci) {
+      const int rpw = cand[ci];
+      if (NS * rpw > 32) break;
+      launch_spmv<T, NS, SEG>(c, w, rpw, I::KM(c, w), I::P(w), I::Q(w), nullptr, nullptr);  // warm
+      AFEM_CUDA(cudaEventRecord(a, s));
+      for (int k = 0; k < 3; ++k) launch_spmv<T, NS, SEG>(c, w, rpw, I::KM(c, w), I::P(w), I::Q(w), nullptr, nullptr);
+      AFEM_CUDA(cudaEventRecord(b, s));
+      AFEM_CUDA(cudaEventSynchronize(b));
+      float ms = 0;
+      AFEM_CUDA(cudaEventElapsedTime(&ms, a, b));
+      tbest[ci] = std::min(tbest[ci], ms);
+    }
   float best = 1e30f;
   int pick = 1;
-  for (int rpw : {1, 2, 4}) {
-    if (NS * rpw > 32) break;
-    launch_spmv<T, NS, SEG>(c, w, rpw, I::KM(c, w), I::P(w), I::Q(w), nullptr, nullptr);  // warm
-    AFEM_CUDA(cudaEventRecord(a, s));
-    for (int k = 0; k < 3; ++k) launch_spmv<T, NS, SEG>(c, w, rpw, I::KM(c, w), I::P(w), I::Q(w), nullptr, nullptr);
-    AFEM_CUDA(cudaEventRecord(b, s));
-    AFEM_CUDA(cudaEventSynchronize(b));
-    float ms = 0;
-    AFEM_CUDA(cudaEventElapsedTime(&ms, a, b));
-    if (ms < best * 0.97f) { best = ms; pick = rpw; }
-  }
+  for (int ci = 0; ci < 3; ++ci)
+    if (tbest[ci] < best * 0.97f) { best = tbest[ci]; pick = cand[ci]; }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   slot = pick;
