@@ -20,8 +20,9 @@ STATUS = {
     -5: "AFEM_EBREAKDOWN", -6: "AFEM_ENONFINITE", -7: "AFEM_ECUDA", -8: "AFEM_ESTATE", -9: "AFEM_ETIMEOUT",
     -10: "AFEM_EIO", -11: "AFEM_ENOPRECOND", -12: "AFEM_ESITE", -13: "AFEM_ESTAGNATION",
 }
+STATUS_CODE = {v: k for k, v in STATUS.items()}
 PRECOND = {"IC": 0, "SSOR": 1, "DIAG": 2, "NONE": 3, "LEARNED": 4, "SSOR_MC": 5, "HYBRID": 6}
-PRECISION = {"fp64": 0, "mixed": 1}
+PRECISION = {"fp64": 0, "mixed": 1, "pc32": 2}
 
 # Every entry point declared in include/afem.h.
 EXPORTS = (
@@ -34,6 +35,7 @@ EXPORTS = (
     "afem_solve_rhs", "afem_jacobian", "afem_sweep_schedule", "afem_coloring", "afem_set_segments",
     "afem_segment_info", "afem_launch_count", "afem_hybrid_matrix", "afem_sites_grid", "afem_site_coeffs_grid",
     "afem_xy_points", "afem_sort_index", "afem_mesh_info", "afem_solution_count", "afem_sites_noalloc",
+    "afem_set_wait_limit", "afem_set_spmv_rows_per_warp", "afem_utm_xy",
     "afem_mpnn_set_base", "afem_precond_apply",
 )
 
@@ -84,6 +86,12 @@ def lib():
     L.afem_precond_apply.restype = C.c_int
     L.afem_sites_noalloc.argtypes = [_vp, C.c_int, _vp, _vp]
     L.afem_sites_noalloc.restype = C.c_int
+    L.afem_utm_xy.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _vp]
+    L.afem_utm_xy.restype = C.c_int
+    L.afem_set_wait_limit.argtypes = [_vp, C.c_uint]
+    L.afem_set_wait_limit.restype = C.c_int
+    L.afem_set_spmv_rows_per_warp.argtypes = [_vp, C.c_int]
+    L.afem_set_spmv_rows_per_warp.restype = C.c_int
     L.afem_sites_grid.argtypes = [_vp, C.c_int, _vp, _vp]
     L.afem_sites_grid.restype = C.c_int
     L.afem_site_coeffs_grid.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp]
@@ -153,6 +161,15 @@ def xy_points(xmin, xmax, ymin, ymax, nx, ny, z):
     out = np.zeros((nx * ny, 3))
     if lib().afem_xy_points(xmin, xmax, ymin, ymax, nx, ny, z, out.ctypes.data_as(_vp)) != 0:
         raise ValueError("xy_points: bad grid")
+    return out
+
+
+def utm_xy(lon, lat, lonorigin, latorigin, zone):
+    """UTMXY: km east/north of the origin in UTM zone `zone` (host only)."""
+    out = np.zeros(2)
+    rc = lib().afem_utm_xy(float(lon), float(lat), float(lonorigin), float(latorigin), int(zone), out.ctypes.data)
+    if rc != AFEM_OK:
+        raise AfemError(rc, "utm_xy: bad zone")
     return out
 
 

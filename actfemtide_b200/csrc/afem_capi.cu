@@ -461,11 +461,38 @@ int afem_export_system(afem_ctx* c, double freq, int isrc, int* n_out, long* iau
   });
 }
 
+namespace {
+void check_opts(const afem_solve_opts* o) {
+  AFEM_REQUIRE(o->precond >= 0 && o->precond <= 6, AFEM_EINVAL, "solve: unknown preconditioner");
+  AFEM_REQUIRE(o->precision >= 0 && o->precision <= 2, AFEM_EINVAL, "solve: unknown precision");
+  AFEM_REQUIRE(o->precision != AFEM_FP32_PRECOND || o->precond == AFEM_PRECOND_SSOR_MC ||
+                   o->precond == AFEM_PRECOND_HYBRID,
+               AFEM_EINVAL, "solve: the FP32 preconditioner applies to SSOR_MC and HYBRID");
+}
+}  // namespace
+
+int afem_set_wait_limit(afem_ctx* c, unsigned polls) {
+  return guarded(c, [&]() {
+    c->wait_limit = polls;
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_set_spmv_rows_per_warp(afem_ctx* c, int rpw) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(rpw == 0 || rpw == 1 || rpw == 2 || rpw == 4, AFEM_EINVAL,
+                 "set_spmv_rows_per_warp: 0 (tuned), 1, 2 or 4");
+    c->spmv_rpw = rpw;
+    afem::reset_spmv_tuning(c);
+    return (int)AFEM_OK;
+  });
+}
+
 int afem_solve(afem_ctx* c, int nsys, const double* freq, const int* src, const afem_solve_opts* opts,
                afem_solve_stats* stats) {
   return guarded(c, [&]() {
     AFEM_REQUIRE(freq && opts, AFEM_EINVAL, "solve: null freq or opts");
-    AFEM_REQUIRE(opts->precond >= 0 && opts->precond <= 6, AFEM_EINVAL, "solve: unknown preconditioner");
+    check_opts(opts);
     afem::reset_status(c);
     return afem::solve_device(c, nsys, freq, src, opts, stats);
   });
@@ -496,6 +523,7 @@ int afem_solve_rhs(afem_ctx* c, int nsys, const double* freq, const double* rhs,
                    afem_solve_stats* stats) {
   return guarded(c, [&]() {
     AFEM_REQUIRE(freq && opts && rhs, AFEM_EINVAL, "solve_rhs: null argument");
+    check_opts(opts);
     afem::reset_status(c);
     afem::SolveExtra ex;
     ex.rhs = rhs;

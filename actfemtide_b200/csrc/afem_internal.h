@@ -225,6 +225,9 @@ struct afem_ctx {
   int last_learned_its = 0;  // iterations the last solve ran with the learned preconditioner
   afem::CtlInfo* ctl = nullptr;
 
+  unsigned wait_limit = 0;   // polls of the sync-free sweeps' bounded wait (0: the built-in limit)
+  int spmv_rpw = 0;          // SpMV rows per warp pinned by the caller (0: chosen by the tuner)
+
   afem::DBuf<afem::DevStatus> status;  // one status word
   afem::Profile prof;
 };
@@ -284,6 +287,7 @@ void load_split_system(afem_ctx* c, int n, const int32_t* INU, const int32_t* IA
 void destroy_work(afem_ctx* c);
 void invalidate_work(afem_ctx* c);          // new matrix values
 void invalidate_pattern_work(afem_ctx* c);  // new pattern
+void reset_spmv_tuning(afem_ctx* c);        // the SpMV rows per warp is chosen again at the next solve
 void get_residual(afem_ctx* c, int k, double* r);  // b - A x of system k after the last solve
 
 // afem_mpnn.cu (learned preconditioner)

@@ -295,6 +295,60 @@ void lift_sites(const Msh& h, std::vector<double>& xyzobs) {
   }
 }
 
+}  // namespace
+
+// Longitude/latitude (deg) to UTM easting/northing (m) in `zone`: the ellipsoidal
+// transverse Mercator of Snyder ("Map Projections -- A Working Manual", USGS
+// Professional Paper 1395, 1987, eqs. 8-9 to 8-13, Clarke 1866 ellipsoid, scale
+// 0.9996, false easting 500 km) in the form utm_geo_tm evaluates it for
+// LONLAT2UTM (src/common/m_param.f90:741-936, called by UTMGMT, :629-661).  One
+// term is kept as the reference has it: the sin(4 phi) coefficient of the
+// meridional arc multiplies 15 e^4/256 by 45 e^6/1024 where Snyder adds them, so
+// northings differ from Snyder's by up to ~17 m; the sites must land where the
+// reference puts them.
+void utm_lonlat2xy(double lon, double lat, int zone, double* x, double* y) {
+  const double pi = 3.141592653589793, degrad = pi / 180.0;
+  const double a_ = 6378206.4, b_ = 6356583.8, k0 = 0.9996;
+  const double e2 = 1.0 - std::pow(b_ / a_, 2.0), e4 = e2 * e2, e6 = e2 * e4, ep2 = e2 / (1.0 - e2);
+  const double cm = zone * 6.0 - 183.0;
+  const double rlat = degrad * lat;
+  double delam = lon - cm;
+  if (delam < -180.0) delam += 360.0;
+  if (delam > 180.0) delam -= 360.0;
+  delam *= degrad;
+  const double f1 = (1.0 - e2 / 4.0 - 3.0 * e4 / 64.0 - 5.0 * e6 / 256.0) * rlat;
+  const double f2 = (3.0 * e2 / 8.0 + 3.0 * e4 / 32.0 + 45.0 * e6 / 1024.0) * std::sin(2.0 * rlat);
+  const double f3 = (15.0 * e4 / 256.0 * 45.0 * e6 / 1024.0) * std::sin(4.0 * rlat);  // the reference's product
+  const double f4 = 35.0 * e6 / 3072.0 * std::sin(6.0 * rlat);
+  const double rm = a_ * (f1 - f2 + f3 - f4);
+  double xx, yy;
+  if (lat == 90.0 || lat == -90.0) {
+    xx = 0.0;
+    yy = k0 * rm;
+  } else {
+    const double sl = std::sin(rlat), cl = std::cos(rlat), tl = std::tan(rlat);
+    const double rn = a_ / std::sqrt(1.0 - e2 * sl * sl);
+    const double t = tl * tl, c = ep2 * cl * cl, A = cl * delam;
+    const double A2 = A * A, A3 = A2 * A, A4 = A2 * A2, A5 = A4 * A, A6 = A4 * A2;
+    xx = k0 * rn * (A + (1.0 - t + c) * A3 / 6.0 + (5.0 - 18.0 * t + t * t + 72.0 * c - 58.0 * ep2) * A5 / 120.0);
+    yy = k0 * (rm + rn * tl * (A2 / 2.0 + (5.0 - t + 9.0 * c + 4.0 * c * c) * A4 / 24.0 +
+                               (61.0 - 58.0 * t + t * t + 600.0 * c - 330.0 * ep2) * A6 / 720.0));
+  }
+  *x = xx + 500000.0;
+  *y = yy;
+}
+
+namespace {
+
+// UTMXY (m_param.f90:609-627): site position in km east/north of the origin, both in UTM zone `zone`
+void utmxy(double lon, double lat, double lonorigin, double latorigin, int zone, double* xkm, double* ykm) {
+  double x, y, x0, y0;
+  utm_lonlat2xy(lon, lat, zone, &x, &y);
+  utm_lonlat2xy(lonorigin, latorigin, zone, &x0, &y0);
+  *xkm = (x - x0) / 1e3;
+  *ykm = (y - y0) / 1e3;
+}
+
 // Fortran Gw.d edit descriptor (G15.7 of OUTOBSFILESFWD) for finite values.
 std::string fortran_g(double x, int w, int d) {
   char buf[64];
@@ -374,8 +428,18 @@ int load_ctl(afem_ctx* c, const char* path) {
   ci->ybound[3] = -ci->ybound[0];
   ci->nobs = (int)r.num("nobs");
   ci->lonlatflag = (int)r.num("lonlatflag");
-  if (ci->lonlatflag == 1) throw Error{AFEM_EIO, "ctl: lonlatflag 1 (UTM sites) is not supported; give xyz (2) or local lon/lat (0)"};
-  r.skip("UTM zone line");
+  AFEM_REQUIRE(ci->lonlatflag >= 0 && ci->lonlatflag <= 2, AFEM_EIO, "ctl: lonlatflag should be 0, 1 or 2");
+  int utm_zone = 0;
+  if (ci->lonlatflag == 1) {
+    // read(input,*) c_param%UTM (character(3)); UTMGMT reads the zone number from its first two characters
+    const std::string z = r.word("UTM zone");
+    const std::string z2 = z.substr(0, 2);
+    char* end = nullptr;
+    utm_zone = (int)std::strtol(z2.c_str(), &end, 10);
+    AFEM_REQUIRE(end != z2.c_str() && utm_zone >= 1 && utm_zone <= 60, AFEM_EIO, "ctl: bad UTM zone '" + z + "'");
+  } else {
+    r.skip("UTM zone line");
+  }
   auto org = r.nums("lonlatorigin", 2);
   ci->lonorigin = org[0];
   ci->latorigin = org[1];
@@ -386,6 +450,12 @@ int load_ctl(afem_ctx* c, const char* path) {
     if (ci->lonlatflag == 0) {
       ci->xyzobs.push_back((v[0] - ci->lonorigin) * d2r * radius * std::cos(ci->latorigin * d2r));
       ci->xyzobs.push_back((v[1] - ci->latorigin) * d2r * radius);
+      ci->xyzobs.push_back(v[2]);
+    } else if (ci->lonlatflag == 1) {  // UTMXY (m_param.f90:316-323)
+      double xk, yk;
+      utmxy(v[0], v[1], ci->lonorigin, ci->latorigin, utm_zone, &xk, &yk);
+      ci->xyzobs.push_back(xk);
+      ci->xyzobs.push_back(yk);
       ci->xyzobs.push_back(v[2]);
     } else {
       ci->xyzobs.insert(ci->xyzobs.end(), v.begin(), v.end());
@@ -592,6 +662,13 @@ void destroy_ctl(afem_ctx* c) {
 }
 
 }  // namespace afem
+
+// Host only: UTMXY of one site (m_param.f90:609-627): km east/north of the origin.
+extern "C" int afem_utm_xy(double lon, double lat, double lonorigin, double latorigin, int zone, double* xy_km) {
+  if (!xy_km || zone < 1 || zone > 60) return AFEM_EINVAL;
+  afem::utmxy(lon, lat, lonorigin, latorigin, zone, &xy_km[0], &xy_km[1]);
+  return AFEM_OK;
+}
 
 // Host-only helpers exported for the test-suite (no device work).
 extern "C" int afem_fortran_g(double x, int w, int d, char* out, int cap) {

@@ -363,9 +363,14 @@ void site_coeffs_range(afem_ctx* c, int nobs, const double* xyz_obs, long t0, lo
                                                          g->nz, g->stack.p, g->ordered.p, obs.p, nobs, best.p);
     count_launch();
   } else {
-    dim3 grid(std::max(1, std::min(2 * c->num_sms, (int)((t1 - t0 + 255) / 256))), nobs);
-    k_find<<<grid, 256, 0, s>>>(c->xyz.p, c->n4.p, t0, t1, obs.p, nobs, best.p);
-    count_launch();
+    // one grid row per site; sites beyond the 65,535 rows of a grid go to further launches
+    constexpr int ROWS = 65535;
+    for (int s0 = 0; s0 < nobs; s0 += ROWS) {
+      const int cnt = std::min(ROWS, nobs - s0);
+      dim3 grid(std::max(1, std::min(2 * c->num_sms, (int)((t1 - t0 + 255) / 256))), cnt);
+      k_find<<<grid, 256, 0, s>>>(c->xyz.p, c->n4.p, t0, t1, obs.p + 3L * s0, cnt, best.p + s0);
+      count_launch();
+    }
   }
   DBuf<int32_t> ditem;
   DBuf<double> dve, dvf;
@@ -484,7 +489,9 @@ static __device__ __align__(256) unsigned char g_sites_scratch[NA_BYTES];
 namespace {
 
 constexpr int NA_MAX_DEVICES = 64;
-unsigned char* g_sites_scratch_ptr[NA_MAX_DEVICES] = {};
+// device address of g_sites_scratch per device, looked up once; atomic because
+// contexts on several host threads may make their first call at the same time
+std::atomic<unsigned char*> g_sites_scratch_ptr[NA_MAX_DEVICES] = {};
 
 __global__ void k_fill_int(int* __restrict__ p, int n, int v) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -503,8 +510,11 @@ void sites_noalloc_device(afem_ctx* c, int nobs, const double* xyz_obs, double* 
                "sites_noalloc: at most " + std::to_string(NOALLOC_SYS) + " solved systems (got " +
                    std::to_string(c->nsys) + ")");
   AFEM_REQUIRE(c->device >= 0 && c->device < NA_MAX_DEVICES, AFEM_EINVAL, "sites_noalloc: device id out of range");
-  unsigned char*& base = g_sites_scratch_ptr[c->device];
-  if (!base) AFEM_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&base), g_sites_scratch));
+  unsigned char* base = g_sites_scratch_ptr[c->device].load(std::memory_order_acquire);
+  if (!base) {  // the device is current (every entry point sets it)
+    AFEM_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&base), g_sites_scratch));
+    g_sites_scratch_ptr[c->device].store(base, std::memory_order_release);
+  }
   double* obs = reinterpret_cast<double*>(base + NA_OBS);
   int* best = reinterpret_cast<int*>(base + NA_BEST);
   int32_t* item = reinterpret_cast<int32_t*>(base + NA_ITEM);

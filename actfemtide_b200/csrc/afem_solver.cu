@@ -30,6 +30,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "afem_hybrid.h"
 #include "afem_internal.h"
@@ -69,6 +70,7 @@ struct Ctrl {
   int iter;        // iterations of the current inner solve
   int maxit;
   double tol;
+  unsigned spin_limit;  // polls of a bounded wait before DEV_TIMEOUT (0: SPIN_LIMIT)
 };
 
 struct SolverWork {
@@ -93,7 +95,8 @@ struct SolverWork {
   int mcb_blocks = 0;               // and of the backward one (fewer registers: more blocks)
   double sd = 1.0;                  // SSOR diagonal scale of the current solve (DD = 1 / (sd D))
   bool no_window = false;           // COCG13_single semantics: no stagnation window, run to the cap
-  bool kmf_valid = false;
+  bool kmf_valid = false;            // kmf matches the assembly
+  bool mcf_valid = false;            // mc_lkmf / mc_ukmf match the assembly
   DBuf<unsigned> flag_f, flag_b;
   DBuf<double> part;                // partial sums [block][sys][4]
   DBuf<double> part2;               // nodal share of rho (hybrid), same layout
@@ -110,7 +113,8 @@ struct SolverWork {
 
 namespace {
 
-__device__ __forceinline__ bool wait_flag(const unsigned* f, unsigned epoch, DevStatus* st, int row) {
+__device__ __forceinline__ bool wait_flag(const unsigned* f, unsigned epoch, DevStatus* st, int row,
+                                          unsigned limit) {
   if (ld_relaxed(f) >= epoch) return true;
   // exponential back-off keeps the poll traffic from crowding L2
   unsigned spins = 0, ns = 32;
@@ -120,7 +124,7 @@ __device__ __forceinline__ bool wait_flag(const unsigned* f, unsigned epoch, Dev
     if (ld_relaxed(f) >= epoch) return true;
     ++spins;
     if ((spins & 63) == 0 && *(volatile int*)&st->code == DEV_TIMEOUT) return false;
-    if (spins > SPIN_LIMIT) {
+    if (spins > limit) {
       raise_status(st, DEV_TIMEOUT, row);
       return false;
     }
@@ -149,6 +153,21 @@ __device__ __forceinline__ void group_reduce(T& a, T& b, T& c, T& d) {
   }
 }
 
+// The values a gather reads may sit in L1 when every row's NS values fill whole
+// 128-byte lines: a line then holds one row only, and a row is read only after
+// this kernel wrote it (earlier colours of a sweep) or never written in it (the
+// SpMV's p), so no SM can hold a stale copy.  Narrower rows share lines with
+// rows still to be written and are read at L2 (ld.cg).
+template <class V, int NS>
+struct GatherL1 {
+  static constexpr bool ok = (NS * sizeof(V)) % 128 == 0;
+};
+template <class V, int NS>
+__device__ __forceinline__ V gather_ld(const V* p) {
+  if constexpr (GatherL1<V, NS>::ok) return *p;
+  else return ldcg(p);
+}
+
 // Sum over a row's entries k0, k0+G, ... < k1 of A_k * v_col(k) for system s, split
 // as t1 = sum K*v and t2 = sum M*v.  Four entries at a time: their columns,
 // then their values and gathers, so four independent gathers are in flight
@@ -165,8 +184,8 @@ __device__ __forceinline__ void row_gather(const int32_t* __restrict__ cols, con
     for (; k + 3 < k1; k += 4) {
       const int j0 = __ldg(cols + k), j1 = __ldg(cols + k + 1), j2 = __ldg(cols + k + 2), j3 = __ldg(cols + k + 3);
       const V a0 = vals[k], a1 = vals[k + 1], a2 = vals[k + 2], a3 = vals[k + 3];
-      const V v0 = ldcg(vec + (long)j0 * NS + s), v1 = ldcg(vec + (long)j1 * NS + s);
-      const V v2 = ldcg(vec + (long)j2 * NS + s), v3 = ldcg(vec + (long)j3 * NS + s);
+      const V v0 = gather_ld<V, NS>(vec + (long)j0 * NS + s), v1 = gather_ld<V, NS>(vec + (long)j1 * NS + s);
+      const V v2 = gather_ld<V, NS>(vec + (long)j2 * NS + s), v3 = gather_ld<V, NS>(vec + (long)j3 * NS + s);
       t1x += a0.x * v0.x; t1y += a0.x * v0.y; t2x += a0.y * v0.x; t2y += a0.y * v0.y;
       t1x += a1.x * v1.x; t1y += a1.x * v1.y; t2x += a1.y * v1.x; t2y += a1.y * v1.y;
       t1x += a2.x * v2.x; t1y += a2.x * v2.y; t2x += a2.y * v2.x; t2y += a2.y * v2.y;
@@ -175,10 +194,22 @@ __device__ __forceinline__ void row_gather(const int32_t* __restrict__ cols, con
   for (; k < k1; k += G) {
     const int j = __ldg(cols + k);
     const V a = vals[k];
-    const V v = ldcg(vec + (long)j * NS + s);
+    const V v = gather_ld<V, NS>(vec + (long)j * NS + s);
     t1x += a.x * v.x; t1y += a.x * v.y;
     t2x += a.y * v.x; t2y += a.y * v.y;
   }
+}
+
+// The contiguous part of [p0, p1) that this block works on; its warps interleave
+// inside it.  Rows near in index are near in the mesh, so the warps of an SM
+// gather from overlapping neighbourhoods and L1 serves the repeats.
+struct Slice {
+  int begin, end;
+};
+__device__ __forceinline__ Slice block_slice(int p0, int p1) {
+  const int per = (p1 - p0 + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int b = p0 + (int)blockIdx.x * per;
+  return Slice{min(b, p1), min(b + per, p1)};
 }
 
 // Block-reduce NS-per-lane doubles into part[blockIdx][s*4 + slot]; lanes with g == 0 hold system s values.
@@ -242,6 +273,7 @@ __global__ void __launch_bounds__(256)
   if (ctrl->done) return;
   constexpr int G = 32 / NS;
   const unsigned epoch = ctrl->epoch;
+  const unsigned lim = ctrl->spin_limit ? ctrl->spin_limit : SPIN_LIMIT;
   const bool update = ctrl->iter > 0;
   const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -294,7 +326,7 @@ __global__ void __launch_bounds__(256)
     for (int k = k0 + g; k < k1; k += G) {
       const int j = col[k];
       const V a = km[k];
-      if (!wait_flag(flag + j, epoch, st, row)) break;
+      if (!wait_flag(flag + j, epoch, st, row, lim)) break;
       const V yj = ldcg(y + (long)j * NS + s);
       t1x += a.x * yj.x; t1y += a.x * yj.y;
       t2x += a.y * yj.x; t2y += a.y * yj.y;
@@ -333,6 +365,7 @@ __global__ void __launch_bounds__(256)
   if (ctrl->done) return;
   constexpr int G = 32 / NS;
   const unsigned epoch = ctrl->epoch;
+  const unsigned lim = ctrl->spin_limit ? ctrl->spin_limit : SPIN_LIMIT;
   const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -354,7 +387,7 @@ __global__ void __launch_bounds__(256)
       for (int k = k0 + g; k < k1; k += G) {
         const int j = col[k];
         const V a = km[k];
-        if (!wait_flag(flag + j, epoch, st, row)) break;
+        if (!wait_flag(flag + j, epoch, st, row, lim)) break;
         const V zj = ldcg(z + (long)j * NS + s);
         t1x += a.x * zj.x; t1y += a.x * zj.y;
         t2x += a.y * zj.x; t2y += a.y * zj.y;
@@ -418,23 +451,34 @@ struct McShape {
   static constexpr int G = LPR / NS;             // entry groups per row
 };
 
-template <class T, int NS, bool SEG = false>
+// 1 / (sd (K_ii + i omega M_ii)): the SSOR diagonal of the system at omega, from the
+// row's (K, M) diagonal pair (COCG13_single.f90:126-130), computed where it is used
+// instead of being read from a per-(row, system) array
+__device__ __forceinline__ double2 ssor_dd(double2 a, double om, double sd) {
+  const double dx = sd * a.x, dy = sd * om * a.y;
+  const double inv = 1.0 / (dx * dx + dy * dy);
+  return make_double2(dx * inv, -dy * inv);
+}
+
+// T: the COCG vectors (r, q); PT: the preconditioner's matrix copy, output y and
+// the values gathered from it (PT = float: the FP32 preconditioner of an FP64 solve)
+template <class T, class PT, int NS, bool SEG = false>
 __global__ void __launch_bounds__(256)
-    k_fwd_mc(const int32_t* __restrict__ lptr, const int32_t* __restrict__ lcol, const typename Cx<T>::V* __restrict__ lkm,
-             int n, typename Cx<T>::V* __restrict__ r, typename Cx<T>::V* __restrict__ y,
-             const typename Cx<T>::V* __restrict__ q, const typename Cx<T>::V* __restrict__ dd,
-             const int32_t* __restrict__ perm,
+    k_fwd_mc(const int32_t* __restrict__ lptr, const int32_t* __restrict__ lcol,
+             const typename Cx<PT>::V* __restrict__ lkm, int n, typename Cx<T>::V* __restrict__ r,
+             typename Cx<PT>::V* __restrict__ y, const typename Cx<T>::V* __restrict__ q,
+             const double2* __restrict__ dkm, double sd, const int32_t* __restrict__ perm,
              const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl,
              double* __restrict__ part, const uint8_t* __restrict__ seg, typename Cx<T>::V* __restrict__ rprev) {
   using V = typename Cx<T>::V;
+  using PV = typename Cx<PT>::V;
   using S = McShape<NS, SEG>;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;  // uniform over the grid
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
   const bool update = ctrl->iter > 0;
   const int lane = threadIdx.x & 31, sub = lane / S::LPR, s = lane % NS, g = (lane % S::LPR) / NS;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;  // warp in block, warps per block
   const int slot = (threadIdx.x >> 5) * S::RPW + sub;
   double om = sc[s].omega;
   double2 al = sc[s].alpha;
@@ -444,10 +488,12 @@ __global__ void __launch_bounds__(256)
   if constexpr (SEG) red = seg_sums<8 * S::RPW, 1>();
   for (int c = 0; c < ncolors; ++c) {
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    for (int pos0 = p0 + warp * S::RPW; pos0 < p1; pos0 += nwarps * S::RPW) {
+    const Slice sl = block_slice(p0, p1);
+    for (int pos0 = sl.begin + wib * S::RPW; pos0 < sl.end; pos0 += nwb * S::RPW) {
       const int pos = pos0 + sub;
-      const bool live = pos < p1;
+      const bool live = pos < sl.end;
       const int row = live ? __ldg(perm + pos) : 0;
+      const double2 dg = live ? __ldg(dkm + pos) : make_double2(1.0, 0.0);
       int sid = s;
       if constexpr (SEG) {
         sid = live ? (int)__ldg(seg + row) : 0;
@@ -468,19 +514,20 @@ __global__ void __launch_bounds__(256)
         if constexpr (SEG) red[slot][sid][0] += v;
         else rr += v;
       }
-      T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
+      PT t1x = 0, t1y = 0, t2x = 0, t2y = 0;
       if (live)
-        row_gather<T, NS, S::G>(lcol, lkm, y, __ldg(lptr + pos) + g, __ldg(lptr + pos + 1), s, t1x, t1y, t2x, t2y);
+        row_gather<PT, NS, S::G>(lcol, lkm, y, __ldg(lptr + pos) + g, __ldg(lptr + pos + 1), s, t1x, t1y, t2x, t2y);
 #pragma unroll
       for (int m = NS; m < S::LPR; m <<= 1) {
         t1x += shfl_xor(t1x, m); t1y += shfl_xor(t1y, m);
         t2x += shfl_xor(t2x, m); t2y += shfl_xor(t2y, m);
       }
       if (live && g == 0) {
-        const T o = (T)om;
-        const T wx = ri.x - (t1x - o * t2y), wy = ri.y - (t1y + o * t2x);
-        const V d = dd[(long)row * NS + s];
-        y[(long)row * NS + s] = Cx<T>::make(wx * d.x - wy * d.y, wx * d.y + wy * d.x);
+        const PT o = (PT)om;
+        const PT wx = (PT)ri.x - (t1x - o * t2y), wy = (PT)ri.y - (t1y + o * t2x);
+        const double2 dd = ssor_dd(dg, om, sd);
+        const PT dx = (PT)dd.x, dy = (PT)dd.y;
+        y[(long)row * NS + s] = Cx<PT>::make(wx * dx - wy * dy, wx * dy + wy * dx);
       }
     }
     grid.sync();
@@ -495,22 +542,24 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-template <class T, int NS, bool SEG = false>
+// Backward sweep in place on z (the forward sweep's y).  r (COCG type T) is read
+// only by packed batches, for their per-mesh rho = r^T z.
+template <class T, class PT, int NS, bool SEG = false>
 __global__ void __launch_bounds__(256)
-    k_bwd_mc(const int32_t* __restrict__ uptr, const int32_t* __restrict__ ucol, const typename Cx<T>::V* __restrict__ ukm,
-             int n, const typename Cx<T>::V* __restrict__ r, typename Cx<T>::V* __restrict__ z,
-             const typename Cx<T>::V* __restrict__ dd, const int32_t* __restrict__ perm,
+    k_bwd_mc(const int32_t* __restrict__ uptr, const int32_t* __restrict__ ucol,
+             const typename Cx<PT>::V* __restrict__ ukm, int n, const typename Cx<T>::V* __restrict__ r,
+             typename Cx<PT>::V* __restrict__ z, const int32_t* __restrict__ perm,
              const int32_t* __restrict__ cptr, int ncolors, SysScal* __restrict__ sc, Ctrl* __restrict__ ctrl,
              double* __restrict__ part, const uint8_t* __restrict__ seg, const double2* __restrict__ dkm,
              double sd) {
   using V = typename Cx<T>::V;
+  using PV = typename Cx<PT>::V;
   using S = McShape<NS, SEG>;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
   const int lane = threadIdx.x & 31, sub = lane / S::LPR, s = lane % NS, g = (lane % S::LPR) / NS;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;  // warp in block, warps per block
   const int slot = (threadIdx.x >> 5) * S::RPW + sub;
   double om = sc[s].omega;
   double rx = 0.0, ry = 0.0;
@@ -518,39 +567,40 @@ __global__ void __launch_bounds__(256)
   if constexpr (SEG) red = seg_sums<8 * S::RPW, 4>();
   for (int c = ncolors - 1; c >= 0; --c) {
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    for (int pos0 = p0 + warp * S::RPW; pos0 < p1; pos0 += nwarps * S::RPW) {
+    const Slice sl = block_slice(p0, p1);
+    for (int pos0 = sl.begin + wib * S::RPW; pos0 < sl.end; pos0 += nwb * S::RPW) {
       const int pos = pos0 + sub;
-      const bool live = pos < p1;
+      const bool live = pos < sl.end;
       const int row = live ? __ldg(perm + pos) : 0;
+      const double2 dg = live ? __ldg(dkm + pos) : make_double2(1.0, 0.0);
       int sid = s;
       if constexpr (SEG) {
         sid = live ? (int)__ldg(seg + row) : 0;
         om = sc[sid].omega;
       }
-      T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
+      PT t1x = 0, t1y = 0, t2x = 0, t2y = 0;
       if (live)
-        row_gather<T, NS, S::G>(ucol, ukm, z, __ldg(uptr + pos) + g, __ldg(uptr + pos + 1), s, t1x, t1y, t2x, t2y);
+        row_gather<PT, NS, S::G>(ucol, ukm, z, __ldg(uptr + pos) + g, __ldg(uptr + pos + 1), s, t1x, t1y, t2x, t2y);
 #pragma unroll
       for (int m = NS; m < S::LPR; m <<= 1) {
         t1x += shfl_xor(t1x, m); t1y += shfl_xor(t1y, m);
         t2x += shfl_xor(t2x, m); t2y += shfl_xor(t2y, m);
       }
       if (live && g == 0) {
-        V zi = z[(long)row * NS + s];
+        PV zi = z[(long)row * NS + s];
         if constexpr (!SEG) {
-          // rho = r^T z = y^T D' y (U = L^T, D' = sd diag(A), y = the forward sweep's output in z);
-          // the diagonal sits in colour-position order, so its load does not wait for the row id
-          const double2 a = dkm[pos];
-          const double dx = sd * a.x, dy = sd * om * a.y;
+          // rho = r^T z = y^T D' y (U = L^T, D' = sd diag(A), y = the forward sweep's output in z)
+          const double dx = sd * dg.x, dy = sd * om * dg.y;
           const double y2x = (double)zi.x * (double)zi.x - (double)zi.y * (double)zi.y;
           const double y2y = 2.0 * (double)zi.x * (double)zi.y;
           rx += dx * y2x - dy * y2y;
           ry += dx * y2y + dy * y2x;
         }
-        const T o = (T)om;
-        const T swx = t1x - o * t2y, swy = t1y + o * t2x;
-        const V d = dd[(long)row * NS + s];
-        zi = Cx<T>::make(zi.x - (d.x * swx - d.y * swy), zi.y - (d.x * swy + d.y * swx));
+        const PT o = (PT)om;
+        const PT swx = t1x - o * t2y, swy = t1y + o * t2x;
+        const double2 dd = ssor_dd(dg, om, sd);
+        const PT dx = (PT)dd.x, dy = (PT)dd.y;
+        zi = Cx<PT>::make(zi.x - (dx * swx - dy * swy), zi.y - (dx * swy + dy * swx));
         z[(long)row * NS + s] = zi;
         if constexpr (SEG) {  // packed batches: per-mesh rho = r^T z
           const V ri = r[(long)row * NS + s];
@@ -591,10 +641,11 @@ __global__ void k_gather_entries(const double2* __restrict__ km, const int32_t* 
 // then z += G u and the rho = r^T z partial sums of the corrected z.
 
 // t_a = sum over the non-Dirichlet edges e at node a of g_ea r_e (g = +1 at the head, -1 at the tail)
-template <class T, int NS>
+// (r in the COCG type T, t in the preconditioner type PT; the sum runs in T)
+template <class T, class PT, int NS>
 __global__ void k_grad_t(int node, const int32_t* __restrict__ nptr, const int32_t* __restrict__ nlist,
                          const uint8_t* __restrict__ bc, const typename Cx<T>::V* __restrict__ r,
-                         typename Cx<T>::V* __restrict__ t, const Ctrl* __restrict__ ctrl) {
+                         typename Cx<PT>::V* __restrict__ t, const Ctrl* __restrict__ ctrl) {
   if (ctrl->done) return;
   const long total = (long)node * NS;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
@@ -607,7 +658,7 @@ __global__ void k_grad_t(int node, const int32_t* __restrict__ nptr, const int32
       if (v & 1) { ax -= re.x; ay -= re.y; }
       else { ax += re.x; ay += re.y; }
     }
-    t[i] = Cx<T>::make(ax, ay);
+    t[i] = Cx<PT>::make((PT)ax, (PT)ay);
   }
 }
 
@@ -630,16 +681,16 @@ __global__ void __launch_bounds__(256)
   if (ctrl->done) return;
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
   const int lane = threadIdx.x & 31, sub = lane / S::LPR, s = lane % NS, g = (lane % S::LPR) / NS;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;  // warp in block, warps per block
   double om = sc[s].omega;
   double tx = 0.0, ty = 0.0;
   for (int cc = 0; cc < ncolors; ++cc) {
     const int c = backward ? ncolors - 1 - cc : cc;
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    for (int pos0 = p0 + warp * S::RPW; pos0 < p1; pos0 += nwarps * S::RPW) {
+    const Slice sl = block_slice(p0, p1);
+    for (int pos0 = sl.begin + wib * S::RPW; pos0 < sl.end; pos0 += nwb * S::RPW) {
       const int pos = pos0 + sub;
-      const bool live = pos < p1;
+      const bool live = pos < sl.end;
       const int row = live ? __ldg(perm + pos) : 0;
       if constexpr (SEG) om = sc[live ? (int)__ldg(seg + row) : 0].omega;
       T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
@@ -701,13 +752,15 @@ __device__ __forceinline__ void seg_warp_add(double (*red)[MAX_SYS][NVAL], int s
 }
 
 // z_e += u_head(e) - u_tail(e) on the non-Dirichlet edges, then rho = r^T z partial sums (slots 0, 1)
-template <class T, int NS, bool SEG>
+// (u, z in the preconditioner type PT, r in the COCG type T)
+template <class T, class PT, int NS, bool SEG>
 __global__ void __launch_bounds__(256)
     k_grad_add(int n, const int32_t* __restrict__ line, const uint8_t* __restrict__ bc,
-               const typename Cx<T>::V* __restrict__ u, typename Cx<T>::V* __restrict__ z,
+               const typename Cx<PT>::V* __restrict__ u, typename Cx<PT>::V* __restrict__ z,
                const typename Cx<T>::V* __restrict__ r, const Ctrl* __restrict__ ctrl, double* __restrict__ part,
                const uint8_t* __restrict__ seg) {
   using V = typename Cx<T>::V;
+  using PV = typename Cx<PT>::V;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;
   const long total = (long)n * NS;
@@ -721,11 +774,11 @@ __global__ void __launch_bounds__(256)
     int sid = -1;
     if (i < total) {
       const int e = (int)(i / NS), s = (int)(i % NS);
-      V zi = z[i];
+      PV zi = z[i];
       if (!__ldg(bc + e)) {
-        const V uh = u[(long)(__ldg(line + 2 * e + 1) - 1) * NS + s];
-        const V ut = u[(long)(__ldg(line + 2 * e) - 1) * NS + s];
-        zi = Cx<T>::make(zi.x + (uh.x - ut.x), zi.y + (uh.y - ut.y));
+        const PV uh = u[(long)(__ldg(line + 2 * e + 1) - 1) * NS + s];
+        const PV ut = u[(long)(__ldg(line + 2 * e) - 1) * NS + s];
+        zi = Cx<PT>::make(zi.x + (uh.x - ut.x), zi.y + (uh.y - ut.y));
         z[i] = zi;
       }
       const V ri = r[i];
@@ -798,12 +851,14 @@ __global__ void k_dd_node(const double2* __restrict__ km, const int32_t* __restr
 // systems whose update is pending (also after the residual check ended the
 // solve).  Hybrid preconditioner with the gradient add folded in (u != nullptr):
 // z_e + u_head(e) - u_tail(e) on the non-Dirichlet edges stands for z.
-template <class T, int NS, bool SEG = false>
-__global__ void k_pupd(int n, const typename Cx<T>::V* __restrict__ z, typename Cx<T>::V* __restrict__ p,
+// (p in the COCG type T; z and u in the preconditioner type PT)
+template <class T, class PT, int NS, bool SEG = false>
+__global__ void k_pupd(int n, const typename Cx<PT>::V* __restrict__ z, typename Cx<T>::V* __restrict__ p,
                        const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl, const uint8_t* __restrict__ seg,
                        double2* __restrict__ x, int nsys, const int32_t* __restrict__ line,
-                       const uint8_t* __restrict__ bc, const typename Cx<T>::V* __restrict__ u) {
+                       const uint8_t* __restrict__ bc, const typename Cx<PT>::V* __restrict__ u) {
   using V = typename Cx<T>::V;
+  using PV = typename Cx<PT>::V;
   const bool done = ctrl->done;
   if (done) {
     if (!x) return;
@@ -827,14 +882,15 @@ __global__ void k_pupd(int n, const typename Cx<T>::V* __restrict__ z, typename 
       x[i] = xi;
     }
     if (done) continue;
-    V zi = z[i];
+    const PV zp = z[i];
+    V zi = Cx<T>::make((T)zp.x, (T)zp.y);
     if (u) {
       const int e = (int)(i / NS);
       if (!__ldg(bc + e)) {
         const int sn = SEG ? 0 : s;
-        const V uh = u[(long)(__ldg(line + 2 * e + 1) - 1) * NS + sn];
-        const V ut = u[(long)(__ldg(line + 2 * e) - 1) * NS + sn];
-        zi = Cx<T>::make(zi.x + (uh.x - ut.x), zi.y + (uh.y - ut.y));
+        const PV uh = u[(long)(__ldg(line + 2 * e + 1) - 1) * NS + sn];
+        const PV ut = u[(long)(__ldg(line + 2 * e) - 1) * NS + sn];
+        zi = Cx<T>::make(zi.x + (T)(uh.x - ut.x), zi.y + (T)(uh.y - ut.y));
       }
     }
     if (first) {
@@ -865,16 +921,16 @@ __global__ void __launch_bounds__(256)
   constexpr int LPR = 32 / RPW;  // lanes per row
   constexpr int G = LPR / NS;    // entry groups per row
   const int lane = threadIdx.x & 31, sub = lane / LPR, s = lane % NS, g = (lane % LPR) / NS;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double om = sc[s].omega;
   double ax = 0.0, ay = 0.0, bb = 0.0;
   double (*red)[MAX_SYS][3] = nullptr;
   if constexpr (SEG) red = seg_sums<8 * RPW, 3>();
   const int slot = (threadIdx.x >> 5) * RPW + sub;
-  for (int row0 = warp * RPW; row0 < n; row0 += nwarps * RPW) {
+  const Slice sl = block_slice(0, n);
+  const int wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;
+  for (int row0 = sl.begin + wib * RPW; row0 < sl.end; row0 += nwb * RPW) {
     const int row = row0 + sub;
-    const bool live = row < n;
+    const bool live = row < sl.end;
     int sid = s;
     if constexpr (SEG) {
       sid = live ? (int)__ldg(seg + row) : 0;
@@ -1069,6 +1125,7 @@ __global__ void __launch_bounds__(256)
   using V = typename Cx<T>::V;
   constexpr int G = 32 / NS;
   const unsigned epoch = ctrl->epoch;
+  const unsigned lim = ctrl->spin_limit ? ctrl->spin_limit : SPIN_LIMIT;
   const int lane = threadIdx.x & 31, s = lane % NS, g = lane / NS;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1081,7 +1138,7 @@ __global__ void __launch_bounds__(256)
     for (int k = k0 + g; k < k1; k += G) {
       const int j = col[k];
       const V a = km[k];
-      if (!wait_flag(flag + j, epoch, st, row)) break;
+      if (!wait_flag(flag + j, epoch, st, row, lim)) break;
       const V d = ldcg(dd + (long)j * NS + s);
       const double2 al = make_double2((double)a.x, om * (double)a.y);
       const double2 a2 = cmul(al, al);
@@ -1141,7 +1198,7 @@ __global__ void k_copy_r<float2>(const double2* __restrict__ in, float2* __restr
 
 // Start of an inner solve: x_inner = 0, ||b||^2 from the partials of the residual SpMV.
 __global__ void k_init_sys(SysScal* sc, Ctrl* ctrl, const double* part, int nblocks, int ns, double tol, int maxit,
-                           const double* omega) {
+                           const double* omega, unsigned spin_limit) {
   const int s = threadIdx.x >> 5;
   if (s < ns) {
     double v[1];
@@ -1155,8 +1212,10 @@ __global__ void k_init_sys(SysScal* sc, Ctrl* ctrl, const double* part, int nblo
       S.rho = S.rho1 = S.alpha = S.beta = S.pq = make_double2(0.0, 0.0);
       S.iter = 0;
       S.xpend = 0;
-      S.active = v[0] > 0.0;
-      S.status = AFEM_OK;
+      // a NaN / Inf in the matrix or the right-hand side shows in ||b - A 0||^2
+      const bool finite = isfinite(v[0]);
+      S.active = finite && v[0] > 0.0;
+      S.status = finite ? AFEM_OK : AFEM_ENONFINITE;
     }
   }
   __syncthreads();
@@ -1165,6 +1224,7 @@ __global__ void k_init_sys(SysScal* sc, Ctrl* ctrl, const double* part, int nblo
     ctrl->iter = 0;
     ctrl->tol = tol;
     ctrl->maxit = maxit;
+    ctrl->spin_limit = spin_limit;
   }
 }
 
@@ -1285,6 +1345,10 @@ int tune_spmv(afem_ctx* c, SolverWork* w) {
   using I = Inner<T, NS>;
   int& slot = sizeof(T) == 8 ? w->rpw64 : w->rpw32;
   if (slot) return slot;
+  if (c->spmv_rpw > 0) {  // pinned by the caller: the same reduction order in every process
+    slot = NS * c->spmv_rpw <= 32 ? c->spmv_rpw : 1;
+    return slot;
+  }
   cudaStream_t s = c->stream;
   cudaEvent_t a, b;
   AFEM_CUDA(cudaEventCreate(&a));
@@ -1315,10 +1379,15 @@ int tune_spmv(afem_ctx* c, SolverWork* w) {
 }
 
 // One COCG iteration (7 launches; the learned preconditioner adds the network's 8).
-template <class T, int NS, bool SEG>
+// T: COCG vectors and the SpMV; PT: the multicolour preconditioner (its matrix
+// copies and vectors); PT differs from T only on the multicolour path.
+template <class T, class PT, int NS, bool SEG>
 void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, cudaEvent_t* ev) {
   using I = Inner<T, NS>;
+  using P = Inner<PT, NS>;
   using V = typename I::V;
+  using PV = typename P::V;
+  constexpr bool same = std::is_same<T, PT>::value;
   cudaStream_t s = c->stream;
   const int n = w->n;
   const int nsys = w->nsys;
@@ -1334,33 +1403,36 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
   // backward nodal sweep sums t^T u, the nodal share of rho
   const bool fold_grad = hyb && !lbase && !SEG;
   if (ev) AFEM_CUDA(cudaEventRecord(ev[0], s));
-  if (mc)  // the multicolour sweep updates r only: x += alpha p moves to the p update
-    launch_coop(k_fwd_mc<T, NS, SEG>, w->mc_blocks, s, (const int32_t*)c->mc_lptr.p, (const int32_t*)c->mc_lcol.p,
-                I::LKM(c, w), n, I::R(w), I::Z(w), (const V*)I::Q(w), (const V*)I::DD(w),
-                (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p,
-                w->part.p, sg, rp);
-  else
+  if (mc) {  // the multicolour sweep updates r only: x += alpha p moves to the p update
+    launch_coop(k_fwd_mc<T, PT, NS, SEG>, w->mc_blocks, s, (const int32_t*)c->mc_lptr.p,
+                (const int32_t*)c->mc_lcol.p, P::LKM(c, w), n, I::R(w), P::Z(w), (const V*)I::Q(w),
+                (const double2*)c->mc_dkm.p, w->sd, (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p,
+                c->ncolors, w->sc.p, w->ctrl.p, w->part.p, sg, rp);
+  } else if constexpr (same) {
     launch_coop(k_fwd<T, NS, SEG>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
                 (const int32_t*)c->diagpos.p, I::KM(c, w), n, I::R(w), I::Z(w), (const V*)I::P(w), (const V*)I::Q(w),
                 w->x.p, (const V*)I::DD(w), w->flag_f.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, rp,
                 (const int32_t*)c->perm_f.p, sg);
+  }
   if (ev) AFEM_CUDA(cudaEventRecord(ev[1], s));
   const int swb = mc ? w->mc_blocks : sweep_blocks;
   k_scal_r<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, swb, nsys, learned ? w->rms.p : nullptr, n,
                                       mc ? 1 : 0);
   count_launch();
-  if (learned && !lbase) mpnn_run<V>(c, NS, w->rms.p, (const V*)I::R(w), I::Z(w), &w->ctrl.p->done);
+  if constexpr (same)
+    if (learned && !lbase) mpnn_run<V>(c, NS, w->rms.p, (const V*)I::R(w), I::Z(w), &w->ctrl.p->done);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[2], s));
-  if (mc)
-    launch_coop(k_bwd_mc<T, NS, SEG>, w->mcb_blocks, s, (const int32_t*)c->mc_uptr.p, (const int32_t*)c->mc_ucol.p,
-                I::UKM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w), (const int32_t*)c->perm_mc.p,
-                (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p, sg,
-                (const double2*)c->mc_dkm.p, w->sd);
-  else
+  if (mc) {
+    launch_coop(k_bwd_mc<T, PT, NS, SEG>, w->mcb_blocks, s, (const int32_t*)c->mc_uptr.p,
+                (const int32_t*)c->mc_ucol.p, P::UKM(c, w), n, (const V*)I::R(w), P::Z(w),
+                (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p,
+                w->part.p, sg, (const double2*)c->mc_dkm.p, w->sd);
+  } else if constexpr (same) {
     launch_coop(k_bwd<T, NS, SEG>, sweep_blocks, s, (const int32_t*)c->rowptr.p, (const int32_t*)c->col.p,
                 (const int32_t*)c->diagpos.p, I::KM(c, w), n, (const V*)I::R(w), I::Z(w), (const V*)I::DD(w),
                 w->flag_b.p, mode, w->sc.p, w->ctrl.p, w->part.p, c->status.p, (const V*)rp,
                 (const int32_t*)c->perm_b.p, sg);
+  }
   if (ev) AFEM_CUDA(cudaEventRecord(ev[3], s));
   int rho_blocks = mc ? w->mcb_blocks : sweep_blocks;
   if (hyb) {
@@ -1369,39 +1441,40 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
     HybridState* h = c->hyb;
     const int node = h->node;
     const uint8_t* hs = SEG ? h->seg.p : nullptr;
-    k_grad_t<T, NS><<<c->num_sms * 8, 256, 0, s>>>(node, h->nptr.p, h->nlist.p, c->bc.p, (const V*)I::R(w), I::HT(w),
-                                                    w->ctrl.p);
+    k_grad_t<T, PT, NS><<<c->num_sms * 8, 256, 0, s>>>(node, h->nptr.p, h->nlist.p, c->bc.p, (const V*)I::R(w),
+                                                        P::HT(w), w->ctrl.p);
     count_launch();
     for (int bwd = 0; bwd < 2; ++bwd)
-      launch_coop(k_nsweep_mc<T, NS, SEG>, w->nmc_blocks, s, (const int32_t*)(bwd ? h->uptr.p : h->lptr.p),
-                  (const int32_t*)(bwd ? h->ucol.p : h->lcol.p), bwd ? I::HUKM(c) : I::HLKM(c),
-                  (const V*)I::HT(w), I::HY(w), (const V*)I::HDD(w), (const int32_t*)h->perm.p,
+      launch_coop(k_nsweep_mc<PT, NS, SEG>, w->nmc_blocks, s, (const int32_t*)(bwd ? h->uptr.p : h->lptr.p),
+                  (const int32_t*)(bwd ? h->ucol.p : h->lcol.p), bwd ? P::HUKM(c) : P::HLKM(c),
+                  (const PV*)P::HT(w), P::HY(w), (const PV*)P::HDD(w), (const int32_t*)h->perm.p,
                   (const int32_t*)h->cptr.p, h->ncolors, (const SysScal*)w->sc.p, (const Ctrl*)w->ctrl.p, hs, bwd,
                   (fold_grad && bwd) ? w->part2.p : (double*)nullptr);
     if (!fold_grad) {
-      k_grad_add<T, NS, SEG><<<w->nblocks, 256, 0, s>>>(n, c->line.p, c->bc.p, (const V*)I::HY(w), I::Z(w),
-                                                          (const V*)I::R(w), w->ctrl.p, w->part.p, sg);
+      k_grad_add<T, PT, NS, SEG><<<w->nblocks, 256, 0, s>>>(n, c->line.p, c->bc.p, (const PV*)P::HY(w), P::Z(w),
+                                                              (const V*)I::R(w), w->ctrl.p, w->part.p, sg);
       count_launch();
       rho_blocks = w->nblocks;
     }
   }
-  if (lbase) {
-    // z += N(r), then rho = r^T z and rprev^T z of the final z for the flexible beta
-    mpnn_run<V>(c, NS, w->rms.p, (const V*)I::R(w), I::Z(w), &w->ctrl.p->done);
-    k_dots<T, NS><<<w->nblocks, 256, 0, s>>>(n, (const V*)I::R(w), (const V*)I::Z(w), (const V*)rp, w->ctrl.p,
-                                             w->part.p);
-    count_launch();
-    rho_blocks = w->nblocks;
-  }
+  if constexpr (same)
+    if (lbase) {
+      // z += N(r), then rho = r^T z and rprev^T z of the final z for the flexible beta
+      mpnn_run<V>(c, NS, w->rms.p, (const V*)I::R(w), I::Z(w), &w->ctrl.p->done);
+      k_dots<T, NS><<<w->nblocks, 256, 0, s>>>(n, (const V*)I::R(w), (const V*)I::Z(w), (const V*)rp, w->ctrl.p,
+                                               w->part.p);
+      count_launch();
+      rho_blocks = w->nblocks;
+    }
   if (ev) AFEM_CUDA(cudaEventRecord(ev[4], s));
   k_scal_rho<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, rho_blocks, nsys, learned ? 1 : 0,
                                         fold_grad ? w->part2.p : (const double*)nullptr, w->nmc_blocks);
   count_launch();
   if (ev) AFEM_CUDA(cudaEventRecord(ev[5], s));
-  k_pupd<T, NS, SEG><<<c->num_sms * 8, 256, 0, s>>>(
-      n, I::Z(w), I::P(w), w->sc.p, w->ctrl.p, sg, mc ? w->x.p : (double2*)nullptr, nsys,
+  k_pupd<T, PT, NS, SEG><<<c->num_sms * 8, 256, 0, s>>>(
+      n, (const PV*)P::Z(w), I::P(w), w->sc.p, w->ctrl.p, sg, mc ? w->x.p : (double2*)nullptr, nsys,
       fold_grad ? (const int32_t*)c->line.p : (const int32_t*)nullptr, fold_grad ? c->bc.p : (const uint8_t*)nullptr,
-      fold_grad ? (const V*)I::HY(w) : (const V*)nullptr);
+      fold_grad ? (const PV*)P::HY(w) : (const PV*)nullptr);
   count_launch();
   if (ev) AFEM_CUDA(cudaEventRecord(ev[6], s));
   launch_spmv<T, NS, SEG>(c, w, sizeof(T) == 8 ? w->rpw64 : w->rpw32, I::KM(c, w), (const V*)I::P(w), I::Q(w),
@@ -1432,9 +1505,13 @@ void true_residual(afem_ctx* c, SolverWork* w, std::vector<double>& rr, std::vec
   for (int k = 0; k < nsys; ++k) { rr[k] = h[2 * k]; bb[k] = h[2 * k + 1]; }
 }
 
-template <class T, int NS, bool SEG>
+// DD of the natural-order sweeps (IC, SSOR, DIAG) in the COCG type T; the
+// multicolour sweeps compute theirs from the diagonal, and the hybrid's nodal
+// diagonal goes to the preconditioner type PT.
+template <class T, class PT, int NS, bool SEG>
 void setup_dd(afem_ctx* c, SolverWork* w, int precond, double sd) {
   using I = Inner<T, NS>;
+  using P = Inner<PT, NS>;
   cudaStream_t s = c->stream;
   const uint8_t* sg = SEG ? c->seg_of_row.p : nullptr;
   if (precond == AFEM_PRECOND_IC) {
@@ -1447,23 +1524,22 @@ void setup_dd(afem_ctx* c, SolverWork* w, int precond, double sd) {
                 (const Ctrl*)w->ctrl.p, c->status.p, (const int32_t*)c->perm_f.p, sg);
     w->epoch_host += 1;
     AFEM_CUDA(cudaMemcpyAsync(&w->ctrl.p->epoch, &w->epoch_host, sizeof(unsigned), cudaMemcpyHostToDevice, s));
-  } else if (precond == AFEM_PRECOND_SSOR || precond == AFEM_PRECOND_DIAG || precond == AFEM_PRECOND_SSOR_MC ||
-             precond == AFEM_PRECOND_HYBRID) {
+  } else if (precond == AFEM_PRECOND_SSOR || precond == AFEM_PRECOND_DIAG) {
     k_dd_diag<T, NS><<<c->num_sms * 8, 256, 0, s>>>(I::KM(c, w), (const int32_t*)c->diagpos.p, w->n, sd,
                                                     (const SysScal*)w->sc.p, I::DD(w), sg);
     count_launch();
   }
   if (precond == AFEM_PRECOND_HYBRID) {
     HybridState* h = c->hyb;
-    k_dd_node<T, NS><<<c->num_sms * 8, 256, 0, s>>>(h->km.p, h->diagpos.p, h->live.p, h->node,
-                                                    (const SysScal*)w->sc.p, I::HDD(w), SEG ? h->seg.p : nullptr);
+    k_dd_node<PT, NS><<<c->num_sms * 8, 256, 0, s>>>(h->km.p, h->diagpos.p, h->live.p, h->node,
+                                                     (const SysScal*)w->sc.p, P::HDD(w), SEG ? h->seg.p : nullptr);
     count_launch();
   }
 }
 
 // Inner COCG from x_inner = 0 on right-hand side r64 (FP64, converted to T).
 // Returns iterations; fills per-system status/resid.
-template <class T, int NS, bool SEG>
+template <class T, class PT, int NS, bool SEG>
 int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond, double tol, int maxit,
                int check_every, const double* d_omega, std::vector<SysScal>& hs, bool* stalled) {
   using I = Inner<T, NS>;
@@ -1483,13 +1559,14 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
                                                           w->part.p, w->r64.p, SEG ? c->seg_of_row.p : nullptr);
     count_launch();
   }
-  k_init_sys<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, nsys, tol, maxit, d_omega);
+  k_init_sys<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, nsys, tol, maxit, d_omega,
+                                       c->wait_limit);
   count_launch();
   const bool use_hyb = precond == AFEM_PRECOND_HYBRID || (precond == AFEM_PRECOND_LEARNED && mpnn_base(c) == 1);
   if (use_hyb) {
     HybridState* h = c->hyb;
     const long nt = (long)h->node * NS;
-    if (sizeof(T) == 8) {
+    if (sizeof(PT) == 8) {
       w->ht.alloc(nt); w->hy.alloc(nt); w->hdd.alloc(nt);
     } else {
       w->htf.alloc(nt); w->hyf.alloc(nt); w->hddf.alloc(nt);
@@ -1512,7 +1589,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
     }
   }
   w->sd = o->sigma_diag > 0 ? o->sigma_diag : 1.0;
-  setup_dd<T, NS, SEG>(c, w, use_hyb ? AFEM_PRECOND_HYBRID : precond, w->sd);
+  setup_dd<T, PT, NS, SEG>(c, w, use_hyb ? AFEM_PRECOND_HYBRID : precond, w->sd);
   const int mode = precond;
   tune_spmv<T, NS, SEG>(c, w);
   const bool learned = mode == AFEM_PRECOND_LEARNED;
@@ -1528,11 +1605,11 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   const int sb2 = coresident_blocks(k_bwd<T, NS, SEG>, c->num_sms);
   const int sblocks = std::min(std::min(sweep_blocks, sb2), w->nblocks);
   if (mode == AFEM_PRECOND_SSOR_MC || use_hyb) {
-    w->mc_blocks = std::min(coresident_blocks(k_fwd_mc<T, NS, SEG>, c->num_sms), w->nblocks);
-    w->mcb_blocks = std::min(coresident_blocks(k_bwd_mc<T, NS, SEG>, c->num_sms), w->nblocks);
+    w->mc_blocks = std::min(coresident_blocks(k_fwd_mc<T, PT, NS, SEG>, c->num_sms), w->nblocks);
+    w->mcb_blocks = std::min(coresident_blocks(k_bwd_mc<T, PT, NS, SEG>, c->num_sms), w->nblocks);
   }
   if (use_hyb)
-    w->nmc_blocks = std::min(coresident_blocks(k_nsweep_mc<T, NS, SEG>, c->num_sms), w->nblocks);
+    w->nmc_blocks = std::min(coresident_blocks(k_nsweep_mc<PT, NS, SEG>, c->num_sms), w->nblocks);
   // every solve starts a fresh flag generation: a solve that stopped inside a
   // chunk left its last forward-sweep flags at the epoch it ended on
   w->epoch_host += 1;
@@ -1557,7 +1634,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
       bool ok = true;
       g_capturing = 1;
       try {
-        for (int k = 0; k < chunk; ++k) enqueue_iteration<T, NS, SEG>(c, w, mode, sblocks, ev_of(k));
+        for (int k = 0; k < chunk; ++k) enqueue_iteration<T, PT, NS, SEG>(c, w, mode, sblocks, ev_of(k));
       } catch (const Error&) {
         ok = false;
       }
@@ -1581,6 +1658,25 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
     if (!gexec) use_graph = false;
   }
   int iter_before = 0;
+  // On an error inside the loop (a device status such as a wait timeout, a CUDA
+  // error) the graph and events are released and the host's flag epoch is brought
+  // up to the device's, so that the next solve's epoch is above every flag written.
+  struct LoopGuard {
+    SolverWork* w;
+    cudaStream_t s;
+    cudaGraphExec_t* g;
+    std::vector<cudaEvent_t>* evs;
+    bool armed = true;
+    ~LoopGuard() {
+      if (!armed) return;
+      if (*g) cudaGraphExecDestroy(*g);
+      for (auto& e : *evs) cudaEventDestroy(e);
+      if (cudaMemcpyAsync(w->h_ctrl, w->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+          cudaStreamSynchronize(s) == cudaSuccess)
+        w->epoch_host = std::max(w->epoch_host, w->h_ctrl->epoch);
+      cudaGetLastError();
+    }
+  } guard{w, s, &gexec, &evs};
   // every chunk either advances the iteration count or ends the solve; the
   // chunk budget is a host-side backstop against a device state that does neither
   const long chunk_budget = (long)maxit / chunk + 4;
@@ -1590,7 +1686,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
       AFEM_CUDA(cudaGraphLaunch(gexec, s));
       count_launch(graph_kernels);
     } else {
-      for (int k = 0; k < chunk; ++k) enqueue_iteration<T, NS, SEG>(c, w, mode, sblocks, ev_of(k));
+      for (int k = 0; k < chunk; ++k) enqueue_iteration<T, PT, NS, SEG>(c, w, mode, sblocks, ev_of(k));
     }
     AFEM_CUDA(cudaMemcpyAsync(w->h_ctrl, w->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
     AFEM_CUDA(cudaStreamSynchronize(s));
@@ -1598,7 +1694,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
     if (prof) {
       // count only iterations that ran to their last kernel
       const int executed = std::min(chunk, w->h_ctrl->iter - iter_before);
-      const char* tag = sizeof(T) == 8 ? "fp64" : "fp32";
+      const char* tag = sizeof(T) == 8 ? (sizeof(PT) == 8 ? "fp64" : "fp64pc32") : "fp32";
       char nf[64], nb[64], nh[64], np_[64], ns_[64];
       const char* kind = SEG ? "seg" : "ns";
       const int cnt = SEG ? nsys : NS;
@@ -1654,6 +1750,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
       }
     }
   }
+  guard.armed = false;
   if (gexec) cudaGraphExecDestroy(gexec);
   for (auto& e : evs) cudaEventDestroy(e);
   w->epoch_host = w->h_ctrl->epoch;
@@ -1668,7 +1765,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
 
 // The solve workspace for NS systems per row (SEG: a packed batch), FP32 copies when mixed.
 template <int NS, bool SEG>
-SolverWork* ensure_work(afem_ctx* c, int nsys, bool mixed) {
+SolverWork* ensure_work(afem_ctx* c, int nsys, bool mixed, bool pc32 = false) {
   SolverWork* w = c->work;
   cudaStream_t s = c->stream;
   const int n = c->nline;
@@ -1696,12 +1793,17 @@ SolverWork* ensure_work(afem_ctx* c, int nsys, bool mixed) {
   }
   w->nsys = nsys;
   if (mixed && w->rf.n != (size_t)total) {
-    w->rf.alloc(total); w->zf.alloc(total); w->pf.alloc(total); w->qf.alloc(total); w->ddf.alloc(total);
+    w->rf.alloc(total); w->pf.alloc(total); w->qf.alloc(total); w->ddf.alloc(total);
   }
+  if ((mixed || pc32) && w->zf.n != (size_t)total) w->zf.alloc(total);
   if (mixed && (!w->kmf_valid || w->kmf.n != (size_t)c->nnz)) {
     w->kmf.alloc(c->nnz);
     k_convert<float2, double2><<<c->num_sms * 8, 256, 0, s>>>(c->km.p, w->kmf.p, c->nnz);
     count_launch();
+    w->kmf_valid = true;
+  }
+  // FP32 copies of the colour-ordered split rows (mixed inner solve, FP32 preconditioner)
+  if ((mixed || pc32) && (!w->mcf_valid || w->mc_lkmf.n != c->mc_lcol.n)) {
     const long nl = (long)c->mc_lcol.n, nu = (long)c->mc_ucol.n;
     w->mc_lkmf.alloc(nl);
     w->mc_ukmf.alloc(nu);
@@ -1713,14 +1815,18 @@ SolverWork* ensure_work(afem_ctx* c, int nsys, bool mixed) {
       k_gather_entries<float2><<<c->num_sms * 8, 256, 0, s>>>(c->km.p, c->mc_usrc.p, nu, w->mc_ukmf.p);
       count_launch();
     }
-    w->kmf_valid = true;
+    w->mcf_valid = true;
   }
   {
     int b1 = 0;
     AFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_spmv<double, NS, 1, SEG>, 256, 0));
     w->nblocks = std::max(1, b1) * c->num_sms;
-    w->nblocks = std::max(w->nblocks, coresident_blocks(k_fwd_mc<double, NS, SEG>, c->num_sms));
-    w->nblocks = std::max(w->nblocks, coresident_blocks(k_bwd_mc<double, NS, SEG>, c->num_sms));
+    w->nblocks = std::max(w->nblocks, coresident_blocks(k_fwd_mc<double, double, NS, SEG>, c->num_sms));
+    w->nblocks = std::max(w->nblocks, coresident_blocks(k_bwd_mc<double, double, NS, SEG>, c->num_sms));
+    if (pc32) {
+      w->nblocks = std::max(w->nblocks, coresident_blocks(k_fwd_mc<double, float, NS, SEG>, c->num_sms));
+      w->nblocks = std::max(w->nblocks, coresident_blocks(k_bwd_mc<double, float, NS, SEG>, c->num_sms));
+    }
     int bf = coresident_blocks(k_fwd<double, NS, SEG>, c->num_sms);
     int bb = coresident_blocks(k_bwd<double, NS, SEG>, c->num_sms);
     w->nblocks = std::max(w->nblocks, std::max(bf, bb));
@@ -1742,7 +1848,8 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
   const long total = (long)n * NS;
   const int nsys = SEG ? c->nseg : NS;
   const bool mixed = o->precision == AFEM_MIXED;
-  SolverWork* w = ensure_work<NS, SEG>(c, nsys, mixed);
+  const bool pc32 = o->precision == AFEM_FP32_PRECOND;
+  SolverWork* w = ensure_work<NS, SEG>(c, nsys, mixed, pc32);
   // ---- right-hand sides and omegas
   {
     DBuf<int> dsrc;
@@ -1820,10 +1927,16 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     if (left <= 0) break;
     int its;
     bool stalled = false;
+    const bool mc_now = precond_now == AFEM_PRECOND_SSOR_MC || precond_now == AFEM_PRECOND_HYBRID;
     if (mixed)
-      its = inner_cocg<float, NS, SEG>(c, w, o, precond_now, inner_tol, left, o->check_every, d_om.p, hs, &stalled);
+      its = inner_cocg<float, float, NS, SEG>(c, w, o, precond_now, inner_tol, left, o->check_every, d_om.p, hs,
+                                              &stalled);
+    else if (pc32 && mc_now)
+      its = inner_cocg<double, float, NS, SEG>(c, w, o, precond_now, inner_tol, left, o->check_every, d_om.p, hs,
+                                               &stalled);
     else
-      its = inner_cocg<double, NS, SEG>(c, w, o, precond_now, inner_tol, left, o->check_every, d_om.p, hs, &stalled);
+      its = inner_cocg<double, double, NS, SEG>(c, w, o, precond_now, inner_tol, left, o->check_every, d_om.p, hs,
+                                                &stalled);
     if (precond_now != AFEM_PRECOND_LEARNED && stalled) {
       for (int k = 0; k < nsys; ++k)
         if (hs[k].active) hs[k].status = AFEM_ESTAGNATION;
@@ -1847,10 +1960,12 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
     rec = 0.0;
     bool all_ok = true, any_fatal = false;
     for (int k = 0; k < nsys; ++k) {
-      const double rel = bb[k] > 0 ? std::sqrt(rr[k] / bb[k]) : 0.0;
+      double rel = bb[k] > 0 ? std::sqrt(rr[k] / bb[k]) : 0.0;
+      if (!std::isfinite(rr[k]) || !std::isfinite(bb[k])) rel = std::nan("");
       worst = std::max(worst, rel);
       rec = std::max(rec, hs[k].resid);
       if (!(rel <= tol)) all_ok = false;
+      if (!std::isfinite(rel)) hs[k].status = AFEM_ENONFINITE;
       if (hs[k].status == AFEM_ENONFINITE || hs[k].status == AFEM_EBREAKDOWN) any_fatal = true;
       status[k] = (rel <= tol) ? AFEM_OK : hs[k].status;
     }
@@ -1977,20 +2092,20 @@ void precond_apply_device(afem_ctx* c, double omega, const double2* r, double2* 
   w->ht.alloc(h->node);
   w->hy.alloc(h->node);
   w->hdd.alloc(h->node);
-  setup_dd<double, 1, false>(c, w, AFEM_PRECOND_HYBRID, 1.0);
-  w->mc_blocks = std::min(std::min(coresident_blocks(k_fwd_mc<double, 1, false>, c->num_sms),
-                                   coresident_blocks(k_bwd_mc<double, 1, false>, c->num_sms)), w->nblocks);
+  setup_dd<double, double, 1, false>(c, w, AFEM_PRECOND_HYBRID, 1.0);
+  w->mc_blocks = std::min(std::min(coresident_blocks(k_fwd_mc<double, double, 1, false>, c->num_sms),
+                                   coresident_blocks(k_bwd_mc<double, double, 1, false>, c->num_sms)), w->nblocks);
   w->nmc_blocks = std::min(coresident_blocks(k_nsweep_mc<double, 1, false>, c->num_sms), w->nblocks);
-  launch_coop(k_fwd_mc<double, 1, false>, w->mc_blocks, s, (const int32_t*)c->mc_lptr.p, (const int32_t*)c->mc_lcol.p,
-              (const double2*)c->mc_lkm.p, n, w->r.p, w->z.p, (const double2*)w->q.p,
-              (const double2*)w->dd.p, (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors,
-              w->sc.p, w->ctrl.p, w->part.p, (const uint8_t*)nullptr, (double2*)nullptr);
-  launch_coop(k_bwd_mc<double, 1, false>, w->mc_blocks, s, (const int32_t*)c->mc_uptr.p, (const int32_t*)c->mc_ucol.p,
-              (const double2*)c->mc_ukm.p, n, (const double2*)w->r.p, w->z.p, (const double2*)w->dd.p,
+  launch_coop(k_fwd_mc<double, double, 1, false>, w->mc_blocks, s, (const int32_t*)c->mc_lptr.p,
+              (const int32_t*)c->mc_lcol.p, (const double2*)c->mc_lkm.p, n, w->r.p, w->z.p, (const double2*)w->q.p,
+              (const double2*)c->mc_dkm.p, 1.0, (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p,
+              c->ncolors, w->sc.p, w->ctrl.p, w->part.p, (const uint8_t*)nullptr, (double2*)nullptr);
+  launch_coop(k_bwd_mc<double, double, 1, false>, w->mc_blocks, s, (const int32_t*)c->mc_uptr.p,
+              (const int32_t*)c->mc_ucol.p, (const double2*)c->mc_ukm.p, n, (const double2*)w->r.p, w->z.p,
               (const int32_t*)c->perm_mc.p, (const int32_t*)c->color_ptr.p, c->ncolors, w->sc.p, w->ctrl.p, w->part.p,
               (const uint8_t*)nullptr, (const double2*)c->mc_dkm.p, 1.0);
-  k_grad_t<double, 1><<<c->num_sms * 8, 256, 0, s>>>(h->node, h->nptr.p, h->nlist.p, c->bc.p, (const double2*)w->r.p,
-                                                      w->ht.p, w->ctrl.p);
+  k_grad_t<double, double, 1><<<c->num_sms * 8, 256, 0, s>>>(h->node, h->nptr.p, h->nlist.p, c->bc.p,
+                                                              (const double2*)w->r.p, w->ht.p, w->ctrl.p);
   count_launch();
   for (int bwd = 0; bwd < 2; ++bwd)
     launch_coop(k_nsweep_mc<double, 1, false>, w->nmc_blocks, s, (const int32_t*)(bwd ? h->uptr.p : h->lptr.p),
@@ -1998,9 +2113,9 @@ void precond_apply_device(afem_ctx* c, double omega, const double2* r, double2* 
                 (const double2*)w->ht.p, w->hy.p, (const double2*)w->hdd.p, (const int32_t*)h->perm.p,
                 (const int32_t*)h->cptr.p, h->ncolors, (const SysScal*)w->sc.p, (const Ctrl*)w->ctrl.p,
                 (const uint8_t*)nullptr, bwd, (double*)nullptr);
-  k_grad_add<double, 1, false><<<w->nblocks, 256, 0, s>>>(n, c->line.p, c->bc.p, (const double2*)w->hy.p, w->z.p,
-                                                          (const double2*)w->r.p, w->ctrl.p, w->part.p,
-                                                          (const uint8_t*)nullptr);
+  k_grad_add<double, double, 1, false><<<w->nblocks, 256, 0, s>>>(n, c->line.p, c->bc.p, (const double2*)w->hy.p,
+                                                                  w->z.p, (const double2*)w->r.p, w->ctrl.p,
+                                                                  w->part.p, (const uint8_t*)nullptr);
   count_launch();
   AFEM_CUDA(cudaMemcpyAsync(z, w->z.p, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
   AFEM_CUDA(cudaStreamSynchronize(s));
@@ -2028,17 +2143,21 @@ void get_residual(afem_ctx* c, int k, double* r) {
 // depends on the pattern only), so repeated solves take the same reduction
 // order and give the same bits.
 void invalidate_work(afem_ctx* c) {
-  if (c->work) c->work->kmf_valid = false;
+  if (c->work) c->work->kmf_valid = c->work->mcf_valid = false;
 }
 
 // A new pattern: also tune the SpMV again (ensure_work re-allocates when the
 // size changes; buffers of the same size are kept).
 void invalidate_pattern_work(afem_ctx* c) {
   if (c->work) {
-    c->work->kmf_valid = false;
+    c->work->kmf_valid = c->work->mcf_valid = false;
     c->work->rpw64 = c->work->rpw32 = 0;
   }
   c->nsys = 0;  // the old solutions belong to the old pattern
+}
+
+void reset_spmv_tuning(afem_ctx* c) {
+  if (c->work) c->work->rpw64 = c->work->rpw32 = 0;
 }
 
 void destroy_work(afem_ctx* c) {

@@ -346,6 +346,14 @@ class Forward:
         return item, ve, vf, iele
 
     # ------------------------------------------------------------ measurement
+    def set_wait_limit(self, polls: int):
+        """Bound of the sync-free sweeps' waits in polls (0: the built-in bound)."""
+        self._check(self._L.afem_set_wait_limit(self.ctx, int(polls)))
+
+    def set_spmv_rows_per_warp(self, rpw: int):
+        """Pin the SpMV's rows per warp (1, 2, 4) for the same bits in every process; 0: tuned."""
+        self._check(self._L.afem_set_spmv_rows_per_warp(self.ctx, int(rpw)))
+
     def set_profiling(self, enable: bool):
         self._check(self._L.afem_set_profiling(self.ctx, int(enable)))
 

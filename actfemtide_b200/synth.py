@@ -331,7 +331,7 @@ def _write_msh(path, xyz, elems, etype):
 
 
 def write_reference_inputs(m: TidalModel, outdir: str, line=None, n6line=None, site_names=None,
-                           plan_view=None) -> str:
+                           plan_view=None, utm_sites=None) -> str:
     """Write model m as the files the reference's tide forward reads; returns the ctl path.
 
     em3d.msh (tetrahedra, tags = elementary volume), polygonz.msh (top-of-earth
@@ -340,6 +340,8 @@ def write_reference_inputs(m: TidalModel, outdir: str, line=None, n6line=None, s
     vxyz_mesh (readfxyz / readvxyz records), cond_test.msh (READCOND: 11 header
     lines, nphys2, index and resistivity), tide_fwd.ctl (readparam's record
     order, labels in the first 20 columns, xyz sites given 1 m below the surface).
+    utm_sites = (zone, lonorigin, latorigin, lonlat): sites given as longitude /
+    latitude (lonlat: nobs x 2 degrees) in UTM zone `zone` (lonlatflag 1).
     """
     import os
     os.makedirs(outdir, exist_ok=True)
@@ -401,10 +403,17 @@ def write_reference_inputs(m: TidalModel, outdir: str, line=None, n6line=None, s
              lab("zmin   [km]") + repr(float(m.bounds["zmin"]))]
     rows += [lab(k) + "0.1" for k in ("sizein [km]", "sizebo [km]", "sigma_obs [km]", "A_obs     [km]",
                                        "dlen_source [km]", "sigma_src [km]", "A_src     [km]")]
-    rows += [lab("# of observatory") + str(m.sites.shape[0]), lab("lonlat(1),xyz (2)") + "2",
-             lab("UTM ZONE") + "none", lab("lonlatorigin") + "0.0 0.0"]
-    for nm, s in zip(names, m.sites):
-        rows += [lab("Name") + nm, lab("xyz") + f"{float(s[0])!r} {float(s[1])!r} {-SITE_DEPTH_KM!r}"]
+    if utm_sites is None:
+        rows += [lab("# of observatory") + str(m.sites.shape[0]), lab("lonlat(1),xyz (2)") + "2",
+                 lab("UTM ZONE") + "none", lab("lonlatorigin") + "0.0 0.0"]
+        for nm, s in zip(names, m.sites):
+            rows += [lab("Name") + nm, lab("xyz") + f"{float(s[0])!r} {float(s[1])!r} {-SITE_DEPTH_KM!r}"]
+    else:
+        zone, lon0, lat0, lonlat = utm_sites
+        rows += [lab("# of observatory") + str(m.sites.shape[0]), lab("lonlat(1),xyz (2)") + "1",
+                 lab("UTM ZONE") + f"{int(zone)}S", lab("lonlatorigin") + f"{float(lon0)!r} {float(lat0)!r}"]
+        for nm, ll in zip(names, lonlat):
+            rows += [lab("Name") + nm, lab("lonlatalt") + f"{float(ll[0])!r} {float(ll[1])!r} {-SITE_DEPTH_KM!r}"]
     if plan_view is None:
         rows += [lab("0:no,1:nxny,2:ntrik") + "0"]
     else:  # (xyfilehead, nx, ny, depth_xy): a constant-depth plan view (ixyflag 1, ixydepth 1)

@@ -61,7 +61,10 @@ typedef enum afem_precond {
 
 typedef enum afem_precision {
   AFEM_FP64 = 0,          /* every kernel in complex FP64 */
-  AFEM_MIXED = 1          /* inner COCG in complex FP32, FP64 iterative refinement outside */
+  AFEM_MIXED = 1,         /* inner COCG in complex FP32, FP64 iterative refinement outside */
+  AFEM_FP32_PRECOND = 2   /* COCG in complex FP64 (SpMV, residuals, x, p, alpha/beta, the true-residual
+                             check) with the multicolour preconditioner (SSOR_MC, HYBRID: its sweeps,
+                             matrix copies, nodal correction and vectors) in complex FP32 */
 } afem_precision;
 
 typedef struct afem_solve_opts {
@@ -178,6 +181,19 @@ int afem_cocg13_single(afem_ctx *ctx, int NP, int NPL, int NPU, double *D, doubl
                        const int32_t *IAL, double *AU, const int32_t *INU, const int32_t *IAU, double *B, double *X,
                        const char *PRECOND, double SIGMA_DIAG, double SIGMA, double *RESID, int *ITER, int *ERROR,
                        int NSET);
+/* Bound of the waits in the sync-free triangular sweeps (IC, SSOR, DIAG set-up
+ * and sweeps in natural row order; COCG13_single's sweeps are serial, so the
+ * reference has no counterpart): after `polls` back-off polls (32 ns doubling to
+ * 1 us) on a row the sweep depends on, the kernel records a timeout, every
+ * waiting row gives up, and the solve returns AFEM_ETIMEOUT with the context
+ * still usable.  0 restores the built-in bound (2^21 polls, about 2 s). */
+int afem_set_wait_limit(afem_ctx *ctx, unsigned polls);
+/* Pin the SpMV's rows per warp (1, 2 or 4; 0: the autotuner picks per pattern
+ * by timing).  The choice sets how a row's products are split over lanes and so
+ * the order of the floating-point additions: with the tuner, two processes may
+ * pick different variants and their results differ in the last bits; a pinned
+ * value gives the same bits in every process.  No counterpart in the reference. */
+int afem_set_spmv_rows_per_warp(afem_ctx *ctx, int rows_per_warp);
 /* Load a system in the same split layout for afem_solve (freq_hz = 1/(2*pi) gives A itself). */
 int afem_set_system(afem_ctx *ctx, int n, const int32_t *INU, const int32_t *IAU, const int32_t *INL,
                     const int32_t *IAL, const double *D, const double *AU, const double *AL, const double *b);
@@ -299,6 +315,11 @@ int afem_ctl_info(afem_ctx *ctx, int *nfreq, double *freq, int *nobs, double *xy
 /* Run every frequency of the loaded ctl and write <outputfolder><site>_<src>.dat
  * exactly as OUTOBSFILESFWD (m_outresp.f90:221-262). */
 int afem_run_ctl(afem_ctx *ctx, const afem_solve_opts *opts);
+/* Host only: a site's position in km east and north of the origin (lonorigin,
+ * latorigin), both projected to UTM zone `zone` (1..60): UTMXY + UTMGMT +
+ * utm_geo_tm (src/common/m_param.f90:609-661, 741-936), which readparam applies
+ * to lonlatflag-1 sites (m_param.f90:316-323).  xy_km[2]. */
+int afem_utm_xy(double lon, double lat, double lonorigin, double latorigin, int zone, double *xy_km);
 /* Fortran Gw.d formatting of x as OUTOBSFILESFWD writes it ('(11g15.7)'); host only. */
 int afem_fortran_g(double x, int w, int d, char *out, int cap);
 

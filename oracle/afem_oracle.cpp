@@ -468,76 +468,76 @@ int orc_assemble_split(long ntet, const double* xyz, const int* n4, const int* n
   return 0;
 }
 
-// COCG13_single (src/solver/COCG13_single.f90:9-340): preconditioned COCG on
-// split D/L/U storage, unconjugated r^T z and p^T q, conjugated norms, stop on
-// the recursive residual ||r||/||b|| <= RESID.  PRECOND "IC" (diagonal-modified
-// IC(0)), "SSOR", "DIAG".  NSET 0 -> ERROR 101 on first use, 1 -> precondition,
-// 2 -> symmetric diagonal scaling as well.  ITER in: max iterations; out: count
-// (MAXIT+1 after a full loop, as the Fortran DO variable).  ERROR -100 at the cap.
-// The reference SAVEs DD/SCALE across calls; here they are fresh each call.
-void orc_cocg13_single(int NP, int NPL, int NPU, double* D_, double* AL_, const int* INL, const int* IAL,
-                       double* AU_, const int* INU, const int* IAU, double* B_, double* X_, const char* PRECOND,
-                       double SIGMA_DIAG, double SIGMA, double* RESID, int* ITER, int* ERROR, int NSET,
-                       double* history) {
-  (void)NPL; (void)NPU;
-  cplx* D = reinterpret_cast<cplx*>(D_);
-  cplx* AL = reinterpret_cast<cplx*>(AL_);
-  cplx* AU = reinterpret_cast<cplx*>(AU_);
-  cplx* B = reinterpret_cast<cplx*>(B_);
-  cplx* X = reinterpret_cast<cplx*>(X_);
-  *ERROR = 0;
-  if (NSET == 0) { *ERROR = 101; return; }
-  std::vector<cplx> R(NP), Z(NP), P(NP);
-  std::vector<cplx>& Q = Z;  // Q shares the Z column (COCG13_single.f90:64-67)
-  std::vector<cplx> DD(NP, 0.0);
-  std::vector<double> SCALE(NP, 1.0);
-  const int MAXIT = *ITER;
-  const double TOL = *RESID;
-  const bool ic = (std::strncmp(PRECOND, "IC", 2) == 0) || (std::strncmp(PRECOND, "ILU", 3) == 0);
-  const bool ssor = std::strncmp(PRECOND, "SSOR", 4) == 0;
-  const bool diag = std::strncmp(PRECOND, "DIAG", 4) == 0;
-  if (NSET >= 1) {
-    if (NSET == 2) {
-      for (int i = 0; i < NP; ++i) SCALE[i] = 1.0 / std::sqrt(std::abs(D[i]));
-      for (int j = 0; j < NP; ++j) {
-        D[j] = std::abs(D[j]) / D[j];
-        for (int i = INU[j]; i < INU[j + 1]; ++i) AU[i] = AU[i] * SCALE[IAU[i] - 1] * SCALE[j];
-        for (int i = INL[j]; i < INL[j + 1]; ++i) AL[i] = AL[i] * SCALE[IAL[i] - 1] * SCALE[j];
-      }
-    }
-    for (int i = 0; i < NP; ++i) B[i] = B[i] * SCALE[i];
-    for (int i = 0; i < NP; ++i) DD[i] = 0.0;
-    if (ic) {
-      for (int i = 0; i < NP; ++i) {
-        cplx W = D[i] * SIGMA_DIAG;
-        for (int k = INL[i]; k < INL[i + 1]; ++k) {
-          cplx SS = AL[k];
-          int id = IAL[k];
-          for (int kk = INU[id - 1]; kk < INU[id]; ++kk) SS = SS + AU[kk] * SIGMA;
-          W = W - AL[k] * SS * DD[id - 1];
-        }
-        DD[i] = cplx(1.0, 0.0) / W;
-      }
-    }
-    if (ssor || diag)
-      for (int i = 0; i < NP; ++i) DD[i] = cplx(1.0, 0.0) / (SIGMA_DIAG * D[i]);
-  }
-  for (int j = 0; j < NP; ++j) {
-    cplx W = B[j] - D[j] * X[j];
-    for (int i = INU[j]; i < INU[j + 1]; ++i) W = W - AU[i] * X[IAU[i] - 1];
-    for (int i = INL[j]; i < INL[j + 1]; ++i) W = W - AL[i] * X[IAL[i] - 1];
-    R[j] = W;
-  }
+}  // extern "C"
+
+namespace {
+
+// COCG13_single (src/solver/COCG13_single.f90:9-340) as a resumable run: the
+// set-up (NSET scaling, DD, initial residual, ||b||^2), one iteration at a time,
+// and the final unscaling.  orc_cocg13_single drives it exactly as the
+// reference's DO loop; orc_cocg_begin/advance/end let a caller time the same
+// iterations in slices (the Krylov state carries over between slices).
+struct CocgRun {
+  int NP = 0;
+  cplx *D = nullptr, *AL = nullptr, *AU = nullptr, *B = nullptr, *X = nullptr;
+  const int *INL = nullptr, *IAL = nullptr, *INU = nullptr, *IAU = nullptr;
+  bool ic = false, ssor = false, diag = false;
+  std::vector<cplx> R, Z, P, DD;
+  std::vector<double> SCALE;
   double BNRM2 = 0.0;
-  for (int i = 0; i < NP; ++i) BNRM2 = BNRM2 + (B[i] * std::conj(B[i])).real();
-  if (BNRM2 == 0.0) {
-    for (int i = 0; i < NP; ++i) X[i] = 0.0;
-    *RESID = 0.0; *ITER = 0;
-    return;
+  cplx RHO1 = 0.0;
+  int iter = 0;  // iterations done
+
+  // COCG13_single.f90:80-180: NSET 2 scaling (in place), DD, R = B - A X, ||B||^2
+  void setup(const char* PRECOND, double SIGMA_DIAG, double SIGMA, int NSET) {
+    R.assign(NP, 0.0);
+    Z.assign(NP, 0.0);
+    P.assign(NP, 0.0);
+    DD.assign(NP, 0.0);
+    SCALE.assign(NP, 1.0);
+    ic = (std::strncmp(PRECOND, "IC", 2) == 0) || (std::strncmp(PRECOND, "ILU", 3) == 0);
+    ssor = std::strncmp(PRECOND, "SSOR", 4) == 0;
+    diag = std::strncmp(PRECOND, "DIAG", 4) == 0;
+    if (NSET >= 1) {
+      if (NSET == 2) {
+        for (int i = 0; i < NP; ++i) SCALE[i] = 1.0 / std::sqrt(std::abs(D[i]));
+        for (int j = 0; j < NP; ++j) {
+          D[j] = std::abs(D[j]) / D[j];
+          for (int i = INU[j]; i < INU[j + 1]; ++i) AU[i] = AU[i] * SCALE[IAU[i] - 1] * SCALE[j];
+          for (int i = INL[j]; i < INL[j + 1]; ++i) AL[i] = AL[i] * SCALE[IAL[i] - 1] * SCALE[j];
+        }
+      }
+      for (int i = 0; i < NP; ++i) B[i] = B[i] * SCALE[i];
+      for (int i = 0; i < NP; ++i) DD[i] = 0.0;
+      if (ic) {
+        for (int i = 0; i < NP; ++i) {
+          cplx W = D[i] * SIGMA_DIAG;
+          for (int k = INL[i]; k < INL[i + 1]; ++k) {
+            cplx SS = AL[k];
+            int id = IAL[k];
+            for (int kk = INU[id - 1]; kk < INU[id]; ++kk) SS = SS + AU[kk] * SIGMA;
+            W = W - AL[k] * SS * DD[id - 1];
+          }
+          DD[i] = cplx(1.0, 0.0) / W;
+        }
+      }
+      if (ssor || diag)
+        for (int i = 0; i < NP; ++i) DD[i] = cplx(1.0, 0.0) / (SIGMA_DIAG * D[i]);
+    }
+    for (int j = 0; j < NP; ++j) {
+      cplx W = B[j] - D[j] * X[j];
+      for (int i = INU[j]; i < INU[j + 1]; ++i) W = W - AU[i] * X[IAU[i] - 1];
+      for (int i = INL[j]; i < INL[j + 1]; ++i) W = W - AL[i] * X[IAL[i] - 1];
+      R[j] = W;
+    }
+    BNRM2 = 0.0;
+    for (int i = 0; i < NP; ++i) BNRM2 = BNRM2 + (B[i] * std::conj(B[i])).real();
   }
-  cplx RHO, RHO1 = 0.0, ALPHA;
-  int iter;
-  for (iter = 1; iter <= MAXIT; ++iter) {
+
+  // One pass of the DO loop body (COCG13_single.f90:195-330); returns RESID.
+  double step() {
+    ++iter;
+    std::vector<cplx>& Q = Z;  // Q shares the Z column (COCG13_single.f90:64-67)
     for (int i = 0; i < NP; ++i) Z[i] = R[i];
     if (ic || ssor) {
       for (int i = 0; i < NP; ++i) {
@@ -555,7 +555,7 @@ void orc_cocg13_single(int NP, int NPL, int NPU, double* D_, double* AL_, const 
       for (int i = 0; i < NP; ++i) Z[i] = R[i] * DD[i];
     cplx RHO0(0.0, 0.0);
     for (int i = 0; i < NP; ++i) RHO0 = RHO0 + R[i] * Z[i];
-    RHO = RHO0;
+    const cplx RHO = RHO0;
     if (iter == 1) {
       for (int i = 0; i < NP; ++i) P[i] = Z[i];
     } else {
@@ -570,24 +570,167 @@ void orc_cocg13_single(int NP, int NPL, int NPU, double* D_, double* AL_, const 
     }
     cplx C10(0.0, 0.0);
     for (int i = 0; i < NP; ++i) C10 = C10 + P[i] * Q[i];
-    ALPHA = RHO / C10;
+    const cplx ALPHA = RHO / C10;
     for (int i = 0; i < NP; ++i) {
       X[i] = X[i] + ALPHA * P[i];
       R[i] = R[i] - ALPHA * Q[i];
     }
     double DNRM2 = 0.0;
     for (int i = 0; i < NP; ++i) DNRM2 = DNRM2 + (R[i] * std::conj(R[i])).real();
-    *RESID = std::sqrt(DNRM2 / BNRM2);
+    RHO1 = RHO;
+    return std::sqrt(DNRM2 / BNRM2);
+  }
+
+  // COCG13_single.f90:332-338: X and B back to the unscaled system
+  void finish() {
+    for (int i = 0; i < NP; ++i) {
+      X[i] = X[i] * SCALE[i];
+      B[i] = B[i] / SCALE[i];
+    }
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+// COCG13_single (src/solver/COCG13_single.f90:9-340): preconditioned COCG on
+// split D/L/U storage, unconjugated r^T z and p^T q, conjugated norms, stop on
+// the recursive residual ||r||/||b|| <= RESID.  PRECOND "IC" (diagonal-modified
+// IC(0)), "SSOR", "DIAG".  NSET 0 -> ERROR 101 on first use, 1 -> precondition,
+// 2 -> symmetric diagonal scaling as well.  ITER in: max iterations; out: count
+// (MAXIT+1 after a full loop, as the Fortran DO variable).  ERROR -100 at the cap.
+// The reference SAVEs DD/SCALE across calls; here they are fresh each call.
+void orc_cocg13_single(int NP, int NPL, int NPU, double* D_, double* AL_, const int* INL, const int* IAL,
+                       double* AU_, const int* INU, const int* IAU, double* B_, double* X_, const char* PRECOND,
+                       double SIGMA_DIAG, double SIGMA, double* RESID, int* ITER, int* ERROR, int NSET,
+                       double* history) {
+  (void)NPL; (void)NPU;
+  *ERROR = 0;
+  if (NSET == 0) { *ERROR = 101; return; }
+  CocgRun run;
+  run.NP = NP;
+  run.D = reinterpret_cast<cplx*>(D_);
+  run.AL = reinterpret_cast<cplx*>(AL_);
+  run.AU = reinterpret_cast<cplx*>(AU_);
+  run.B = reinterpret_cast<cplx*>(B_);
+  run.X = reinterpret_cast<cplx*>(X_);
+  run.INL = INL; run.IAL = IAL; run.INU = INU; run.IAU = IAU;
+  const int MAXIT = *ITER;
+  const double TOL = *RESID;
+  run.setup(PRECOND, SIGMA_DIAG, SIGMA, NSET);
+  if (run.BNRM2 == 0.0) {
+    for (int i = 0; i < NP; ++i) run.X[i] = 0.0;
+    *RESID = 0.0; *ITER = 0;
+    return;
+  }
+  int iter;
+  for (iter = 1; iter <= MAXIT; ++iter) {
+    *RESID = run.step();
     if (history) history[iter - 1] = *RESID;
     if (*RESID <= TOL) break;
     if (iter == MAXIT) *ERROR = -100;
-    RHO1 = RHO;
   }
   *ITER = iter;
-  for (int i = 0; i < NP; ++i) {
-    X[i] = X[i] * SCALE[i];
-    B[i] = B[i] / SCALE[i];
+  run.finish();
+}
+
+// The same solver in slices (measurement of the reference's solver on a bounded
+// sample): begin does COCG13_single's set-up on the caller's arrays (kept
+// borrowed until end; NSET 2 scales them in place), advance runs k more
+// iterations of the same loop and returns the recursive residual, end unscales
+// X (and B) and frees the state.  Returns nullptr when ||b|| = 0 or NSET = 0.
+void* orc_cocg_begin(int NP, double* D_, double* AL_, const int* INL, const int* IAL, double* AU_, const int* INU,
+                     const int* IAU, double* B_, double* X_, const char* PRECOND, double SIGMA_DIAG, int NSET) {
+  if (NSET == 0) return nullptr;
+  CocgRun* run = new CocgRun();
+  run->NP = NP;
+  run->D = reinterpret_cast<cplx*>(D_);
+  run->AL = reinterpret_cast<cplx*>(AL_);
+  run->AU = reinterpret_cast<cplx*>(AU_);
+  run->B = reinterpret_cast<cplx*>(B_);
+  run->X = reinterpret_cast<cplx*>(X_);
+  run->INL = INL; run->IAL = IAL; run->INU = INU; run->IAU = IAU;
+  run->setup(PRECOND, SIGMA_DIAG, 0.0, NSET);
+  if (run->BNRM2 == 0.0) {
+    delete run;
+    return nullptr;
   }
+  return run;
+}
+
+double orc_cocg_advance(void* h, int k) {
+  CocgRun* run = static_cast<CocgRun*>(h);
+  double resid = -1.0;
+  for (int i = 0; i < k; ++i) resid = run->step();
+  return resid;
+}
+
+int orc_cocg_iterations(void* h) { return static_cast<CocgRun*>(h)->iter; }
+
+void orc_cocg_end(void* h) {
+  CocgRun* run = static_cast<CocgRun*>(h);
+  run->finish();
+  delete run;
+}
+
+// utm_geo_tm, LONLAT2UTM branch (src/common/m_param.f90:741-936): Snyder's
+// ellipsoidal transverse Mercator on Clarke 1866, k0 0.9996, false easting
+// 500 km.  reference_series = 1 keeps the reference's sin(4 phi) coefficient
+// (15 e4/256 * 45 e6/1024, a product), 0 uses Snyder's sum (for checking the
+// restatement against Snyder's published worked example).
+void orc_utm_lonlat2xy(double rlon_deg, double rlat_deg, int zone, int reference_series, double* rx, double* ry) {
+  const double PI = 3.141592653589793;
+  const double degrad = PI / 180.0;
+  const double semimaj = 6378206.4, semimin = 6356583.8, scfa = 0.9996, north = 0.0, east = 500000.0;
+  const double e2 = 1.0 - std::pow(semimin / semimaj, 2.0);
+  const double e4 = e2 * e2, e6 = e2 * e4, ep2 = e2 / (1.0 - e2);
+  const double dlon = rlon_deg, dlat = rlat_deg;
+  const double cm = (double)zone * 6.0 - 183.0;
+  const double rlat = degrad * dlat;
+  double delam = dlon - cm;
+  if (delam < -180.0) delam = delam + 360.0;
+  if (delam > 180.0) delam = delam - 360.0;
+  delam = delam * degrad;
+  double f1 = (1.0 - e2 / 4.0 - 3.0 * e4 / 64.0 - 5.0 * e6 / 256) * rlat;
+  double f2 = 3.0 * e2 / 8.0 + 3.0 * e4 / 32.0 + 45.0 * e6 / 1024.0;
+  f2 = f2 * std::sin(2.0 * rlat);
+  double f3 = reference_series ? 15.0 * e4 / 256.0 * 45.0 * e6 / 1024.0 : 15.0 * e4 / 256.0 + 45.0 * e6 / 1024.0;
+  f3 = f3 * std::sin(4.0 * rlat);
+  double f4 = 35.0 * e6 / 3072.0;
+  f4 = f4 * std::sin(6.0 * rlat);
+  const double rm = semimaj * (f1 - f2 + f3 - f4);
+  double xx, yy;
+  if (dlat == 90.0 || dlat == -90.0) {
+    xx = 0.0;
+    yy = scfa * rm;
+  } else {
+    const double rn = semimaj / std::sqrt(1.0 - e2 * std::pow(std::sin(rlat), 2));
+    const double t = std::pow(std::tan(rlat), 2);
+    const double c = ep2 * std::pow(std::cos(rlat), 2);
+    const double a = std::cos(rlat) * delam;
+    f1 = (1.0 - t + c) * std::pow(a, 3) / 6.0;
+    f2 = 5.0 - 18.0 * t + std::pow(t, 2) + 72.0 * c - 58.0 * ep2;
+    f2 = f2 * std::pow(a, 5) / 120.0;
+    xx = scfa * rn * (a + f1 + f2);
+    f1 = std::pow(a, 2) / 2.0;
+    f2 = 5.0 - t + 9.0 * c + 4.0 * std::pow(c, 2);
+    f2 = f2 * std::pow(a, 4) / 24.0;
+    f3 = 61.0 - 58.0 * t + std::pow(t, 2) + 600.0 * c - 330.0 * ep2;
+    f3 = f3 * std::pow(a, 6) / 720.0;
+    yy = scfa * (rm + rn * std::tan(rlat) * (f1 + f2 + f3));
+  }
+  *rx = xx + east;
+  *ry = yy + north;
+}
+
+// UTMXY (src/common/m_param.f90:609-627): (x - xorigin)/1e3, (y - yorigin)/1e3 [km]
+void orc_utmxy(double lon, double lat, double lonorigin, double latorigin, int zone, double* xy) {
+  double x, y, xo, yo;
+  orc_utm_lonlat2xy(lon, lat, zone, 1, &x, &y);
+  orc_utm_lonlat2xy(lonorigin, latorigin, zone, 1, &xo, &yo);
+  xy[0] = (x - xo) / 1.0e3;
+  xy[1] = (y - yo) / 1.0e3;
 }
 
 // ||b - A x|| / ||b|| on split storage (the build's acceptance criterion).

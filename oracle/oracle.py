@@ -60,6 +60,20 @@ def lib():
         L.orc_cocg13_single.argtypes = [C.c_int, C.c_int, C.c_int, _c128p, _c128p, _i32p, _i32p, _c128p, _i32p, _i32p,
                                         _c128p, _c128p, C.c_char_p, C.c_double, C.c_double, C.POINTER(C.c_double),
                                         C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.c_void_p]
+        L.orc_cocg_begin.restype = C.c_void_p
+        L.orc_cocg_begin.argtypes = [C.c_int, _c128p, _c128p, _i32p, _i32p, _c128p, _i32p, _i32p, _c128p, _c128p,
+                                     C.c_char_p, C.c_double, C.c_int]
+        L.orc_cocg_advance.restype = C.c_double
+        L.orc_cocg_advance.argtypes = [C.c_void_p, C.c_int]
+        L.orc_cocg_iterations.restype = C.c_int
+        L.orc_cocg_iterations.argtypes = [C.c_void_p]
+        L.orc_cocg_end.restype = None
+        L.orc_cocg_end.argtypes = [C.c_void_p]
+        L.orc_utm_lonlat2xy.restype = None
+        L.orc_utm_lonlat2xy.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_double)]
+        L.orc_utmxy.restype = None
+        L.orc_utmxy.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _f64p]
         L.orc_true_residual.restype = C.c_double
         L.orc_true_residual.argtypes = [C.c_int, _c128p, _c128p, _i32p, _i32p, _c128p, _i32p, _i32p, _c128p, _c128p]
         L.orc_findelement0.restype = C.c_long
@@ -200,10 +214,55 @@ def cocg13_single(A: Assembled, b=None, x0=None, precond="IC", resid=1e-8, maxit
     return out
 
 
+class CocgSlices:
+    """COCG13_single run in slices: the same iterations as cocg13_single, with the
+    Krylov state kept between advance() calls (the reference's solver timed on a
+    bounded sample).  A is read, not modified (NSET 1); b defaults to A.b."""
+
+    def __init__(self, A: Assembled, b=None, precond="SSOR", sigma_diag=1.0):
+        self.A = A
+        self.b = (A.b if b is None else np.asarray(b, np.complex128)).copy()
+        self.x = np.zeros(A.n, np.complex128)
+        self.h = lib().orc_cocg_begin(A.n, A.D, A.AL, A.INL, A.IAL, A.AU, A.INU, A.IAU, self.b, self.x,
+                                      precond.encode(), sigma_diag, 1)
+        if not self.h:
+            raise ValueError("CocgSlices: ||b|| = 0")
+        self.resid = 1.0
+
+    def advance(self, k: int) -> float:
+        """k more iterations (ctypes releases the GIL, so threads run in parallel)."""
+        self.resid = lib().orc_cocg_advance(self.h, int(k))
+        return self.resid
+
+    @property
+    def iterations(self) -> int:
+        return lib().orc_cocg_iterations(self.h)
+
+    def close(self):
+        if self.h:
+            lib().orc_cocg_end(self.h)
+            self.h = None
+        return self.x
+
+
 def true_residual(A: Assembled, x, b=None):
     B = A.b if b is None else _c(b, np.complex128)
     return lib().orc_true_residual(A.n, A.D, A.AL, A.INL, A.IAL, A.AU, A.INU, A.IAU, _c(B, np.complex128),
                                    _c(x, np.complex128))
+
+
+def utm_lonlat2xy(lon, lat, zone, reference_series=True):
+    """utm_geo_tm LONLAT2UTM: easting, northing [m]; reference_series=False uses Snyder's series."""
+    x = C.c_double(); y = C.c_double()
+    lib().orc_utm_lonlat2xy(float(lon), float(lat), int(zone), int(bool(reference_series)), C.byref(x), C.byref(y))
+    return x.value, y.value
+
+
+def utmxy(lon, lat, lonorigin, latorigin, zone):
+    """UTMXY: km east/north of the origin."""
+    out = np.zeros(2)
+    lib().orc_utmxy(float(lon), float(lat), float(lonorigin), float(latorigin), int(zone), out)
+    return out
 
 
 def findelement0(m, x3):

@@ -55,3 +55,47 @@ def test_adjoint_jacobian_matches_finite_differences(gpulib):
             scale = np.abs(J).max()
             assert np.abs(J[:, t] - g).max() <= 1e-5 * scale + 1e-4 * np.abs(g).max(), (t, J[:, t], g)
         fw.set_cond(m.sigma_air, m.sigma_ocean, 1, sigma_file=m.sigma_land)
+
+
+def test_adjoint_128_rhs_on_training_mesh(gpulib):
+    """The Jacobian workload at its stated size: 64 sites x 2 horizontal E components = 128 adjoint
+    right-hand sides on the 32x32x24 mesh (179,800 edges), solved in 8 batches of 16, and the
+    resulting dE/dlog(sigma) checked against central differences (step 1e-4) on 20 cells."""
+    from actfemtide_b200.forward import Forward
+    grid = np.linspace(-35.0, 35.0, 8)
+    m = synth.tidal_box(32, 32, 24, seed=5, grf=True, block=False, site_grid=grid, name="box32x32x24")
+    f = m.freqs[0]
+    sites = m.sites
+    assert sites.shape[0] == 64
+    with Forward(0) as fw:
+        fw.load_model(m)
+        fw.assemble()
+        assert fw.solve(f, precond="HYBRID", tol=1e-12).ok
+        x = fw.solution(0)
+        base = fw.sites(sites)[0]
+        C = fw.adjoint_sources(f, sites)           # (n, 128)
+        assert C.shape[1] == 128
+        np.testing.assert_allclose(C.T @ x, base[3:5].T.ravel(), rtol=1e-10, atol=1e-14)
+        J = np.zeros((128, m.ntet), np.complex128)
+        for b0 in range(0, 128, 16):
+            r = fw.solve_rhs(np.full(16, f), C[:, b0:b0 + 16], precond="HYBRID", tol=1e-12)
+            assert r.ok, (b0, r)
+            J[b0:b0 + 16] = fw.jacobian(f, x, 16)
+        rng = np.random.default_rng(1)
+        land = np.arange(m.nphys1, m.ntet)
+        sens = np.abs(J[:, land]).max(axis=0)
+        cells = np.concatenate([land[np.argsort(sens)[-10:]], rng.choice(land, 10, replace=False)])
+        h = 1e-4
+        scale = np.abs(J).max()
+        for t in cells:
+            fd = []
+            for sgn in (1, -1):
+                sl = m.sigma_land.copy()
+                sl[t - m.nphys1] *= np.exp(sgn * h)
+                fw.set_cond(m.sigma_air, m.sigma_ocean, 1, sigma_file=sl)
+                fw.assemble()
+                assert fw.solve(f, precond="HYBRID", tol=1e-12).ok
+                fd.append(fw.sites(sites)[0][3:5].T.ravel())
+            g = (fd[0] - fd[1]) / (2 * h)
+            assert np.abs(J[:, t] - g).max() <= 1e-5 * scale + 1e-4 * np.abs(g).max(), t
+        fw.set_cond(m.sigma_air, m.sigma_ocean, 1, sigma_file=m.sigma_land)

@@ -84,3 +84,47 @@ def test_ctl_plan_view_matches_oracle(gpulib, oracle, short_dir):
     big = amp[0].T > 1e-3 * amp[0].max()
     dphi = (vals[:, :, 1][big] - ph[0].T[big] + 180.0) % 360.0 - 180.0
     assert np.all(np.abs(dphi) <= 1e-3)
+
+
+def _lonlat_of(oracle, xy_km, zone, lon0, lat0):
+    """Longitude/latitude whose UTMXY position is xy_km (Newton on the oracle's UTMXY)."""
+    ll = np.array([lon0, lat0]) + np.array([xy_km[0] / 100.0, xy_km[1] / 111.0])
+    for _ in range(20):
+        f = oracle.utmxy(ll[0], ll[1], lon0, lat0, zone) - xy_km
+        h = 1e-6
+        J = np.stack([(oracle.utmxy(ll[0] + h, ll[1], lon0, lat0, zone) - oracle.utmxy(ll[0] - h, ll[1], lon0, lat0,
+                                                                                         zone)) / (2 * h),
+                      (oracle.utmxy(ll[0], ll[1] + h, lon0, lat0, zone) - oracle.utmxy(ll[0], ll[1] - h, lon0, lat0,
+                                                                                         zone)) / (2 * h)], axis=1)
+        ll = ll - np.linalg.solve(J, f)
+    return ll
+
+
+def test_ctl_utm_sites_match_xyz_sites(gpulib, oracle, short_dir):
+    """lonlatflag 1: the same sites given as longitude/latitude in UTM zone 54 (UTMXY) land where the
+    xyz sites are and give the same site files."""
+    import shutil
+    from actfemtide_b200.forward import Forward
+    m = synth.tidal_box(4, 4, 6, seed=3, site_grid=(-6.0, 0.0, 6.0), half_km=12.0)
+    m.freqs = np.array([1.0 / 44714.0])
+    of = oracle.OracleForward(m)
+    zone, lon0, lat0 = 54, 139.8, 28.3
+    lonlat = np.array([_lonlat_of(oracle, s[:2], zone, lon0, lat0) for s in m.sites])
+    d_xyz = os.path.join(short_dir, "a")
+    d_utm = os.path.join(short_dir, "b")
+    ctl_a = synth.write_reference_inputs(m, d_xyz, of.line, of.n6line)
+    ctl_b = synth.write_reference_inputs(m, d_utm, of.line, of.n6line, utm_sites=(zone, lon0, lat0, lonlat))
+    with Forward(0) as fw:
+        fw.load_ctl(ctl_b)
+        _, xyz_b = fw.ctl_info()
+        np.testing.assert_allclose(xyz_b[:, :2], m.sites[:, :2], atol=1e-9)
+        for s, ll in zip(xyz_b, lonlat):
+            np.testing.assert_allclose(s[:2], oracle.utmxy(ll[0], ll[1], lon0, lat0, zone), atol=1e-12)
+        fw.run_ctl(precond="SSOR", tol=1e-10)
+        fw.load_ctl(ctl_a)
+        fw.run_ctl(precond="SSOR", tol=1e-10)
+    for s in range(m.sites.shape[0]):
+        a = np.loadtxt(os.path.join(d_xyz, f"S{s + 1:03d}_S1.dat"))
+        b = np.loadtxt(os.path.join(d_utm, f"S{s + 1:03d}_S1.dat"))
+        np.testing.assert_allclose(b, a, rtol=1e-5, atol=1e-6 * np.abs(a).max())
+    shutil.rmtree(d_xyz, ignore_errors=True)

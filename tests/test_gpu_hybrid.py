@@ -85,7 +85,7 @@ def test_nodal_matrix_is_the_galerkin_product(fw, grf_model):
         assert np.all(np.abs(dev - ref) <= 1e-12 * bound)
 
 
-@pytest.mark.parametrize("precision", ["fp64"])
+@pytest.mark.parametrize("precision", ["fp64", "pc32"])
 def test_hybrid_cocg_matches_oracle(fw, grf_model, precision):
     m, of, ref = grf_model
     fw.load_model(m)
@@ -116,11 +116,45 @@ def test_hybrid_batched_matches_single(fw, grf_model):
         assert _rel(outb[k], fw.sites(m.sites)[0]) <= 1e-6
 
 
-def test_hybrid_box20_iterations(fw):
-    """On the 20x20x20 model SSOR-COCG needs ~2,550 iterations; the correction cuts that several-fold."""
+@pytest.fixture(scope="module")
+def box20_ref(oracle):
+    """The 20x20x20 model and the oracle's SSOR-COCG (the reference's own solver) at 1e-10."""
     m = synth.small_model()
+    of = oracle.OracleForward(m)
+    A = of.assemble(m.freqs[0])
+    r = oracle.cocg13_single(A, precond="SSOR", resid=1e-10, maxit=100000)
+    assert r["error"] == 0
+    ref, _, _ = of.sites(r["x"], m.freqs[0])
+    return m, A, ref[0]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "pc32"])
+def test_hybrid_box20_sites(fw, oracle, box20_ref, precision):
+    """SSOR-COCG needs ~2,550 iterations on the 20x20x20 model; the corrected COCG several-fold fewer,
+    and its site fields match the reference solver's to 1e-6 (FP64 preconditioner and FP32 one)."""
+    m, A, ref = box20_ref
     fw.load_model(m)
     fw.assemble()
-    r = fw.solve(m.freqs[0], precond="HYBRID", tol=1e-8, maxit=20000)
-    assert r.ok and r.resid_true <= 1e-8
+    r = fw.solve(m.freqs[0], precond="HYBRID", precision=precision, tol=1e-8, maxit=20000)
+    assert r.ok and r.resid_true <= 1e-8, r
     assert r.iterations < 1000, r.iterations
+    assert oracle.true_residual(A, fw.solution(0)) <= 1.01e-8
+    assert _rel(fw.sites(m.sites)[0], ref) <= 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp64", "pc32"])
+def test_hybrid_box20_batch_of_16_sites(fw, oracle, box20_ref, precision):
+    """The benchmark's batch shape (8 periods x 2 source patterns) on the 20x20x20 model, with system 0
+    at the M2 period of the reference solve: its site fields within 1e-6 of the reference solver's."""
+    m, A, ref = box20_ref
+    m2 = synth.tidal_box(20, 20, 20, seed=1000, name="box20")
+    fw.load_model(m, sources=[(m.F, m.v), (m2.F, m2.v)])
+    fw.assemble()
+    freqs = 1.0 / (3600.0 * np.array(synth.BATCH_PERIODS_H))
+    freqs[0] = m.freqs[0]
+    f = np.concatenate([freqs, freqs])
+    src = np.repeat([0, 1], 8).astype(np.int32)
+    r = fw.solve(f, srcs=src, precond="HYBRID", precision=precision, tol=1e-8, maxit=20000)
+    assert r.ok and r.resid_true <= 1e-8, r
+    assert oracle.true_residual(A, fw.solution(0)) <= 1.01e-8
+    assert _rel(fw.sites(m.sites, nsys=16)[0], ref) <= 1e-6

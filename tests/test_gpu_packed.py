@@ -120,3 +120,33 @@ def test_packed_errors(fw, parts):
     # clearing the declaration returns to a single system
     fw.set_segments(None)
     assert fw.segment_info()[0].shape == (1,)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "pc32"])
+def test_packed_24_uneven_meshes_full_size(fw, oracle, precision):
+    """The batched workload's second batch at its stated size: 24 meshes of n x n x round(3n/4) cells,
+    n uniform in 8..32, each with its own seeded log-normal subsurface, in one packed solve.  Every
+    mesh's solution is checked by the oracle's FP64 true residual of that mesh's own assembly, and its
+    site fields against a separate device solve of the mesh alone (1e-6)."""
+    parts = synth.uneven_models(24, seed=0)
+    ns_ = sorted(m.dims[0] for m in parts)
+    assert len(parts) == 24 and ns_[0] >= 8 and ns_[-1] <= 32
+    sites = parts[0].sites
+    sep = []
+    for m in parts:
+        fw.load_model(m)
+        fw.assemble()
+        r = fw.solve(m.freqs[0], precond="HYBRID", tol=1e-8, maxit=20000)
+        assert r.ok and r.resid_true <= 1e-8, (m.name, r)
+        sep.append(fw.sites(sites)[0])
+    pk = synth.pack(parts)
+    fw.load_packed(pk)
+    fw.assemble()
+    freqs = np.array([m.freqs[0] for m in parts])
+    res = fw.solve(freqs, np.zeros(24, int), precond="HYBRID", precision=precision, tol=1e-8, maxit=20000)
+    assert res.ok and res.resid_true <= 1e-8, res
+    out = fw.sites(sites, nsys=24)
+    for k, m in enumerate(parts):
+        A = oracle.OracleForward(m).assemble(m.freqs[0])
+        assert oracle.true_residual(A, fw.solution(k)) <= 1.01e-8, m.name
+        assert _rel(out[k], sep[k]) <= 1e-6, m.name

@@ -13,6 +13,7 @@ import pytest
 
 from actfemtide_b200 import synth
 from actfemtide_b200.capi import AfemError
+from parity_util import assert_system_close
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -35,27 +36,6 @@ def box20(oracle):
     r = oracle.cocg13_single(A, precond="SSOR", resid=1e-10, maxit=100000)
     ref, _, _ = of.sites(r["x"], m.freqs[0])
     return m, of, A, ref
-
-
-def assert_system_close(sys_gpu, A, rtol=1e-12):
-    n = A.n
-    # per-row scale: largest |entry| of the row
-    scale = np.abs(A.D).copy()
-    for i in range(n):
-        for k in range(A.INU[i], A.INU[i + 1]):
-            scale[i] = max(scale[i], abs(A.AU[k]))
-        for k in range(A.INL[i], A.INL[i + 1]):
-            scale[i] = max(scale[i], abs(A.AL[k]))
-    ru = np.repeat(np.arange(n), np.diff(A.INU))
-    rl = np.repeat(np.arange(n), np.diff(A.INL))
-    assert np.all(np.abs(sys_gpu["D"] - A.D) <= rtol * scale)
-    assert np.all(np.abs(sys_gpu["AU"] - A.AU) <= rtol * scale[ru])
-    assert np.all(np.abs(sys_gpu["AL"] - A.AL) <= rtol * scale[rl])
-    # real part (curl-curl) is computed in the reference's operation order: bit-exact
-    assert np.array_equal(sys_gpu["D"].real, A.D.real)
-    assert np.array_equal(sys_gpu["AU"].real, A.AU.real)
-    bscale = np.abs(A.b).max()
-    assert np.all(np.abs(sys_gpu["b"] - A.b) <= rtol * bscale)
 
 
 @pytest.mark.parametrize("maker", [synth.tiny_model, synth.small_model])
@@ -134,12 +114,13 @@ def test_ssor_cocg_box20_sites(fw, oracle, box20):
     assert np.abs(out - ref).max() <= 1e-6 * np.abs(ref).max()
 
 
-def test_multicolour_ssor_box20(fw, box20):
-    """SSOR in colour order (split-row sweeps) converges to the same site fields."""
+@pytest.mark.parametrize("precision", ["fp64", "pc32"])
+def test_multicolour_ssor_box20(fw, box20, precision):
+    """SSOR in colour order (split-row sweeps, FP64 or FP32 sweeps) converges to the same site fields."""
     m, of, A, ref = box20
     fw.load_model(m)
     fw.assemble()
-    res = fw.solve(m.freqs[0], precond="SSOR_MC", tol=1e-8, maxit=40000)
+    res = fw.solve(m.freqs[0], precond="SSOR_MC", precision=precision, tol=1e-8, maxit=40000)
     assert res.ok and res.resid_true <= 1e-8, res
     out = fw.sites(m.sites)
     assert np.abs(out - ref).max() <= 1e-6 * np.abs(ref).max()
