@@ -315,7 +315,8 @@ void jacobian_device(afem_ctx* c, double freq, const double* x_host, int nadj, d
 // afem_sites.cu
 void site_coeffs_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item, double* val_e, double* val_f,
                         int32_t* iele);
-void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out, bool grid = false);
+// grid: FINDELEWITHGRID search over a 300 x 300 x grid_nz grid list (PREPOBSCOEFF_XY: 50, _XYSBTM: 300)
+void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out, bool grid = false, int grid_nz = 50);
 void site_coeffs_grid_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item, double* val_e,
                              double* val_f, int32_t* iele);
 void sort_index_heap(int n, int32_t* na, double* ra);  // SORT_INDEX (sort_index.f90:13-56)

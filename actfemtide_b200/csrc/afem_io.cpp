@@ -8,6 +8,7 @@
 // (PREPZSRCOBS), :470-527 (SETNPHYS1INDEX2COND), :570-626 (CALOBSRESP);
 // src/common/m_outresp.f90:221-262 (OUTOBSFILESFWD).
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -34,10 +35,18 @@ struct CtlInfo {
   double sigma_air = 1e-8;
   std::vector<double> sigma_land;
   int nodes = 0;
-  // plan view (ixyflag = 1): OUTFREQFILES2 files <outputfolder><xyfilehead><freq>_S<k>.dat
+  // plan view (ixyflag = 1, 2): OUTFREQFILES2 files <outputfolder><xyfilehead><freq>_S<k>.dat
   std::string xyfilehead;
   int xy_nx = 0, xy_ny = 0, ixydepth = 0;
   double depth_xy = 0.0;
+  // seafloor plan views (ixydepth 2, ixyflag 2): the polygon_ki triangle mesh and ki23dptr,
+  // its nodes' surface and seafloor nodes of the 3-D mesh (READKI23DPTR, 1-based)
+  std::string pokimsh, ki23dfile;
+  std::vector<double> ki_xyz;
+  std::vector<int32_t> ki_n3, ki23dptr;
+  std::vector<double> xyz3d;  // 3-D mesh nodes (PREPZOBS heights, XYSBTM points, GENXYZMINMAX)
+  std::vector<double> F, v;   // readfxyz / readvxyz records of the ocean nodes (IXYHOUT)
+  bool seafloor() const { return ixyflag == 2 || (ixyflag == 1 && ixydepth == 2); }
 };
 
 namespace {
@@ -349,6 +358,96 @@ void utmxy(double lon, double lat, double lonorigin, double latorigin, int zone,
   *ykm = (y - y0) / 1e3;
 }
 
+// The 2-D grid list of a triangle mesh and its point search (allocate_2Dgrid_list,
+// gen2Dgridforlist, classifytri2grd, findtriwithgrid, FINDTRI; src/common/
+// m_triangle.f90:11-260), as PREPZOBS uses it to find the seafloor under a
+// plan-view point: nx x ny boxes over [xmin, xmax] x [ymin, ymax] (the 3-D mesh's
+// node extent), each triangle listed in the box of its centroid (strictly
+// inside; a centroid on a box boundary stops the reference), the list in
+// SORT_INDEX (heap) order; a point's box is half-open (lo, hi], and shells of
+// boxes grow around it until a listed triangle holds the point.
+struct TriGrid {
+  int nx = 0, ny = 0;
+  std::vector<double> xg, yg;     // nx+1 / ny+1 boundaries
+  std::vector<int32_t> stack;     // 0..nx*ny: triangles in boxes <= b
+  std::vector<int32_t> ordered;   // 0-based triangle ids in list order
+};
+
+TriGrid make_tri_grid(const std::vector<double>& xyz, const std::vector<int32_t>& n3, const double mm[4], int nx,
+                      int ny) {
+  TriGrid g;
+  g.nx = nx;
+  g.ny = ny;
+  g.xg.resize(nx + 1);
+  g.yg.resize(ny + 1);
+  for (int i = 0; i <= ny; ++i) g.yg[i] = (double)i * (mm[3] - mm[2]) / (double)ny + mm[2];
+  for (int i = 0; i <= nx; ++i) g.xg[i] = (double)i * (mm[1] - mm[0]) / (double)nx + mm[0];
+  const long ntri = (long)n3.size() / 3;
+  // strict box of a centroid coordinate: g[i-1] < v < g[i], 1-based i, 0 if none
+  auto sbox = [](const std::vector<double>& gr, double v) {
+    const int pos = (int)(std::lower_bound(gr.begin(), gr.end(), v) - gr.begin());  // count of gr < v
+    return (pos >= 1 && pos < (int)gr.size() && v < gr[pos]) ? pos : 0;
+  };
+  std::vector<double> order(ntri);
+  std::vector<int32_t> index(ntri);
+  for (long t = 0; t < ntri; ++t) {
+    double x2[2] = {0.0, 0.0};
+    for (int j = 0; j < 3; ++j)
+      for (int c = 0; c < 2; ++c) x2[c] = x2[c] + xyz[3L * (n3[3 * t + j] - 1) + c] / 3.0;
+    const int iy = sbox(g.yg, x2[1]), ix = sbox(g.xg, x2[0]);
+    AFEM_REQUIRE(ix && iy, AFEM_EIO,
+                 "seafloor plan view: a polygon_ki triangle's centroid lies on a box boundary or outside the "
+                 "3-D mesh (classifytri2grd)");
+    order[t] = (double)((long)nx * (iy - 1) + ix);
+    index[t] = (int32_t)(t + 1);
+  }
+  sort_index_heap((int)ntri, index.data(), order.data());
+  g.stack.assign((long)nx * ny + 1, 0);
+  for (long t = 0; t < ntri; ++t) g.stack[(long)order[t]] += 1;
+  for (long b = 1; b <= (long)nx * ny; ++b) g.stack[b] += g.stack[b - 1];
+  g.ordered.resize(ntri);
+  for (long t = 0; t < ntri; ++t) g.ordered[t] = index[t] - 1;
+  return g;
+}
+
+// findtriwithgrid + FINDTRI: 0-based triangle holding (x, y) and its coordinates a[3]; false if none
+bool find_tri(const TriGrid& g, const std::vector<double>& xyz, const std::vector<int32_t>& n3, double x, double y,
+              int* tri, double a[3]) {
+  auto hbox = [](const std::vector<double>& gr, double v) {  // gr[i-1] < v <= gr[i]
+    const int pos = (int)(std::lower_bound(gr.begin(), gr.end(), v) - gr.begin());
+    return (pos >= 1 && pos < (int)gr.size()) ? pos : 0;
+  };
+  const int iy = hbox(g.yg, y), ix = hbox(g.xg, x);
+  if (!ix || !iy) return false;
+  for (int iside = 0; iside <= std::max(g.nx, g.ny); ++iside) {  // the reference grows iside without bound
+    for (int k = std::max(iy - iside, 1); k <= std::min(iy + iside, g.ny); ++k)
+      for (int j = std::max(ix - iside, 1); j <= std::min(ix + iside, g.nx); ++j) {
+        if (iy - (iside - 1) <= k && k <= iy + (iside - 1) && ix - (iside - 1) <= j && j <= ix + (iside - 1))
+          continue;
+        const long idx = (long)g.nx * (k - 1) + j;
+        for (int q = g.stack[idx - 1]; q < g.stack[idx]; ++q) {
+          const int t = g.ordered[q];
+          const double* p[3];
+          for (int m = 0; m < 3; ++m) p[m] = &xyz[3L * (n3[3 * t + m] - 1)];
+          const double x12[2] = {p[1][0] - p[0][0], p[1][1] - p[0][1]};
+          const double x13[2] = {p[2][0] - p[0][0], p[2][1] - p[0][1]};
+          const double x23[2] = {p[2][0] - p[1][0], p[2][1] - p[1][1]};
+          const double v1[2] = {x - p[0][0], y - p[0][1]};
+          const double v2[2] = {x - p[1][0], y - p[1][1]};
+          const double a0 = (x13[0] * x12[1] - x13[1] * x12[0]);
+          a[1] = (x13[0] * v1[1] - x13[1] * v1[0]) / a0;
+          a[2] = (v1[0] * x12[1] - v1[1] * x12[0]) / a0;
+          a[0] = (v2[0] * x23[1] - v2[1] * x23[0]) / a0;
+          if (a[0] >= 0.0 && a[1] >= 0.0 && a[2] >= 0.0) {
+            *tri = t;
+            return true;
+          }
+        }
+      }
+  }
+  return false;
+}
+
 // Fortran Gw.d edit descriptor (G15.7 of OUTOBSFILESFWD) for finite values.
 std::string fortran_g(double x, int w, int d) {
   char buf[64];
@@ -462,19 +561,21 @@ int load_ctl(afem_ctx* c, const char* path) {
     }
   }
   ci->ixyflag = (int)r.num("ixyflag");
+  AFEM_REQUIRE(ci->ixyflag >= 0 && ci->ixyflag <= 2, AFEM_EIO, "ctl: ixyflag should be 0, 1 or 2");
   if (ci->ixyflag == 1) {
     ci->xyfilehead = r.word("xyfilehead");
     auto nxy = r.nums("nx ny", 2);
     ci->xy_nx = (int)nxy[0];
     ci->xy_ny = (int)nxy[1];
     ci->ixydepth = (int)r.num("ixydepth");
+    AFEM_REQUIRE(ci->ixydepth == 1 || ci->ixydepth == 2, AFEM_EIO, "ctl: ixydepth should be 1 or 2");
     if (ci->ixydepth == 1) ci->depth_xy = r.num("depth_xy");
-    r.skip("pokimsh");
-    r.skip("ki23dfile");
+    ci->pokimsh = r.str("pokimsh");
+    ci->ki23dfile = r.str("ki23dfile");
   } else if (ci->ixyflag == 2) {
-    r.skip("xyfilehead");
-    r.skip("pokimsh");
-    r.skip("ki23dfile");
+    ci->xyfilehead = r.word("xyfilehead");
+    ci->pokimsh = r.str("pokimsh");
+    ci->ki23dfile = r.str("ki23dfile");
   }
   ci->nsource = (int)r.num("nsource");
   for (int i = 0; i < ci->nsource; ++i) {
@@ -498,6 +599,29 @@ int load_ctl(afem_ctx* c, const char* path) {
   // mesh, surface, ocean node count, edges
   Msh g = read_msh(ci->g_meshfile, true, false);
   Msh h = read_msh(ci->z_meshfile, false, true);
+  ci->xyz3d = g.xyz;
+  if (ci->seafloor()) {
+    // READMESH_TOTAL(ki_mesh, pokimsh) + READKI23DPTR (n_ebfem_bxyz_mpi.f90:67-70, 305-328); the
+    // constant-depth view does not use them, so they are read only for the seafloor views
+    Msh k = read_msh(ci->pokimsh, false, true);
+    ci->ki_xyz = k.xyz;
+    ci->ki_n3 = k.n3;
+    std::ifstream f(ci->ki23dfile);
+    AFEM_REQUIRE((bool)f, AFEM_EIO, "cannot open ki23dfile " + ci->ki23dfile);
+    long ndat = 0;
+    AFEM_REQUIRE((bool)(f >> ndat), AFEM_EIO, "no count in " + ci->ki23dfile);
+    AFEM_REQUIRE(ndat == k.node, AFEM_EIO, "ki23dfile: the count differs from the polygon_ki node count");
+    ci->ki23dptr.resize(2 * ndat);
+    for (long i = 0; i < 2 * ndat; ++i) {
+      std::string tok;
+      AFEM_REQUIRE((bool)(f >> tok), AFEM_EIO, "truncated " + ci->ki23dfile);
+      ci->ki23dptr[i] = (int32_t)fnum(tok);  // read as real(8), used as integer(4)
+      AFEM_REQUIRE(ci->ki23dptr[i] >= 1 && ci->ki23dptr[i] <= g.node, AFEM_EIO,
+                   "ki23dfile: a node id outside the 3-D mesh");
+    }
+    for (int32_t id : ci->ki_n3)
+      AFEM_REQUIRE(id >= 1 && id <= k.node, AFEM_EIO, "polygon_ki mesh: a triangle node id out of range");
+  }
   ci->nodes = count_msh_nodes(ci->ocean_meshfile);
   lift_sites(h, ci->xyzobs);
   std::vector<int32_t> line, n6;
@@ -514,7 +638,8 @@ int load_ctl(afem_ctx* c, const char* path) {
                      ci->sigma_land.empty() ? nullptr : ci->sigma_land.data(), (int)sigma_file.size(),
                      sigma_file.empty() ? nullptr : sigma_file.data());
   if (rc) throw Error{rc, c->err};
-  std::vector<double> F, v;
+  std::vector<double>& F = ci->F;
+  std::vector<double>& v = ci->v;
   read_fv(ci->fxyz_file, ci->vxyz_file, ci->nodes, F, v);
   rc = afem_set_source(c, 0, ci->nodes, F.data(), v.data());
   if (rc) throw Error{rc, c->err};
@@ -567,6 +692,129 @@ std::string fortran_f(double x, int w, int d) {
   return s;
 }
 
+namespace {
+
+// GENXYZMINMAX (n_ebfem_bxyz_mpi.f90:533-565): xmin, xmax, ymin, ymax of the 3-D mesh nodes
+void xy_extent(const std::vector<double>& xyz, double mm[4]) {
+  mm[0] = mm[1] = xyz[0];
+  mm[2] = mm[3] = xyz[1];
+  for (size_t i = 0; i < xyz.size() / 3; ++i) {
+    mm[0] = std::min(mm[0], xyz[3 * i]);
+    mm[1] = std::max(mm[1], xyz[3 * i]);
+    mm[2] = std::min(mm[2], xyz[3 * i + 1]);
+    mm[3] = std::max(mm[3], xyz[3 * i + 1]);
+  }
+}
+
+// PREPZOBS with iflag 1 (n_ebfem_bxyz_mpi.f90:1181-1267): each plan-view point goes
+// 1 m below the seafloor under it (the polygon_ki triangle holding it, interpolating
+// the heights of its nodes' seafloor nodes ki23dptr(2,:)); the same three nodes and
+// weights are IXYHOUT's coeff_vF row of the point.
+void prepzobs(const CtlInfo* ci, std::vector<double>& xy, std::vector<int32_t>& item, std::vector<double>& val) {
+  const int np = (int)xy.size() / 3;
+  double mm[4];
+  xy_extent(ci->xyz3d, mm);
+  const TriGrid g = make_tri_grid(ci->ki_xyz, ci->ki_n3, mm, 200, 200);
+  item.resize(3L * np);
+  val.resize(3L * np);
+  for (int p = 0; p < np; ++p) {
+    int t = 0;
+    double a[3];
+    AFEM_REQUIRE(find_tri(g, ci->ki_xyz, ci->ki_n3, xy[3L * p], xy[3L * p + 1], &t, a), AFEM_EIO,
+                 "seafloor plan view: a point lies outside the polygon_ki mesh (findtriwithgrid)");
+    double z[3];
+    for (int j = 0; j < 3; ++j) {
+      const int m = ci->ki23dptr[2L * (ci->ki_n3[3L * t + j] - 1) + 1];
+      item[3L * p + j] = m;
+      val[3L * p + j] = a[j];
+      z[j] = ci->xyz3d[3L * (m - 1) + 2];
+    }
+    xy[3L * p + 2] = a[0] * z[0] + a[1] * z[1] + a[2] * z[2] - 0.001;
+  }
+}
+
+// PREPOBSCOEFF_XYSBTM's points (n_ebfem_bxyz_mpi.f90:1064-1078): per polygon_ki
+// triangle the mean of its nodes' seafloor nodes, raised by 1 m, with coeff_vF
+// weights 1/3 on those nodes.
+void xysbtm_points(const CtlInfo* ci, std::vector<double>& xy, std::vector<int32_t>& item, std::vector<double>& val) {
+  const long ntri = (long)ci->ki_n3.size() / 3;
+  xy.assign(3 * ntri, 0.0);
+  item.resize(3 * ntri);
+  val.resize(3 * ntri);
+  const double up[3] = {0.0, 0.0, 0.001};
+  for (long i = 0; i < ntri; ++i) {
+    double x3[3] = {0.0, 0.0, 0.0};
+    for (int j = 0; j < 3; ++j) {
+      const int m = ci->ki23dptr[2L * (ci->ki_n3[3 * i + j] - 1) + 1];
+      for (int c = 0; c < 3; ++c) x3[c] = x3[c] + ci->xyz3d[3L * (m - 1) + c] / 3.0 + up[c] / 3.0;
+      item[3 * i + j] = m;
+      val[3 * i + j] = 1.0 / 3.0;
+    }
+    for (int c = 0; c < 3; ++c) xy[3 * i + c] = x3[c];
+  }
+}
+
+// IXYHOUT (n_ebfem_bxyz_mpi.f90:192-302): the depth-integrated ocean current of each
+// plan-view point, <outputfolder>ixyh_xy2D<freq>.dat with 26 E15.7 columns: x, y, z,
+// sigma h E, sigma h (v x F), their sum, h v (x, y, complex), B (3 complex), h.
+// fields: complex bx, by, bz, ex, ey of source 1 (5 x np); the reference reads them
+// back from amplitude and phase, and takes sigma_ocean from the default-real 3.3.
+void write_ixyhout(const CtlInfo* ci, double freq, const std::vector<double>& xy, const double* fields,
+                   const std::vector<int32_t>& item, const std::vector<double>& val) {
+  const int np = (int)xy.size() / 3;
+  const double pi = 4.0 * std::atan(1.0), d2r = pi / 180.0, r2d = 180.0 / pi;
+  const double sig = (double)3.3f;
+  using cx = std::complex<double>;
+  auto vnode = [&](int m, int c) {  // readvxyz: ocean nodes 1..nodes, zero beyond
+    return m <= ci->nodes ? cx(ci->v[6L * (m - 1) + 2 * c], ci->v[6L * (m - 1) + 2 * c + 1]) : cx(0.0, 0.0);
+  };
+  auto fnode = [&](int m, int c) { return m <= ci->nodes ? ci->F[3L * (m - 1) + c] : 0.0; };
+  const std::string num = trim(fortran_e(freq, 9, 2));
+  const std::string fn = rtrim(ci->outputfolder.substr(0, 70)) + "ixyh_xy2D" + num + ".dat";
+  FILE* f = std::fopen(fn.c_str(), "w");
+  if (!f) throw Error{AFEM_EIO, "cannot write " + fn};
+  for (int i = 0; i < np; ++i) {
+    double h = -xy[3L * i + 2];
+    if (h <= 0.0) h = 0.0;
+    cx rec[5];
+    for (int comp = 0; comp < 5; ++comp) {
+      const double re = fields[2 * ((long)comp * np + i)], im = fields[2 * ((long)comp * np + i) + 1];
+      const double amp = std::sqrt(std::pow(re, 2.0) + std::pow(im, 2.0));
+      const double ph = std::atan2(im, re) * r2d;
+      rec[comp] = amp * std::exp(cx(0.0, ph * d2r));
+    }
+    cx vf[3] = {0.0, 0.0, 0.0}, vh[2] = {0.0, 0.0};
+    for (int k = 0; k < 3; ++k) {
+      const int m = item[3L * i + k];
+      const double w = val[3L * i + k];
+      const cx v1 = vnode(m, 0), v2 = vnode(m, 1), v3 = vnode(m, 2);
+      const double F1 = fnode(m, 0), F2 = fnode(m, 1), F3 = fnode(m, 2);
+      const cx c1 = v2 * F3 - v3 * F2, c2 = v3 * F1 - v1 * F3, c3 = v1 * F2 - v2 * F1;  // cr_outer(v, F)
+      vf[0] = vf[0] + w * c1;
+      vf[1] = vf[1] + w * c2;
+      vf[2] = vf[2] + w * c3;
+      vh[0] = vh[0] + w * v1;
+      vh[1] = vh[1] + w * v2;
+    }
+    cx out[9];
+    for (int c = 0; c < 2; ++c) {
+      out[c] = sig * h * rec[3 + c];                         // ixyh_e
+      out[2 + c] = sig * h * vf[c] * 1e-3;                   // ixyh_vF
+      out[4 + c] = sig * h * (rec[3 + c] + vf[c] * 1e-3);    // ixyh
+      out[6 + c] = h * vh[c];                                // vh_obs
+    }
+    std::string row;
+    for (int j = 0; j < 3; ++j) row += fortran_e(xy[3L * i + j], 15, 7);
+    for (int j = 0; j < 8; ++j) row += fortran_e(out[j].real(), 15, 7) + fortran_e(out[j].imag(), 15, 7);
+    for (int c = 0; c < 3; ++c) row += fortran_e(rec[c].real(), 15, 7) + fortran_e(rec[c].imag(), 15, 7);
+    row += fortran_e(h, 15, 7);
+    std::fprintf(f, "%s\n", row.c_str());
+  }
+  std::fclose(f);
+}
+
+}  // namespace
+
 // Frequency loop of n_ebfem_bxyz (n_ebfem_bxyz_mpi.f90:144-183): one forward
 // solve per frequency, CALOBSEBCOMP, then OUTOBSFILESFWD.  GENMAT fills
 // right-hand-side column 1 only, so sources 2..nsr have zero fields.
@@ -574,20 +822,29 @@ int run_ctl(afem_ctx* c, const afem_solve_opts* o) {
   AFEM_REQUIRE(c->ctl, AFEM_ESTATE, "run_ctl: no ctl loaded");
   AFEM_REQUIRE(o, AFEM_EINVAL, "run_ctl: null options");
   CtlInfo* ci = c->ctl;
-  AFEM_REQUIRE(ci->ixyflag == 0 || (ci->ixyflag == 1 && ci->ixydepth == 1), AFEM_EIO,
-               "run_ctl: plan views on the seafloor (ixyflag 2, or ixydepth 2) need the polygon_ki mesh (PREPZOBS); "
-               "only the constant-depth plan view (ixyflag 1, ixydepth 1) is supported");
   int rc = afem_assemble(c);
   if (rc) throw Error{rc, c->err};
   const int nf = (int)ci->freq.size(), nobs = ci->nobs;
-  // plan-view points of PREPOBSCOEFF_XY: the cells of [xbound(2), xbound(3)] x [ybound(2), ybound(3)]
+  // plan-view points: PREPOBSCOEFF_XY's cells of [xbound(2), xbound(3)] x [ybound(2), ybound(3)]
+  // at depth_xy (ixydepth 1) or 1 m below the seafloor (ixydepth 2, PREPZOBS), or
+  // PREPOBSCOEFF_XYSBTM's polygon_ki triangles (ixyflag 2); the seafloor views also
+  // write IXYHOUT's file (with ixydepth 1 the reference's IXYHOUT reads coeff_vF rows
+  // that nothing built, so that file is not written there)
   std::vector<double> xy;
-  const int nxy = ci->ixyflag == 1 ? ci->xy_nx * ci->xy_ny : 0;
-  if (nxy > 0) {
+  std::vector<int32_t> vf_item;
+  std::vector<double> vf_val;
+  int nxy = 0, grid_nz = 50;
+  if (ci->ixyflag == 1) {
+    nxy = ci->xy_nx * ci->xy_ny;
     xy.resize(3L * nxy);
-    rc = afem_xy_points(ci->xbound[1], ci->xbound[2], ci->ybound[1], ci->ybound[2], ci->xy_nx, ci->xy_ny, ci->depth_xy,
-                        xy.data());
+    rc = afem_xy_points(ci->xbound[1], ci->xbound[2], ci->ybound[1], ci->ybound[2], ci->xy_nx, ci->xy_ny,
+                        ci->ixydepth == 1 ? ci->depth_xy : 0.0, xy.data());
     if (rc) throw Error{rc, "run_ctl: plan-view grid"};
+    if (ci->ixydepth == 2) prepzobs(ci, xy, vf_item, vf_val);
+  } else if (ci->ixyflag == 2) {
+    xysbtm_points(ci, xy, vf_item, vf_val);
+    nxy = (int)xy.size() / 3;
+    grid_nz = 300;  // PREPOBSCOEFF_XYSBTM's grid list (n_ebfem_bxyz_mpi.f90:1097)
   }
   std::vector<double> amp((size_t)nf * 5 * nobs), ph((size_t)nf * 5 * nobs);
   const double pi = 4.0 * std::atan(1.0), r2d = 180.0 / pi;
@@ -602,8 +859,8 @@ int run_ctl(afem_ctx* c, const afem_solve_opts* o) {
     if (nxy > 0) {
       // OUTFREQFILES2 (m_outresp.f90:181-217): x, y, z and (amp, phase) of bx..ey per plan-view point
       std::vector<double> o2(2L * 5 * nxy);
-      rc = afem_sites_grid(c, nxy, xy.data(), o2.data());
-      if (rc) throw Error{rc, c->err};
+      reset_status(c);
+      sites_device(c, nxy, xy.data(), o2.data(), true, grid_nz);
       const std::string num = fortran_e(ci->freq[i], 9, 2);
       for (int k = 0; k < ci->nsource; ++k) {
         // the reference assembles the name in a character(50) variable
@@ -627,6 +884,7 @@ int run_ctl(afem_ctx* c, const afem_solve_opts* o) {
         }
         std::fclose(f);
       }
+      if (ci->seafloor()) write_ixyhout(ci, ci->freq[i], xy, o2.data(), vf_item, vf_val);
     }
     for (int comp = 0; comp < 5; ++comp)
       for (int s = 0; s < nobs; ++s) {

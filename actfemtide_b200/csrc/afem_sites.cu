@@ -289,10 +289,12 @@ namespace {
 // gengridforlist + classifyelement2grd (m_mesh_type.f90:73-202) on the host:
 // the grid over the node extent (GENXYZMINMAX) widened by 1 km, each
 // tetrahedron's box by its centroid, the list sorted by box with SORT_INDEX.
-void build_grid(afem_ctx* c) {
+void build_grid(afem_ctx* c, int nz) {
   if (!c->grid) c->grid = new GridList();
   GridList* g = c->grid;
-  if (g->ready) return;
+  if (g->ready && g->nz == nz) return;
+  g->nz = nz;
+  g->ready = false;
   cudaStream_t s = c->stream;
   const int node = c->node, ntet = c->ntet;
   std::vector<double> xyz(3L * node);
@@ -348,7 +350,7 @@ void build_grid(afem_ctx* c) {
 }
 
 void site_coeffs_range(afem_ctx* c, int nobs, const double* xyz_obs, long t0, long t1, int32_t* item, double* val_e,
-                       double* val_f, int32_t* iele, bool grid_search = false) {
+                       double* val_f, int32_t* iele, bool grid_search = false, int grid_nz = 50) {
   cudaStream_t s = c->stream;
   DBuf<double> obs;
   obs.upload(xyz_obs, 3L * nobs, s);
@@ -357,7 +359,7 @@ void site_coeffs_range(afem_ctx* c, int nobs, const double* xyz_obs, long t0, lo
   std::vector<int> init(nobs, 0x7fffffff);
   AFEM_CUDA(cudaMemcpyAsync(best.p, init.data(), sizeof(int) * nobs, cudaMemcpyHostToDevice, s));
   if (grid_search) {
-    build_grid(c);
+    build_grid(c, grid_nz);
     GridList* g = c->grid;
     k_find_grid<<<(nobs * 32 + 127) / 128, 128, 0, s>>>(c->xyz.p, c->n4.p, g->xg.p, g->yg.p, g->zg.p, g->nx, g->ny,
                                                          g->nz, g->stack.p, g->ordered.p, obs.p, nobs, best.p);
@@ -410,7 +412,7 @@ void grid_destroy(afem_ctx* c) {
   c->grid = nullptr;
 }
 
-void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out, bool grid) {
+void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out, bool grid, int grid_nz) {
   AFEM_REQUIRE(c->nsys > 0 && c->X.p, AFEM_ESTATE, "sites: no solution");
   cudaStream_t s = c->stream;
   if (c->sol_packed) {
@@ -444,7 +446,7 @@ void sites_device(afem_ctx* c, int nobs, const double* xyz_obs, double* out, boo
   }
   std::vector<int32_t> item(6L * nobs);
   std::vector<double> ve(18L * nobs), vf(18L * nobs);
-  site_coeffs_range(c, nobs, xyz_obs, 0, c->ntet, item.data(), ve.data(), vf.data(), nullptr, grid);
+  site_coeffs_range(c, nobs, xyz_obs, 0, c->ntet, item.data(), ve.data(), vf.data(), nullptr, grid, grid_nz);
   DBuf<int32_t> ditem;
   DBuf<double> dve, dvf, dom;
   ditem.upload(item.data(), item.size(), s);

@@ -331,7 +331,7 @@ def _write_msh(path, xyz, elems, etype):
 
 
 def write_reference_inputs(m: TidalModel, outdir: str, line=None, n6line=None, site_names=None,
-                           plan_view=None, utm_sites=None) -> str:
+                           plan_view=None, utm_sites=None, seafloor_view=None) -> str:
     """Write model m as the files the reference's tide forward reads; returns the ctl path.
 
     em3d.msh (tetrahedra, tags = elementary volume), polygonz.msh (top-of-earth
@@ -342,6 +342,12 @@ def write_reference_inputs(m: TidalModel, outdir: str, line=None, n6line=None, s
     order, labels in the first 20 columns, xyz sites given 1 m below the surface).
     utm_sites = (zone, lonorigin, latorigin, lonlat): sites given as longitude /
     latitude (lonlat: nobs x 2 degrees) in UTM zone `zone` (lonlatflag 1).
+    plan_view = (xyfilehead, nx, ny, depth): the nx x ny plan view (ixyflag 1) at a
+    constant depth (ixydepth 1), or 1 m below the seafloor when depth is None
+    (ixydepth 2); seafloor_view = xyfilehead: the polygon_ki triangles' plan view
+    (ixyflag 2).  The seafloor views also get polygon_ki.msh (the surface grid's
+    triangles) and ki23dptr.dat (each of its nodes' 3-D surface node at z = 0 and
+    seafloor node at the top of the solid earth; the mesh needs a node layer there).
     """
     import os
     os.makedirs(outdir, exist_ok=True)
@@ -362,6 +368,15 @@ def write_reference_inputs(m: TidalModel, outdir: str, line=None, n6line=None, s
             tris.append((1, (a, b, b + 1)))
             tris.append((1, (a, b + 1, a + 1)))
     _write_msh(p("polygonz.msh"), sxyz, tris, 2)
+    if seafloor_view is not None or (plan_view is not None and plan_view[3] is None):
+        _write_msh(p("polygon_ki.msh"), np.stack([X.ravel(), Y.ravel(), np.zeros(X.size)], axis=1), tris, 2)
+        key = {tuple(np.round(c, 6)): i + 1 for i, c in enumerate(m.xyz)}
+        with open(p("ki23dptr.dat"), "w") as f:
+            f.write(f"{sxyz.shape[0]}\n")
+            for x, y, zs in sxyz:
+                top = key[(round(float(x), 6), round(float(y), 6), 0.0)]
+                bot = key[(round(float(x), 6), round(float(y), 6), round(float(zs), 6))]
+                f.write(f"{top} {bot}\n")
     _write_msh(p("ocean.msh"), m.xyz[: m.nodes], [], 4)
     if line is not None:
         with open(p("lineinfo.dat"), "w") as f:
@@ -414,13 +429,19 @@ def write_reference_inputs(m: TidalModel, outdir: str, line=None, n6line=None, s
                  lab("UTM ZONE") + f"{int(zone)}S", lab("lonlatorigin") + f"{float(lon0)!r} {float(lat0)!r}"]
         for nm, ll in zip(names, lonlat):
             rows += [lab("Name") + nm, lab("lonlatalt") + f"{float(ll[0])!r} {float(ll[1])!r} {-SITE_DEPTH_KM!r}"]
-    if plan_view is None:
+    if seafloor_view is not None:  # ixyflag 2: the polygon_ki triangles 1 m above the seafloor
+        rows += [lab("0:no,1:nxny,2:ntrik") + "2", lab("xyfilehead") + seafloor_view,
+                 lab("pokimsh") + p("polygon_ki.msh"), lab("ki23dfile") + p("ki23dptr.dat")]
+    elif plan_view is None:
         rows += [lab("0:no,1:nxny,2:ntrik") + "0"]
-    else:  # (xyfilehead, nx, ny, depth_xy): a constant-depth plan view (ixyflag 1, ixydepth 1)
+    else:  # (xyfilehead, nx, ny, depth_xy): ixyflag 1, at depth_xy (ixydepth 1) or on the seafloor (2)
         head, pnx, pny, depth = plan_view
-        rows += [lab("0:no,1:nxny,2:ntrik") + "1", lab("xyfilehead") + head, lab("nx ny") + f"{pnx} {pny}",
-                 lab("ixydepth") + "1", lab("depth_xy [km]") + repr(float(depth)), lab("pokimsh") + p("polygon_ki.msh"),
-                 lab("ki23dfile") + p("ki23dptr.dat")]
+        rows += [lab("0:no,1:nxny,2:ntrik") + "1", lab("xyfilehead") + head, lab("nx ny") + f"{pnx} {pny}"]
+        if depth is None:
+            rows += [lab("ixydepth") + "2"]
+        else:
+            rows += [lab("ixydepth") + "1", lab("depth_xy [km]") + repr(float(depth))]
+        rows += [lab("pokimsh") + p("polygon_ki.msh"), lab("ki23dfile") + p("ki23dptr.dat")]
     rows += [lab("# of sources") + "1", lab("Source Name") + "S1",
              lab("source start point") + "0.0 0.0 -0.001", lab("source end   point") + "0.1 0.0 -0.001",
              lab("Elcetric current[A]") + "0.0", lab("sigma_air    [S/m]") + repr(float(m.sigma_air)),

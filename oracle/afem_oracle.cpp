@@ -824,9 +824,10 @@ struct GridList {
   std::vector<int> ordered;         // 1-based tetrahedron ids, ordered[1..ntet]
 };
 
-GridList make_grid_list(const double* xyz, long node, long ntet, const int* n4) {
+GridList make_grid_list(const double* xyz, long node, long ntet, const int* n4, int nz = 50) {
   GridList g;
-  g.nx = 300; g.ny = 300; g.nz = 50;  // PREPOBSCOEFF_XY (n_ebfem_bxyz_mpi.f90:793)
+  // PREPOBSCOEFF_XY (n_ebfem_bxyz_mpi.f90:822): 300 x 300 x 50; PREPOBSCOEFF_XYSBTM (:1097): 300 x 300 x 300
+  g.nx = 300; g.ny = 300; g.nz = nz;
   // GENXYZMINMAX (src/src_inv_ap/n_inv_ap.f90:1175-1205)
   double xmin = xyz[0], xmax = xyz[0], ymin = xyz[1], ymax = xyz[1], zmin = xyz[2], zmax = xyz[2];
   for (long i = 0; i < node; ++i) {
@@ -959,6 +960,122 @@ long orc_prepobscoeff_grid(const double* xyz, long node, long ntet, const int* n
     if (iele == 0) return -(s + 1);
     if (iele_out) iele_out[s] = (int)iele;
     coeff_rows(xyz, n4, n6line, nobs, s, iele - 1, x3, item, val_e, val_f);
+  }
+  return 0;
+}
+
+// The same with the grid list's vertical box count nz (XYSBTM's 300).
+long orc_prepobscoeff_grid_nz(const double* xyz, long node, long ntet, const int* n4, const int* n6line, int nobs,
+                              const double* xyzobs, int nz, int* item, double* val_e, double* val_f, int* iele_out) {
+  GridList g = make_grid_list(xyz, node, ntet, n4, nz);
+  for (int s = 0; s < nobs; ++s) {
+    const double* x3 = xyzobs + 3 * s;
+    long iele = findelewithgrid(g, xyz, n4, x3);
+    if (iele == 0) return -(s + 1);
+    if (iele_out) iele_out[s] = (int)iele;
+    coeff_rows(xyz, n4, n6line, nobs, s, iele - 1, x3, item, val_e, val_f);
+  }
+  return 0;
+}
+
+// Triangle search of PREPZOBS (n_ebfem_bxyz_mpi.f90:1218-1223) over a 2-D mesh:
+// allocate_2Dgrid_list + gen2Dgridforlist + classifytri2grd + findtriwithgrid +
+// FINDTRI (src/common/m_triangle.f90:11-260).  xyz: 3 per node (x, y used);
+// n3: 3 per triangle, 1-based; minmax: xmin, xmax, ymin, ymax (GENXYZMINMAX of
+// the 3-D mesh, not widened here); nx x ny boxes.  Per point: iele (1-based) and
+// a3.  Returns 0; -(j+1) when point j lies in no box or in no triangle of the
+// shells searched (the reference stops or searches forever); -1000000 - t when
+// triangle t's centroid lies on a box boundary (the reference stops).
+long orc_findtri_grid(const double* xyz, long ntri, const int* n3, const double* minmax, int nx, int ny, int npts,
+                      const double* pts, int* iele_out, double* a3_out) {
+  // gen2Dgridforlist (:28-54)
+  std::vector<double> xg(nx + 2, 0.0), yg(ny + 2, 0.0);
+  const double xmin = minmax[0], xmax = minmax[1], ymin = minmax[2], ymax = minmax[3];
+  for (int i = 1; i <= ny + 1; ++i) yg[i] = (i - 1) * (ymax - ymin) / (double)(float)ny + ymin;
+  for (int i = 1; i <= nx + 1; ++i) xg[i] = (i - 1) * (xmax - xmin) / (double)(float)nx + xmin;
+  // classifytri2grd (:56-131): the centroid's box, strict on both sides
+  std::vector<double> order(ntri + 1, 0.0);
+  std::vector<int> index(ntri);
+  for (long ii = 1; ii <= ntri; ++ii) {
+    double x2[2] = {0.0, 0.0};
+    for (int j = 0; j < 3; ++j)
+      for (int c = 0; c < 2; ++c) x2[c] = x2[c] + xyz[3L * (n3[(ii - 1) * 3 + j] - 1) + c] / 3.0;
+    int ix = 0, iy = 0;
+    for (int j = 1; j <= ny && !ix; ++j) {
+      if (yg[j] < x2[1] && x2[1] < yg[j + 1]) {
+        iy = j;
+        for (int i = 1; i <= nx; ++i)
+          if (xg[i] < x2[0] && x2[0] < xg[i + 1]) { ix = i; break; }
+      }
+    }
+    if (!ix) return -1000000 - ii;
+    order[ii] = (nx * (iy - 1) + ix) * 1.0;
+    index[ii - 1] = (int)ii;
+  }
+  sort_index((int)ntri, index.data(), order.data() + 1);
+  std::vector<int> ordered(ntri + 1, 0);
+  for (long i = 1; i <= ntri; ++i) ordered[i] = index[i - 1];
+  const long nxy = (long)nx * ny;
+  std::vector<int> stack(nxy + 1, 0);
+  long ipre = 0, ii = 0;
+  for (ii = 0; ii <= nxy - 1; ++ii) {
+    for (;;) {
+      if (ipre == ntri) goto done;
+      if (order[ipre] < order[ipre + 1]) {
+        stack[ii] = (int)ipre;
+        if (ii + 1 == (long)order[ipre + 1]) ipre = ipre + 1;
+        break;
+      } else {
+        ipre = ipre + 1;
+      }
+    }
+  }
+done:
+  for (long k = ii; k <= nxy; ++k) stack[k] = (int)ntri;
+  // findtriwithgrid (:133-204) per point: the box (half-open), then growing shells
+  for (int p = 0; p < npts; ++p) {
+    const double* x2 = pts + 2L * p;
+    int ix = 0, iy = 0;
+    for (int k = 1; k <= ny && !ix; ++k) {
+      if (yg[k] < x2[1] && x2[1] <= yg[k + 1]) {
+        iy = k;
+        for (int j = 1; j <= nx; ++j)
+          if (xg[j] < x2[0] && x2[0] <= xg[j + 1]) { ix = j; break; }
+      }
+    }
+    if (!ix) return -(p + 1);
+    long found = 0;
+    double a[3] = {0.0, 0.0, 0.0};
+    std::vector<int> elist;
+    for (int iside = 0; iside <= std::max(nx, ny) && !found; ++iside) {
+      elist.clear();
+      for (int k = std::max(iy - iside, 1); k <= std::min(iy + iside, ny); ++k)
+        for (int j = std::max(ix - iside, 1); j <= std::min(ix + iside, nx); ++j) {
+          if (iy - (iside - 1) <= k && k <= iy + (iside - 1) && ix - (iside - 1) <= j && j <= ix + (iside - 1))
+            continue;
+          const long idx = (long)nx * (k - 1) + j;
+          const int num = stack[idx] - stack[idx - 1];
+          for (int i = 1; i <= num; ++i) elist.push_back(ordered[stack[idx - 1] + i]);
+        }
+      // FINDTRI (:208-258): the first listed triangle with all three coordinates >= 0
+      for (int t : elist) {
+        const double* P[3];
+        for (int j = 0; j < 3; ++j) P[j] = xyz + 3L * (n3[(t - 1) * 3 + j] - 1);
+        const double x12[2] = {P[1][0] - P[0][0], P[1][1] - P[0][1]};
+        const double x13[2] = {P[2][0] - P[0][0], P[2][1] - P[0][1]};
+        const double x23[2] = {P[2][0] - P[1][0], P[2][1] - P[1][1]};
+        const double v1[2] = {x2[0] - P[0][0], x2[1] - P[0][1]};
+        const double v2[2] = {x2[0] - P[1][0], x2[1] - P[1][1]};
+        const double a0 = (x13[0] * x12[1] - x13[1] * x12[0]);
+        a[1] = (x13[0] * v1[1] - x13[1] * v1[0]) / a0;
+        a[2] = (v1[0] * x12[1] - v1[1] * x12[0]) / a0;
+        a[0] = (v2[0] * x23[1] - v2[1] * x23[0]) / a0;
+        if (a[0] >= 0.0 && a[1] >= 0.0 && a[2] >= 0.0) { found = t; break; }
+      }
+    }
+    if (!found) return -(p + 1);
+    iele_out[p] = (int)found;
+    for (int j = 0; j < 3; ++j) a3_out[3L * p + j] = a[j];
   }
   return 0;
 }

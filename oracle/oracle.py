@@ -83,6 +83,12 @@ def lib():
         L.orc_prepobscoeff_grid.restype = C.c_long
         L.orc_prepobscoeff_grid.argtypes = [_f64p, C.c_long, C.c_long, _i32p, _i32p, C.c_int, _f64p, _i32p, _f64p,
                                             _f64p, _i32p]
+        L.orc_prepobscoeff_grid_nz.restype = C.c_long
+        L.orc_prepobscoeff_grid_nz.argtypes = [_f64p, C.c_long, C.c_long, _i32p, _i32p, C.c_int, _f64p, C.c_int,
+                                               _i32p, _f64p, _f64p, _i32p]
+        L.orc_findtri_grid.restype = C.c_long
+        L.orc_findtri_grid.argtypes = [_f64p, C.c_long, _i32p, _f64p, C.c_int, C.c_int, C.c_int, _f64p, _i32p,
+                                       _f64p]
         L.orc_calobsebcomp.restype = None
         L.orc_calobsebcomp.argtypes = [C.c_int, C.c_int, C.c_double, _c128p, C.c_int, _i32p, _f64p, _f64p, _c128p,
                                        _f64p, _f64p]
@@ -295,6 +301,95 @@ def prepobscoeff_grid(m, n6line, sites):
     if rc != 0:
         raise RuntimeError(f"site {-rc} is outside the mesh")
     return item, ve, vf, iele
+
+
+def prepobscoeff_grid_nz(m, n6line, sites, nz):
+    """prepobscoeff_grid with the grid list's nz boxes in z (PREPOBSCOEFF_XYSBTM uses 300)."""
+    sites = _c(sites, np.float64)
+    nobs = sites.shape[0]
+    item = np.zeros((nobs, 6), np.int32)
+    ve = np.zeros((3, nobs, 6)); vf = np.zeros((3, nobs, 6)); iele = np.zeros(nobs, np.int32)
+    rc = lib().orc_prepobscoeff_grid_nz(_c(m.xyz, np.float64).reshape(-1), m.node, m.ntet, _c(m.n4, np.int32),
+                                        _c(n6line, np.int32), nobs, sites.reshape(-1), int(nz), item, ve, vf, iele)
+    if rc != 0:
+        raise RuntimeError(f"site {-rc} is outside the mesh")
+    return item, ve, vf, iele
+
+
+def findtri_grid(xyz, n3, minmax, pts2, nx=200, ny=200):
+    """findtriwithgrid over a triangle mesh (m_triangle.f90:11-260): 1-based triangle and a3 per point."""
+    pts2 = _c(np.asarray(pts2)[:, :2], np.float64)
+    npts = pts2.shape[0]
+    iele = np.zeros(npts, np.int32)
+    a3 = np.zeros((npts, 3))
+    rc = lib().orc_findtri_grid(_c(xyz, np.float64).reshape(-1), int(n3.shape[0]), _c(n3, np.int32).reshape(-1),
+                                _c(minmax, np.float64), nx, ny, npts, pts2.reshape(-1), iele, a3)
+    if rc != 0:
+        raise RuntimeError(f"findtri_grid failed: {rc}")
+    return iele, a3
+
+
+def xyz_minmax(xyz):
+    """GENXYZMINMAX (n_ebfem_bxyz_mpi.f90:533-565): node extent xmin, xmax, ymin, ymax, zmin, zmax."""
+    return np.array([xyz[:, 0].min(), xyz[:, 0].max(), xyz[:, 1].min(), xyz[:, 1].max(), xyz[:, 2].min(),
+                     xyz[:, 2].max()])
+
+
+def prepzobs(xyz3d, ki_xyz, ki_n3, ki23dptr, pts):
+    """PREPZOBS with iflag 1 (n_ebfem_bxyz_mpi.f90:1181-1267): each plan-view point 1 m below the seafloor
+    under it (the triangle of the polygon_ki mesh that holds it, its nodes' seafloor nodes ki23dptr(2,:)),
+    and the coeff_vF rows (3 seafloor nodes, the triangle's coordinates).  Returns xyz, items (1-based), vals."""
+    iele, a3 = findtri_grid(ki_xyz, ki_n3, xyz_minmax(xyz3d)[:4], pts, 200, 200)
+    m = ki23dptr[ki_n3[iele - 1] - 1, 1]  # (npts, 3) 1-based 3-D seafloor nodes
+    out = np.array(pts, np.float64).copy()
+    z = xyz3d[:, 2]
+    out[:, 2] = a3[:, 0] * z[m[:, 0] - 1] + a3[:, 1] * z[m[:, 1] - 1] + a3[:, 2] * z[m[:, 2] - 1] - 0.001
+    return out, m.astype(np.int32), a3
+
+
+def xysbtm_points(xyz3d, ki_n3, ki23dptr):
+    """PREPOBSCOEFF_XYSBTM's points (n_ebfem_bxyz_mpi.f90:1064-1078): per polygon_ki triangle, the mean of its
+    three seafloor nodes raised by 1 m, and coeff_vF rows of 1/3 on those nodes."""
+    m = ki23dptr[ki_n3 - 1, 1].astype(np.int32)  # (ntri, 3)
+    x3 = np.zeros((ki_n3.shape[0], 3))
+    up = np.array([0.0, 0.0, 0.001])
+    for j in range(3):
+        x3 = x3 + xyz3d[m[:, j] - 1] / 3.0 + up / 3.0
+    return x3, m, np.full(m.shape, 1.0 / 3.0)
+
+
+def ixyhout(pts, fields5, F, v, items, vals):
+    """IXYHOUT (n_ebfem_bxyz_mpi.f90:192-302): the 26 columns of ixyh_xy2D<freq>.dat per plan-view point.
+
+    fields5: complex (5, npts) bx, by, bz, ex, ey of source 1; F (node, 3) nT and v (node, 3) m/s over the
+    3-D mesh nodes (zero past the ocean nodes), items/vals the coeff_vF rows."""
+    pi = 4.0 * np.arctan(1.0)
+    d2r, r2d = pi / 180.0, 180.0 / pi
+    amp = np.sqrt(fields5.real ** 2.0 + fields5.imag ** 2.0)
+    ph = np.arctan2(fields5.imag, fields5.real) * r2d
+    rec = amp * np.exp(1j * ph * d2r)             # CALOBSRESP amp/phase read back as in IXYHOUT
+    bxyz, exy = rec[0:3], rec[3:5]
+    sig = float(np.float32(3.3))                    # sigma_ocean = 3.3, a default-real literal
+    h = -np.asarray(pts)[:, 2]
+    h = np.where(h <= 0.0, 0.0, h)
+    vF = np.stack([v[:, 1] * F[:, 2] - v[:, 2] * F[:, 1], v[:, 2] * F[:, 0] - v[:, 0] * F[:, 2],
+                   v[:, 0] * F[:, 1] - v[:, 1] * F[:, 0]])
+    npts = len(h)
+    vF_obs = np.zeros((3, npts), np.complex128)
+    vh = np.zeros((2, npts), np.complex128)
+    for k in range(items.shape[1]):               # mul_matcrs_cv, in the row's entry order
+        vF_obs = vF_obs + vals[:, k] * vF[:, items[:, k] - 1]
+        vh = vh + vals[:, k] * v[items[:, k] - 1, :2].T
+    ixyh = sig * h * (exy + vF_obs[:2] * 1e-3)
+    ixyh_e = sig * h * exy
+    ixyh_vF = sig * h * vF_obs[:2] * 1e-3
+    vh = h * vh
+    cols = [np.asarray(pts)[:, j] for j in range(3)]
+    for arr in (ixyh_e, ixyh_vF, ixyh, vh, bxyz):
+        for c in range(arr.shape[0]):
+            cols += [arr[c].real, arr[c].imag]
+    cols.append(h)
+    return np.stack(cols, axis=1)
 
 
 def calobsebcomp(fs, omega, item, ve, vf):

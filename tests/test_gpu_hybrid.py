@@ -158,3 +158,29 @@ def test_hybrid_box20_batch_of_16_sites(fw, oracle, box20_ref, precision):
     assert r.ok and r.resid_true <= 1e-8, r
     assert oracle.true_residual(A, fw.solution(0)) <= 1.01e-8
     assert _rel(fw.sites(m.sites, nsys=16)[0], ref) <= 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp64", "pc32"])
+def test_batched_hybrid_matches_direct_solve_32x32x24(fw, precision):
+    """The batched gradient-corrected solve (16 systems, 8 periods x 2 velocity patterns) on the 32x32x24 mesh
+    (179,800 edges): the site fields of systems 0 and 12 within 1e-6 of a direct solve (SciPy SuperLU, the
+    stand-in for the reference's PARDISO) of the oracle's assembly, committed by
+    tests/golden/make_superlu_fixture.py."""
+    import os
+    import sys
+    here = os.path.join(os.path.dirname(__file__), "golden")
+    sys.path.insert(0, here)
+    import make_superlu_fixture as msf
+    g = np.load(os.path.join(here, "box32x32x24_superlu.npz"))
+    m, m2 = msf.models()
+    f, src = msf.batch_freqs(m)
+    assert np.array_equal(g["sites"], m.sites)
+    fw.load_model(m, sources=[(m.F, m.v), (m2.F, m2.v)])
+    fw.assemble()
+    r = fw.solve(f, srcs=src, precond="HYBRID", precision=precision, tol=1e-8, maxit=20000)
+    assert r.ok and r.resid_true <= 1e-8, r
+    out = fw.sites(m.sites, nsys=16)
+    for k in (0, 12):
+        assert float(g[f"freq_{k}"]) == f[k]
+        assert float(g[f"resid_{k}"]) <= 1e-10
+        assert _rel(out[k], g[f"sites_{k}"]) <= 1e-6, (k, _rel(out[k], g[f"sites_{k}"]))
