@@ -50,7 +50,6 @@ struct Cx<float> {
   __host__ __device__ static V make(float a, float b) { return make_float2(a, b); }
 };
 
-constexpr int MAX_NS = 16;   // systems sharing one matrix (lanes of a warp)
 constexpr int MAX_SYS = 32;  // systems of one solve: NS, or the meshes of a packed batch
 constexpr unsigned SPIN_LIMIT = 1u << 21;  // x ~1 us back-off: a wait gives up after ~2 s
 
@@ -90,7 +89,8 @@ struct SolverWork {
   DBuf<double2> ht, hy, hdd;        // gradient-space correction: nodal rhs, solution, 1/diag (FP64 inner)
   DBuf<float2> htf, hyf, hddf;      // the same for the FP32 inner solve
   int nmc_blocks = 0;               // co-resident grid of the nodal multicolour sweeps
-  int rpw64 = 0, rpw32 = 0;         // SpMV rows per warp chosen by tune_spmv (0 = not tuned)
+  int rpw64 = 0, rpw32 = 0;         // SpMV rows per warp chosen by tune_spmv (0 = not tuned; 8: 4 systems per lane)
+  int spmv_grid[2][4] = {};         // one-wave grid of each SpMV variant (FP64 / FP32), 0 = not known yet
   int mc_blocks = 0;                // co-resident grid of the forward multicolour sweep
   int mcb_blocks = 0;               // and of the backward one (fewer registers: more blocks)
   double sd = 1.0;                  // SSOR diagonal scale of the current solve (DD = 1 / (sd D))
@@ -444,12 +444,148 @@ __global__ void __launch_bounds__(256)
 // entries, so a row per lane keeps 32/NS rows' dependent loads in flight per
 // warp (the sweeps are latency-bound, not bandwidth-bound).  Packed batches
 // keep 4 rows per warp so that each row's per-mesh sums have their own slot.
+// With 16 systems a lane carries SPL of them (2 by default): a row's 16 values are
+// read by its 16/SPL lanes as one contiguous run, and a warp works on 2*SPL rows at
+// once (SPL times the independent load chains of a lane per system), with the row's
+// column indices and matrix values loaded by 16/SPL lanes instead of 16.
+#ifndef AFEM_MC_SPL
+#define AFEM_MC_SPL 2  // systems per lane at 16 systems (1, 2 or 4)
+#endif
+constexpr int MC_MIN_BLOCKS = 4;
+
 template <int NS, bool SEG = false>
 struct McShape {
-  static constexpr int RPW = SEG ? 4 : 32 / NS;  // rows per warp
-  static constexpr int LPR = 32 / RPW;           // lanes per row
-  static constexpr int G = LPR / NS;             // entry groups per row
+  static constexpr int SPL = (NS == 16 && !SEG) ? AFEM_MC_SPL : 1;  // systems per lane
+  static constexpr int NG = NS / SPL;                      // lanes of a row that hold different systems
+  static constexpr int RPW = SEG ? 4 : 32 / NG;            // rows per warp
+  static constexpr int LPR = 32 / RPW;                     // lanes per row
+  static constexpr int G = LPR / NG;                       // entry groups per row
 };
+
+// Minimum resident blocks of 256 threads asked of the compiler: the 4-systems-per-lane
+// kernels get at most 64 registers a thread, so that 4 blocks (32 warps, 256 rows) stay
+// resident per SM; the lane-per-system kernels keep the compiler's choice.
+template <int NS, bool SEG>
+constexpr int mc_min_blocks() {
+  return McShape<NS, SEG>::SPL > 1 ? MC_MIN_BLOCKS : 0;
+}
+
+// SPL consecutive complex values of one row (systems s0 .. s0+SPL-1) at p, 16-byte loads;
+// GATHER: a neighbour's values (L1 or L2, see GatherL1), else the row's own (plain load).
+template <class V, int NS, int SPL, bool GATHER>
+__device__ __forceinline__ void load_spl(const V* p, V (&v)[SPL]) {
+  if constexpr (SPL > 1 && sizeof(V) == 8) {  // float2 pairs as float4
+#pragma unroll
+    for (int i = 0; i < SPL; i += 2) {
+      const float4* q = reinterpret_cast<const float4*>(p + i);
+      float4 f;
+      if constexpr (GATHER && !GatherL1<V, NS>::ok) f = __ldcg(q);
+      else f = *q;
+      v[i] = V{f.x, f.y};
+      v[i + 1] = V{f.z, f.w};
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < SPL; ++i) {
+      if constexpr (GATHER) v[i] = gather_ld<V, NS>(p + i);
+      else v[i] = p[i];
+    }
+  }
+}
+template <class V, int SPL>
+__device__ __forceinline__ void store_spl(V* p, const V (&v)[SPL]) {
+  if constexpr (SPL > 1 && sizeof(V) == 8) {
+#pragma unroll
+    for (int i = 0; i < SPL; i += 2)
+      *reinterpret_cast<float4*>(p + i) = make_float4(v[i].x, v[i].y, v[i + 1].x, v[i + 1].y);
+  } else {
+#pragma unroll
+    for (int i = 0; i < SPL; ++i) p[i] = v[i];
+  }
+}
+
+// row_gather for a lane carrying SPL systems: sums A_k v_col(k) for systems s0..s0+SPL-1
+// over entries k0, k0+G, ... < k1, two entries' loads in flight (SPL = 1: row_gather).
+template <class T, int NS, int G, int SPL>
+__device__ __forceinline__ void row_gather_spl(const int32_t* __restrict__ cols,
+                                               const typename Cx<T>::V* __restrict__ vals,
+                                               const typename Cx<T>::V* vec, int k0, int k1, int s0,
+                                               T (&t1x)[SPL], T (&t1y)[SPL], T (&t2x)[SPL], T (&t2y)[SPL]) {
+  using V = typename Cx<T>::V;
+  if constexpr (SPL == 1) {
+    row_gather<T, NS, G>(cols, vals, vec, k0, k1, s0, t1x[0], t1y[0], t2x[0], t2y[0]);
+  } else {
+    int k = k0;
+    if constexpr (G == 1)
+      for (; k + 1 < k1; k += 2) {
+        const int j0 = __ldg(cols + k), j1 = __ldg(cols + k + 1);
+        const V a0 = vals[k], a1 = vals[k + 1];
+        V v0[SPL], v1[SPL];
+        load_spl<V, NS, SPL, true>(vec + (long)j0 * NS + s0, v0);
+        load_spl<V, NS, SPL, true>(vec + (long)j1 * NS + s0, v1);
+#pragma unroll
+        for (int i = 0; i < SPL; ++i) {
+          t1x[i] += a0.x * v0[i].x; t1y[i] += a0.x * v0[i].y; t2x[i] += a0.y * v0[i].x; t2y[i] += a0.y * v0[i].y;
+          t1x[i] += a1.x * v1[i].x; t1y[i] += a1.x * v1[i].y; t2x[i] += a1.y * v1[i].x; t2y[i] += a1.y * v1[i].y;
+        }
+      }
+    for (; k < k1; k += G) {
+      const int j = __ldg(cols + k);
+      const V a = vals[k];
+      V v[SPL];
+      load_spl<V, NS, SPL, true>(vec + (long)j * NS + s0, v);
+#pragma unroll
+      for (int i = 0; i < SPL; ++i) {
+        t1x[i] += a.x * v[i].x; t1y[i] += a.x * v[i].y; t2x[i] += a.y * v[i].x; t2y[i] += a.y * v[i].y;
+      }
+    }
+  }
+}
+
+// Sum the G entry groups of a row (lanes of one row that hold the same systems).
+template <class T, int SPL, int NG, int LPR>
+__device__ __forceinline__ void group_sum(T (&a)[SPL], T (&b)[SPL], T (&c)[SPL], T (&d)[SPL]) {
+#pragma unroll
+  for (int m = NG; m < LPR; m <<= 1)
+#pragma unroll
+    for (int i = 0; i < SPL; ++i) {
+      a[i] += shfl_xor(a[i], m); b[i] += shfl_xor(b[i], m);
+      c[i] += shfl_xor(c[i], m); d[i] += shfl_xor(d[i], m);
+    }
+}
+
+// Block partial sums when a lane carries systems s0..s0+SPL-1 (values nonzero only
+// on lanes with g == 0): the rows of each warp are folded with shuffles, the lanes
+// of its first row hand their systems' values to shared memory, and threads s < NS
+// add the warps in order into part[blockIdx][s][slot].
+template <int NS, int SPL, int LPR, int NVAL>
+__device__ __forceinline__ void block_partials_spl(double (&v)[SPL][NVAL], int s0, bool g0, double* part) {
+  __shared__ double red[8][NS][NVAL];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int m = LPR; m < 32; m <<= 1)
+#pragma unroll
+    for (int i = 0; i < SPL; ++i)
+#pragma unroll
+      for (int k = 0; k < NVAL; ++k) v[i][k] += __shfl_xor_sync(0xffffffffu, v[i][k], m);
+  if (lane < LPR && g0)
+#pragma unroll
+    for (int i = 0; i < SPL; ++i)
+#pragma unroll
+      for (int k = 0; k < NVAL; ++k) red[w][s0 + i][k] = v[i][k];
+  __syncthreads();
+  if (threadIdx.x < NS) {
+    const int sy = threadIdx.x;
+    double acc[NVAL];
+#pragma unroll
+    for (int k = 0; k < NVAL; ++k) acc[k] = 0.0;
+    for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww)
+#pragma unroll
+      for (int k = 0; k < NVAL; ++k) acc[k] += red[ww][sy][k];
+#pragma unroll
+    for (int k = 0; k < NVAL; ++k) part[((long)blockIdx.x * MAX_SYS + sy) * 4 + k] = acc[k];
+  }
+}
 
 // 1 / (sd (K_ii + i omega M_ii)): the SSOR diagonal of the system at omega, from the
 // row's (K, M) diagonal pair (COCG13_single.f90:126-130), computed where it is used
@@ -463,7 +599,7 @@ __device__ __forceinline__ double2 ssor_dd(double2 a, double om, double sd) {
 // T: the COCG vectors (r, q); PT: the preconditioner's matrix copy, output y and
 // the values gathered from it (PT = float: the FP32 preconditioner of an FP64 solve)
 template <class T, class PT, int NS, bool SEG = false>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
     k_fwd_mc(const int32_t* __restrict__ lptr, const int32_t* __restrict__ lcol,
              const typename Cx<PT>::V* __restrict__ lkm, int n, typename Cx<T>::V* __restrict__ r,
              typename Cx<PT>::V* __restrict__ y, const typename Cx<T>::V* __restrict__ q,
@@ -473,17 +609,25 @@ __global__ void __launch_bounds__(256)
   using V = typename Cx<T>::V;
   using PV = typename Cx<PT>::V;
   using S = McShape<NS, SEG>;
+  constexpr int SPL = S::SPL;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;  // uniform over the grid
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
   const bool update = ctrl->iter > 0;
-  const int lane = threadIdx.x & 31, sub = lane / S::LPR, s = lane % NS, g = (lane % S::LPR) / NS;
+  const int lane = threadIdx.x & 31, sub = lane / S::LPR, ql = lane % S::LPR;
+  const int s0 = (ql % S::NG) * SPL, g = ql / S::NG;
   const int wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;  // warp in block, warps per block
-  const int slot = (threadIdx.x >> 5) * S::RPW + sub;
-  double om = sc[s].omega;
-  double2 al = sc[s].alpha;
-  bool act = sc[s].active;
-  double rr = 0.0;
+  const int slot = wib * S::RPW + sub;
+  double om[SPL], rr[SPL][1];
+  double2 al[SPL];
+  bool act[SPL];
+#pragma unroll
+  for (int i = 0; i < SPL; ++i) {
+    om[i] = sc[s0 + i].omega;
+    al[i] = sc[s0 + i].alpha;
+    act[i] = sc[s0 + i].active;
+    rr[i][0] = 0.0;
+  }
   double (*red)[MAX_SYS][1] = nullptr;
   if constexpr (SEG) red = seg_sums<8 * S::RPW, 1>();
   for (int c = 0; c < ncolors; ++c) {
@@ -494,40 +638,57 @@ __global__ void __launch_bounds__(256)
       const bool live = pos < sl.end;
       const int row = live ? __ldg(perm + pos) : 0;
       const double2 dg = live ? __ldg(dkm + pos) : make_double2(1.0, 0.0);
-      int sid = s;
+      int sid = s0;
       if constexpr (SEG) {
         sid = live ? (int)__ldg(seg + row) : 0;
-        om = sc[sid].omega;
-        al = sc[sid].alpha;
-        act = sc[sid].active;
+        om[0] = sc[sid].omega;
+        al[0] = sc[sid].alpha;
+        act[0] = sc[sid].active;
       }
-      V ri = live ? r[(long)row * NS + s] : Cx<T>::make(0, 0);
-      if (rprev && live && g == 0) rprev[(long)row * NS + s] = ri;  // flexible COCG keeps r_k
-      if (live && update && act && g == 0) {  // x += alpha p follows in the p update
-        const V qi = q[(long)row * NS + s];
-        ri = Cx<T>::make((T)((double)ri.x - (al.x * (double)qi.x - al.y * (double)qi.y)),
-                         (T)((double)ri.y - (al.x * (double)qi.y + al.y * (double)qi.x)));
-        r[(long)row * NS + s] = ri;
-      }
-      if (live && g == 0) {
-        const double v = (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
-        if constexpr (SEG) red[slot][sid][0] += v;
-        else rr += v;
-      }
-      PT t1x = 0, t1y = 0, t2x = 0, t2y = 0;
-      if (live)
-        row_gather<PT, NS, S::G>(lcol, lkm, y, __ldg(lptr + pos) + g, __ldg(lptr + pos + 1), s, t1x, t1y, t2x, t2y);
+      V ri[SPL];
+      if (live) load_spl<V, NS, SPL, false>(r + (long)row * NS + s0, ri);
+      else
 #pragma unroll
-      for (int m = NS; m < S::LPR; m <<= 1) {
-        t1x += shfl_xor(t1x, m); t1y += shfl_xor(t1y, m);
-        t2x += shfl_xor(t2x, m); t2y += shfl_xor(t2y, m);
+        for (int i = 0; i < SPL; ++i) ri[i] = Cx<T>::make(0, 0);
+      if (rprev && live && g == 0) store_spl<V, SPL>(rprev + (long)row * NS + s0, ri);  // flexible COCG keeps r_k
+      if (live && update && g == 0) {  // x += alpha p follows in the p update
+        V qi[SPL];
+        load_spl<V, NS, SPL, false>(q + (long)row * NS + s0, qi);
+        bool any = false;
+#pragma unroll
+        for (int i = 0; i < SPL; ++i)
+          if (act[i]) {
+            any = true;
+            ri[i] = Cx<T>::make((T)((double)ri[i].x - (al[i].x * (double)qi[i].x - al[i].y * (double)qi[i].y)),
+                                (T)((double)ri[i].y - (al[i].x * (double)qi[i].y + al[i].y * (double)qi[i].x)));
+          }
+        if (any) store_spl<V, SPL>(r + (long)row * NS + s0, ri);
       }
+      if (live && g == 0)
+#pragma unroll
+        for (int i = 0; i < SPL; ++i) {
+          const double v = (double)ri[i].x * (double)ri[i].x + (double)ri[i].y * (double)ri[i].y;
+          if constexpr (SEG) red[slot][sid][0] += v;
+          else rr[i][0] += v;
+        }
+      PT t1x[SPL], t1y[SPL], t2x[SPL], t2y[SPL];
+#pragma unroll
+      for (int i = 0; i < SPL; ++i) t1x[i] = t1y[i] = t2x[i] = t2y[i] = 0;
+      if (live)
+        row_gather_spl<PT, NS, S::G, SPL>(lcol, lkm, y, __ldg(lptr + pos) + g, __ldg(lptr + pos + 1), s0, t1x, t1y,
+                                          t2x, t2y);
+      group_sum<PT, SPL, S::NG, S::LPR>(t1x, t1y, t2x, t2y);
       if (live && g == 0) {
-        const PT o = (PT)om;
-        const PT wx = (PT)ri.x - (t1x - o * t2y), wy = (PT)ri.y - (t1y + o * t2x);
-        const double2 dd = ssor_dd(dg, om, sd);
-        const PT dx = (PT)dd.x, dy = (PT)dd.y;
-        y[(long)row * NS + s] = Cx<PT>::make(wx * dx - wy * dy, wx * dy + wy * dx);
+        PV yo[SPL];
+#pragma unroll
+        for (int i = 0; i < SPL; ++i) {
+          const PT o = (PT)om[i];
+          const PT wx = (PT)ri[i].x - (t1x[i] - o * t2y[i]), wy = (PT)ri[i].y - (t1y[i] + o * t2x[i]);
+          const double2 dd = ssor_dd(dg, om[i], sd);
+          const PT dx = (PT)dd.x, dy = (PT)dd.y;
+          yo[i] = Cx<PT>::make(wx * dx - wy * dy, wx * dy + wy * dx);
+        }
+        store_spl<PV, SPL>(y + (long)row * NS + s0, yo);
       }
     }
     grid.sync();
@@ -535,17 +696,14 @@ __global__ void __launch_bounds__(256)
   if constexpr (SEG) {
     seg_partials<8 * S::RPW, 1>(red, part);
   } else {
-#pragma unroll
-    for (int m = S::LPR; m < 32; m <<= 1) rr += __shfl_xor_sync(0xffffffffu, rr, m);
-    double v[1] = {rr};
-    block_partials<NS, 1>(v, part);
+    block_partials_spl<NS, SPL, S::LPR, 1>(rr, s0, g == 0, part);
   }
 }
 
 // Backward sweep in place on z (the forward sweep's y).  r (COCG type T) is read
 // only by packed batches, for their per-mesh rho = r^T z.
 template <class T, class PT, int NS, bool SEG = false>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
     k_bwd_mc(const int32_t* __restrict__ uptr, const int32_t* __restrict__ ucol,
              const typename Cx<PT>::V* __restrict__ ukm, int n, const typename Cx<T>::V* __restrict__ r,
              typename Cx<PT>::V* __restrict__ z, const int32_t* __restrict__ perm,
@@ -555,14 +713,20 @@ __global__ void __launch_bounds__(256)
   using V = typename Cx<T>::V;
   using PV = typename Cx<PT>::V;
   using S = McShape<NS, SEG>;
+  constexpr int SPL = S::SPL;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
-  const int lane = threadIdx.x & 31, sub = lane / S::LPR, s = lane % NS, g = (lane % S::LPR) / NS;
+  const int lane = threadIdx.x & 31, sub = lane / S::LPR, ql = lane % S::LPR;
+  const int s0 = (ql % S::NG) * SPL, g = ql / S::NG;
   const int wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;  // warp in block, warps per block
-  const int slot = (threadIdx.x >> 5) * S::RPW + sub;
-  double om = sc[s].omega;
-  double rx = 0.0, ry = 0.0;
+  const int slot = wib * S::RPW + sub;
+  double om[SPL], rh[SPL][4];
+#pragma unroll
+  for (int i = 0; i < SPL; ++i) {
+    om[i] = sc[s0 + i].omega;
+    rh[i][0] = rh[i][1] = rh[i][2] = rh[i][3] = 0.0;
+  }
   double (*red)[MAX_SYS][4] = nullptr;
   if constexpr (SEG) red = seg_sums<8 * S::RPW, 4>();
   for (int c = ncolors - 1; c >= 0; --c) {
@@ -573,39 +737,42 @@ __global__ void __launch_bounds__(256)
       const bool live = pos < sl.end;
       const int row = live ? __ldg(perm + pos) : 0;
       const double2 dg = live ? __ldg(dkm + pos) : make_double2(1.0, 0.0);
-      int sid = s;
+      int sid = s0;
       if constexpr (SEG) {
         sid = live ? (int)__ldg(seg + row) : 0;
-        om = sc[sid].omega;
+        om[0] = sc[sid].omega;
       }
-      PT t1x = 0, t1y = 0, t2x = 0, t2y = 0;
-      if (live)
-        row_gather<PT, NS, S::G>(ucol, ukm, z, __ldg(uptr + pos) + g, __ldg(uptr + pos + 1), s, t1x, t1y, t2x, t2y);
+      PT t1x[SPL], t1y[SPL], t2x[SPL], t2y[SPL];
 #pragma unroll
-      for (int m = NS; m < S::LPR; m <<= 1) {
-        t1x += shfl_xor(t1x, m); t1y += shfl_xor(t1y, m);
-        t2x += shfl_xor(t2x, m); t2y += shfl_xor(t2y, m);
-      }
+      for (int i = 0; i < SPL; ++i) t1x[i] = t1y[i] = t2x[i] = t2y[i] = 0;
+      if (live)
+        row_gather_spl<PT, NS, S::G, SPL>(ucol, ukm, z, __ldg(uptr + pos) + g, __ldg(uptr + pos + 1), s0, t1x, t1y,
+                                          t2x, t2y);
+      group_sum<PT, SPL, S::NG, S::LPR>(t1x, t1y, t2x, t2y);
       if (live && g == 0) {
-        PV zi = z[(long)row * NS + s];
-        if constexpr (!SEG) {
-          // rho = r^T z = y^T D' y (U = L^T, D' = sd diag(A), y = the forward sweep's output in z)
-          const double dx = sd * dg.x, dy = sd * om * dg.y;
-          const double y2x = (double)zi.x * (double)zi.x - (double)zi.y * (double)zi.y;
-          const double y2y = 2.0 * (double)zi.x * (double)zi.y;
-          rx += dx * y2x - dy * y2y;
-          ry += dx * y2y + dy * y2x;
+        PV zi[SPL];
+        load_spl<PV, NS, SPL, false>(z + (long)row * NS + s0, zi);
+#pragma unroll
+        for (int i = 0; i < SPL; ++i) {
+          if constexpr (!SEG) {
+            // rho = r^T z = y^T D' y (U = L^T, D' = sd diag(A), y = the forward sweep's output in z)
+            const double dx = sd * dg.x, dy = sd * om[i] * dg.y;
+            const double y2x = (double)zi[i].x * (double)zi[i].x - (double)zi[i].y * (double)zi[i].y;
+            const double y2y = 2.0 * (double)zi[i].x * (double)zi[i].y;
+            rh[i][0] += dx * y2x - dy * y2y;
+            rh[i][1] += dx * y2y + dy * y2x;
+          }
+          const PT o = (PT)om[i];
+          const PT swx = t1x[i] - o * t2y[i], swy = t1y[i] + o * t2x[i];
+          const double2 dd = ssor_dd(dg, om[i], sd);
+          const PT dx = (PT)dd.x, dy = (PT)dd.y;
+          zi[i] = Cx<PT>::make(zi[i].x - (dx * swx - dy * swy), zi[i].y - (dx * swy + dy * swx));
         }
-        const PT o = (PT)om;
-        const PT swx = t1x - o * t2y, swy = t1y + o * t2x;
-        const double2 dd = ssor_dd(dg, om, sd);
-        const PT dx = (PT)dd.x, dy = (PT)dd.y;
-        zi = Cx<PT>::make(zi.x - (dx * swx - dy * swy), zi.y - (dx * swy + dy * swx));
-        z[(long)row * NS + s] = zi;
+        store_spl<PV, SPL>(z + (long)row * NS + s0, zi);
         if constexpr (SEG) {  // packed batches: per-mesh rho = r^T z
-          const V ri = r[(long)row * NS + s];
-          red[slot][sid][0] += (double)ri.x * (double)zi.x - (double)ri.y * (double)zi.y;
-          red[slot][sid][1] += (double)ri.x * (double)zi.y + (double)ri.y * (double)zi.x;
+          const V ri = r[(long)row * NS + s0];
+          red[slot][sid][0] += (double)ri.x * (double)zi[0].x - (double)ri.y * (double)zi[0].y;
+          red[slot][sid][1] += (double)ri.x * (double)zi[0].y + (double)ri.y * (double)zi[0].x;
         }
       }
     }
@@ -614,13 +781,7 @@ __global__ void __launch_bounds__(256)
   if constexpr (SEG) {
     seg_partials<8 * S::RPW, 4>(red, part);
   } else {
-#pragma unroll
-    for (int m = S::LPR; m < 32; m <<= 1) {
-      rx += __shfl_xor_sync(0xffffffffu, rx, m);
-      ry += __shfl_xor_sync(0xffffffffu, ry, m);
-    }
-    double v[4] = {rx, ry, 0.0, 0.0};
-    block_partials<NS, 4>(v, part);
+    block_partials_spl<NS, SPL, S::LPR, 4>(rh, s0, g == 0, part);
   }
 }
 
@@ -668,7 +829,7 @@ __global__ void k_grad_t(int node, const int32_t* __restrict__ nptr, const int32
 // part (backward, nullable): partial sums of t^T y over the final y, the share
 // r^T G u of rho = r^T (z + G u) (since t = G^T r), slots 0, 1.
 template <class T, int NS, bool SEG>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
     k_nsweep_mc(const int32_t* __restrict__ xptr, const int32_t* __restrict__ xcol,
                 const typename Cx<T>::V* __restrict__ xkm, const typename Cx<T>::V* __restrict__ t,
                 typename Cx<T>::V* __restrict__ y, const typename Cx<T>::V* __restrict__ dd,
@@ -677,13 +838,19 @@ __global__ void __launch_bounds__(256)
                 int backward, double* __restrict__ part) {
   using V = typename Cx<T>::V;
   using S = McShape<NS, SEG>;
+  constexpr int SPL = S::SPL;
   static_assert(!SEG || NS == 1, "packed batches hold one system per row");
   if (ctrl->done) return;
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
-  const int lane = threadIdx.x & 31, sub = lane / S::LPR, s = lane % NS, g = (lane % S::LPR) / NS;
+  const int lane = threadIdx.x & 31, sub = lane / S::LPR, ql = lane % S::LPR;
+  const int s0 = (ql % S::NG) * SPL, g = ql / S::NG;
   const int wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;  // warp in block, warps per block
-  double om = sc[s].omega;
-  double tx = 0.0, ty = 0.0;
+  double om[SPL], tu[SPL][4];
+#pragma unroll
+  for (int i = 0; i < SPL; ++i) {
+    om[i] = sc[s0 + i].omega;
+    tu[i][0] = tu[i][1] = tu[i][2] = tu[i][3] = 0.0;
+  }
   for (int cc = 0; cc < ncolors; ++cc) {
     const int c = backward ? ncolors - 1 - cc : cc;
     const int p0 = cptr[c], p1 = cptr[c + 1];
@@ -692,46 +859,53 @@ __global__ void __launch_bounds__(256)
       const int pos = pos0 + sub;
       const bool live = pos < sl.end;
       const int row = live ? __ldg(perm + pos) : 0;
-      if constexpr (SEG) om = sc[live ? (int)__ldg(seg + row) : 0].omega;
-      T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
-      if (live)
-        row_gather<T, NS, S::G>(xcol, xkm, y, __ldg(xptr + pos) + g, __ldg(xptr + pos + 1), s, t1x, t1y, t2x, t2y);
+      if constexpr (SEG) om[0] = sc[live ? (int)__ldg(seg + row) : 0].omega;
+      T t1x[SPL], t1y[SPL], t2x[SPL], t2y[SPL];
 #pragma unroll
-      for (int m = NS; m < S::LPR; m <<= 1) {
-        t1x += shfl_xor(t1x, m); t1y += shfl_xor(t1y, m);
-        t2x += shfl_xor(t2x, m); t2y += shfl_xor(t2y, m);
-      }
+      for (int i = 0; i < SPL; ++i) t1x[i] = t1y[i] = t2x[i] = t2y[i] = 0;
+      if (live)
+        row_gather_spl<T, NS, S::G, SPL>(xcol, xkm, y, __ldg(xptr + pos) + g, __ldg(xptr + pos + 1), s0, t1x, t1y,
+                                         t2x, t2y);
+      group_sum<T, SPL, S::NG, S::LPR>(t1x, t1y, t2x, t2y);
       if (live && g == 0) {
-        const T o = (T)om;
-        const T sx = t1x - o * t2y, sy = t1y + o * t2x;
-        const V d = dd[(long)row * NS + s];
+        const long base = (long)row * NS + s0;
+        V d[SPL], yo[SPL];
+        load_spl<V, NS, SPL, false>(dd + base, d);
         if (!backward) {
-          const V ti = t[(long)row * NS + s];
-          const T wx = ti.x - sx, wy = ti.y - sy;
-          y[(long)row * NS + s] = Cx<T>::make(wx * d.x - wy * d.y, wx * d.y + wy * d.x);
+          V ti[SPL];
+          load_spl<V, NS, SPL, false>(t + base, ti);
+#pragma unroll
+          for (int i = 0; i < SPL; ++i) {
+            const T o = (T)om[i];
+            const T sx = t1x[i] - o * t2y[i], sy = t1y[i] + o * t2x[i];
+            const T wx = ti[i].x - sx, wy = ti[i].y - sy;
+            yo[i] = Cx<T>::make(wx * d[i].x - wy * d[i].y, wx * d[i].y + wy * d[i].x);
+          }
         } else {
-          const V yi = y[(long)row * NS + s];
-          const V yn = Cx<T>::make(yi.x - (d.x * sx - d.y * sy), yi.y - (d.x * sy + d.y * sx));
-          y[(long)row * NS + s] = yn;
+          V yi[SPL];
+          load_spl<V, NS, SPL, false>(y + base, yi);
+#pragma unroll
+          for (int i = 0; i < SPL; ++i) {
+            const T o = (T)om[i];
+            const T sx = t1x[i] - o * t2y[i], sy = t1y[i] + o * t2x[i];
+            yo[i] = Cx<T>::make(yi[i].x - (d[i].x * sx - d[i].y * sy), yi[i].y - (d[i].x * sy + d[i].y * sx));
+          }
           if (part) {
-            const V ti = t[(long)row * NS + s];
-            tx += (double)ti.x * (double)yn.x - (double)ti.y * (double)yn.y;
-            ty += (double)ti.x * (double)yn.y + (double)ti.y * (double)yn.x;
+            V ti[SPL];
+            load_spl<V, NS, SPL, false>(t + base, ti);
+#pragma unroll
+            for (int i = 0; i < SPL; ++i) {
+              tu[i][0] += (double)ti[i].x * (double)yo[i].x - (double)ti[i].y * (double)yo[i].y;
+              tu[i][1] += (double)ti[i].x * (double)yo[i].y + (double)ti[i].y * (double)yo[i].x;
+            }
           }
         }
+        store_spl<V, SPL>(y + base, yo);
       }
     }
     grid.sync();
   }
-  if (part) {  // uniform over the grid
-#pragma unroll
-    for (int m = S::LPR; m < 32; m <<= 1) {
-      tx += __shfl_xor_sync(0xffffffffu, tx, m);
-      ty += __shfl_xor_sync(0xffffffffu, ty, m);
-    }
-    double v[4] = {tx, ty, 0.0, 0.0};
-    block_partials<NS, 4>(v, part);
-  }
+  if (part) block_partials_spl<NS, SPL, S::LPR, 4>(tu, s0, g == 0, part);  // uniform over the grid
 }
 
 // Packed batches: the lanes of a warp hold rows of possibly different meshes;
@@ -906,23 +1080,30 @@ __global__ void k_pupd(int n, const typename Cx<PT>::V* __restrict__ z, typename
 
 // q = A p (COCG13_single.f90:273-288) and p^T q partial sums.  With
 // resid_mode, computes r = b - A x in FP64 instead and ||r||^2 (and ||b||^2).
-// RPW rows per warp: lane = sub * (32/RPW) + g * NS + s, so rows of ~16
-// nonzeros do not leave half a warp idle (RPW is picked by tune_spmv).
-template <class T, int NS, int RPW = 1, bool SEG = false>
-__global__ void __launch_bounds__(256)
+// RPW rows per warp, SPL systems per lane: lane = sub * (32/RPW) + g * (NS/SPL) +
+// s0/SPL, so rows of ~16 nonzeros do not leave half a warp idle (RPW and SPL are
+// picked by tune_spmv; SPL = 4 at 16 systems gives 8 rows per warp).
+template <class T, int NS, int RPW = 1, bool SEG = false, int SPL = 1>
+__global__ void __launch_bounds__(256, (SPL > 1 ? MC_MIN_BLOCKS : 0))
     k_spmv(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
            const typename Cx<T>::V* __restrict__ km, int n, const typename Cx<T>::V* __restrict__ p,
            typename Cx<T>::V* __restrict__ q, const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl,
            double* __restrict__ part, const typename Cx<T>::V* __restrict__ bvec, const uint8_t* __restrict__ seg) {
   using V = typename Cx<T>::V;
-  static_assert(NS * RPW <= 32, "rows per warp times systems must fit a warp");
-  static_assert(!SEG || NS == 1, "packed batches hold one system per row");
+  constexpr int NG = NS / SPL;   // lanes of a row that hold different systems
+  static_assert(NG * RPW <= 32, "rows per warp times lanes per row must fit a warp");
+  static_assert(!SEG || (NS == 1 && SPL == 1), "packed batches hold one system per row");
   if (ctrl && ctrl->done) return;
   constexpr int LPR = 32 / RPW;  // lanes per row
-  constexpr int G = LPR / NS;    // entry groups per row
-  const int lane = threadIdx.x & 31, sub = lane / LPR, s = lane % NS, g = (lane % LPR) / NS;
-  double om = sc[s].omega;
-  double ax = 0.0, ay = 0.0, bb = 0.0;
+  constexpr int G = LPR / NG;    // entry groups per row
+  const int lane = threadIdx.x & 31, sub = lane / LPR, ql = lane % LPR;
+  const int s0 = (ql % NG) * SPL, g = ql / NG;
+  double om[SPL];
+#pragma unroll
+  for (int i = 0; i < SPL; ++i) om[i] = sc[s0 + i].omega;
+  double acc[SPL][3];
+#pragma unroll
+  for (int i = 0; i < SPL; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.0;
   double (*red)[MAX_SYS][3] = nullptr;
   if constexpr (SEG) red = seg_sums<8 * RPW, 3>();
   const int slot = (threadIdx.x >> 5) * RPW + sub;
@@ -931,59 +1112,54 @@ __global__ void __launch_bounds__(256)
   for (int row0 = sl.begin + wib * RPW; row0 < sl.end; row0 += nwb * RPW) {
     const int row = row0 + sub;
     const bool live = row < sl.end;
-    int sid = s;
+    int sid = s0;
     if constexpr (SEG) {
       sid = live ? (int)__ldg(seg + row) : 0;
-      om = sc[sid].omega;
+      om[0] = sc[sid].omega;
     }
     const int k0 = live ? rowptr[row] : 0, k1 = live ? rowptr[row + 1] : 0;
-    T t1x = 0, t1y = 0, t2x = 0, t2y = 0;
-    row_gather<T, NS, G>(col, km, p, k0 + g, k1, s, t1x, t1y, t2x, t2y);
+    T t1x[SPL], t1y[SPL], t2x[SPL], t2y[SPL];
 #pragma unroll
-    for (int m = NS; m < LPR; m <<= 1) {
-      t1x += shfl_xor(t1x, m); t1y += shfl_xor(t1y, m);
-      t2x += shfl_xor(t2x, m); t2y += shfl_xor(t2y, m);
-    }
+    for (int i = 0; i < SPL; ++i) t1x[i] = t1y[i] = t2x[i] = t2y[i] = 0;
+    row_gather_spl<T, NS, G, SPL>(col, km, p, k0 + g, k1, s0, t1x, t1y, t2x, t2y);
+    group_sum<T, SPL, NG, LPR>(t1x, t1y, t2x, t2y);
     if (g == 0 && live) {
-      const T o = (T)om;
-      const V qi = Cx<T>::make(t1x - o * t2y, t1y + o * t2x);
-      double e0, e1 = 0.0, e2 = 0.0;
+      const long base = (long)row * NS + s0;
+      V qi[SPL], own[SPL];
+#pragma unroll
+      for (int i = 0; i < SPL; ++i) {
+        const T o = (T)om[i];
+        qi[i] = Cx<T>::make(t1x[i] - o * t2y[i], t1y[i] + o * t2x[i]);
+      }
       if (bvec) {  // r = b - A x
-        const V bi = bvec[(long)row * NS + s];
-        const V ri = Cx<T>::make(bi.x - qi.x, bi.y - qi.y);
-        q[(long)row * NS + s] = ri;
-        e0 = (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
-        e2 = (double)bi.x * (double)bi.x + (double)bi.y * (double)bi.y;
+        load_spl<V, NS, SPL, false>(bvec + base, own);
+#pragma unroll
+        for (int i = 0; i < SPL; ++i) {
+          const V ri = Cx<T>::make(own[i].x - qi[i].x, own[i].y - qi[i].y);
+          qi[i] = ri;
+          const double e0 = (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
+          const double e2 = (double)own[i].x * (double)own[i].x + (double)own[i].y * (double)own[i].y;
+          if constexpr (SEG) { red[slot][sid][0] += e0; red[slot][sid][2] += e2; }
+          else { acc[i][0] += e0; acc[i][2] += e2; }
+        }
       } else {
-        q[(long)row * NS + s] = qi;
-        const V pi = p[(long)row * NS + s];
-        e0 = (double)pi.x * (double)qi.x - (double)pi.y * (double)qi.y;
-        e1 = (double)pi.x * (double)qi.y + (double)pi.y * (double)qi.x;
+        load_spl<V, NS, SPL, false>(p + base, own);
+#pragma unroll
+        for (int i = 0; i < SPL; ++i) {
+          const double e0 = (double)own[i].x * (double)qi[i].x - (double)own[i].y * (double)qi[i].y;
+          const double e1 = (double)own[i].x * (double)qi[i].y + (double)own[i].y * (double)qi[i].x;
+          if constexpr (SEG) { red[slot][sid][0] += e0; red[slot][sid][1] += e1; }
+          else { acc[i][0] += e0; acc[i][1] += e1; }
+        }
       }
-      if constexpr (SEG) {
-        red[slot][sid][0] += e0;
-        red[slot][sid][1] += e1;
-        red[slot][sid][2] += e2;
-      } else {
-        ax += e0;
-        ay += e1;
-        bb += e2;
-      }
+      store_spl<V, SPL>(q + base, qi);
     }
   }
   if constexpr (SEG) {
     seg_partials<8 * RPW, 3>(red, part);
     return;
   }
-  // fold the RPW rows of the warp onto lanes 0..NS-1
-#pragma unroll
-  for (int m = LPR; m < 32; m <<= 1) {
-    ax += shfl_xor(ax, m);
-    ay += shfl_xor(ay, m);
-    bb += shfl_xor(bb, m);
-  }
-  double v[3] = {ax, ay, bb};
-  block_partials<NS, 3>(v, part);
+  block_partials_spl<NS, SPL, LPR, 3>(acc, s0, g == 0, part);
 }
 
 // ------------------------------------------------------------------ scalar kernels
@@ -1317,23 +1493,52 @@ struct Inner<float, NS> {
   static const V* UKM(afem_ctx*, SolverWork* w) { return w->mc_ukmf.p; }
 };
 
+// Co-resident blocks of a kernel on this device (256 threads), at most `cap`: a
+// persistent grid of that size runs in one wave with every block's slice of rows.
+template <class K>
+int one_wave_grid(afem_ctx* c, K kernel, int cap) {
+  int per_sm = 0;
+  AFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0));
+  return std::max(1, std::min(cap, std::max(1, per_sm) * c->num_sms));
+}
+
+// The SpMV variants: rpw rows per warp with a lane per system (1, 2, 4), or, at 16
+// systems, 8 rows per warp with 4 systems per lane (rpw = 8).  Returns the grid it
+// used (the number of partial sums its consumer adds).
 template <class T, int NS, bool SEG>
-void launch_spmv(afem_ctx* c, SolverWork* w, int rpw, const typename Cx<T>::V* km, const typename Cx<T>::V* p,
-                 typename Cx<T>::V* q, const Ctrl* ctrl, const typename Cx<T>::V* bvec) {
+int launch_spmv(afem_ctx* c, SolverWork* w, int rpw, const typename Cx<T>::V* km, const typename Cx<T>::V* p,
+                typename Cx<T>::V* q, const Ctrl* ctrl, const typename Cx<T>::V* bvec) {
   cudaStream_t s = c->stream;
   const int n = w->n;
   const int32_t* rp = c->rowptr.p;
   const int32_t* cl = c->col.p;
   const uint8_t* sg = SEG ? c->seg_of_row.p : nullptr;
-  if (rpw == 4 && NS * 4 <= 32)
-    k_spmv<T, NS, (NS * 4 <= 32 ? 4 : 1), SEG><<<w->nblocks, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p,
-                                                                           bvec, sg);
-  else if (rpw == 2 && NS * 2 <= 32)
-    k_spmv<T, NS, (NS * 2 <= 32 ? 2 : 1), SEG><<<w->nblocks, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p,
-                                                                           bvec, sg);
-  else
-    k_spmv<T, NS, 1, SEG><<<w->nblocks, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p, bvec, sg);
+  const int vi = rpw == 8 ? 3 : rpw == 4 ? 2 : rpw == 2 ? 1 : 0;
+  int& grid = w->spmv_grid[sizeof(T) == 8 ? 0 : 1][vi];
+  if constexpr (NS == 16 && !SEG) {
+    if (rpw == 8) {  // AFEM_MC_SPL systems per lane, 2 * AFEM_MC_SPL rows per warp
+      auto k = k_spmv<T, NS, 2 * AFEM_MC_SPL, SEG, AFEM_MC_SPL>;
+      if (!grid) grid = one_wave_grid(c, k, w->nblocks);
+      k<<<grid, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p, bvec, sg);
+      count_launch();
+      return grid;
+    }
+  }
+  if (rpw == 4 && NS * 4 <= 32) {
+    auto k = k_spmv<T, NS, (NS * 4 <= 32 ? 4 : 1), SEG>;
+    if (!grid) grid = one_wave_grid(c, k, w->nblocks);
+    k<<<grid, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p, bvec, sg);
+  } else if (rpw == 2 && NS * 2 <= 32) {
+    auto k = k_spmv<T, NS, (NS * 2 <= 32 ? 2 : 1), SEG>;
+    if (!grid) grid = one_wave_grid(c, k, w->nblocks);
+    k<<<grid, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p, bvec, sg);
+  } else {
+    auto k = k_spmv<T, NS, 1, SEG>;
+    if (!grid) grid = one_wave_grid(c, k, w->nblocks);
+    k<<<grid, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p, bvec, sg);
+  }
   count_launch();
+  return grid;
 }
 
 // Rows-per-warp autotuner: times each variant on this matrix (q = A p with the
@@ -1345,20 +1550,21 @@ int tune_spmv(afem_ctx* c, SolverWork* w) {
   using I = Inner<T, NS>;
   int& slot = sizeof(T) == 8 ? w->rpw64 : w->rpw32;
   if (slot) return slot;
+  auto valid = [](int rpw) { return rpw == 8 ? (NS == 16 && !SEG) : NS * rpw <= 32; };
   if (c->spmv_rpw > 0) {  // pinned by the caller: the same reduction order in every process
-    slot = NS * c->spmv_rpw <= 32 ? c->spmv_rpw : 1;
+    slot = valid(c->spmv_rpw) ? c->spmv_rpw : 1;
     return slot;
   }
   cudaStream_t s = c->stream;
   cudaEvent_t a, b;
   AFEM_CUDA(cudaEventCreate(&a));
   AFEM_CUDA(cudaEventCreate(&b));
-  const int cand[3] = {1, 2, 4};
-  float tbest[3] = {1e30f, 1e30f, 1e30f};
+  const int cand[4] = {1, 2, 4, 8};
+  float tbest[4] = {1e30f, 1e30f, 1e30f, 1e30f};
   for (int round = 0; round < 3; ++round)
-    for (int ci = 0; ci < 3; ++ci) {
+    for (int ci = 0; ci < 4; ++ci) {
       const int rpw = cand[ci];
-      if (NS * rpw > 32) break;
+      if (!valid(rpw)) continue;
       launch_spmv<T, NS, SEG>(c, w, rpw, I::KM(c, w), I::P(w), I::Q(w), nullptr, nullptr);  // warm
       AFEM_CUDA(cudaEventRecord(a, s));
       for (int k = 0; k < 3; ++k) launch_spmv<T, NS, SEG>(c, w, rpw, I::KM(c, w), I::P(w), I::Q(w), nullptr, nullptr);
@@ -1370,7 +1576,7 @@ int tune_spmv(afem_ctx* c, SolverWork* w) {
     }
   float best = 1e30f;
   int pick = 1;
-  for (int ci = 0; ci < 3; ++ci)
+  for (int ci = 0; ci < 4; ++ci)
     if (tbest[ci] < best * 0.97f) { best = tbest[ci]; pick = cand[ci]; }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
@@ -1477,10 +1683,10 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
       fold_grad ? (const PV*)P::HY(w) : (const PV*)nullptr);
   count_launch();
   if (ev) AFEM_CUDA(cudaEventRecord(ev[6], s));
-  launch_spmv<T, NS, SEG>(c, w, sizeof(T) == 8 ? w->rpw64 : w->rpw32, I::KM(c, w), (const V*)I::P(w), I::Q(w),
-                          w->ctrl.p, (const V*)nullptr);
+  const int spmv_grid = launch_spmv<T, NS, SEG>(c, w, sizeof(T) == 8 ? w->rpw64 : w->rpw32, I::KM(c, w),
+                                                (const V*)I::P(w), I::Q(w), w->ctrl.p, (const V*)nullptr);
   if (ev) AFEM_CUDA(cudaEventRecord(ev[7], s));
-  k_scal_pq<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, w->nblocks, nsys);
+  k_scal_pq<<<1, 32 * MAX_SYS, 0, s>>>(w->sc.p, w->ctrl.p, w->part.p, spmv_grid, nsys);
   count_launch();
 }
 

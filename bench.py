@@ -496,6 +496,20 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+_PINNED = []  # pinned host tensors behind the numpy views handed out by _pinned
+
+
+def _pinned(torch, a):
+    """A pinned (page-locked) host copy of a, so the host->device copies of the e2e pass are DMA copies."""
+    a = np.ascontiguousarray(a)
+    t = torch.empty(a.shape, dtype=getattr(torch, {"float64": "float64", "int32": "int32", "complex128": "complex128"}[
+        str(a.dtype)]), pin_memory=True)
+    out = t.numpy()
+    out[...] = a
+    _PINNED.append(t)
+    return out
+
+
 def plain_same_gpu(fw, job, cap):
     """The reference's solver (COCG13_single: FP64, natural row order) with SSOR and with its
     diagonal-modified IC(0), system 0 of the workload alone, capped at `cap` iterations."""

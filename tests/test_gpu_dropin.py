@@ -107,6 +107,11 @@ def test_ctl_utm_sites_match_xyz_sites(gpulib, oracle, short_dir):
     from actfemtide_b200.forward import Forward
     m = synth.tidal_box(4, 4, 6, seed=3, site_grid=(-6.0, 0.0, 6.0), half_km=12.0)
     m.freqs = np.array([1.0 / 44714.0])
+    # sites strictly inside tetrahedra: on a shared face the fields of neighbouring elements differ
+    # (B is constant per element), and the converted positions differ from the xyz ones in the last bits
+    sx, sy = np.meshgrid([-4.37, 1.91, 3.23], [-2.71, 0.83, 4.57], indexing="ij")
+    sx, sy = sx.ravel(), sy.ravel()
+    m.sites = np.stack([sx, sy, synth.surface_z(sx, sy) - synth.SITE_DEPTH_KM], axis=1)
     of = oracle.OracleForward(m)
     zone, lon0, lat0 = 54, 139.8, 28.3
     lonlat = np.array([_lonlat_of(oracle, s[:2], zone, lon0, lat0) for s in m.sites])
