@@ -10,8 +10,9 @@
 //   a_ij = K_ij/(s_i s_j), b_ij = omega M_ij/(s_i s_j)
 //   h <- h + relu(X W_l + c_l)   (l = 0..5, GEMM 144 x 48 on the tensor cores)
 //   z_i = r_i/s_i^2 + rms * (o_i0 + i o_i1)/s_i,  o = h W_out  (Jacobi term + learned correction)
-// One fused kernel per layer: a warp per row aggregates its neighbours into a
-// shared-memory tile, then every warp multiplies its 16 x 144 tile by W_l with
+// One fused kernel per layer: each warp aggregates its 16 rows' neighbours (four
+// rows at a time, 8 lanes per row) into a shared-memory tile, then every warp
+// multiplies its 16 x 144 tile by W_l with
 // mma.sync.m16n8k16 (BF16 in, FP32 accumulate) and applies bias, ReLU and the
 // residual in registers.
 #include <cuda_bf16.h>
@@ -123,37 +124,78 @@ __global__ void __launch_bounds__(128)
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double om = omega[sy];
   const int r0 = blockIdx.x * ROWS + w * 16;
-  // ---- aggregate: lanes 0..23 own features 2*lane, 2*lane+1
-  for (int rr = 0; rr < 16; ++rr) {
+  // ---- aggregate: four rows of the warp's 16 at a time, 8 lanes per row, each lane
+  // owning features 6*l8 .. 6*l8+5 (words 3*l8 .. 3*l8+2 of a row's 24); two
+  // neighbours' loads in flight per row; each feature sums its neighbours in entry order
+  const int sub = lane >> 3, l8 = lane & 7;
+  for (int rr = sub; rr < 16; rr += 4) {
     const int row = r0 + rr;
     unsigned* xrow = reinterpret_cast<unsigned*>(xs + (w * 16 + rr) * XS);
     if (row < n) {
-      float aa0 = 0.f, aa1 = 0.f, ab0 = 0.f, ab1 = 0.f;
-      unsigned own = 0;
+      float aa[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, ab[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      const unsigned* own = reinterpret_cast<const unsigned*>(h_in + (base + row) * H) + 3 * l8;
+      const unsigned o0 = own[0], o1 = own[1], o2 = own[2];
       const float si = s[base + row];
-      if (lane < 24) own = reinterpret_cast<const unsigned*>(h_in + (base + row) * H)[lane];
-      for (int k = rowptr[row]; k < rowptr[row + 1]; ++k) {
-        const int j = col[k];
-        if (j == row) continue;
-        const double2 a = km[k];
-        const float sj = s[base + j];
-        const float inv = 1.0f / (si * sj);
-        const float wa = (float)a.x * inv, wb = (float)(om * a.y) * inv;
-        if (lane < 24) {
-          const float2 hj = unpack_bf16(reinterpret_cast<const unsigned*>(h_in + (base + j) * H)[lane]);
-          aa0 += wa * hj.x; aa1 += wa * hj.y;
-          ab0 += wb * hj.x; ab1 += wb * hj.y;
+      const int k1 = rowptr[row + 1];
+      int k = rowptr[row];
+      for (; k + 1 < k1; k += 2) {
+        const int ja = col[k], jb = col[k + 1];
+        const double2 ea = km[k], eb = km[k + 1];
+        const float sa = s[base + ja], sb = s[base + jb];
+        const unsigned* pa = reinterpret_cast<const unsigned*>(h_in + (base + ja) * H) + 3 * l8;
+        const unsigned* pb = reinterpret_cast<const unsigned*>(h_in + (base + jb) * H) + 3 * l8;
+        const unsigned ua[3] = {pa[0], pa[1], pa[2]}, ub[3] = {pb[0], pb[1], pb[2]};
+        if (ja != row) {
+          const float inv = 1.0f / (si * sa);
+          const float wa = (float)ea.x * inv, wb = (float)(om * ea.y) * inv;
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            const float2 hj = unpack_bf16(ua[q]);
+            aa[2 * q] += wa * hj.x; aa[2 * q + 1] += wa * hj.y;
+            ab[2 * q] += wb * hj.x; ab[2 * q + 1] += wb * hj.y;
+          }
+        }
+        if (jb != row) {
+          const float inv = 1.0f / (si * sb);
+          const float wa = (float)eb.x * inv, wb = (float)(om * eb.y) * inv;
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            const float2 hj = unpack_bf16(ub[q]);
+            aa[2 * q] += wa * hj.x; aa[2 * q + 1] += wa * hj.y;
+            ab[2 * q] += wb * hj.x; ab[2 * q + 1] += wb * hj.y;
+          }
         }
       }
-      if (lane < 24) {
-        xrow[lane] = own;
-        xrow[24 + lane] = pack_bf16(aa0, aa1);
-        xrow[48 + lane] = pack_bf16(ab0, ab1);
+      if (k < k1) {
+        const int j = col[k];
+        if (j != row) {
+          const double2 e = km[k];
+          const float inv = 1.0f / (si * s[base + j]);
+          const float wa = (float)e.x * inv, wb = (float)(om * e.y) * inv;
+          const unsigned* pj = reinterpret_cast<const unsigned*>(h_in + (base + j) * H) + 3 * l8;
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            const float2 hj = unpack_bf16(pj[q]);
+            aa[2 * q] += wa * hj.x; aa[2 * q + 1] += wa * hj.y;
+            ab[2 * q] += wb * hj.x; ab[2 * q + 1] += wb * hj.y;
+          }
+        }
       }
-    } else if (lane < 24) {
-      xrow[lane] = 0u;
-      xrow[24 + lane] = 0u;
-      xrow[48 + lane] = 0u;
+      xrow[3 * l8] = o0;
+      xrow[3 * l8 + 1] = o1;
+      xrow[3 * l8 + 2] = o2;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        xrow[24 + 3 * l8 + q] = pack_bf16(aa[2 * q], aa[2 * q + 1]);
+        xrow[48 + 3 * l8 + q] = pack_bf16(ab[2 * q], ab[2 * q + 1]);
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        xrow[3 * l8 + q] = 0u;
+        xrow[24 + 3 * l8 + q] = 0u;
+        xrow[48 + 3 * l8 + q] = 0u;
+      }
     }
   }
   __syncthreads();

@@ -200,16 +200,28 @@ __device__ __forceinline__ void row_gather(const int32_t* __restrict__ cols, con
   }
 }
 
-// The contiguous part of [p0, p1) that this block works on; its warps interleave
-// inside it.  Rows near in index are near in the mesh, so the warps of an SM
-// gather from overlapping neighbourhoods and L1 serves the repeats.
-struct Slice {
-  int begin, end;
-};
-__device__ __forceinline__ Slice block_slice(int p0, int p1) {
-  const int per = (p1 - p0 + (int)gridDim.x - 1) / (int)gridDim.x;
-  const int b = p0 + (int)blockIdx.x * per;
-  return Slice{min(b, p1), min(b + per, p1)};
+// Row schedule of the persistent kernels: [p0, p1) is cut into chunks of CH
+// rounds of the block's warps (CH * warps * RPW rows), dealt to the blocks
+// round-robin.  All SMs then work inside a band of gridDim * chunk rows that
+// moves through the range (the neighbours they gather stay in L2), and inside a
+// chunk the warps of one SM gather from overlapping neighbourhoods (L1 serves
+// the repeats).  CH = 1 is a plain grid-wide stride.
+#ifndef AFEM_SWEEP_CHUNK
+#define AFEM_SWEEP_CHUNK 2  // rounds per chunk in the multicolour sweeps
+#endif
+#ifndef AFEM_SPMV_CHUNK
+#define AFEM_SPMV_CHUNK 16  // rounds per chunk in the SpMV
+#endif
+// Calls body(pos0) for the first row of every warp round of this block; the round's
+// rows are pos0 + sub for sub < RPW, live below `end` (passed to body as well).
+template <int RPW, int CH, class F>
+__device__ __forceinline__ void for_rows(int p0, int p1, F body) {
+  const int wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;
+  const int chunk = CH * nwb * RPW;
+  for (int cb = p0 + (int)blockIdx.x * chunk; cb < p1; cb += (int)gridDim.x * chunk) {
+    const int ce = min(cb + chunk, p1);
+    for (int pos0 = cb + wib * RPW; pos0 < ce; pos0 += nwb * RPW) body(pos0, ce);
+  }
 }
 
 // Block-reduce NS-per-lane doubles into part[blockIdx][s*4 + slot]; lanes with g == 0 hold system s values.
@@ -616,8 +628,7 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
   const bool update = ctrl->iter > 0;
   const int lane = threadIdx.x & 31, sub = lane / S::LPR, ql = lane % S::LPR;
   const int s0 = (ql % S::NG) * SPL, g = ql / S::NG;
-  const int wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;  // warp in block, warps per block
-  const int slot = wib * S::RPW + sub;
+  const int slot = (threadIdx.x >> 5) * S::RPW + sub;  // this row's per-warp slot
   double om[SPL], rr[SPL][1];
   double2 al[SPL];
   bool act[SPL];
@@ -632,10 +643,9 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
   if constexpr (SEG) red = seg_sums<8 * S::RPW, 1>();
   for (int c = 0; c < ncolors; ++c) {
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    const Slice sl = block_slice(p0, p1);
-    for (int pos0 = sl.begin + wib * S::RPW; pos0 < sl.end; pos0 += nwb * S::RPW) {
+    for_rows<S::RPW, AFEM_SWEEP_CHUNK>(p0, p1, [&](int pos0, int cend) {
       const int pos = pos0 + sub;
-      const bool live = pos < sl.end;
+      const bool live = pos < cend;
       const int row = live ? __ldg(perm + pos) : 0;
       const double2 dg = live ? __ldg(dkm + pos) : make_double2(1.0, 0.0);
       int sid = s0;
@@ -690,7 +700,7 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
         }
         store_spl<PV, SPL>(y + (long)row * NS + s0, yo);
       }
-    }
+    });
     grid.sync();
   }
   if constexpr (SEG) {
@@ -719,8 +729,7 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
   const int lane = threadIdx.x & 31, sub = lane / S::LPR, ql = lane % S::LPR;
   const int s0 = (ql % S::NG) * SPL, g = ql / S::NG;
-  const int wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;  // warp in block, warps per block
-  const int slot = wib * S::RPW + sub;
+  const int slot = (threadIdx.x >> 5) * S::RPW + sub;  // this row's per-warp slot
   double om[SPL], rh[SPL][4];
 #pragma unroll
   for (int i = 0; i < SPL; ++i) {
@@ -731,10 +740,9 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
   if constexpr (SEG) red = seg_sums<8 * S::RPW, 4>();
   for (int c = ncolors - 1; c >= 0; --c) {
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    const Slice sl = block_slice(p0, p1);
-    for (int pos0 = sl.begin + wib * S::RPW; pos0 < sl.end; pos0 += nwb * S::RPW) {
+    for_rows<S::RPW, AFEM_SWEEP_CHUNK>(p0, p1, [&](int pos0, int cend) {
       const int pos = pos0 + sub;
-      const bool live = pos < sl.end;
+      const bool live = pos < cend;
       const int row = live ? __ldg(perm + pos) : 0;
       const double2 dg = live ? __ldg(dkm + pos) : make_double2(1.0, 0.0);
       int sid = s0;
@@ -775,7 +783,7 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
           red[slot][sid][1] += (double)ri.x * (double)zi[0].y + (double)ri.y * (double)zi[0].x;
         }
       }
-    }
+    });
     grid.sync();
   }
   if constexpr (SEG) {
@@ -844,7 +852,6 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
   cooperative_groups::grid_group grid = cooperative_groups::this_grid();
   const int lane = threadIdx.x & 31, sub = lane / S::LPR, ql = lane % S::LPR;
   const int s0 = (ql % S::NG) * SPL, g = ql / S::NG;
-  const int wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;  // warp in block, warps per block
   double om[SPL], tu[SPL][4];
 #pragma unroll
   for (int i = 0; i < SPL; ++i) {
@@ -854,10 +861,9 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
   for (int cc = 0; cc < ncolors; ++cc) {
     const int c = backward ? ncolors - 1 - cc : cc;
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    const Slice sl = block_slice(p0, p1);
-    for (int pos0 = sl.begin + wib * S::RPW; pos0 < sl.end; pos0 += nwb * S::RPW) {
+    for_rows<S::RPW, AFEM_SWEEP_CHUNK>(p0, p1, [&](int pos0, int cend) {
       const int pos = pos0 + sub;
-      const bool live = pos < sl.end;
+      const bool live = pos < cend;
       const int row = live ? __ldg(perm + pos) : 0;
       if constexpr (SEG) om[0] = sc[live ? (int)__ldg(seg + row) : 0].omega;
       T t1x[SPL], t1y[SPL], t2x[SPL], t2y[SPL];
@@ -902,7 +908,7 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
         }
         store_spl<V, SPL>(y + base, yo);
       }
-    }
+    });
     grid.sync();
   }
   if (part) block_partials_spl<NS, SPL, S::LPR, 4>(tu, s0, g == 0, part);  // uniform over the grid
@@ -1107,11 +1113,9 @@ __global__ void __launch_bounds__(256, (SPL > 1 ? MC_MIN_BLOCKS : 0))
   double (*red)[MAX_SYS][3] = nullptr;
   if constexpr (SEG) red = seg_sums<8 * RPW, 3>();
   const int slot = (threadIdx.x >> 5) * RPW + sub;
-  const Slice sl = block_slice(0, n);
-  const int wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;
-  for (int row0 = sl.begin + wib * RPW; row0 < sl.end; row0 += nwb * RPW) {
+  for_rows<RPW, AFEM_SPMV_CHUNK>(0, n, [&](int row0, int cend) {
     const int row = row0 + sub;
-    const bool live = row < sl.end;
+    const bool live = row < cend;
     int sid = s0;
     if constexpr (SEG) {
       sid = live ? (int)__ldg(seg + row) : 0;
@@ -1154,7 +1158,7 @@ __global__ void __launch_bounds__(256, (SPL > 1 ? MC_MIN_BLOCKS : 0))
       }
       store_spl<V, SPL>(q + base, qi);
     }
-  }
+  });
   if constexpr (SEG) {
     seg_partials<8 * RPW, 3>(red, part);
     return;
@@ -1909,7 +1913,7 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
       snprintf(nb, sizeof nb, "cocg_bwd_sweep%s_%s_%s%d", mcs ? "_mc" : "", tag, kind, cnt);
       snprintf(nh, sizeof nh, "cocg_nodal_correction_%s_%s%d", tag, kind, cnt);
       snprintf(np_, sizeof np_, "cocg_p_update_%s_%s%d", tag, kind, cnt);
-      snprintf(ns_, sizeof ns_, "cocg_spmv_%s_%s%d", tag, kind, cnt);
+      snprintf(ns_, sizeof ns_, "cocg_spmv_%s_%s%d_rpw%d", tag, kind, cnt, sizeof(T) == 8 ? w->rpw64 : w->rpw32);
       for (int k = 0; k < executed; ++k) {
         float a = 0, b = 0, h = 0, d = 0, e = 0;
         cudaEvent_t* E = &evs[8L * k];
