@@ -831,6 +831,59 @@ __global__ void k_grad_t(int node, const int32_t* __restrict__ nptr, const int32
   }
 }
 
+// k_grad_t for 16 systems: a thread takes 4 systems of one node (16-byte loads of
+// r, the node's edge list read once for its 4 systems), two edges in flight; each
+// system's sum runs over the edges in list order as in k_grad_t.
+template <class T, class PT, int NS>
+__global__ void k_grad_t_spl(int node, const int32_t* __restrict__ nptr, const int32_t* __restrict__ nlist,
+                             const uint8_t* __restrict__ bc, const typename Cx<T>::V* __restrict__ r,
+                             typename Cx<PT>::V* __restrict__ t, const Ctrl* __restrict__ ctrl) {
+  using V = typename Cx<T>::V;
+  using PV = typename Cx<PT>::V;
+  constexpr int SP = 4, GPR = NS / SP;
+  if (ctrl->done) return;
+  const long total = (long)node * GPR;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int a = (int)(i / GPR), s0 = (int)(i % GPR) * SP;
+    T ax[SP], ay[SP];
+#pragma unroll
+    for (int j = 0; j < SP; ++j) ax[j] = ay[j] = 0;
+    const int q1 = __ldg(nptr + a + 1);
+    int q = __ldg(nptr + a);
+    auto add = [&](int v, const V (&re)[SP]) {
+      if (v & 1) {
+#pragma unroll
+        for (int j = 0; j < SP; ++j) { ax[j] -= re[j].x; ay[j] -= re[j].y; }
+      } else {
+#pragma unroll
+        for (int j = 0; j < SP; ++j) { ax[j] += re[j].x; ay[j] += re[j].y; }
+      }
+    };
+    for (; q + 1 < q1; q += 2) {
+      const int va = __ldg(nlist + q), vb = __ldg(nlist + q + 1);
+      const int ea = va >> 1, eb = vb >> 1;
+      const bool ka = !__ldg(bc + ea), kb = !__ldg(bc + eb);
+      V ra[SP], rb[SP];
+      if (ka) load_spl<V, NS, SP, false>(r + (long)ea * NS + s0, ra);
+      if (kb) load_spl<V, NS, SP, false>(r + (long)eb * NS + s0, rb);
+      if (ka) add(va, ra);
+      if (kb) add(vb, rb);
+    }
+    if (q < q1) {
+      const int v = __ldg(nlist + q), e = v >> 1;
+      if (!__ldg(bc + e)) {
+        V re[SP];
+        load_spl<V, NS, SP, false>(r + (long)e * NS + s0, re);
+        add(v, re);
+      }
+    }
+    PV out[SP];
+#pragma unroll
+    for (int j = 0; j < SP; ++j) out[j] = Cx<PT>::make((PT)ax[j], (PT)ay[j]);
+    store_spl<PV, SP>(t + (long)a * NS + s0, out);
+  }
+}
+
 // One multicolour SSOR sweep on the nodal matrix, over its colour-ordered split
 // rows (as the edge sweeps): forward y_a = (t_a - sum_{col(b)<col(a)} A_ab y_b) dd_a,
 // backward (in place) y_a -= dd_a sum_{col(b)>col(a)} A_ab y_b.  Grid barrier between colours.
@@ -1080,6 +1133,84 @@ __global__ void k_pupd(int n, const typename Cx<PT>::V* __restrict__ z, typename
       if (!have_p) pi = p[i];
       p[i] = Cx<T>::make((T)((double)zi.x + (be.x * (double)pi.x - be.y * (double)pi.y)),
                          (T)((double)zi.y + (be.x * (double)pi.y + be.y * (double)pi.x)));
+    }
+  }
+}
+
+// k_pupd for 16 systems sharing a matrix: a thread takes 4 systems of one row
+// (16-byte loads, the systems' scalars held in registers, the row's edge and
+// Dirichlet data read once for its 4 systems).  The grid-stride is a multiple of
+// 4, so a thread keeps the same 4 systems throughout.
+template <class T, class PT, int NS>
+__global__ void k_pupd_spl(int n, const typename Cx<PT>::V* __restrict__ z, typename Cx<T>::V* __restrict__ p,
+                           const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl, double2* __restrict__ x,
+                           int nsys, const int32_t* __restrict__ line, const uint8_t* __restrict__ bc,
+                           const typename Cx<PT>::V* __restrict__ u) {
+  using V = typename Cx<T>::V;
+  using PV = typename Cx<PT>::V;
+  constexpr int SP = 4, GPR = NS / SP;  // systems per thread, threads per row
+  const bool done = ctrl->done;
+  if (done) {
+    if (!x) return;
+    bool any = false;
+    for (int k = 0; k < nsys; ++k) any |= sc[k].xpend != 0;
+    if (!any) return;
+  }
+  const bool first = ctrl->iter == 0;
+  const long total = (long)n * GPR;
+  const long stride = (long)gridDim.x * blockDim.x;
+  const long i0 = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int s0 = (int)(i0 % GPR) * SP;
+  double2 al[SP], be[SP];
+  bool xp[SP], anyx = false;
+#pragma unroll
+  for (int j = 0; j < SP; ++j) {
+    xp[j] = x && sc[s0 + j].xpend;
+    al[j] = sc[s0 + j].alpha;
+    be[j] = sc[s0 + j].beta;
+    anyx |= xp[j];
+  }
+  for (long i = i0; i < total; i += stride) {
+    const int e = (int)(i / GPR);
+    const long base = (long)e * NS + s0;
+    V pi[SP];
+    bool have_p = false;
+    if (anyx) {
+      load_spl<V, NS, SP, false>(p + base, pi);
+      have_p = true;
+#pragma unroll
+      for (int j = 0; j < SP; ++j)
+        if (xp[j]) {
+          double2 xi = x[base + j];
+          xi.x += al[j].x * (double)pi[j].x - al[j].y * (double)pi[j].y;
+          xi.y += al[j].x * (double)pi[j].y + al[j].y * (double)pi[j].x;
+          x[base + j] = xi;
+        }
+    }
+    if (done) continue;
+    PV zp[SP];
+    load_spl<PV, NS, SP, false>(z + base, zp);
+    V zi[SP];
+#pragma unroll
+    for (int j = 0; j < SP; ++j) zi[j] = Cx<T>::make((T)zp[j].x, (T)zp[j].y);
+    if (u && !__ldg(bc + e)) {
+      PV uh[SP], ut[SP];
+      load_spl<PV, NS, SP, false>(u + (long)(__ldg(line + 2 * e + 1) - 1) * NS + s0, uh);
+      load_spl<PV, NS, SP, false>(u + (long)(__ldg(line + 2 * e) - 1) * NS + s0, ut);
+#pragma unroll
+      for (int j = 0; j < SP; ++j)
+        zi[j] = Cx<T>::make(zi[j].x + (T)(uh[j].x - ut[j].x), zi[j].y + (T)(uh[j].y - ut[j].y));
+    }
+    if (first) {
+      store_spl<V, SP>(p + base, zi);
+    } else {
+      if (!have_p) load_spl<V, NS, SP, false>(p + base, pi);
+      V po[SP];
+#pragma unroll
+      for (int j = 0; j < SP; ++j)
+        po[j] = Cx<T>::make((T)((double)zi[j].x + (be[j].x * (double)pi[j].x - be[j].y * (double)pi[j].y)),
+                            (T)((double)zi[j].y + (be[j].x * (double)pi[j].y + be[j].y * (double)pi[j].x)));
+      store_spl<V, SP>(p + base, po);
     }
   }
 }
@@ -1651,8 +1782,12 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
     HybridState* h = c->hyb;
     const int node = h->node;
     const uint8_t* hs = SEG ? h->seg.p : nullptr;
-    k_grad_t<T, PT, NS><<<c->num_sms * 8, 256, 0, s>>>(node, h->nptr.p, h->nlist.p, c->bc.p, (const V*)I::R(w),
-                                                        P::HT(w), w->ctrl.p);
+    if constexpr (NS == 16 && !SEG)
+      k_grad_t_spl<T, PT, NS><<<c->num_sms * 8, 256, 0, s>>>(node, h->nptr.p, h->nlist.p, c->bc.p,
+                                                              (const V*)I::R(w), P::HT(w), w->ctrl.p);
+    else
+      k_grad_t<T, PT, NS><<<c->num_sms * 8, 256, 0, s>>>(node, h->nptr.p, h->nlist.p, c->bc.p, (const V*)I::R(w),
+                                                          P::HT(w), w->ctrl.p);
     count_launch();
     for (int bwd = 0; bwd < 2; ++bwd)
       launch_coop(k_nsweep_mc<PT, NS, SEG>, w->nmc_blocks, s, (const int32_t*)(bwd ? h->uptr.p : h->lptr.p),
@@ -1681,10 +1816,16 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
                                         fold_grad ? w->part2.p : (const double*)nullptr, w->nmc_blocks);
   count_launch();
   if (ev) AFEM_CUDA(cudaEventRecord(ev[5], s));
-  k_pupd<T, PT, NS, SEG><<<c->num_sms * 8, 256, 0, s>>>(
-      n, (const PV*)P::Z(w), I::P(w), w->sc.p, w->ctrl.p, sg, mc ? w->x.p : (double2*)nullptr, nsys,
-      fold_grad ? (const int32_t*)c->line.p : (const int32_t*)nullptr, fold_grad ? c->bc.p : (const uint8_t*)nullptr,
-      fold_grad ? (const PV*)P::HY(w) : (const PV*)nullptr);
+  if constexpr (NS == 16 && !SEG)
+    k_pupd_spl<T, PT, NS><<<c->num_sms * 8, 256, 0, s>>>(
+        n, (const PV*)P::Z(w), I::P(w), w->sc.p, w->ctrl.p, mc ? w->x.p : (double2*)nullptr, nsys,
+        fold_grad ? (const int32_t*)c->line.p : (const int32_t*)nullptr,
+        fold_grad ? c->bc.p : (const uint8_t*)nullptr, fold_grad ? (const PV*)P::HY(w) : (const PV*)nullptr);
+  else
+    k_pupd<T, PT, NS, SEG><<<c->num_sms * 8, 256, 0, s>>>(
+        n, (const PV*)P::Z(w), I::P(w), w->sc.p, w->ctrl.p, sg, mc ? w->x.p : (double2*)nullptr, nsys,
+        fold_grad ? (const int32_t*)c->line.p : (const int32_t*)nullptr, fold_grad ? c->bc.p : (const uint8_t*)nullptr,
+        fold_grad ? (const PV*)P::HY(w) : (const PV*)nullptr);
   count_launch();
   if (ev) AFEM_CUDA(cudaEventRecord(ev[6], s));
   const int spmv_grid = launch_spmv<T, NS, SEG>(c, w, sizeof(T) == 8 ? w->rpw64 : w->rpw32, I::KM(c, w),
