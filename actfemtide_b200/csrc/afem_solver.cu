@@ -212,15 +212,33 @@ __device__ __forceinline__ void row_gather(const int32_t* __restrict__ cols, con
 #ifndef AFEM_SPMV_CHUNK
 #define AFEM_SPMV_CHUNK 16  // rounds per chunk in the SpMV
 #endif
-// Calls body(pos0) for the first row of every warp round of this block; the round's
-// rows are pos0 + sub for sub < RPW, live below `end` (passed to body as well).
+// The first row of this warp's first round in for_rows<RPW, CH>(p0, ..).
+template <int RPW, int CH>
+__device__ __forceinline__ int first_round(int p0) {
+  return p0 + (int)blockIdx.x * CH * (int)(blockDim.x >> 5) * RPW + (int)(threadIdx.x >> 5) * RPW;
+}
+
+// Calls body(pos0, end, next) for every warp round of this block: the round's rows
+// are pos0 + sub (sub < RPW), live below `end`; `next` is the first row of the
+// warp's following round (-1 after the last), so that a body can load the next
+// rows' indices while it gathers for the current ones.
 template <int RPW, int CH, class F>
 __device__ __forceinline__ void for_rows(int p0, int p1, F body) {
   const int wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;
-  const int chunk = CH * nwb * RPW;
-  for (int cb = p0 + (int)blockIdx.x * chunk; cb < p1; cb += (int)gridDim.x * chunk) {
+  const int chunk = CH * nwb * RPW, cstride = (int)gridDim.x * chunk;
+  int cb = p0 + (int)blockIdx.x * chunk, pos0 = cb + wib * RPW;
+  if (cb < p1 && pos0 >= min(cb + chunk, p1)) cb = p1;  // no round of this warp in the (last, partial) chunk
+  while (cb < p1) {
     const int ce = min(cb + chunk, p1);
-    for (int pos0 = cb + wib * RPW; pos0 < ce; pos0 += nwb * RPW) body(pos0, ce);
+    int ncb = cb, npos = pos0 + nwb * RPW;
+    if (npos >= ce) {
+      ncb = cb + cstride;
+      npos = ncb + wib * RPW;
+      if (ncb < p1 && npos >= min(ncb + chunk, p1)) ncb = p1;
+    }
+    body(pos0, ce, ncb < p1 ? npos : -1);
+    cb = ncb;
+    pos0 = npos;
   }
 }
 
@@ -630,30 +648,38 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
   const int s0 = (ql % S::NG) * SPL, g = ql / S::NG;
   const int slot = (threadIdx.x >> 5) * S::RPW + sub;  // this row's per-warp slot
   double om[SPL], rr[SPL][1];
-  double2 al[SPL];
-  bool act[SPL];
 #pragma unroll
   for (int i = 0; i < SPL; ++i) {
     om[i] = sc[s0 + i].omega;
-    al[i] = sc[s0 + i].alpha;
-    act[i] = sc[s0 + i].active;
     rr[i][0] = 0.0;
   }
   double (*red)[MAX_SYS][1] = nullptr;
   if constexpr (SEG) red = seg_sums<8 * S::RPW, 1>();
   for (int c = 0; c < ncolors; ++c) {
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    for_rows<S::RPW, AFEM_SWEEP_CHUNK>(p0, p1, [&](int pos0, int cend) {
+    // the next row's id, diagonal pair and pointers, loaded one round ahead
+    int nrow = 0, nk0 = 0, nk1 = 0;
+    double2 ndg = make_double2(1.0, 0.0);
+    auto fetch = [&](int ps) {
+      if (ps < p1) {
+        nrow = __ldg(perm + ps);
+        ndg = __ldg(dkm + ps);
+        nk0 = __ldg(lptr + ps);
+        nk1 = __ldg(lptr + ps + 1);
+      }
+    };
+    fetch(first_round<S::RPW, AFEM_SWEEP_CHUNK>(p0) + sub);
+    for_rows<S::RPW, AFEM_SWEEP_CHUNK>(p0, p1, [&](int pos0, int cend, int next) {
       const int pos = pos0 + sub;
       const bool live = pos < cend;
-      const int row = live ? __ldg(perm + pos) : 0;
-      const double2 dg = live ? __ldg(dkm + pos) : make_double2(1.0, 0.0);
+      const int row = live ? nrow : 0;
+      const int k0 = nk0, k1 = nk1;
+      const double2 dg = live ? ndg : make_double2(1.0, 0.0);
+      if (next >= 0) fetch(next + sub);
       int sid = s0;
       if constexpr (SEG) {
         sid = live ? (int)__ldg(seg + row) : 0;
         om[0] = sc[sid].omega;
-        al[0] = sc[sid].alpha;
-        act[0] = sc[sid].active;
       }
       V ri[SPL];
       if (live) load_spl<V, NS, SPL, false>(r + (long)row * NS + s0, ri);
@@ -667,10 +693,11 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
         bool any = false;
 #pragma unroll
         for (int i = 0; i < SPL; ++i)
-          if (act[i]) {
+          if (sc[sid + i].active) {  // the system's scalars (read-only here, L1)
             any = true;
-            ri[i] = Cx<T>::make((T)((double)ri[i].x - (al[i].x * (double)qi[i].x - al[i].y * (double)qi[i].y)),
-                                (T)((double)ri[i].y - (al[i].x * (double)qi[i].y + al[i].y * (double)qi[i].x)));
+            const double2 al = sc[sid + i].alpha;
+            ri[i] = Cx<T>::make((T)((double)ri[i].x - (al.x * (double)qi[i].x - al.y * (double)qi[i].y)),
+                                (T)((double)ri[i].y - (al.x * (double)qi[i].y + al.y * (double)qi[i].x)));
           }
         if (any) store_spl<V, SPL>(r + (long)row * NS + s0, ri);
       }
@@ -685,7 +712,7 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
 #pragma unroll
       for (int i = 0; i < SPL; ++i) t1x[i] = t1y[i] = t2x[i] = t2y[i] = 0;
       if (live)
-        row_gather_spl<PT, NS, S::G, SPL>(lcol, lkm, y, __ldg(lptr + pos) + g, __ldg(lptr + pos + 1), s0, t1x, t1y,
+        row_gather_spl<PT, NS, S::G, SPL>(lcol, lkm, y, k0 + g, k1, s0, t1x, t1y,
                                           t2x, t2y);
       group_sum<PT, SPL, S::NG, S::LPR>(t1x, t1y, t2x, t2y);
       if (live && g == 0) {
@@ -740,11 +767,25 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
   if constexpr (SEG) red = seg_sums<8 * S::RPW, 4>();
   for (int c = ncolors - 1; c >= 0; --c) {
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    for_rows<S::RPW, AFEM_SWEEP_CHUNK>(p0, p1, [&](int pos0, int cend) {
+    // the next row's id, diagonal pair and pointers, loaded one round ahead
+    int nrow = 0, nk0 = 0, nk1 = 0;
+    double2 ndg = make_double2(1.0, 0.0);
+    auto fetch = [&](int ps) {
+      if (ps < p1) {
+        nrow = __ldg(perm + ps);
+        ndg = __ldg(dkm + ps);
+        nk0 = __ldg(uptr + ps);
+        nk1 = __ldg(uptr + ps + 1);
+      }
+    };
+    fetch(first_round<S::RPW, AFEM_SWEEP_CHUNK>(p0) + sub);
+    for_rows<S::RPW, AFEM_SWEEP_CHUNK>(p0, p1, [&](int pos0, int cend, int next) {
       const int pos = pos0 + sub;
       const bool live = pos < cend;
-      const int row = live ? __ldg(perm + pos) : 0;
-      const double2 dg = live ? __ldg(dkm + pos) : make_double2(1.0, 0.0);
+      const int row = live ? nrow : 0;
+      const int k0 = nk0, k1 = nk1;
+      const double2 dg = live ? ndg : make_double2(1.0, 0.0);
+      if (next >= 0) fetch(next + sub);
       int sid = s0;
       if constexpr (SEG) {
         sid = live ? (int)__ldg(seg + row) : 0;
@@ -754,7 +795,7 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
 #pragma unroll
       for (int i = 0; i < SPL; ++i) t1x[i] = t1y[i] = t2x[i] = t2y[i] = 0;
       if (live)
-        row_gather_spl<PT, NS, S::G, SPL>(ucol, ukm, z, __ldg(uptr + pos) + g, __ldg(uptr + pos + 1), s0, t1x, t1y,
+        row_gather_spl<PT, NS, S::G, SPL>(ucol, ukm, z, k0 + g, k1, s0, t1x, t1y,
                                           t2x, t2y);
       group_sum<PT, SPL, S::NG, S::LPR>(t1x, t1y, t2x, t2y);
       if (live && g == 0) {
@@ -914,16 +955,30 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
   for (int cc = 0; cc < ncolors; ++cc) {
     const int c = backward ? ncolors - 1 - cc : cc;
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    for_rows<S::RPW, AFEM_SWEEP_CHUNK>(p0, p1, [&](int pos0, int cend) {
+    // the next row's id and pointers, loaded one round ahead
+    int nrow = 0, nk0 = 0, nk1 = 0;
+
+    auto fetch = [&](int ps) {
+      if (ps < p1) {
+        nrow = __ldg(perm + ps);
+
+        nk0 = __ldg(xptr + ps);
+        nk1 = __ldg(xptr + ps + 1);
+      }
+    };
+    fetch(first_round<S::RPW, AFEM_SWEEP_CHUNK>(p0) + sub);
+    for_rows<S::RPW, AFEM_SWEEP_CHUNK>(p0, p1, [&](int pos0, int cend, int next) {
       const int pos = pos0 + sub;
       const bool live = pos < cend;
-      const int row = live ? __ldg(perm + pos) : 0;
+      const int row = live ? nrow : 0;
+      const int k0 = nk0, k1 = nk1;
+      if (next >= 0) fetch(next + sub);
       if constexpr (SEG) om[0] = sc[live ? (int)__ldg(seg + row) : 0].omega;
       T t1x[SPL], t1y[SPL], t2x[SPL], t2y[SPL];
 #pragma unroll
       for (int i = 0; i < SPL; ++i) t1x[i] = t1y[i] = t2x[i] = t2y[i] = 0;
       if (live)
-        row_gather_spl<T, NS, S::G, SPL>(xcol, xkm, y, __ldg(xptr + pos) + g, __ldg(xptr + pos + 1), s0, t1x, t1y,
+        row_gather_spl<T, NS, S::G, SPL>(xcol, xkm, y, k0 + g, k1, s0, t1x, t1y,
                                          t2x, t2y);
       group_sum<T, SPL, S::NG, S::LPR>(t1x, t1y, t2x, t2y);
       if (live && g == 0) {
@@ -1244,7 +1299,14 @@ __global__ void __launch_bounds__(256, (SPL > 1 ? MC_MIN_BLOCKS : 0))
   double (*red)[MAX_SYS][3] = nullptr;
   if constexpr (SEG) red = seg_sums<8 * RPW, 3>();
   const int slot = (threadIdx.x >> 5) * RPW + sub;
-  for_rows<RPW, AFEM_SPMV_CHUNK>(0, n, [&](int row0, int cend) {
+  // row pointers of the warp's next row, loaded one round ahead
+  int nk0 = 0, nk1 = 0;
+  {
+    const int wib = threadIdx.x >> 5;
+    const int first = (int)blockIdx.x * AFEM_SPMV_CHUNK * (int)(blockDim.x >> 5) * RPW + wib * RPW + sub;
+    if (first < n) { nk0 = __ldg(rowptr + first); nk1 = __ldg(rowptr + first + 1); }
+  }
+  for_rows<RPW, AFEM_SPMV_CHUNK>(0, n, [&](int row0, int cend, int next) {
     const int row = row0 + sub;
     const bool live = row < cend;
     int sid = s0;
@@ -1252,7 +1314,8 @@ __global__ void __launch_bounds__(256, (SPL > 1 ? MC_MIN_BLOCKS : 0))
       sid = live ? (int)__ldg(seg + row) : 0;
       om[0] = sc[sid].omega;
     }
-    const int k0 = live ? rowptr[row] : 0, k1 = live ? rowptr[row + 1] : 0;
+    const int k0 = live ? nk0 : 0, k1 = live ? nk1 : 0;
+    if (next >= 0 && next + sub < n) { nk0 = __ldg(rowptr + next + sub); nk1 = __ldg(rowptr + next + sub + 1); }
     T t1x[SPL], t1y[SPL], t2x[SPL], t2y[SPL];
 #pragma unroll
     for (int i = 0; i < SPL; ++i) t1x[i] = t1y[i] = t2x[i] = t2y[i] = 0;

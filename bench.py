@@ -15,8 +15,9 @@ Methods (preconditioner, precision, systems per step): plain = SSOR-COCG
 FP64, one system (the reference's solver on the device, natural row order);
 plain-mc = the multicolour SSOR; hybrid = multicolour SSOR plus the
 gradient-space (nodal) correction; mixed = hybrid with FP32 inner COCG
-under FP64 refinement; batched / batched-mixed = 8 tidal periods x 2 source
-patterns = 16 systems per solve; learned* = flexible COCG with the learned
+under FP64 refinement; *-pc32 = FP64 COCG with the preconditioner in FP32;
+batched / batched-mixed / batched-pc32 = 8 tidal periods x 2 source patterns =
+16 systems per solve (batched-pc32 is the default); learned* = flexible COCG with the learned
 network (flexible COCG, z = H(r) + N(r) over the gradient-corrected SSOR H when
 that checkpoint exists); packed = 24 uneven meshes (n x n x 3n/4, n in 8..32)
 in one solve.
@@ -51,7 +52,7 @@ UNIT = "s/solve"
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of a kernel from an
 # ncu capture on the 48x48x32 model (532,352 edges), scaled to the bench's model by its rows
 TRAFFIC = {}
-DEFAULT_METHOD = "batched"
+DEFAULT_METHOD = "batched-pc32"
 TOL = 1e-8
 FALLBACK_HBM_GBS = 6650.0
 
@@ -339,7 +340,8 @@ def run_gpu(args):
     if "learned" in args.method:
         # the network over the gradient-corrected SSOR when that checkpoint exists, else the Jacobi-base one
         from actfemtide_b200 import learned
-        ckpt = learned.HYBRID_CKPT if os.path.exists(learned.HYBRID_CKPT + ".json") else learned.DEFAULT_CKPT
+        ckpt = args.ckpt or (learned.HYBRID_CKPT if os.path.exists(learned.HYBRID_CKPT + ".json")
+                             else learned.DEFAULT_CKPT)
         fw.mpnn_set_params(learned.load(ckpt))
         fw.mpnn_set_base(learned.load_base(ckpt) == 1)
     n = fw.nline
@@ -742,6 +744,7 @@ def main():
     p.add_argument("--ref-step-seconds", type=float, default=8.0,
                    help="reference arm: wall seconds of one step's slice of iterations")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--ckpt", default=None, help="learned methods: checkpoint path (without extension)")
     args = p.parse_args()
     if args.impl == "reference":
         run_reference(args)
