@@ -207,10 +207,13 @@ __device__ __forceinline__ void row_gather(const int32_t* __restrict__ cols, con
 // chunk the warps of one SM gather from overlapping neighbourhoods (L1 serves
 // the repeats).  CH = 1 is a plain grid-wide stride.
 #ifndef AFEM_SWEEP_CHUNK
-#define AFEM_SWEEP_CHUNK 2  // rounds per chunk in the multicolour sweeps
+#define AFEM_SWEEP_CHUNK 1  // rounds per chunk in the multicolour sweeps
+#endif
+#ifndef AFEM_GRADT_SPL
+#define AFEM_GRADT_SPL 1  // nodal right-hand side with four systems per thread at 16 systems
 #endif
 #ifndef AFEM_SPMV_CHUNK
-#define AFEM_SPMV_CHUNK 16  // rounds per chunk in the SpMV
+#define AFEM_SPMV_CHUNK 4  // rounds per chunk in the SpMV
 #endif
 // The first row of this warp's first round in for_rows<RPW, CH>(p0, ..).
 template <int RPW, int CH>
@@ -1845,7 +1848,7 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
     HybridState* h = c->hyb;
     const int node = h->node;
     const uint8_t* hs = SEG ? h->seg.p : nullptr;
-    if constexpr (NS == 16 && !SEG)
+    if constexpr (NS == 16 && !SEG && AFEM_GRADT_SPL)
       k_grad_t_spl<T, PT, NS><<<c->num_sms * 8, 256, 0, s>>>(node, h->nptr.p, h->nlist.p, c->bc.p,
                                                               (const V*)I::R(w), P::HT(w), w->ctrl.p);
     else

@@ -344,6 +344,8 @@ def run_gpu(args):
                              else learned.DEFAULT_CKPT)
         fw.mpnn_set_params(learned.load(ckpt))
         fw.mpnn_set_base(learned.load_base(ckpt) == 1)
+    if args.spmv_rpw:
+        fw.set_spmv_rows_per_warp(args.spmv_rpw)
     n = fw.nline
     INU, IAU, INL, IAL = fw.export_pattern()
     nnz = n + 2 * len(IAU)
@@ -744,6 +746,7 @@ def main():
     p.add_argument("--ref-step-seconds", type=float, default=8.0,
                    help="reference arm: wall seconds of one step's slice of iterations")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--spmv-rpw", type=int, default=0, help="pin the SpMV's rows per warp (1, 2, 4, 8); 0: tuned")
     p.add_argument("--ckpt", default=None, help="learned methods: checkpoint path (without extension)")
     args = p.parse_args()
     if args.impl == "reference":
