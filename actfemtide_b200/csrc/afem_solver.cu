@@ -209,9 +209,6 @@ __device__ __forceinline__ void row_gather(const int32_t* __restrict__ cols, con
 #ifndef AFEM_SWEEP_CHUNK
 #define AFEM_SWEEP_CHUNK 1  // rounds per chunk in the multicolour sweeps
 #endif
-#ifndef AFEM_GRADT_SPL
-#define AFEM_GRADT_SPL 1  // nodal right-hand side with four systems per thread at 16 systems
-#endif
 #ifndef AFEM_SPMV_CHUNK
 #define AFEM_SPMV_CHUNK 4  // rounds per chunk in the SpMV
 #endif
@@ -872,59 +869,6 @@ __global__ void k_grad_t(int node, const int32_t* __restrict__ nptr, const int32
       else { ax += re.x; ay += re.y; }
     }
     t[i] = Cx<PT>::make((PT)ax, (PT)ay);
-  }
-}
-
-// k_grad_t for 16 systems: a thread takes 4 systems of one node (16-byte loads of
-// r, the node's edge list read once for its 4 systems), two edges in flight; each
-// system's sum runs over the edges in list order as in k_grad_t.
-template <class T, class PT, int NS>
-__global__ void k_grad_t_spl(int node, const int32_t* __restrict__ nptr, const int32_t* __restrict__ nlist,
-                             const uint8_t* __restrict__ bc, const typename Cx<T>::V* __restrict__ r,
-                             typename Cx<PT>::V* __restrict__ t, const Ctrl* __restrict__ ctrl) {
-  using V = typename Cx<T>::V;
-  using PV = typename Cx<PT>::V;
-  constexpr int SP = 4, GPR = NS / SP;
-  if (ctrl->done) return;
-  const long total = (long)node * GPR;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-    const int a = (int)(i / GPR), s0 = (int)(i % GPR) * SP;
-    T ax[SP], ay[SP];
-#pragma unroll
-    for (int j = 0; j < SP; ++j) ax[j] = ay[j] = 0;
-    const int q1 = __ldg(nptr + a + 1);
-    int q = __ldg(nptr + a);
-    auto add = [&](int v, const V (&re)[SP]) {
-      if (v & 1) {
-#pragma unroll
-        for (int j = 0; j < SP; ++j) { ax[j] -= re[j].x; ay[j] -= re[j].y; }
-      } else {
-#pragma unroll
-        for (int j = 0; j < SP; ++j) { ax[j] += re[j].x; ay[j] += re[j].y; }
-      }
-    };
-    for (; q + 1 < q1; q += 2) {
-      const int va = __ldg(nlist + q), vb = __ldg(nlist + q + 1);
-      const int ea = va >> 1, eb = vb >> 1;
-      const bool ka = !__ldg(bc + ea), kb = !__ldg(bc + eb);
-      V ra[SP], rb[SP];
-      if (ka) load_spl<V, NS, SP, false>(r + (long)ea * NS + s0, ra);
-      if (kb) load_spl<V, NS, SP, false>(r + (long)eb * NS + s0, rb);
-      if (ka) add(va, ra);
-      if (kb) add(vb, rb);
-    }
-    if (q < q1) {
-      const int v = __ldg(nlist + q), e = v >> 1;
-      if (!__ldg(bc + e)) {
-        V re[SP];
-        load_spl<V, NS, SP, false>(r + (long)e * NS + s0, re);
-        add(v, re);
-      }
-    }
-    PV out[SP];
-#pragma unroll
-    for (int j = 0; j < SP; ++j) out[j] = Cx<PT>::make((PT)ax[j], (PT)ay[j]);
-    store_spl<PV, SP>(t + (long)a * NS + s0, out);
   }
 }
 
@@ -1848,12 +1792,8 @@ void enqueue_iteration(afem_ctx* c, SolverWork* w, int mode, int sweep_blocks, c
     HybridState* h = c->hyb;
     const int node = h->node;
     const uint8_t* hs = SEG ? h->seg.p : nullptr;
-    if constexpr (NS == 16 && !SEG && AFEM_GRADT_SPL)
-      k_grad_t_spl<T, PT, NS><<<c->num_sms * 8, 256, 0, s>>>(node, h->nptr.p, h->nlist.p, c->bc.p,
-                                                              (const V*)I::R(w), P::HT(w), w->ctrl.p);
-    else
-      k_grad_t<T, PT, NS><<<c->num_sms * 8, 256, 0, s>>>(node, h->nptr.p, h->nlist.p, c->bc.p, (const V*)I::R(w),
-                                                          P::HT(w), w->ctrl.p);
+    k_grad_t<T, PT, NS><<<c->num_sms * 8, 256, 0, s>>>(node, h->nptr.p, h->nlist.p, c->bc.p, (const V*)I::R(w),
+                                                        P::HT(w), w->ctrl.p);
     count_launch();
     for (int bwd = 0; bwd < 2; ++bwd)
       launch_coop(k_nsweep_mc<PT, NS, SEG>, w->nmc_blocks, s, (const int32_t*)(bwd ? h->uptr.p : h->lptr.p),
