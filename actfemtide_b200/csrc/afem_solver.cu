@@ -500,11 +500,49 @@ constexpr int mc_min_blocks() {
   return McShape<NS, SEG>::SPL > 1 ? MC_MIN_BLOCKS : 0;
 }
 
-// SPL consecutive complex values of one row (systems s0 .. s0+SPL-1) at p, 16-byte loads;
-// GATHER: a neighbour's values (L1 or L2, see GatherL1), else the row's own (plain load).
-template <class V, int NS, int SPL, bool GATHER>
+// Two consecutive complex doubles (32 bytes, 32-byte aligned) in one 256-bit access
+// (sm_100 ld/st .v4.f64).  A row's 16 FP64 values are then read by 8 lanes as two
+// whole 128-byte lines per instruction instead of 16-byte pieces at a 32-byte
+// stride, which halves the L1 wavefronts of a gather.  CG: at L2 only (ld.cg).
+// RO: the data are not written during the launch, and the load may be scheduled
+// freely; otherwise (values other threads write between grid barriers, as in the
+// sweeps) the load is also a compiler memory barrier, so it is never moved across a
+// grid barrier or a store.
+template <bool CG, bool RO>
+__device__ __forceinline__ void ld_v4d(const double2* p, double2& a, double2& b) {
+  if constexpr (RO) {
+    if constexpr (CG)
+      asm("ld.global.cg.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y) : "l"(p));
+    else
+      asm("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y) : "l"(p));
+  } else {
+    if constexpr (CG)
+      asm volatile("ld.global.cg.v4.f64 {%0,%1,%2,%3}, [%4];"
+                   : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y) : "l"(p) : "memory");
+    else
+      asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];"
+                   : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y) : "l"(p) : "memory");
+  }
+}
+__device__ __forceinline__ void st_v4d(double2* p, double2 a, double2 b) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(a.x), "d"(a.y), "d"(b.x), "d"(b.y)
+               : "memory");
+}
+
+#ifndef AFEM_V4D
+#define AFEM_V4D 1  // 256-bit accesses for FP64 pairs (0: two 128-bit accesses)
+#endif
+
+// SPL consecutive complex values of one row (systems s0 .. s0+SPL-1) at p: FP32 pairs
+// as one 16-byte load, FP64 pairs as one 32-byte load (s0 even, rows 256-byte aligned);
+// GATHER: a neighbour's values (L1 or L2, see GatherL1), else the row's own (plain load);
+// RO: values nothing writes during the launch (see ld_v4d).
+template <class V, int NS, int SPL, bool GATHER, bool RO = false>
 __device__ __forceinline__ void load_spl(const V* p, V (&v)[SPL]) {
-  if constexpr (SPL > 1 && sizeof(V) == 8) {  // float2 pairs as float4
+  if constexpr (AFEM_V4D && SPL > 1 && sizeof(V) == 16) {  // double2 pairs as 32 bytes
+#pragma unroll
+    for (int i = 0; i < SPL; i += 2) ld_v4d<GATHER && !GatherL1<V, NS>::ok, RO>(p + i, v[i], v[i + 1]);
+  } else if constexpr (SPL > 1 && sizeof(V) == 8) {  // float2 pairs as float4
 #pragma unroll
     for (int i = 0; i < SPL; i += 2) {
       const float4* q = reinterpret_cast<const float4*>(p + i);
@@ -524,7 +562,10 @@ __device__ __forceinline__ void load_spl(const V* p, V (&v)[SPL]) {
 }
 template <class V, int SPL>
 __device__ __forceinline__ void store_spl(V* p, const V (&v)[SPL]) {
-  if constexpr (SPL > 1 && sizeof(V) == 8) {
+  if constexpr (AFEM_V4D && SPL > 1 && sizeof(V) == 16) {
+#pragma unroll
+    for (int i = 0; i < SPL; i += 2) st_v4d(p + i, v[i], v[i + 1]);
+  } else if constexpr (SPL > 1 && sizeof(V) == 8) {
 #pragma unroll
     for (int i = 0; i < SPL; i += 2)
       *reinterpret_cast<float4*>(p + i) = make_float4(v[i].x, v[i].y, v[i + 1].x, v[i + 1].y);
@@ -536,7 +577,7 @@ __device__ __forceinline__ void store_spl(V* p, const V (&v)[SPL]) {
 
 // row_gather for a lane carrying SPL systems: sums A_k v_col(k) for systems s0..s0+SPL-1
 // over entries k0, k0+G, ... < k1, two entries' loads in flight (SPL = 1: row_gather).
-template <class T, int NS, int G, int SPL>
+template <class T, int NS, int G, int SPL, bool RO = false>
 __device__ __forceinline__ void row_gather_spl(const int32_t* __restrict__ cols,
                                                const typename Cx<T>::V* __restrict__ vals,
                                                const typename Cx<T>::V* vec, int k0, int k1, int s0,
@@ -551,8 +592,8 @@ __device__ __forceinline__ void row_gather_spl(const int32_t* __restrict__ cols,
         const int j0 = __ldg(cols + k), j1 = __ldg(cols + k + 1);
         const V a0 = vals[k], a1 = vals[k + 1];
         V v0[SPL], v1[SPL];
-        load_spl<V, NS, SPL, true>(vec + (long)j0 * NS + s0, v0);
-        load_spl<V, NS, SPL, true>(vec + (long)j1 * NS + s0, v1);
+        load_spl<V, NS, SPL, true, RO>(vec + (long)j0 * NS + s0, v0);
+        load_spl<V, NS, SPL, true, RO>(vec + (long)j1 * NS + s0, v1);
 #pragma unroll
         for (int i = 0; i < SPL; ++i) {
           t1x[i] += a0.x * v0[i].x; t1y[i] += a0.x * v0[i].y; t2x[i] += a0.y * v0[i].x; t2y[i] += a0.y * v0[i].y;
@@ -563,7 +604,7 @@ __device__ __forceinline__ void row_gather_spl(const int32_t* __restrict__ cols,
       const int j = __ldg(cols + k);
       const V a = vals[k];
       V v[SPL];
-      load_spl<V, NS, SPL, true>(vec + (long)j * NS + s0, v);
+      load_spl<V, NS, SPL, true, RO>(vec + (long)j * NS + s0, v);
 #pragma unroll
       for (int i = 0; i < SPL; ++i) {
         t1x[i] += a.x * v[i].x; t1y[i] += a.x * v[i].y; t2x[i] += a.y * v[i].x; t2y[i] += a.y * v[i].y;
@@ -1139,10 +1180,11 @@ __global__ void k_pupd(int n, const typename Cx<PT>::V* __restrict__ z, typename
   }
 }
 
-// k_pupd for 16 systems sharing a matrix: a thread takes 4 systems of one row
-// (16-byte loads, the systems' scalars held in registers, the row's edge and
-// Dirichlet data read once for its 4 systems).  The grid-stride is a multiple of
-// 4, so a thread keeps the same 4 systems throughout.
+// k_pupd for 16 systems sharing a matrix: a thread takes 2 consecutive systems of
+// one row, so the 8 threads of a row read and write its FP64 values (p, x) as one
+// 256-byte run of 32-byte accesses and its FP32 values (z, u) as one 128-byte run
+// of 16-byte accesses; the systems' scalars stay in registers.  The grid-stride is
+// a multiple of 8, so a thread keeps the same 2 systems throughout.
 template <class T, class PT, int NS>
 __global__ void k_pupd_spl(int n, const typename Cx<PT>::V* __restrict__ z, typename Cx<T>::V* __restrict__ p,
                            const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl, double2* __restrict__ x,
@@ -1150,7 +1192,7 @@ __global__ void k_pupd_spl(int n, const typename Cx<PT>::V* __restrict__ z, type
                            const typename Cx<PT>::V* __restrict__ u) {
   using V = typename Cx<T>::V;
   using PV = typename Cx<PT>::V;
-  constexpr int SP = 4, GPR = NS / SP;  // systems per thread, threads per row
+  constexpr int SP = 2, GPR = NS / SP;  // systems per thread, threads per row
   const bool done = ctrl->done;
   if (done) {
     if (!x) return;
@@ -1180,14 +1222,15 @@ __global__ void k_pupd_spl(int n, const typename Cx<PT>::V* __restrict__ z, type
     if (anyx) {
       load_spl<V, NS, SP, false>(p + base, pi);
       have_p = true;
+      double2 xi[SP];
+      load_spl<double2, NS, SP, false>(x + base, xi);
 #pragma unroll
       for (int j = 0; j < SP; ++j)
         if (xp[j]) {
-          double2 xi = x[base + j];
-          xi.x += al[j].x * (double)pi[j].x - al[j].y * (double)pi[j].y;
-          xi.y += al[j].x * (double)pi[j].y + al[j].y * (double)pi[j].x;
-          x[base + j] = xi;
+          xi[j].x += al[j].x * (double)pi[j].x - al[j].y * (double)pi[j].y;
+          xi[j].y += al[j].x * (double)pi[j].y + al[j].y * (double)pi[j].x;
         }
+      store_spl<double2, SP>(x + base, xi);  // a system not pending keeps its value
     }
     if (done) continue;
     PV zp[SP];
@@ -1237,12 +1280,15 @@ __global__ void __launch_bounds__(256, (SPL > 1 ? MC_MIN_BLOCKS : 0))
   constexpr int G = LPR / NG;    // entry groups per row
   const int lane = threadIdx.x & 31, sub = lane / LPR, ql = lane % LPR;
   const int s0 = (ql % NG) * SPL, g = ql / NG;
-  double om[SPL];
+  // SPL > 1 never runs in resid_mode (the true residual uses one system per lane):
+  // two sums per system (p^T q) keep the 64-register variant free of spills
+  constexpr int NACC = SPL > 1 ? 2 : 3;
+  double om1 = sc[s0].omega;  // SPL = 1: this lane's system (SEG: set per row)
+  double acc[SPL][NACC];
 #pragma unroll
-  for (int i = 0; i < SPL; ++i) om[i] = sc[s0 + i].omega;
-  double acc[SPL][3];
+  for (int i = 0; i < SPL; ++i)
 #pragma unroll
-  for (int i = 0; i < SPL; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.0;
+    for (int k = 0; k < NACC; ++k) acc[i][k] = 0.0;
   double (*red)[MAX_SYS][3] = nullptr;
   if constexpr (SEG) red = seg_sums<8 * RPW, 3>();
   const int slot = (threadIdx.x >> 5) * RPW + sub;
@@ -1259,24 +1305,24 @@ __global__ void __launch_bounds__(256, (SPL > 1 ? MC_MIN_BLOCKS : 0))
     int sid = s0;
     if constexpr (SEG) {
       sid = live ? (int)__ldg(seg + row) : 0;
-      om[0] = sc[sid].omega;
+      om1 = sc[sid].omega;
     }
     const int k0 = live ? nk0 : 0, k1 = live ? nk1 : 0;
     if (next >= 0 && next + sub < n) { nk0 = __ldg(rowptr + next + sub); nk1 = __ldg(rowptr + next + sub + 1); }
     T t1x[SPL], t1y[SPL], t2x[SPL], t2y[SPL];
 #pragma unroll
     for (int i = 0; i < SPL; ++i) t1x[i] = t1y[i] = t2x[i] = t2y[i] = 0;
-    row_gather_spl<T, NS, G, SPL>(col, km, p, k0 + g, k1, s0, t1x, t1y, t2x, t2y);
+    row_gather_spl<T, NS, G, SPL, true>(col, km, p, k0 + g, k1, s0, t1x, t1y, t2x, t2y);
     group_sum<T, SPL, NG, LPR>(t1x, t1y, t2x, t2y);
     if (g == 0 && live) {
       const long base = (long)row * NS + s0;
       V qi[SPL], own[SPL];
 #pragma unroll
       for (int i = 0; i < SPL; ++i) {
-        const T o = (T)om[i];
+        const T o = (T)(SPL == 1 ? om1 : __ldg(&sc[s0 + i].omega));
         qi[i] = Cx<T>::make(t1x[i] - o * t2y[i], t1y[i] + o * t2x[i]);
       }
-      if (bvec) {  // r = b - A x
+      if (SPL == 1 && bvec) {  // r = b - A x
         load_spl<V, NS, SPL, false>(bvec + base, own);
 #pragma unroll
         for (int i = 0; i < SPL; ++i) {
@@ -1285,10 +1331,10 @@ __global__ void __launch_bounds__(256, (SPL > 1 ? MC_MIN_BLOCKS : 0))
           const double e0 = (double)ri.x * (double)ri.x + (double)ri.y * (double)ri.y;
           const double e2 = (double)own[i].x * (double)own[i].x + (double)own[i].y * (double)own[i].y;
           if constexpr (SEG) { red[slot][sid][0] += e0; red[slot][sid][2] += e2; }
-          else { acc[i][0] += e0; acc[i][2] += e2; }
+          else { acc[i][0] += e0; acc[i][NACC - 1] += e2; }
         }
       } else {
-        load_spl<V, NS, SPL, false>(p + base, own);
+        load_spl<V, NS, SPL, false, true>(p + base, own);
 #pragma unroll
         for (int i = 0; i < SPL; ++i) {
           const double e0 = (double)own[i].x * (double)qi[i].x - (double)own[i].y * (double)qi[i].y;
@@ -1304,7 +1350,7 @@ __global__ void __launch_bounds__(256, (SPL > 1 ? MC_MIN_BLOCKS : 0))
     seg_partials<8 * RPW, 3>(red, part);
     return;
   }
-  block_partials_spl<NS, SPL, LPR, 3>(acc, s0, g == 0, part);
+  block_partials_spl<NS, SPL, LPR, NACC>(acc, s0, g == 0, part);
 }
 
 // ------------------------------------------------------------------ scalar kernels
@@ -1661,7 +1707,7 @@ int launch_spmv(afem_ctx* c, SolverWork* w, int rpw, const typename Cx<T>::V* km
   const int vi = rpw == 8 ? 3 : rpw == 4 ? 2 : rpw == 2 ? 1 : 0;
   int& grid = w->spmv_grid[sizeof(T) == 8 ? 0 : 1][vi];
   if constexpr (NS == 16 && !SEG) {
-    if (rpw == 8) {  // AFEM_MC_SPL systems per lane, 2 * AFEM_MC_SPL rows per warp
+    if (rpw == 8 && !bvec) {  // AFEM_MC_SPL systems per lane, 2 * AFEM_MC_SPL rows per warp (q = A p only)
       auto k = k_spmv<T, NS, 2 * AFEM_MC_SPL, SEG, AFEM_MC_SPL>;
       if (!grid) grid = one_wave_grid(c, k, w->nblocks);
       k<<<grid, 256, 0, s>>>(rp, cl, km, n, p, q, w->sc.p, ctrl, w->part.p, bvec, sg);

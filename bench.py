@@ -359,6 +359,14 @@ def run_gpu(args):
         out = fw.sites(job.sites, nsys=ns)
         return res, out
 
+    if args.profile_case:
+        # profiler case: one assembly + solve (capped at --maxit) + sites, no timing, no JSON bench line
+        res, _ = step()
+        print(f"profile case {args.workload}: iterations {res.iterations}, true residual {res.resid_true:.3e}, "
+              f"status {res.status}", flush=True)
+        fw.close()
+        return
+
     for _ in range(args.warmup):
         res, _ = step()
         if not res.ok and not args.allow_unconverged:
@@ -748,6 +756,8 @@ def main():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--spmv-rpw", type=int, default=0, help="pin the SpMV's rows per warp (1, 2, 4, 8); 0: tuned")
     p.add_argument("--ckpt", default=None, help="learned methods: checkpoint path (without extension)")
+    p.add_argument("--profile-case", action="store_true",
+                   help="for profiler captures: one assembly and solve capped at --maxit, then exit (no bench line)")
     args = p.parse_args()
     if args.impl == "reference":
         run_reference(args)
