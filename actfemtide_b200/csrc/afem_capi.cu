@@ -480,8 +480,8 @@ int afem_set_wait_limit(afem_ctx* c, unsigned polls) {
 
 int afem_set_spmv_rows_per_warp(afem_ctx* c, int rpw) {
   return guarded(c, [&]() {
-    AFEM_REQUIRE(rpw == 0 || rpw == 1 || rpw == 2 || rpw == 4 || rpw == 8, AFEM_EINVAL,
-                 "set_spmv_rows_per_warp: 0 (tuned), 1, 2, 4 or 8");
+    AFEM_REQUIRE(rpw == 0 || rpw == 1 || rpw == 2 || rpw == 4 || rpw == 8 || rpw == 16, AFEM_EINVAL,
+                 "set_spmv_rows_per_warp: 0 (tuned), 1, 2, 4, 8 or 16 (tiles staged in shared memory)");
     c->spmv_rpw = rpw;
     afem::reset_spmv_tuning(c);
     return (int)AFEM_OK;

@@ -196,6 +196,13 @@ struct afem_ctx {
   afem::DBuf<double2> mc_lkm, mc_ukm, mc_dkm;
   long mc_vals_gen = -1;        // assembly generation of mc_lkm / mc_ukm / mc_dkm
   bool schedule_ready = false;
+  // tiled SpMV (16 systems): per tile of 32 rows its distinct columns and the entries'
+  // positions among them (k_spt_build); spt_fb flags tiles summed from global memory
+  afem::DBuf<int32_t> spt_ptr, spt_uniq;
+  afem::DBuf<uint16_t> spt_lidx;
+  afem::DBuf<uint8_t> spt_fb;
+  int spt_ntiles = 0;
+  bool spt_ready = false;
 
   // values: A(omega) = K + i*omega*M, stored interleaved (K_k, M_k)
   afem::DBuf<double2> km;       // nnz

@@ -90,7 +90,7 @@ struct SolverWork {
   DBuf<float2> htf, hyf, hddf;      // the same for the FP32 inner solve
   int nmc_blocks = 0;               // co-resident grid of the nodal multicolour sweeps
   int rpw64 = 0, rpw32 = 0;         // SpMV rows per warp chosen by tune_spmv (0 = not tuned; 8: 4 systems per lane)
-  int spmv_grid[2][4] = {};         // one-wave grid of each SpMV variant (FP64 / FP32), 0 = not known yet
+  int spmv_grid[2][5] = {};         // one-wave grid of each SpMV variant (FP64 / FP32), 0 = not known yet
   int mc_blocks = 0;                // co-resident grid of the forward multicolour sweep
   int mcb_blocks = 0;               // and of the backward one (fewer registers: more blocks)
   double sd = 1.0;                  // SSOR diagonal scale of the current solve (DD = 1 / (sd D))
@@ -613,6 +613,58 @@ __device__ __forceinline__ void row_gather_spl(const int32_t* __restrict__ cols,
   }
 }
 
+// Row sums for rows whose LPR lanes hold different systems (G == 1): the row's columns
+// and values are loaded once, lane m of the row taking entry m of each block of LPR
+// entries (one coalesced load per row instead of LPR copies of every entry), and are
+// handed to the row's other lanes by shuffles; a block's gathers are then issued
+// BATCH at a time before their products are summed, so a row waits on one column
+// load and len/BATCH gathers instead of a column load before every pair of gathers.
+// Warp-uniform (shuffles): every lane runs the blocks of the longest row of its warp,
+// len = 0 for a lane whose row is not live.  Each lane adds its row's entries in CSR
+// order, as row_gather_spl does, so the sums are the same bits.
+#ifndef AFEM_COOP_GATHER
+#define AFEM_COOP_GATHER 1
+#endif
+template <class T, int NS, int SPL, int LPR, int BATCH>
+__device__ __forceinline__ void row_gather_coop(const int32_t* __restrict__ cols,
+                                                const typename Cx<T>::V* __restrict__ vals,
+                                                const typename Cx<T>::V* vec, int k0, int len, int s0,
+                                                T (&t1x)[SPL], T (&t1y)[SPL], T (&t2x)[SPL], T (&t2y)[SPL]) {
+  using V = typename Cx<T>::V;
+  static_assert(LPR % BATCH == 0 && LPR <= 32, "a batch stays inside a block");
+  const int ql = threadIdx.x & (LPR - 1);
+  const int maxlen = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
+  for (int b = 0; b < maxlen; b += LPR) {
+    const bool have = b + ql < len;
+    const int jm = have ? __ldg(cols + k0 + b + ql) : 0;
+    const V am = have ? vals[k0 + b + ql] : Cx<T>::make(0, 0);
+    const int nb = min(LPR, maxlen - b);
+    for (int e0 = 0; e0 < nb; e0 += BATCH) {
+      V a[BATCH], v[BATCH][SPL];
+#pragma unroll
+      for (int u = 0; u < BATCH; ++u) {
+        const int e = e0 + u;
+        const int j = __shfl_sync(0xffffffffu, jm, e, LPR);
+        a[u] = Cx<T>::make(__shfl_sync(0xffffffffu, am.x, e, LPR), __shfl_sync(0xffffffffu, am.y, e, LPR));
+        if (b + e < len) {
+          load_spl<V, NS, SPL, true>(vec + (long)j * NS + s0, v[u]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < SPL; ++i) v[u][i] = Cx<T>::make(0, 0);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < BATCH; ++u)
+        if (b + e0 + u < len)
+#pragma unroll
+          for (int i = 0; i < SPL; ++i) {
+            t1x[i] += a[u].x * v[u][i].x; t1y[i] += a[u].x * v[u][i].y;
+            t2x[i] += a[u].y * v[u][i].x; t2y[i] += a[u].y * v[u][i].y;
+          }
+    }
+  }
+}
+
 // Sum the G entry groups of a row (lanes of one row that hold the same systems).
 template <class T, int SPL, int NG, int LPR>
 __device__ __forceinline__ void group_sum(T (&a)[SPL], T (&b)[SPL], T (&c)[SPL], T (&d)[SPL]) {
@@ -752,7 +804,10 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
       PT t1x[SPL], t1y[SPL], t2x[SPL], t2y[SPL];
 #pragma unroll
       for (int i = 0; i < SPL; ++i) t1x[i] = t1y[i] = t2x[i] = t2y[i] = 0;
-      if (live)
+      if constexpr (AFEM_COOP_GATHER && S::G == 1 && S::LPR == 8 && !SEG)
+        row_gather_coop<PT, NS, SPL, S::LPR, (sizeof(PT) == 4 ? 4 : 2)>(lcol, lkm, y, k0, live ? k1 - k0 : 0, s0,
+                                                                        t1x, t1y, t2x, t2y);
+      else if (live)
         row_gather_spl<PT, NS, S::G, SPL>(lcol, lkm, y, k0 + g, k1, s0, t1x, t1y,
                                           t2x, t2y);
       group_sum<PT, SPL, S::NG, S::LPR>(t1x, t1y, t2x, t2y);
@@ -835,7 +890,10 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
       PT t1x[SPL], t1y[SPL], t2x[SPL], t2y[SPL];
 #pragma unroll
       for (int i = 0; i < SPL; ++i) t1x[i] = t1y[i] = t2x[i] = t2y[i] = 0;
-      if (live)
+      if constexpr (AFEM_COOP_GATHER && S::G == 1 && S::LPR == 8 && !SEG)
+        row_gather_coop<PT, NS, SPL, S::LPR, (sizeof(PT) == 4 ? 4 : 2)>(ucol, ukm, z, k0, live ? k1 - k0 : 0, s0,
+                                                                        t1x, t1y, t2x, t2y);
+      else if (live)
         row_gather_spl<PT, NS, S::G, SPL>(ucol, ukm, z, k0 + g, k1, s0, t1x, t1y,
                                           t2x, t2y);
       group_sum<PT, SPL, S::NG, S::LPR>(t1x, t1y, t2x, t2y);
@@ -965,7 +1023,10 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
       T t1x[SPL], t1y[SPL], t2x[SPL], t2y[SPL];
 #pragma unroll
       for (int i = 0; i < SPL; ++i) t1x[i] = t1y[i] = t2x[i] = t2y[i] = 0;
-      if (live)
+      if constexpr (AFEM_COOP_GATHER && S::G == 1 && S::LPR == 8 && !SEG)
+        row_gather_coop<T, NS, SPL, S::LPR, (sizeof(T) == 4 ? 4 : 2)>(xcol, xkm, y, k0, live ? k1 - k0 : 0, s0, t1x,
+                                                                      t1y, t2x, t2y);
+      else if (live)
         row_gather_spl<T, NS, S::G, SPL>(xcol, xkm, y, k0 + g, k1, s0, t1x, t1y,
                                          t2x, t2y);
       group_sum<T, SPL, S::NG, S::LPR>(t1x, t1y, t2x, t2y);
@@ -1353,6 +1414,177 @@ __global__ void __launch_bounds__(256, (SPL > 1 ? MC_MIN_BLOCKS : 0))
   block_partials_spl<NS, SPL, LPR, NACC>(acc, s0, g == 0, part);
 }
 
+// ------------------------------------------------------------------ tiled SpMV (16 systems, FP64)
+// Rows in tiles of SPT_ROWS consecutive rows.  The distinct columns of a tile's
+// entries (the rows of p its sums gather: ~154 for the ~520 entries of 32 rows of a
+// tetrahedral edge mesh) are listed once (spt_uniq from spt_ptr[t]), and every entry
+// holds the position of its column in that list (spt_lidx, 16 bits).  The tile's
+// block copies those p rows into shared memory with independent, coalesced 256-bit
+// loads, then each row sums its entries in CSR order from shared memory: a row's
+// gathers no longer wait on global loads one pair at a time, and each distinct p row
+// crosses L2 once per tile instead of once per entry.  A tile with more than
+// SPT_UCAP distinct columns (or more entries than the builder's table takes) is
+// flagged and summed from global memory as in k_spmv.  The sums, and so q, are the
+// same bits as k_spmv's two-systems-per-lane variant (same entry order, same FMAs).
+constexpr int SPT_ROWS = 32;    // rows per tile: 8 warps x 4 rows
+constexpr int SPT_UCAP = 192;   // distinct columns staged per tile (48 KB of FP64 p rows)
+constexpr int SPT_HASH = 2048;  // builder's open-addressing table; tiles of > SPT_HASH/2 entries fall back
+constexpr int SPT_PIECES = (SPT_UCAP * 8 + 255) / 256;  // 32-byte pieces a thread copies at most
+#ifndef SPT_GROUP
+#define SPT_GROUP 3  // pieces a thread has in flight while staging
+#endif
+
+__device__ __forceinline__ unsigned spt_hash(int j) { return ((unsigned)j * 2654435761u) >> 21; }  // 11 bits
+
+// One block per tile (grid-stride).  fill = false: count[t] = distinct columns, or 0
+// with fb[t] = 1 when the tile falls back; fill = true: list the columns from
+// ptr[t] and the entries' positions.  Positions depend on the order of the atomic
+// insertions; the SpMV's result does not (it sums in CSR order).
+__global__ void __launch_bounds__(256) k_spt_build(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                                                   int n, int ntiles, bool fill, int32_t* __restrict__ count,
+                                                   uint8_t* __restrict__ fb, const int32_t* __restrict__ ptr,
+                                                   int32_t* __restrict__ uniq, uint16_t* __restrict__ lidx) {
+  __shared__ int32_t key[SPT_HASH];
+  __shared__ int32_t pos[SPT_HASH];
+  __shared__ int nu;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int r0 = t * SPT_ROWS, r1 = min(r0 + SPT_ROWS, n);
+    const int k0 = rowptr[r0], k1 = rowptr[r1];
+    const bool big = k1 - k0 > SPT_HASH / 2;  // keeps the table at most half full: every probe ends
+    for (int i = threadIdx.x; i < SPT_HASH; i += blockDim.x) key[i] = -1;
+    if (threadIdx.x == 0) nu = 0;
+    __syncthreads();
+    if (!big)
+      for (int k = k0 + (int)threadIdx.x; k < k1; k += blockDim.x) {
+        const int j = col[k];
+        unsigned h = spt_hash(j);
+        for (;;) {
+          const int prev = atomicCAS(&key[h], -1, j);
+          if (prev == -1) { pos[h] = atomicAdd(&nu, 1); break; }
+          if (prev == j) break;
+          h = (h + 1) & (SPT_HASH - 1);
+        }
+      }
+    __syncthreads();
+    const bool over = big || nu > SPT_UCAP;
+    if (!fill) {
+      if (threadIdx.x == 0) { count[t] = over ? 0 : nu; fb[t] = over ? 1 : 0; }
+    } else if (!over) {
+      const int u0 = ptr[t];
+      for (int h = threadIdx.x; h < SPT_HASH; h += blockDim.x)
+        if (key[h] >= 0) uniq[u0 + pos[h]] = key[h];
+      for (int k = k0 + (int)threadIdx.x; k < k1; k += blockDim.x) {
+        const int j = col[k];
+        unsigned h = spt_hash(j);
+        while (key[h] != j) h = (h + 1) & (SPT_HASH - 1);
+        lidx[k] = (uint16_t)pos[h];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// 3 blocks of 256 threads per SM: 80 registers without spills, 3 x 48 KB of staged rows.
+template <int NS>
+__global__ void __launch_bounds__(256, 3)
+    k_spmv_tile(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                const double2* __restrict__ km, int n, const int32_t* __restrict__ sptr,
+                const int32_t* __restrict__ suniq, const uint16_t* __restrict__ slidx,
+                const uint8_t* __restrict__ sfb, int ntiles, const double2* __restrict__ p,
+                double2* __restrict__ q, const SysScal* __restrict__ sc, const Ctrl* __restrict__ ctrl,
+                double* __restrict__ part) {
+  static_assert(NS == 16, "tiles hold 16 systems per row");
+  constexpr int SPL = 2, LPR = NS / SPL;  // 8 lanes per row, 2 systems per lane, 4 rows per warp
+  // SPT_UCAP rows x NS values; a row's system 2m + h sits at 8h + m, so the 8 lanes of
+  // a row read its values for their first (second) systems as one 128-byte run
+  extern __shared__ double2 sp[];
+  if (ctrl && ctrl->done) return;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, sub = lane / LPR, ql = lane % LPR;
+  const int s0 = ql * SPL;
+  double acc[SPL][2];
+#pragma unroll
+  for (int i = 0; i < SPL; ++i) acc[i][0] = acc[i][1] = 0.0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const bool fb = __ldg(sfb + t) != 0;  // block-uniform
+    if (!fb) {
+      const int u0 = __ldg(sptr + t), nu = __ldg(sptr + t + 1) - u0;
+      // piece i: 32 bytes (systems 2(i%8), +1) of the tile's column i/8; a thread's
+      // pieces in groups of SPT_GROUP loads in flight, then their stores
+#pragma unroll
+      for (int m0 = 0; m0 < SPT_PIECES; m0 += SPT_GROUP) {
+        double2 va[SPT_GROUP], vb[SPT_GROUP];
+#pragma unroll
+        for (int m = 0; m < SPT_GROUP; ++m) {
+          const int i = (int)threadIdx.x + 256 * (m0 + m);
+          if (m0 + m < SPT_PIECES && i < nu * 8) {
+            const int j = __ldg(suniq + u0 + (i >> 3));
+            ld_v4d<false, true>(p + (long)j * NS + (i & 7) * 2, va[m], vb[m]);
+          }
+        }
+#pragma unroll
+        for (int m = 0; m < SPT_GROUP; ++m) {
+          const int i = (int)threadIdx.x + 256 * (m0 + m);
+          if (m0 + m < SPT_PIECES && i < nu * 8) {
+            sp[(i >> 3) * NS + (i & 7)] = va[m];
+            sp[(i >> 3) * NS + 8 + (i & 7)] = vb[m];
+          }
+        }
+      }
+      __syncthreads();
+    }
+    const int row = t * SPT_ROWS + wib * 4 + sub;
+    if (row < n) {
+      const int k0 = __ldg(rowptr + row), k1 = __ldg(rowptr + row + 1);
+      double t1x[SPL], t1y[SPL], t2x[SPL], t2y[SPL];
+#pragma unroll
+      for (int i = 0; i < SPL; ++i) t1x[i] = t1y[i] = t2x[i] = t2y[i] = 0.0;
+      if (!fb) {
+        int k = k0;
+        for (; k + 1 < k1; k += 2) {
+          const int l0 = __ldg(slidx + k), l1 = __ldg(slidx + k + 1);
+          const double2 a0 = km[k], a1 = km[k + 1];
+          const double2* v0 = sp + l0 * NS + ql;
+          const double2* v1 = sp + l1 * NS + ql;
+#pragma unroll
+          for (int i = 0; i < SPL; ++i) {
+            const double2 w0 = v0[8 * i], w1 = v1[8 * i];
+            t1x[i] += a0.x * w0.x; t1y[i] += a0.x * w0.y; t2x[i] += a0.y * w0.x; t2y[i] += a0.y * w0.y;
+            t1x[i] += a1.x * w1.x; t1y[i] += a1.x * w1.y; t2x[i] += a1.y * w1.x; t2y[i] += a1.y * w1.y;
+          }
+        }
+        if (k < k1) {
+          const int l0 = __ldg(slidx + k);
+          const double2 a = km[k];
+          const double2* v = sp + l0 * NS + ql;
+#pragma unroll
+          for (int i = 0; i < SPL; ++i) {
+            const double2 w = v[8 * i];
+            t1x[i] += a.x * w.x; t1y[i] += a.x * w.y; t2x[i] += a.y * w.x; t2y[i] += a.y * w.y;
+          }
+        }
+      } else {
+        row_gather_spl<double, NS, 1, SPL, true>(col, km, p, k0, k1, s0, t1x, t1y, t2x, t2y);
+      }
+      const long base = (long)row * NS + s0;
+      double2 qi[SPL], own[SPL];
+#pragma unroll
+      for (int i = 0; i < SPL; ++i) {
+        const double o = __ldg(&sc[s0 + i].omega);
+        qi[i] = make_double2(t1x[i] - o * t2y[i], t1y[i] + o * t2x[i]);
+      }
+      load_spl<double2, NS, SPL, false, true>(p + base, own);
+#pragma unroll
+      for (int i = 0; i < SPL; ++i) {
+        acc[i][0] += own[i].x * qi[i].x - own[i].y * qi[i].y;
+        acc[i][1] += own[i].x * qi[i].y + own[i].y * qi[i].x;
+      }
+      store_spl<double2, SPL>(q + base, qi);
+    }
+    __syncthreads();  // the next tile overwrites the staged rows
+  }
+  block_partials_spl<NS, SPL, LPR, 2>(acc, s0, true, part);
+}
+
 // ------------------------------------------------------------------ scalar kernels
 __device__ __forceinline__ void sum_partials(const double* part, int nblocks, int s, int k, double* out,
                                              int nvals) {
@@ -1687,15 +1919,42 @@ struct Inner<float, NS> {
 // Co-resident blocks of a kernel on this device (256 threads), at most `cap`: a
 // persistent grid of that size runs in one wave with every block's slice of rows.
 template <class K>
-int one_wave_grid(afem_ctx* c, K kernel, int cap) {
+int one_wave_grid(afem_ctx* c, K kernel, int cap, size_t smem = 0) {
   int per_sm = 0;
-  AFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0));
+  AFEM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem));
   return std::max(1, std::min(cap, std::max(1, per_sm) * c->num_sms));
 }
 
 // The SpMV variants: rpw rows per warp with a lane per system (1, 2, 4), or, at 16
 // systems, 8 rows per warp with 4 systems per lane (rpw = 8).  Returns the grid it
 // used (the number of partial sums its consumer adds).
+// Build the tiled SpMV's column lists once per pattern (two passes of k_spt_build:
+// count, scan, fill).  Synchronises the stream; called before any graph capture.
+void ensure_spmv_tiles(afem_ctx* c) {
+  if (c->spt_ready) return;
+  cudaStream_t s = c->stream;
+  const int n = c->nline;
+  const int ntiles = (n + SPT_ROWS - 1) / SPT_ROWS;
+  c->spt_ptr.alloc(ntiles + 1);
+  c->spt_fb.alloc(ntiles);
+  DBuf<int32_t> cnt;
+  cnt.alloc(ntiles);
+  const int grid = std::max(1, std::min(ntiles, c->num_sms * 8));
+  k_spt_build<<<grid, 256, 0, s>>>(c->rowptr.p, c->col.p, n, ntiles, false, cnt.p, c->spt_fb.p, nullptr, nullptr,
+                                   nullptr);
+  count_launch();
+  long total = 0;
+  exclusive_scan(cnt.p, c->spt_ptr.p, ntiles, s, &total);
+  c->spt_uniq.alloc(std::max(1L, total));
+  c->spt_lidx.alloc(std::max(1L, c->nnz));
+  k_spt_build<<<grid, 256, 0, s>>>(c->rowptr.p, c->col.p, n, ntiles, true, nullptr, c->spt_fb.p, c->spt_ptr.p,
+                                   c->spt_uniq.p, c->spt_lidx.p);
+  count_launch();
+  AFEM_CUDA(cudaStreamSynchronize(s));
+  c->spt_ntiles = ntiles;
+  c->spt_ready = true;
+}
+
 template <class T, int NS, bool SEG>
 int launch_spmv(afem_ctx* c, SolverWork* w, int rpw, const typename Cx<T>::V* km, const typename Cx<T>::V* p,
                 typename Cx<T>::V* q, const Ctrl* ctrl, const typename Cx<T>::V* bvec) {
@@ -1704,8 +1963,23 @@ int launch_spmv(afem_ctx* c, SolverWork* w, int rpw, const typename Cx<T>::V* km
   const int32_t* rp = c->rowptr.p;
   const int32_t* cl = c->col.p;
   const uint8_t* sg = SEG ? c->seg_of_row.p : nullptr;
-  const int vi = rpw == 8 ? 3 : rpw == 4 ? 2 : rpw == 2 ? 1 : 0;
+  const int vi = rpw == 16 ? 4 : rpw == 8 ? 3 : rpw == 4 ? 2 : rpw == 2 ? 1 : 0;
   int& grid = w->spmv_grid[sizeof(T) == 8 ? 0 : 1][vi];
+  if constexpr (NS == 16 && !SEG && sizeof(T) == 8) {
+    if (rpw == 16 && !bvec) {  // tiles staged in shared memory (built by ensure_spmv_tiles)
+      AFEM_REQUIRE(c->spt_ready, AFEM_ESTATE, "SpMV: tiles not built");
+      auto k = k_spmv_tile<NS>;
+      constexpr size_t smem = sizeof(double2) * SPT_UCAP * NS;
+      if (!grid) {
+        AFEM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        grid = one_wave_grid(c, k, w->nblocks, smem);
+      }
+      k<<<grid, 256, smem, s>>>(rp, cl, (const double2*)km, n, c->spt_ptr.p, c->spt_uniq.p, c->spt_lidx.p,
+                                c->spt_fb.p, c->spt_ntiles, (const double2*)p, (double2*)q, w->sc.p, ctrl, w->part.p);
+      count_launch();
+      return grid;
+    }
+  }
   if constexpr (NS == 16 && !SEG) {
     if (rpw == 8 && !bvec) {  // AFEM_MC_SPL systems per lane, 2 * AFEM_MC_SPL rows per warp (q = A p only)
       auto k = k_spmv<T, NS, 2 * AFEM_MC_SPL, SEG, AFEM_MC_SPL>;
@@ -1741,7 +2015,11 @@ int tune_spmv(afem_ctx* c, SolverWork* w) {
   using I = Inner<T, NS>;
   int& slot = sizeof(T) == 8 ? w->rpw64 : w->rpw32;
   if (slot) return slot;
-  auto valid = [](int rpw) { return rpw == 8 ? (NS == 16 && !SEG) : NS * rpw <= 32; };
+  auto valid = [](int rpw) {
+    return rpw == 16 ? (NS == 16 && !SEG && sizeof(T) == 8) : rpw == 8 ? (NS == 16 && !SEG) : NS * rpw <= 32;
+  };
+  // the tiles are built here, outside any graph capture (the build synchronises)
+  if (valid(16) && (c->spmv_rpw == 0 || c->spmv_rpw == 16)) ensure_spmv_tiles(c);
   if (c->spmv_rpw > 0) {  // pinned by the caller: the same reduction order in every process
     slot = valid(c->spmv_rpw) ? c->spmv_rpw : 1;
     return slot;
@@ -1750,10 +2028,10 @@ int tune_spmv(afem_ctx* c, SolverWork* w) {
   cudaEvent_t a, b;
   AFEM_CUDA(cudaEventCreate(&a));
   AFEM_CUDA(cudaEventCreate(&b));
-  const int cand[4] = {1, 2, 4, 8};
-  float tbest[4] = {1e30f, 1e30f, 1e30f, 1e30f};
+  const int cand[5] = {1, 2, 4, 8, 16};
+  float tbest[5] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
   for (int round = 0; round < 3; ++round)
-    for (int ci = 0; ci < 4; ++ci) {
+    for (int ci = 0; ci < 5; ++ci) {
       const int rpw = cand[ci];
       if (!valid(rpw)) continue;
       launch_spmv<T, NS, SEG>(c, w, rpw, I::KM(c, w), I::P(w), I::Q(w), nullptr, nullptr);  // warm
@@ -1767,7 +2045,7 @@ int tune_spmv(afem_ctx* c, SolverWork* w) {
     }
   float best = 1e30f;
   int pick = 1;
-  for (int ci = 0; ci < 4; ++ci)
+  for (int ci = 0; ci < 5; ++ci)
     if (tbest[ci] < best * 0.97f) { best = tbest[ci]; pick = cand[ci]; }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
@@ -2552,6 +2830,7 @@ void invalidate_work(afem_ctx* c) {
 // A new pattern: also tune the SpMV again (ensure_work re-allocates when the
 // size changes; buffers of the same size are kept).
 void invalidate_pattern_work(afem_ctx* c) {
+  c->spt_ready = false;
   if (c->work) {
     c->work->kmf_valid = c->work->mcf_valid = false;
     c->work->rpw64 = c->work->rpw32 = 0;

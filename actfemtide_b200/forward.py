@@ -351,7 +351,9 @@ class Forward:
         self._check(self._L.afem_set_wait_limit(self.ctx, int(polls)))
 
     def set_spmv_rows_per_warp(self, rpw: int):
-        """Pin the SpMV's rows per warp (1, 2, 4) for the same bits in every process; 0: tuned."""
+        """Pin the SpMV variant for the same bits in every process: 1, 2, 4 rows per warp, 8 (two
+        systems per lane, 16-system batches), 16 (tiles staged in shared memory, 16-system FP64
+        batches); a variant that does not fit the batch falls back to 1; 0: tuned."""
         self._check(self._L.afem_set_spmv_rows_per_warp(self.ctx, int(rpw)))
 
     def set_profiling(self, enable: bool):

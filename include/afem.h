@@ -188,9 +188,10 @@ int afem_cocg13_single(afem_ctx *ctx, int NP, int NPL, int NPU, double *D, doubl
  * waiting row gives up, and the solve returns AFEM_ETIMEOUT with the context
  * still usable.  0 restores the built-in bound (2^21 polls, about 2 s). */
 int afem_set_wait_limit(afem_ctx *ctx, unsigned polls);
-/* Pin the SpMV's rows per warp (1, 2, 4, or 8 = four systems per lane, for
- * 16-system batches; a value that does not fit the batch falls back to 1; 0: the
- * autotuner picks per pattern by timing).  The choice sets how a row's products are split over lanes and so
+/* Pin the SpMV variant: rows per warp 1, 2 or 4; 8 = two systems per lane and four
+ * rows per warp (16-system batches); 16 = tiles of 32 rows whose distinct p rows are
+ * staged in shared memory (16-system FP64 batches).  A value that does not fit the
+ * batch falls back to 1; 0: the autotuner picks per pattern by timing.  The choice sets how a row's products are split over lanes and so
  * the order of the floating-point additions: with the tuner, two processes may
  * pick different variants and their results differ in the last bits; a pinned
  * value gives the same bits in every process.  No counterpart in the reference. */
