@@ -470,13 +470,6 @@ __global__ void __launch_bounds__(256)
 // warp (lane = sub * 32/RPW + g * NS + s), which keeps several rows' loads in
 // flight per warp.  One persistent cooperative kernel per sweep with a grid
 // barrier between colours; no flags, no waits.
-// Consecutive colour passes of a sweep walk their positions in opposite directions
-// (rows of one colour are independent, so the order inside a colour changes no
-// value): a pass then starts where the previous one ended, on the neighbour values
-// that pass wrote last and L2 still holds.
-#ifndef AFEM_ALT_DIR
-#define AFEM_ALT_DIR 1
-#endif
 // A lane per (row, system): the earlier- or later-colour part of a row holds ~8
 // entries, so a row per lane keeps 32/NS rows' dependent loads in flight per
 // warp (the sweeps are latency-bound, not bandwidth-bound).  Packed batches
@@ -639,10 +632,7 @@ __device__ __forceinline__ void row_gather_spl(const int32_t* __restrict__ cols,
 #ifndef AFEM_COOP_GATHER
 #define AFEM_COOP_GATHER 1
 #endif
-#ifndef AFEM_SPMV_COOP
-#define AFEM_SPMV_COOP 0  // the SpMV's two-systems variant with the cooperative gather
-#endif
-template <class T, int NS, int SPL, int LPR, int BATCH, bool RO = false>
+template <class T, int NS, int SPL, int LPR, int BATCH>
 __device__ __forceinline__ void row_gather_coop(const int32_t* __restrict__ cols,
                                                 const typename Cx<T>::V* __restrict__ vals,
                                                 const typename Cx<T>::V* vec, int k0, int len, int s0,
@@ -664,7 +654,7 @@ __device__ __forceinline__ void row_gather_coop(const int32_t* __restrict__ cols
         const int j = __shfl_sync(0xffffffffu, jm, e, LPR);
         a[u] = Cx<T>::make(__shfl_sync(0xffffffffu, am.x, e, LPR), __shfl_sync(0xffffffffu, am.y, e, LPR));
         if (b + e < len) {
-          load_spl<V, NS, SPL, true, RO>(vec + (long)j * NS + s0, v[u]);
+          load_spl<V, NS, SPL, true>(vec + (long)j * NS + s0, v[u]);
         } else {
 #pragma unroll
           for (int i = 0; i < SPL; ++i) v[u][i] = Cx<T>::make(0, 0);
@@ -767,17 +757,15 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
   if constexpr (SEG) red = seg_sums<8 * S::RPW, 1>();
   for (int c = 0; c < ncolors; ++c) {
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    const bool rev = AFEM_ALT_DIR && (c & 1);
     // the next row's id, diagonal pair and pointers, loaded one round ahead
     int nrow = 0, nk0 = 0, nk1 = 0;
     double2 ndg = make_double2(1.0, 0.0);
     auto fetch = [&](int ps) {
       if (ps < p1) {
-        const int q = rev ? p0 + p1 - 1 - ps : ps;
-        nrow = __ldg(perm + q);
-        ndg = __ldg(dkm + q);
-        nk0 = __ldg(lptr + q);
-        nk1 = __ldg(lptr + q + 1);
+        nrow = __ldg(perm + ps);
+        ndg = __ldg(dkm + ps);
+        nk0 = __ldg(lptr + ps);
+        nk1 = __ldg(lptr + ps + 1);
       }
     };
     fetch(first_round<S::RPW, AFEM_SWEEP_CHUNK>(p0) + sub);
@@ -879,17 +867,15 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
   if constexpr (SEG) red = seg_sums<8 * S::RPW, 4>();
   for (int c = ncolors - 1; c >= 0; --c) {
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    const bool rev = AFEM_ALT_DIR && ((ncolors - 1 - c) & 1);
     // the next row's id, diagonal pair and pointers, loaded one round ahead
     int nrow = 0, nk0 = 0, nk1 = 0;
     double2 ndg = make_double2(1.0, 0.0);
     auto fetch = [&](int ps) {
       if (ps < p1) {
-        const int q = rev ? p0 + p1 - 1 - ps : ps;
-        nrow = __ldg(perm + q);
-        ndg = __ldg(dkm + q);
-        nk0 = __ldg(uptr + q);
-        nk1 = __ldg(uptr + q + 1);
+        nrow = __ldg(perm + ps);
+        ndg = __ldg(dkm + ps);
+        nk0 = __ldg(uptr + ps);
+        nk1 = __ldg(uptr + ps + 1);
       }
     };
     fetch(first_round<S::RPW, AFEM_SWEEP_CHUNK>(p0) + sub);
@@ -1016,15 +1002,15 @@ __global__ void __launch_bounds__(256, (mc_min_blocks<NS, SEG>()))
   for (int cc = 0; cc < ncolors; ++cc) {
     const int c = backward ? ncolors - 1 - cc : cc;
     const int p0 = cptr[c], p1 = cptr[c + 1];
-    const bool rev = AFEM_ALT_DIR && (cc & 1);
     // the next row's id and pointers, loaded one round ahead
     int nrow = 0, nk0 = 0, nk1 = 0;
+
     auto fetch = [&](int ps) {
       if (ps < p1) {
-        const int q = rev ? p0 + p1 - 1 - ps : ps;
-        nrow = __ldg(perm + q);
-        nk0 = __ldg(xptr + q);
-        nk1 = __ldg(xptr + q + 1);
+        nrow = __ldg(perm + ps);
+
+        nk0 = __ldg(xptr + ps);
+        nk1 = __ldg(xptr + ps + 1);
       }
     };
     fetch(first_round<S::RPW, AFEM_SWEEP_CHUNK>(p0) + sub);
@@ -1388,10 +1374,7 @@ __global__ void __launch_bounds__(256, (SPL > 1 ? MC_MIN_BLOCKS : 0))
     T t1x[SPL], t1y[SPL], t2x[SPL], t2y[SPL];
 #pragma unroll
     for (int i = 0; i < SPL; ++i) t1x[i] = t1y[i] = t2x[i] = t2y[i] = 0;
-    if constexpr (AFEM_SPMV_COOP && SPL > 1 && G == 1)
-      row_gather_coop<T, NS, SPL, LPR, 2, true>(col, km, p, k0, live ? k1 - k0 : 0, s0, t1x, t1y, t2x, t2y);
-    else
-      row_gather_spl<T, NS, G, SPL, true>(col, km, p, k0 + g, k1, s0, t1x, t1y, t2x, t2y);
+    row_gather_spl<T, NS, G, SPL, true>(col, km, p, k0 + g, k1, s0, t1x, t1y, t2x, t2y);
     group_sum<T, SPL, NG, LPR>(t1x, t1y, t2x, t2y);
     if (g == 0 && live) {
       const long base = (long)row * NS + s0;
