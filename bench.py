@@ -49,9 +49,18 @@ METRIC = "s per complex edge-FEM solve to 1e-8 residual: learned+batched vs plai
 PLAIN_96 = {"iterations": 30000, "converged": False, "resid_true_at_cap": 6.843e-05, "ms_per_iteration": 15.862,
             "seconds_at_cap": 475.9}
 UNIT = "s/solve"
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of a kernel from an
-# ncu capture on the 48x48x32 model (532,352 edges), scaled to the bench's model by its rows
-TRAFFIC = {}
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of a kernel, from a
+# one-pass ncu capture of the 96x96x64 batch itself (4,193,536 rows; two iterations, the mean):
+# `python bench.py --profile-case --workload large --maxit 60 --spmv-rpw 8` under
+# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum`.  Scaled by rows for other models.
+_T96 = "ncu one-pass dram bytes of a launch on this 96x96x64 batch (profile case, FP32 preconditioner)"
+TRAFFIC = {
+    "cocg_spmv_fp64pc32_ns16_rpw8": {"bytes": 4.085e9, "rows": 4193536, "source": _T96},
+    "cocg_fwd_sweep_mc_fp64pc32_ns16": {"bytes": 5.877e9, "rows": 4193536, "source": _T96},
+    "cocg_bwd_sweep_mc_fp64pc32_ns16": {"bytes": 3.163e9, "rows": 4193536, "source": _T96},
+    "cocg_p_update_fp64pc32_ns16": {"bytes": 4.931e9, "rows": 4193536, "source": _T96},
+    "cocg_nodal_correction_fp64pc32_ns16": {"bytes": 1.991e9, "rows": 4193536, "source": _T96},
+}
 DEFAULT_METHOD = "batched-pc32"
 TOL = 1e-8
 FALLBACK_HBM_GBS = 6650.0
