@@ -44,7 +44,8 @@ typedef enum afem_status {
   AFEM_EIO = -10,           /* file could not be read or parsed */
   AFEM_ENOPRECOND = -11,    /* NSET = 0 (COCG13_single ERROR = 101) */
   AFEM_ESITE = -12,         /* a site lies outside every tetrahedron (FINDELEMENT0) */
-  AFEM_ESTAGNATION = -13    /* residual stopped decreasing */
+  AFEM_ESTAGNATION = -13    /* the true residual stopped decreasing above the tolerance (the
+                               solutions of the last refinement are kept) */
 } afem_status;
 
 /* Preconditioners of COCG13_single (COCG13_single.f90:107-130, 202-241). */
