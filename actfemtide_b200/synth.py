@@ -80,17 +80,18 @@ class TidalModel:
         return s
 
 
-def kuhn_box(nx: int, ny: int, nz: int, xb=(-50.0, 50.0), yb=(-50.0, 50.0), zb=(-50.0, 50.0)):
+def kuhn_box(nx: int, ny: int, nz: int, xb=(-50.0, 50.0), yb=(-50.0, 50.0), zb=(-50.0, 50.0), zs=None):
     """Nodes and Kuhn-split tetrahedra of an nx*ny*nz hex box.
 
     Returns (xyz, n4, hex_of_tet, centroid) with n4 0-based here; every
     tetrahedron is oriented so that the reference's signed volume
     ``volume(xx(:,1), xx(:,5), -xx(:,4))`` (``src/solver/m_fem_util.f90:22``)
-    is positive.
+    is positive.  ``zs`` (nz+1 ascending levels) replaces the uniform z spacing.
     """
     xs = np.linspace(xb[0], xb[1], nx + 1)
     ys = np.linspace(yb[0], yb[1], ny + 1)
-    zs = np.linspace(zb[0], zb[1], nz + 1)
+    zs = np.linspace(zb[0], zb[1], nz + 1) if zs is None else np.asarray(zs, dtype=np.float64)
+    assert zs.shape == (nz + 1,)
     X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
     xyz = np.stack([X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")], axis=1)
 
@@ -451,3 +452,67 @@ def write_reference_inputs(m: TidalModel, outdir: str, line=None, n6line=None, s
         f.write("## forward control file written by actfemtide_b200.synth\n")
         f.write("\n".join(rows) + "\n")
     return ctl
+
+
+# ----------------------------------------------------------------------------- magnetotelluric models
+MT_FREQS_HZ = (0.1, 0.03, 0.01, 0.003)
+
+
+def graded_levels(top: float, first: float, ratio: float, n: int) -> np.ndarray:
+    """n cell boundaries below 0 down to -top (or above, for top < 0 reversed by the caller):
+    first cell `first` km thick, each next one `ratio` times thicker, scaled to end at |top|."""
+    d = first * ratio ** np.arange(n)
+    d *= abs(top) / d.sum()
+    return np.concatenate([[0.0], np.cumsum(d)])
+
+
+def mt_box(nx: int, ny: int, n_air: int, n_earth: int, *, half_km: float = 50.0, air_km: float = 50.0,
+           earth_km: float = 50.0, first_km: float = 1.0, ratio: float = 1.25, sigma: float = 0.1,
+           block_sigma: float | None = None, grf: bool = False, seed: int = 0, site_grid=None, freqs=None,
+           name: str = "mt_box") -> TidalModel:
+    """A magnetotelluric model on a Kuhn box over [-half_km, half_km]^2 with graded vertical cells
+    (n_air above z = 0 up to air_km, n_earth below down to -earth_km, finest at the surface).
+
+    Physical tags as the MT program reads them (``n4flag(:,1)``,
+    ``src/src_3DMT/forward_3DMT.f90:240``): air (centroid z > 0) tag 1 with
+    1e-8 S/m; earth tag 3 with a per-element conductivity (condflag 1): `sigma`,
+    or with ``grf`` a log10-normal random field (mean log10(sigma), std 0.5,
+    correlation 8 km), optionally a block of `block_sigma` at x in [5,15],
+    y in [-5,5], z in [-15,-5] km (tag 4).  Earth tetrahedra come last, as
+    ``sigma(iele - nphys1)`` expects.  Sites 1 m below the surface on
+    `site_grid` (default 5x5 over +-30 km); no tidal source (``nodes`` = 0).
+    """
+    za = graded_levels(air_km, first_km, ratio, n_air)
+    ze = graded_levels(earth_km, first_km, ratio, n_earth)
+    zs = np.concatenate([0.0 - ze[::-1], za[1:]])
+    xyz, tets, hex_of_tet, cen = kuhn_box(nx, ny, n_air + n_earth, (-half_km, half_km), (-half_km, half_km),
+                                          zs=zs)
+    cx, cy, cz = cen[:, 0], cen[:, 1], cen[:, 2]
+    tag = np.where(cz > 0.0, 1, 3).astype(np.int32)
+    sig = np.full(tets.shape[0], float(sigma))
+    if grf:
+        rng = np.random.default_rng(seed)
+        hx = 2 * half_km / nx
+        g = gaussian_random_field((nx, ny, n_air + n_earth), (hx, hx, hx), 8.0, rng)
+        logs = np.clip(math.log10(sigma) + 0.5 * g.ravel(order="F"), -4.0, 0.5)
+        sig = np.where(tag == 3, 10.0 ** logs[hex_of_tet], sig)
+    if block_sigma is not None:
+        inb = (cx >= 5) & (cx <= 15) & (cy >= -5) & (cy <= 5) & (cz >= -15) & (cz <= -5) & (tag == 3)
+        tag[inb] = 4
+        sig[inb] = block_sigma
+    order = np.concatenate([np.nonzero(tag == 1)[0], np.nonzero(tag >= 3)[0]])
+    tets = tets[order]; tag = tag[order]; sig = sig[order]
+    if site_grid is None:
+        site_grid = (-30.0, -15.0, 0.0, 15.0, 30.0)
+    gx, gy = np.meshgrid(np.asarray(site_grid, dtype=np.float64), np.asarray(site_grid, dtype=np.float64),
+                         indexing="ij")
+    sites = np.stack([gx.ravel(), gy.ravel(), np.full(gx.size, -SITE_DEPTH_KM)], axis=1)
+    land = tag >= 3
+    return TidalModel(
+        name=name, xyz=np.ascontiguousarray(xyz), n4=np.ascontiguousarray((tets + 1).astype(np.int32)),
+        tag=tag, sigma_land=np.ascontiguousarray(sig[land]), nodes=0, F=np.zeros((0, 3)),
+        v=np.zeros((0, 3), np.complex128),
+        freqs=np.asarray(MT_FREQS_HZ if freqs is None else freqs, dtype=np.float64),
+        sites=np.ascontiguousarray(sites),
+        bounds=dict(zmin=float(zs[0]), zmax=float(zs[-1]), xout=half_km, yout=half_km), seed=seed,
+        dims=(nx, ny, n_air + n_earth))

@@ -25,8 +25,8 @@ _c128p = np.ctypeslib.ndpointer(dtype=np.complex128, flags="C_CONTIGUOUS")
 
 
 def build(force: bool = False) -> str:
-    src = os.path.join(HERE, "afem_oracle.cpp")
-    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+    srcs = [os.path.join(HERE, f) for f in ("afem_oracle.cpp", "afem_oracle_mt.cpp", "Makefile")]
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(map(os.path.getmtime, srcs)):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
 
@@ -92,6 +92,24 @@ def lib():
         L.orc_calobsebcomp.restype = None
         L.orc_calobsebcomp.argtypes = [C.c_int, C.c_int, C.c_double, _c128p, C.c_int, _i32p, _f64p, _f64p, _c128p,
                                        _f64p, _f64p]
+        L.orc_mt_surfaces.restype = C.c_void_p
+        L.orc_mt_surfaces.argtypes = [C.c_int, _f64p, C.c_long, _i32p, C.c_int, _i32p, _i32p]
+        L.orc_mt_free.argtypes = [C.c_void_p]
+        L.orc_mt_error.restype = C.c_int
+        L.orc_mt_error.argtypes = [C.c_void_p]
+        L.orc_mt_minmax.argtypes = [C.c_void_p, _f64p]
+        L.orc_mt_surface_sizes.argtypes = [C.c_void_p, C.c_int] + [C.POINTER(C.c_int)] * 3
+        L.orc_mt_surface_get.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 7
+        L.orc_mt_cond2d.restype = C.c_long
+        L.orc_mt_cond2d.argtypes = [C.c_void_p, C.c_int, _i32p, C.c_double, C.c_int, C.c_double, C.c_long, _f64p,
+                                    _f64p]
+        L.orc_mt_face_system.restype = C.c_int
+        L.orc_mt_face_system.argtypes = [C.c_void_p, C.c_int, _f64p, C.c_double, C.c_int, C.POINTER(C.c_long)] + \
+            [C.c_void_p] * 10
+        L.orc_mt_genbcmt.argtypes = [C.c_void_p, C.c_double, C.c_int, _c128p, _c128p, _c128p, _c128p, _c128p, _u8p]
+        L.orc_mt_set_bc3d.argtypes = [C.c_int, C.c_int, _c128p, _c128p, _i32p, _i32p, _c128p, _i32p, _i32p, _c128p,
+                                      _u8p, _c128p]
+        L.orc_mt_calrespmt.argtypes = [C.c_int, C.c_double, _c128p, _c128p, _f64p, _f64p]
         _LIB = L
     return _LIB
 
@@ -423,3 +441,140 @@ class OracleForward:
         item, ve, vf, _ = prepobscoeff(self.m, self.n6line, self.m.sites)
         omega = 2.0 * (4.0 * np.arctan(1.0)) * freq
         return calobsebcomp(x, omega, item, ve, vf)
+
+
+# ----------------------------------------------------------------------------- 3-D MT forward
+def mt_sigma(m):
+    """GENMAT_MT's conductivity per tetrahedron (src/src_3DMT/forward_3DMT.f90:239-252): physical tags
+    1 and 2 -> sigma_air, >= 3 -> the per-element file value (condflag 1)."""
+    return resolve_sigma(m.tag, m.sigma_air, m.sigma_air, 1, None, m.nphys1, m.sigma_land)
+
+
+class Face:
+    """The 2-D TM system of one side surface at one frequency (split storage, after SET_BC_ICCG)."""
+
+    def __init__(self, A: Assembled, rf, gval, line3d, flag):
+        self.A, self.rf, self.gval, self.line3d, self.flag = A, rf, gval, line3d, flag
+
+    def solve(self):
+        """The direct solve the reference leaves to PARDISO (forward_2DTM.f90:160), here SuperLU."""
+        import scipy.sparse.linalg as sla
+        return sla.spsolve(self.A.to_scipy().tocsc(), self.rf)
+
+
+class MTOracle:
+    """EXTRACT6SURFACES, the 2-D TM boundary solves, GENBCMT, GENMAT_MT + SET_BC_3DJoint and
+    CALRESPMT (src/src_3DMT/n_ebfem_3DMT.f90:38-113) on a model m with numbering (line, n6line)."""
+
+    def __init__(self, m, line, n6line):
+        self.m = m
+        self.line = _c(line, np.int32)
+        self.n6line = _c(n6line, np.int32)
+        self.nline = self.line.shape[0]
+        self.h = lib().orc_mt_surfaces(m.node, _c(m.xyz, np.float64).reshape(-1), m.ntet, _c(m.n4, np.int32),
+                                       self.nline, self.line, self.n6line)
+        err = lib().orc_mt_error(self.h)
+        if err != 0:
+            raise RuntimeError(f"orc_mt_surfaces failed: {err}")
+        self.pat = pattern(self.nline, self.n6line)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_mt_free(self.h)
+            self.h = None
+
+    def minmax(self):
+        mm = np.zeros(6)
+        lib().orc_mt_minmax(self.h, mm)
+        return mm
+
+    def surface(self, j: int) -> dict:
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        lib().orc_mt_surface_sizes(self.h, j, C.byref(a), C.byref(b), C.byref(c))
+        node, ntri, nl = a.value, b.value, c.value
+        d = dict(x1x2=np.zeros((node, 2)), n3=np.zeros((ntri, 3), np.int32), n3line=np.zeros((ntri, 3), np.int32),
+                 tet=np.zeros(ntri, np.int32), line=np.zeros((nl, 2), np.int32), line3d=np.zeros(nl, np.int32),
+                 flag=np.zeros(nl, np.int32))
+        lib().orc_mt_surface_get(self.h, j, *[d[k].ctypes.data for k in ("x1x2", "n3", "n3line", "tet", "line",
+                                                                         "line3d", "flag")])
+        return d
+
+    def cond2d(self, j: int):
+        m = self.m
+        ntri = self.surface(j)["tet"].shape[0]
+        out = np.zeros(ntri)
+        rc = lib().orc_mt_cond2d(self.h, j, _c(m.tag, np.int32), m.sigma_air, 1, 0.0, m.nphys1,
+                                 _c(m.sigma_land, np.float64), out)
+        if rc != 0:
+            raise RuntimeError(f"cond3dto2d: triangle {-rc} has no conductivity")
+        return out
+
+    def face(self, j: int, freq: float, apply_bc: bool = True) -> Face:
+        cond = self.cond2d(j)
+        tot = C.c_long(0)
+        L = lib()
+        nul = [None] * 10
+        rc = L.orc_mt_face_system(self.h, j, cond, float(freq), int(apply_bc), C.byref(tot), *nul)
+        s = self.surface(j)
+        n = s["line3d"].shape[0]
+        INU = np.zeros(n + 1, np.int32); INL = np.zeros(n + 1, np.int32)
+        IAU = np.zeros(tot.value, np.int32); IAL = np.zeros(tot.value, np.int32)
+        D = np.zeros(n, np.complex128); AU = np.zeros(tot.value, np.complex128); AL = np.zeros(tot.value, np.complex128)
+        rf = np.zeros(n, np.complex128); bc = np.zeros(n, np.uint8); gv = np.zeros(n, np.complex128)
+        rc = L.orc_mt_face_system(self.h, j, cond, float(freq), int(apply_bc), C.byref(tot),
+                                  *[x.ctypes.data for x in (INU, IAU, INL, IAL, D, AU, AL, rf, bc, gv)])
+        if rc != 0:
+            raise RuntimeError(f"orc_mt_face_system({j}) rc={rc}")
+        return Face(Assembled(D, AU, AL, rf, bc, INU, IAU, INL, IAL), rf, gv, s["line3d"], s["flag"])
+
+    def boundary(self, freq: float, bs=None):
+        """GENBCMT after the four 2-D solves: (Avalue (2, nline) complex, line_bc (nline,)) and the bs used."""
+        if bs is None:
+            bs = [self.face(j, freq).solve() for j in (2, 3, 4, 5)]
+        av = np.zeros((2, self.nline), np.complex128)
+        bc = np.zeros(self.nline, np.uint8)
+        lib().orc_mt_genbcmt(self.h, 2.0 * np.pi * freq, self.nline, *[_c(b, np.complex128) for b in bs], av, bc)
+        return av, bc, bs
+
+    def system(self, freq: float, av, bc):
+        """INITIALIZE + GENMAT_MT + COPY_UL_ICCG12 + SET_BC_3DJoint: the split system and rf (2, nline)."""
+        import types
+        m = self.m
+        src = types.SimpleNamespace(**{k: getattr(m, k) for k in ("node", "xyz", "ntet", "n4", "tag", "bounds")})
+        src.nodes = 0
+        src.F = np.zeros((1, 3)); src.v = np.zeros((1, 3), np.complex128)
+        A = forward_assemble(src, self.line, self.n6line, self.pat, freq, mt_sigma(m), apply_bc=False)
+        rf = np.zeros((2, self.nline), np.complex128)
+        lib().orc_mt_set_bc3d(self.nline, 2, A.D, A.AL, A.INL, A.IAL, A.AU, A.INU, A.IAU, _c(av, np.complex128),
+                              _c(bc, np.uint8), rf)
+        A.bc = _c(bc, np.uint8)
+        return A, rf
+
+    def forward(self, freqs, sites, solver="direct", tol=1e-10):
+        """Fields at the sites for both polarisations, impedances and apparent resistivity/phase:
+        be (nfreq, 2, 5, nobs), z (nfreq, 4, nobs), rho, pha (nfreq, 4, nobs), and the solutions."""
+        import scipy.sparse.linalg as sla
+        item, ve, vf, _ = prepobscoeff(self.m, self.n6line, sites)
+        nobs = item.shape[0]
+        out = dict(be=[], z=[], rho=[], pha=[], x=[], resid=[])
+        for f in np.atleast_1d(freqs):
+            av, bc, _ = self.boundary(f)
+            A, rf = self.system(f, av, bc)
+            X = np.zeros((2, self.nline), np.complex128)
+            if solver == "direct":
+                lu = sla.splu(A.to_scipy().tocsc())
+                for k in range(2):
+                    X[k] = lu.solve(rf[k])
+            else:
+                for k in range(2):
+                    X[k] = cocg13_single(A, b=rf[k], precond="SSOR", resid=tol, maxit=200000)["x"]
+            om = 2.0 * np.pi * f
+            be = np.zeros((2, 5, nobs), np.complex128)
+            lib().orc_calobsebcomp(self.nline, 2, om, X.reshape(-1), nobs, item, ve, vf, be, np.zeros(10 * nobs),
+                                   np.zeros(10 * nobs))
+            z = np.zeros((4, nobs), np.complex128); rho = np.zeros((4, nobs)); pha = np.zeros((4, nobs))
+            lib().orc_mt_calrespmt(nobs, om, be, z, rho, pha)
+            out["be"].append(be); out["z"].append(z); out["rho"].append(rho); out["pha"].append(pha)
+            out["x"].append(X)
+            out["resid"].append([true_residual(A, X[k], rf[k]) for k in range(2)])
+        return {k: np.asarray(v) for k, v in out.items()}
