@@ -18,9 +18,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3"]
 # Files whose arithmetic must round like the serial reference (no FMA contraction).
-NOFMA = {"afem_assemble.cu", "afem_sites.cu", "afem_adjoint.cu"}
+NOFMA = {"afem_assemble.cu", "afem_sites.cu", "afem_adjoint.cu", "afem_mt.cu"}
 SOURCES = ["afem_capi.cu", "afem_mesh.cu", "afem_assemble.cu", "afem_solver.cu", "afem_sites.cu", "afem_mpnn.cu",
-           "afem_adjoint.cu", "afem_hybrid.cu", "afem_io.cpp"]
+           "afem_adjoint.cu", "afem_hybrid.cu", "afem_mt.cu", "afem_io.cpp"]
 HEADERS = ["afem_internal.h", "afem_hybrid.h", os.path.join("..", "..", "include", "afem.h")]
 
 

@@ -36,7 +36,7 @@ EXPORTS = (
     "afem_segment_info", "afem_launch_count", "afem_hybrid_matrix", "afem_sites_grid", "afem_site_coeffs_grid",
     "afem_xy_points", "afem_sort_index", "afem_mesh_info", "afem_solution_count", "afem_sites_noalloc",
     "afem_set_wait_limit", "afem_set_spmv_rows_per_warp", "afem_utm_xy",
-    "afem_mpnn_set_base", "afem_precond_apply",
+    "afem_mpnn_set_base", "afem_precond_apply", "afem_mt_forward", "afem_mt_boundary", "afem_mt_face",
 )
 
 
@@ -49,6 +49,12 @@ class SolveOpts(C.Structure):
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("resid_recursive", C.c_double),
                 ("resid_true", C.c_double), ("seconds", C.c_double), ("status", C.c_int)]
+
+
+class MtCond(C.Structure):
+    """afem_mt_cond: the MT forward's conductivity (GENMAT_MT / COND3DTO2D selections)."""
+    _fields_ = [("sigma_air", C.c_double), ("condflag", C.c_int), ("nvolume", C.c_int), ("sigma_land", C.c_void_p),
+                ("nphys2", C.c_int), ("sigma_file", C.c_void_p), ("tag_phys", C.c_void_p)]
 
 
 class AfemError(RuntimeError):
@@ -144,6 +150,14 @@ def lib():
     L.afem_set_profiling.argtypes = [_vp, C.c_int]
     L.afem_profile_count.argtypes = [_vp]
     L.afem_profile_entry.argtypes = [_vp, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_long)]
+    L.afem_mt_forward.argtypes = [_vp, C.POINTER(MtCond), C.c_int, _vp, C.c_int, _vp, C.POINTER(SolveOpts), _vp, _vp,
+                                  _vp, _vp, C.POINTER(SolveStats)]
+    L.afem_mt_forward.restype = C.c_int
+    L.afem_mt_boundary.argtypes = [_vp, C.POINTER(MtCond), C.c_double, _vp, _vp]
+    L.afem_mt_boundary.restype = C.c_int
+    L.afem_mt_face.argtypes = [_vp, C.POINTER(MtCond), C.c_int, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_long),
+                               _vp, _vp, _vp, _vp, _vp, _vp]
+    L.afem_mt_face.restype = C.c_int
     for name in ("afem_set_mesh", "afem_get_lines", "afem_set_cond", "afem_set_sigma", "afem_set_source",
                  "afem_set_bounds", "afem_assemble", "afem_export_system", "afem_solve", "afem_get_solution",
                  "afem_sites", "afem_site_coeffs", "afem_load_ctl", "afem_ctl_info", "afem_run_ctl",

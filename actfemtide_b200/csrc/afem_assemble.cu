@@ -259,3 +259,94 @@ void assemble_device(afem_ctx* c) {
 }
 
 }  // namespace afem
+
+namespace afem {
+namespace {
+
+// SET_BC_3DJoint's lifting (src/src_3DMT/forward_3DMT.f90:581-596) on the uncleared
+// system: rhs[k*n + e] = g_k[e] on a Dirichlet row; otherwise -(D*g_k[e] + the row's
+// products in ascending column order), the order of the reference's AL then AU loops.
+__global__ void k_lift_dirichlet(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                                 const int32_t* __restrict__ diagpos, const double2* __restrict__ km,
+                                 const uint8_t* __restrict__ bc, int n, int nsys,
+                                 const double* __restrict__ omega, const double2* __restrict__ g,
+                                 double2* __restrict__ rhs) {
+  const long total = (long)n * nsys;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(q / n), e = (int)(q % n);
+    const double2* gk = g + (long)k * n;
+    if (bc[e]) {
+      rhs[q] = gk[e];
+      continue;
+    }
+    const double om = omega[k];
+    double2 t = make_double2(0.0, 0.0);
+    {
+      const int dpos = diagpos[e];
+      const double ar = km[dpos].x, ai = om * km[dpos].y;
+      const double2 v = gk[e];
+      t = make_double2(ar * v.x - ai * v.y, ar * v.y + ai * v.x);
+    }
+    for (int p = rowptr[e]; p < rowptr[e + 1]; ++p) {
+      const int c = col[p];
+      if (c == e) continue;
+      const double ar = km[p].x, ai = om * km[p].y;
+      const double2 v = gk[c];
+      t = make_double2(t.x + (ar * v.x - ai * v.y), t.y + (ar * v.y + ai * v.x));
+    }
+    rhs[q] = make_double2(0.0 - t.x, 0.0 - t.y);
+  }
+}
+
+// SET_BC_3DJoint's matrix part (forward_3DMT.f90:599-620): Dirichlet rows become the
+// identity row, Dirichlet columns of the other rows are cleared.
+__global__ void k_apply_dirichlet(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                                  const uint8_t* __restrict__ bc, int n, double2* __restrict__ km) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const bool dr = bc[e] != 0;
+    for (int p = rowptr[e]; p < rowptr[e + 1]; ++p) {
+      const int c = col[p];
+      if (dr) km[p] = make_double2(c == e ? 1.0 : 0.0, 0.0);
+      else if (bc[c]) km[p] = make_double2(0.0, 0.0);
+    }
+  }
+}
+
+}  // namespace
+
+void assemble_dirichlet_device(afem_ctx* c, const uint8_t* bc, int nsys, const double* omega_host,
+                               const double2* g) {
+  AFEM_REQUIRE(c->pattern_ready, AFEM_ESTATE, "assemble: pattern not built");
+  AFEM_REQUIRE(c->sigma_set, AFEM_ESTATE, "assemble: conductivity not set");
+  AFEM_REQUIRE(nsys >= 1, AFEM_EINVAL, "assemble: no system");
+  cudaStream_t s = c->stream;
+  const int n = c->nline;
+  // K and M with every row complete: no Dirichlet flag for the element gather
+  DBuf<uint8_t> nobc;
+  nobc.alloc(n);
+  nobc.zero(s);
+  SrcArgs sa{};
+  sa.nsrc = 0;
+  c->km.alloc(c->nnz);
+  c->rhs.alloc((size_t)n * nsys);
+  c->rhs_nsrc = nsys;
+  k_assemble_rows<<<(n + 127) / 128, 128, 0, s>>>(c->xyz.p, c->n4.p, c->tag.p, c->n6line.p, c->sigma.p, c->etp.p,
+                                                  c->etl.p, c->rowptr.p, c->col.p, nobc.p, n, sa, c->km.p, c->rhs.p,
+                                                  c->status.p);
+  count_launch();
+  check_status(c, "assemble");
+  DBuf<double> om;
+  om.upload(omega_host, nsys, s);
+  k_lift_dirichlet<<<c->num_sms * 8, 256, 0, s>>>(c->rowptr.p, c->col.p, c->diagpos.p, c->km.p, bc, n, nsys, om.p,
+                                                  g, c->rhs.p);
+  count_launch();
+  k_apply_dirichlet<<<c->num_sms * 8, 256, 0, s>>>(c->rowptr.p, c->col.p, bc, n, c->km.p);
+  count_launch();
+  c->bc.alloc(n);
+  AFEM_CUDA(cudaMemcpyAsync(c->bc.p, bc, n, cudaMemcpyDeviceToDevice, s));
+  AFEM_CUDA(cudaStreamSynchronize(s));
+  c->assembled = true;
+  c->assemble_gen += 1;
+}
+
+}  // namespace afem

@@ -27,6 +27,7 @@ void check_status(afem_ctx* c, const char* what) {
     case DEV_NOTFOUND: code = AFEM_EPATTERN; kind = "id not found"; break;
     case DEV_DEGREE: code = AFEM_EPATTERN; kind = "adjacency longer than the kernel limit"; break;
     case DEV_NOSIGMA: code = AFEM_EINVAL; kind = "no conductivity for tag"; break;
+    case DEV_PIVOT: code = AFEM_EBREAKDOWN; kind = "zero or non-finite pivot"; break;
     default: break;
   }
   char buf[256];
@@ -155,6 +156,7 @@ void afem_destroy(afem_ctx* c) {
   afem::mpnn_destroy(c);
   afem::hybrid_destroy(c);
   afem::grid_destroy(c);
+  afem::mt_destroy(c);
   for (auto* s : c->src) delete s;
   c->src.clear();
     if (c->stream) {
@@ -206,6 +208,7 @@ int afem_set_mesh(afem_ctx* c, int node, const double* xyz, int ntet, const int3
     afem::hybrid_invalidate(c);
     afem::invalidate_pattern_work(c);
     if (c->grid) c->grid->ready = false;
+    afem::mt_destroy(c);
     afem::reset_status(c);
     if (nline > 0) {
       c->nline = nline;
@@ -819,3 +822,32 @@ int afem_run_ctl(afem_ctx* c, const afem_solve_opts* o) {
 }
 
 }  // extern "C"
+
+// ---- 3-D MT forward
+int afem_mt_forward(afem_ctx* c, const afem_mt_cond* cond, int nfreq, const double* freq, int nobs,
+                    const double* xyz_obs, const afem_solve_opts* opts, double* be, double* z, double* rho,
+                    double* pha, afem_solve_stats* stats) {
+  return guarded(c, [&]() {
+    AFEM_REQUIRE(opts, AFEM_EINVAL, "mt_forward: null options");
+    check_opts(opts);
+    afem::reset_status(c);
+    return afem::mt_forward_device(c, cond, nfreq, freq, nobs, xyz_obs, opts, be, z, rho, pha, stats);
+  });
+}
+
+int afem_mt_boundary(afem_ctx* c, const afem_mt_cond* cond, double freq, double* av, uint8_t* bc) {
+  return guarded(c, [&]() {
+    afem::reset_status(c);
+    afem::mt_boundary_device(c, cond, freq, av, bc);
+    return (int)AFEM_OK;
+  });
+}
+
+int afem_mt_face(afem_ctx* c, const afem_mt_cond* cond, int j, double freq, int* n, long* nnz, int32_t* line3d,
+                 int32_t* rowptr, int32_t* col, double* val, double* rhs, double* bs) {
+  return guarded(c, [&]() {
+    afem::reset_status(c);
+    afem::mt_face_device(c, cond, j, freq, n, nnz, line3d, rowptr, col, val, rhs, bs);
+    return (int)AFEM_OK;
+  });
+}

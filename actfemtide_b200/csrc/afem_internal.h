@@ -75,7 +75,8 @@ enum DevErr : int {
   DEV_TIMEOUT = 3,     // bounded wait expired
   DEV_NOTFOUND = 4,    // id missing (edge search / pattern slot)
   DEV_DEGREE = 5,      // adjacency longer than the kernel's limit
-  DEV_NOSIGMA = 6      // tetrahedron tag selects no conductivity
+  DEV_NOSIGMA = 6,     // tetrahedron tag selects no conductivity
+  DEV_PIVOT = 7        // zero or non-finite pivot in a direct factorisation
 };
 
 struct DevStatus {
@@ -143,6 +144,7 @@ inline void count_launch(long n = 1) {
 struct SolverWork;   // afem_solver.cu
 struct MpnnState;    // afem_mpnn.cu
 struct HybridState;  // afem_hybrid.cu
+struct MtState;      // afem_mt.cu
 
 }  // namespace afem
 
@@ -231,6 +233,7 @@ struct afem_ctx {
   afem::GridList* grid = nullptr;   // element locator of the plan-view sites
   int last_learned_its = 0;  // iterations the last solve ran with the learned preconditioner
   afem::CtlInfo* ctl = nullptr;
+  afem::MtState* mt = nullptr;   // boundary surfaces of the MT forward (built per mesh)
 
   unsigned wait_limit = 0;   // polls of the sync-free sweeps' bounded wait (0: the built-in limit)
   int spmv_rpw = 0;          // SpMV rows per warp pinned by the caller (0: chosen by the tuner)
@@ -318,6 +321,21 @@ double mpnn_train_host(afem_ctx* c, double freq, int nsamp, const double* r_host
 
 // afem_adjoint.cu
 void jacobian_device(afem_ctx* c, double freq, const double* x_host, int nadj, double* J_host);
+
+// afem_assemble.cu: the system with non-zero Dirichlet values g_k (SET_BC_3DJoint): K and M
+// without the boundary rows cleared, rhs column k = -A(omega_k) g_k on interior rows and g_k on
+// Dirichlet rows, then the Dirichlet rows and columns cleared.  bc, g: device; g[k*nline + row].
+void assemble_dirichlet_device(afem_ctx* c, const uint8_t* bc, int nsys, const double* omega_host,
+                               const double2* g);
+
+// afem_mt.cu (3-D MT forward)
+void mt_destroy(afem_ctx* c);
+int mt_forward_device(afem_ctx* c, const afem_mt_cond* cond, int nfreq, const double* freq, int nobs,
+                      const double* xyz_obs, const afem_solve_opts* o, double* be, double* z, double* rho,
+                      double* pha, afem_solve_stats* st);
+void mt_boundary_device(afem_ctx* c, const afem_mt_cond* cond, double freq, double* av, uint8_t* bc);
+void mt_face_device(afem_ctx* c, const afem_mt_cond* cond, int j, double freq, int* n, long* nnz, int32_t* line3d,
+                    int32_t* rowptr, int32_t* col, double* val, double* rhs, double* bs);
 
 // afem_sites.cu
 void site_coeffs_device(afem_ctx* c, int nobs, const double* xyz_obs, int32_t* item, double* val_e, double* val_f,

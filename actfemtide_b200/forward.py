@@ -402,3 +402,76 @@ def amp_phase(c):
     """CALOBSRESP's amplitude and phase in degrees (n_ebfem_bxyz_mpi.f90:611-626)."""
     c = np.asarray(c)
     return np.sqrt(c.real ** 2 + c.imag ** 2), np.arctan2(c.imag, c.real) * (180.0 / (4.0 * np.arctan(1.0)))
+
+
+@dataclass
+class MTResult:
+    """afem_mt_forward's outputs: be (nfreq, 2, 5, nobs) fields of the Ex / Ey polarisations
+    (bx, by, bz, ex, ey), z (nfreq, 4, nobs) impedances Zxx, Zxy, Zyx, Zyy in (mV/km)/nT,
+    rho / pha (nfreq, 4, nobs) apparent resistivity (Ohm m) and phase (degrees)."""
+    be: np.ndarray
+    z: np.ndarray
+    rho: np.ndarray
+    pha: np.ndarray
+    solve: SolveResult
+
+
+class MTForward(Forward):
+    """The 3-D MT forward (src/src_3DMT/n_ebfem_3DMT.f90) over the same device context: a mesh,
+    a conductivity (afem_mt_cond), frequencies and sites."""
+
+    def set_mt_cond(self, sigma_air, condflag=1, sigma_land=None, sigma_file=None, tag_phys=None):
+        self._keep = [None if a is None else _c(a, dt) for a, dt in
+                      ((sigma_land, np.float64), (sigma_file, np.float64), (tag_phys, np.int32))]
+        sl, sf, tg = self._keep
+        self._cond = capi.MtCond(float(sigma_air), int(condflag), 0 if sl is None else len(sl),
+                                 None if sl is None else sl.ctypes.data, 0 if sf is None else len(sf),
+                                 None if sf is None else sf.ctypes.data, None if tg is None else tg.ctypes.data)
+
+    def load_mt_model(self, m, with_lines=None):
+        """A synthetic MT model (actfemtide_b200.synth.mt_box): mesh with physical tags, per-element sigma."""
+        if with_lines is not None:
+            self.set_mesh(m.xyz, m.n4, m.tag, *with_lines)
+        else:
+            self.set_mesh(m.xyz, m.n4, m.tag)
+        self.set_mt_cond(m.sigma_air, 1, sigma_file=m.sigma_land)
+
+    def mt_forward(self, freqs, sites, precond="HYBRID", precision="fp64", tol=1e-8, maxit=100000,
+                   use_graph=True) -> MTResult:
+        f = _c(np.atleast_1d(freqs), np.float64)
+        o = _c(sites, np.float64)
+        nf, nobs = len(f), o.shape[0]
+        be = np.zeros((nf, 2, 5, nobs), np.complex128)
+        z = np.zeros((nf, 4, nobs), np.complex128)
+        rho = np.zeros((nf, 4, nobs)); pha = np.zeros((nf, 4, nobs))
+        opts = SolveOpts(capi.PRECOND[precond], capi.PRECISION[precision], tol, maxit, 1.0, 0, 0.0, int(use_graph))
+        st = SolveStats()
+        rc = self._L.afem_mt_forward(self.ctx, C.byref(self._cond), nf, ptr(f), nobs, ptr(o), C.byref(opts), ptr(be),
+                                     ptr(z), ptr(rho), ptr(pha), C.byref(st))
+        if rc not in (capi.AFEM_OK, -4, -13):
+            self._check(rc)
+        res = SolveResult(st.iterations, st.refinements, st.resid_recursive, st.resid_true, st.seconds, rc)
+        self._sizes()
+        return MTResult(be, z, rho, pha, res)
+
+    def mt_boundary(self, freq):
+        """GENBCMT's values at freq: (av (2, nline) complex, bc (nline,) uint8)."""
+        av = np.zeros((2, self.nline), np.complex128)
+        bc = np.zeros(self.nline, np.uint8)
+        self._check(self._L.afem_mt_boundary(self.ctx, C.byref(self._cond), float(freq), ptr(av), ptr(bc)))
+        return av, bc
+
+    def mt_face(self, j, freq):
+        """The 2-D TM system of side surface j at freq in the device's band order:
+        dict(line3d, A (scipy CSR), rhs, bs)."""
+        import scipy.sparse as sp
+        n = C.c_int(0); nnz = C.c_long(0)
+        self._check(self._L.afem_mt_face(self.ctx, C.byref(self._cond), int(j), float(freq), C.byref(n),
+                                         C.byref(nnz), None, None, None, None, None, None))
+        n, nnz = n.value, nnz.value
+        line3d = np.zeros(n, np.int32); rp = np.zeros(n + 1, np.int32); cl = np.zeros(nnz, np.int32)
+        val = np.zeros(nnz, np.complex128); rhs = np.zeros(n, np.complex128); bs = np.zeros(n, np.complex128)
+        self._check(self._L.afem_mt_face(self.ctx, C.byref(self._cond), int(j), float(freq), C.byref(C.c_int()),
+                                         C.byref(C.c_long()), ptr(line3d), ptr(rp), ptr(cl), ptr(val), ptr(rhs),
+                                         ptr(bs)))
+        return dict(line3d=line3d, A=sp.csr_matrix((val, cl, rp), shape=(n, n)), rhs=rhs, bs=bs)

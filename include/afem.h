@@ -306,6 +306,52 @@ int afem_sweep_schedule(int n, const int32_t *rowptr, const int32_t *col, const 
  * (rows sorted by colour), cptr[ncolors+1] (cptr must hold 256).  Returns ncolors. */
 int afem_coloring(int n, const int32_t *rowptr, const int32_t *col, uint8_t *color, int32_t *perm, int32_t *cptr);
 
+/* ---- 3-D MT forward ------------------------------------------------------------ */
+/* Conductivity of the MT forward as READPARAM_MT + SETNPHYS1INDEX2COND deliver it
+ * (src/src_3DMT/m_param_mt.f90, n_ebfem_3DMT.f90:291-340).  The 3-D system uses
+ * GENMAT_MT's selection (forward_3DMT.f90:239-252): tags 1 and 2 -> sigma_air,
+ * tag j >= 3 -> sigma_land[j-2] (condflag 0) or sigma_file[t-nphys1-1] for 1-based
+ * tetrahedron t (condflag 1, nphys2 values, the land tetrahedra last).  The 2-D
+ * side faces use COND3DTO2D's (src/src_2D/m_surface_type.f90:76-120): tag 1 ->
+ * sigma_air, tag 2 -> 3.31 (a default-real literal there), tag >= 3 ->
+ * sigma_land[0] or the file value of the triangle's tetrahedron. */
+typedef struct afem_mt_cond {
+  double sigma_air;
+  int condflag;               /* 0: per tag, 1: per element */
+  int nvolume;                /* entries of sigma_land (condflag 0) */
+  const double *sigma_land;
+  int nphys2;                 /* entries of sigma_file (condflag 1): the tetrahedra with tag >= 3 */
+  const double *sigma_file;
+  const int32_t *tag_phys;    /* physical tags n4flag(:,1), ntet values; NULL: the tags of afem_set_mesh */
+} afem_mt_cond;
+
+/* Replaces the frequency loop of program ebfem_3DMT (src/src_3DMT/n_ebfem_3DMT.f90:85-113):
+ * per frequency the 2-D TM boundary solves of the four side faces (forward_2DTM,
+ * src/src_2D/forward_2DTM.f90:17-170; a banded LDL^T on the device in place of PARDISO),
+ * GENBCMT + GENMAT_MT + SET_BC_3DJoint (forward_3DMT.f90:5-88, 92-177, 553-623), the solve of
+ * the Ex and Ey polarisations of every frequency in batches (in place of solvePARDISO),
+ * CALOBSEBCOMP at the sites and CALRESPMT (n_ebfem_3DMT.f90:179-237).  Outputs (any may be
+ * NULL): be[((f*2 + pol)*5 + c)*nobs + s] complex (c = bx, by, bz, ex, ey; pol 0 = Ex
+ * source, 1 = Ey), z[(f*4 + k)*nobs + s] complex (k = xx, xy, yx, yy, Z = E B^-1 in
+ * (mV/km)/nT), rho[(f*4 + k)*nobs + s] (Ohm m) and pha[...] (degrees).  The context's
+ * conductivity, matrix and right-hand sides become the MT ones (column 2f+pol is frequency
+ * f, polarisation pol; afem_export_system shows them); the last batch's solutions stay for
+ * afem_get_solution.  stats: iterations summed over the batches, worst residuals. */
+int afem_mt_forward(afem_ctx *ctx, const afem_mt_cond *cond, int nfreq, const double *freq_hz, int nobs,
+                    const double *xyz_obs, const afem_solve_opts *opts, double *be_complex, double *z_complex,
+                    double *rho, double *pha, afem_solve_stats *stats);
+/* GENBCMT's Dirichlet values at one frequency after the four 2-D solves (for parity checks):
+ * av[pol*nline + i] complex (Avalue_bc(i, pol+1)), bc[nline] (line_bc(:,1)).  Either may be NULL. */
+int afem_mt_boundary(afem_ctx *ctx, const afem_mt_cond *cond, double freq_hz, double *av_complex, uint8_t *bc);
+/* The 2-D TM system of side surface j (2 north, 3 west, 4 south, 5 east) at one frequency,
+ * after GENBC2D + SET_BC_ICCG, over the surface's lines in the device's band order:
+ * line3d[n] (1-based 3-D line ids), full CSR rowptr[n+1] / col[nnz] (0-based, ascending) /
+ * val[nnz] complex, rhs[n] complex and the solution bs[n] complex.  Call with line3d NULL to
+ * get *n and *nnz only.  (GENMAT2DTM, forward_2DTM.f90:253-363.) */
+int afem_mt_face(afem_ctx *ctx, const afem_mt_cond *cond, int j, double freq_hz, int *n, long *nnz,
+                 int32_t *line3d, int32_t *rowptr, int32_t *col, double *val_complex, double *rhs_complex,
+                 double *bs_complex);
+
 /* ---- drop-in driver --------------------------------------------------------- */
 /* Replaces the rank-0 input stage of program n_ebfem_bxyz (n_ebfem_bxyz_mpi.f90:55-90):
  * reads the forward ctl file (readcontrolfile + readparam, m_param.f90:145-446,
