@@ -97,6 +97,7 @@ void load_split_system(afem_ctx* c, int n, const int32_t* INU, const int32_t* IA
   AFEM_CUDA(cudaStreamSynchronize(s));
   c->pattern_ready = true;
   c->schedule_ready = false;
+  c->levels_ready = false;
   c->assembled = true;
   c->assemble_gen += 1;
   afem::hybrid_invalidate(c);

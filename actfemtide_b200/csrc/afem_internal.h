@@ -197,7 +197,8 @@ struct afem_ctx {
   afem::DBuf<int32_t> mc_dsrc;  // CSR index of the diagonal of the row at each colour position
   afem::DBuf<double2> mc_lkm, mc_ukm, mc_dkm;
   long mc_vals_gen = -1;        // assembly generation of mc_lkm / mc_ukm / mc_dkm
-  bool schedule_ready = false;
+  bool schedule_ready = false;  // colouring and colour-ordered split rows
+  bool levels_ready = false;    // perm_f / perm_b (natural-order sweeps only)
   // tiled SpMV (16 systems): per tile of 32 rows its distinct columns and the entries'
   // positions among them (k_spt_build); spt_fb flags tiles summed from global memory
   afem::DBuf<int32_t> spt_ptr, spt_uniq;
@@ -247,7 +248,7 @@ namespace afem {
 // afem_mesh.cu
 void build_lines_device(afem_ctx* c);     // MKLINE_V2 + MKN6 on the device
 void build_pattern_device(afem_ctx* c);   // adjacency + full CSR pattern
-void build_schedule(afem_ctx* c);         // sweep level schedules from the pattern
+void build_schedule(afem_ctx* c, bool levels);  // colouring + split rows; the level schedules when asked
 void exclusive_scan(const int32_t* in, int32_t* out, int n, cudaStream_t s, long* total_host);
 int compute_coloring(int n, const int32_t* rp, const int32_t* cl, uint8_t* color, int32_t* perm, int32_t* cptr,
                      int max_colors);  // greedy distance-1 colouring, rows sorted by colour

@@ -337,6 +337,7 @@ void build_pattern_device(afem_ctx* c) {
   check_status(c, "pattern: fill");
   c->pattern_ready = true;
   c->schedule_ready = false;
+  c->levels_ready = false;
 }
 
 // Dependency levels of the two triangular sweeps (computed once per pattern on
@@ -405,18 +406,25 @@ int compute_coloring(int n, const int32_t* rp, const int32_t* cl, uint8_t* color
   return nc;
 }
 
-void build_schedule(afem_ctx* c) {
-  if (c->schedule_ready) return;
+void build_schedule(afem_ctx* c, bool levels) {
+  if (c->schedule_ready && (!levels || c->levels_ready)) return;
   const int n = c->nline;
   cudaStream_t s = c->stream;
-  std::vector<int32_t> rp(n + 1), dp(n), cl(c->nnz), pf(n), pb(n);
+  std::vector<int32_t> rp(n + 1), dp(n), cl(c->nnz);
   c->rowptr.download(rp.data(), n + 1, s);
   c->diagpos.download(dp.data(), n, s);
   c->col.download(cl.data(), c->nnz, s);
   AFEM_CUDA(cudaStreamSynchronize(s));
-  compute_schedule(n, rp.data(), dp.data(), cl.data(), pf.data(), pb.data(), &c->levels_f, &c->levels_b);
-  c->perm_f.upload(pf.data(), n, s);
-  c->perm_b.upload(pb.data(), n, s);
+  if (levels && !c->levels_ready) {
+    // the natural-order sweeps' dependency levels (IC, SSOR, DIAG, none)
+    std::vector<int32_t> pf(n), pb(n);
+    compute_schedule(n, rp.data(), dp.data(), cl.data(), pf.data(), pb.data(), &c->levels_f, &c->levels_b);
+    c->perm_f.upload(pf.data(), n, s);
+    c->perm_b.upload(pb.data(), n, s);
+    AFEM_CUDA(cudaStreamSynchronize(s));
+    c->levels_ready = true;
+  }
+  if (c->schedule_ready) return;
   std::vector<uint8_t> color(n);
   std::vector<int32_t> pm(n), cptr(256);
   const int nc = compute_coloring(n, rp.data(), cl.data(), color.data(), pm.data(), cptr.data(), 255);

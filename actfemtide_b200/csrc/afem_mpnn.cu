@@ -10,8 +10,9 @@
 //   a_ij = K_ij/(s_i s_j), b_ij = omega M_ij/(s_i s_j)
 //   h <- h + relu(X W_l + c_l)   (l = 0..5, GEMM 144 x 48 on the tensor cores)
 //   z_i = r_i/s_i^2 + rms * (o_i0 + i o_i1)/s_i,  o = h W_out  (Jacobi term + learned correction)
-// One fused kernel per layer: each warp aggregates its 16 rows' neighbours (four
-// rows at a time, 8 lanes per row) into a shared-memory tile, then every warp
+// One fused kernel per layer: each warp aggregates its 16 rows' neighbours (five
+// rows at a time, 6 lanes per row, 16-byte loads) into a shared-memory tile, with the
+// message weights of every matrix entry computed once per solve, then every warp
 // multiplies its 16 x 144 tile by W_l with
 // mma.sync.m16n8k16 (BF16 in, FP32 accumulate) and applies bias, ReLU and the
 // residual in registers.
@@ -78,6 +79,30 @@ __global__ void k_rowinfo(const double2* __restrict__ km, const int32_t* __restr
   feat[i] = make_float4((float)(ar / mag), (float)(ai / mag), bc ? (float)bc[row] : 0.f, 1.f);
 }
 
+// The message weights of every matrix entry for one omega per system, computed once per solve
+// (every layer of every application reuses them): ew[sy*nnz + k] = (K_ij, omega M_ij)/(s_i s_j)
+// for j != i, 0 on the diagonal (which the aggregation leaves out).
+__global__ void k_edge_w(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                         const double2* __restrict__ km, const float* __restrict__ s,
+                         const double* __restrict__ omega, int n, int ns, long nnz, float2* __restrict__ ew) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)n * ns) return;
+  const int row = (int)(i % n), sy = (int)(i / n);
+  const float si = s[i];
+  const double om = omega[sy];
+  float2* out = ew + (long)sy * nnz;
+  for (int k = rowptr[row]; k < rowptr[row + 1]; ++k) {
+    const int j = col[k];
+    if (j == row) {
+      out[k] = make_float2(0.f, 0.f);
+      continue;
+    }
+    const double2 e = km[k];
+    const float inv = 1.0f / (si * s[(long)sy * n + j]);
+    out[k] = make_float2((float)e.x * inv, (float)(om * e.y) * inv);
+  }
+}
+
 // h0 = x W_in (FP32 FMA, K = 8), rows x systems in one launch.
 template <class V>
 __global__ void k_encode(const V* __restrict__ r, int n, int ns, const float* __restrict__ s,
@@ -108,10 +133,19 @@ __global__ void k_encode(const V* __restrict__ r, int n, int ns, const float* __
 
 // One message-passing layer for rows x systems (blockIdx.y = system).
 // save_x / save_y (training) keep the layer input tile and the pre-activation.
+__device__ __forceinline__ void agg_add8(float (&aa)[8], float (&ab)[8], float2 w, uint4 u) {
+  const unsigned q[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float2 hj = unpack_bf16(q[k]);
+    aa[2 * k] += w.x * hj.x; aa[2 * k + 1] += w.x * hj.y;
+    ab[2 * k] += w.y * hj.x; ab[2 * k + 1] += w.y * hj.y;
+  }
+}
+
 __global__ void __launch_bounds__(128)
-    k_layer(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const double2* __restrict__ km,
-            const float* __restrict__ s, const double* __restrict__ omega, int n,
-            const __nv_bfloat16* __restrict__ h_in, __nv_bfloat16* __restrict__ h_out,
+    k_layer(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col, const float2* __restrict__ ew,
+            long nnz, int n, const __nv_bfloat16* __restrict__ h_in, __nv_bfloat16* __restrict__ h_out,
             const __nv_bfloat16* __restrict__ wt,  // W_l transposed, bf16 [H][XW]
             const float* __restrict__ bias, __nv_bfloat16* __restrict__ save_x, __nv_bfloat16* __restrict__ save_y,
             const int* skip) {
@@ -122,79 +156,59 @@ __global__ void __launch_bounds__(128)
   const long base = (long)sy * n;
   for (int k = threadIdx.x; k < H * XW; k += blockDim.x) ws[(k / XW) * XS + (k % XW)] = wt[k];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const double om = omega[sy];
   const int r0 = blockIdx.x * ROWS + w * 16;
-  // ---- aggregate: four rows of the warp's 16 at a time, 8 lanes per row, each lane
-  // owning features 6*l8 .. 6*l8+5 (words 3*l8 .. 3*l8+2 of a row's 24); two
-  // neighbours' loads in flight per row; each feature sums its neighbours in entry order
-  const int sub = lane >> 3, l8 = lane & 7;
-  for (int rr = sub; rr < 16; rr += 4) {
-    const int row = r0 + rr;
-    unsigned* xrow = reinterpret_cast<unsigned*>(xs + (w * 16 + rr) * XS);
-    if (row < n) {
-      float aa[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, ab[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      const unsigned* own = reinterpret_cast<const unsigned*>(h_in + (base + row) * H) + 3 * l8;
-      const unsigned o0 = own[0], o1 = own[1], o2 = own[2];
-      const float si = s[base + row];
-      const int k1 = rowptr[row + 1];
-      int k = rowptr[row];
-      for (; k + 1 < k1; k += 2) {
-        const int ja = col[k], jb = col[k + 1];
-        const double2 ea = km[k], eb = km[k + 1];
-        const float sa = s[base + ja], sb = s[base + jb];
-        const unsigned* pa = reinterpret_cast<const unsigned*>(h_in + (base + ja) * H) + 3 * l8;
-        const unsigned* pb = reinterpret_cast<const unsigned*>(h_in + (base + jb) * H) + 3 * l8;
-        const unsigned ua[3] = {pa[0], pa[1], pa[2]}, ub[3] = {pb[0], pb[1], pb[2]};
-        if (ja != row) {
-          const float inv = 1.0f / (si * sa);
-          const float wa = (float)ea.x * inv, wb = (float)(om * ea.y) * inv;
+  // ---- aggregate: each warp its own 16 rows, five at a time with six lanes per row; lane
+  // sub of a row owns features 8*sub .. 8*sub+7, one 16-byte word of the row's 96 bytes, so
+  // a neighbour's row is one load per lane (three full sectors); four neighbours in flight;
+  // each feature sums its neighbours in entry order
+  {
+    const int slot = lane / 6, sub = lane - 6 * (lane / 6);
+    const float2* ewr = ew + (long)sy * nnz;
+    for (int pass = 0; pass < 4; ++pass) {
+      const int rr = pass * 5 + slot;
+      if (slot >= 5 || rr >= 16) continue;
+      const int row = r0 + rr;
+      unsigned* xrow = reinterpret_cast<unsigned*>(xs + (w * 16 + rr) * XS);
+      if (row < n) {
+        float aa[8], ab[8];
 #pragma unroll
-          for (int q = 0; q < 3; ++q) {
-            const float2 hj = unpack_bf16(ua[q]);
-            aa[2 * q] += wa * hj.x; aa[2 * q + 1] += wa * hj.y;
-            ab[2 * q] += wb * hj.x; ab[2 * q + 1] += wb * hj.y;
-          }
+        for (int q = 0; q < 8; ++q) { aa[q] = 0.f; ab[q] = 0.f; }
+        const uint4 o = reinterpret_cast<const uint4*>(h_in + (base + row) * H)[sub];
+        const int k1 = rowptr[row + 1];
+        int k = rowptr[row];
+        for (; k + 3 < k1; k += 4) {
+          int j[4];
+          float2 wk[4];
+          uint4 u[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) { j[q] = col[k + q]; wk[q] = ewr[k + q]; }
+#pragma unroll
+          for (int q = 0; q < 4; ++q) u[q] = reinterpret_cast<const uint4*>(h_in + (base + j[q]) * H)[sub];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) agg_add8(aa, ab, wk[q], u[q]);
         }
-        if (jb != row) {
-          const float inv = 1.0f / (si * sb);
-          const float wa = (float)eb.x * inv, wb = (float)(om * eb.y) * inv;
-#pragma unroll
-          for (int q = 0; q < 3; ++q) {
-            const float2 hj = unpack_bf16(ub[q]);
-            aa[2 * q] += wa * hj.x; aa[2 * q + 1] += wa * hj.y;
-            ab[2 * q] += wb * hj.x; ab[2 * q + 1] += wb * hj.y;
-          }
+        for (; k < k1; ++k) {
+          const int j = col[k];
+          const float2 wk = ewr[k];
+          const uint4 u = reinterpret_cast<const uint4*>(h_in + (base + j) * H)[sub];
+          agg_add8(aa, ab, wk, u);
         }
-      }
-      if (k < k1) {
-        const int j = col[k];
-        if (j != row) {
-          const double2 e = km[k];
-          const float inv = 1.0f / (si * s[base + j]);
-          const float wa = (float)e.x * inv, wb = (float)(om * e.y) * inv;
-          const unsigned* pj = reinterpret_cast<const unsigned*>(h_in + (base + j) * H) + 3 * l8;
+        xrow[4 * sub] = o.x;
+        xrow[4 * sub + 1] = o.y;
+        xrow[4 * sub + 2] = o.z;
+        xrow[4 * sub + 3] = o.w;
 #pragma unroll
-          for (int q = 0; q < 3; ++q) {
-            const float2 hj = unpack_bf16(pj[q]);
-            aa[2 * q] += wa * hj.x; aa[2 * q + 1] += wa * hj.y;
-            ab[2 * q] += wb * hj.x; ab[2 * q + 1] += wb * hj.y;
-          }
+        for (int q = 0; q < 4; ++q) {
+          xrow[24 + 4 * sub + q] = pack_bf16(aa[2 * q], aa[2 * q + 1]);
+          xrow[48 + 4 * sub + q] = pack_bf16(ab[2 * q], ab[2 * q + 1]);
         }
-      }
-      xrow[3 * l8] = o0;
-      xrow[3 * l8 + 1] = o1;
-      xrow[3 * l8 + 2] = o2;
+      } else {
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        xrow[24 + 3 * l8 + q] = pack_bf16(aa[2 * q], aa[2 * q + 1]);
-        xrow[48 + 3 * l8 + q] = pack_bf16(ab[2 * q], ab[2 * q + 1]);
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        xrow[3 * l8 + q] = 0u;
-        xrow[24 + 3 * l8 + q] = 0u;
-        xrow[48 + 3 * l8 + q] = 0u;
+        for (int q = 0; q < 4; ++q) {
+          xrow[4 * sub + q] = 0u;
+          xrow[24 + 4 * sub + q] = 0u;
+          xrow[48 + 4 * sub + q] = 0u;
+        }
       }
     }
   }
@@ -604,6 +618,7 @@ struct MpnnState {
   int ns = 0;
   DBuf<float> s;
   DBuf<float4> feat;
+  DBuf<float2> ew;                       // message weights per (system, matrix entry), per solve
   DBuf<double> omega, rms;
   DBuf<__nv_bfloat16> h[L + 1];          // activations (training keeps all; inference ping-pongs 0/1)
   DBuf<__nv_bfloat16> sx[L], sy[L];      // saved layer inputs / pre-activations (training)
@@ -661,6 +676,10 @@ void rowinfo(afem_ctx* c, MpnnState* S, int ns) {
   k_rowinfo<<<blocks(rows, 256), 256, 0, c->stream>>>(c->km.p, c->diagpos.p, c->bc.p, c->nline, S->omega.p, ns, S->s.p,
                                                        S->feat.p);
   count_launch();
+  S->ew.alloc((size_t)ns * c->nnz);
+  k_edge_w<<<blocks(rows, 128), 128, 0, c->stream>>>(c->rowptr.p, c->col.p, c->km.p, S->s.p, S->omega.p, c->nline, ns,
+                                                     c->nnz, S->ew.p);
+  count_launch();
 }
 
 template <class V>
@@ -676,7 +695,7 @@ void forward(afem_ctx* c, MpnnState* S, int ns, const V* r, V* z, bool train, co
   for (int l = 0; l < L; ++l) {
     const __nv_bfloat16* hin = train ? S->h[l].p : S->h[l & 1].p;
     __nv_bfloat16* hout = train ? S->h[l + 1].p : S->h[(l + 1) & 1].p;
-    k_layer<<<grid, 128, 0, st>>>(c->rowptr.p, c->col.p, c->km.p, S->s.p, S->omega.p, n, hin, hout,
+    k_layer<<<grid, 128, 0, st>>>(c->rowptr.p, c->col.p, S->ew.p, c->nnz, n, hin, hout,
                                   S->wt.p + (size_t)l * XW * H, S->small.p + FIN * H + l * H,
                                   train ? S->sx[l].p : nullptr, train ? S->sy[l].p : nullptr, skip);
     count_launch();

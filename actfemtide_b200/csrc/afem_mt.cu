@@ -387,12 +387,13 @@ __global__ void __launch_bounds__(512) k_band_ldlt(const BandSys* __restrict__ s
       y[k + d] = csub(y[k + d], cmul(l, yk));
     }
     __syncthreads();
-    const int tot = m * m;
-    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
-      const int j = idx / m + 1, i = idx - (j - 1) * m + 1;
-      if (i < j) continue;
-      double2* p = L + (long)(k + j) * ld + (i - j);
-      *p = csub(*p, cmul(lb[i], cb[j]));
+    // trailing update A[k+i][k+j] -= l_i * c_j (j <= i): warps take the columns k+j in turn,
+    // lanes run down a column (contiguous in the band)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int j = 1 + warp; j <= m; j += nw) {
+      const double2 cj = cb[j];
+      double2* colp = L + (long)(k + j) * ld - j;
+      for (int i = j + lane; i <= m; i += 32) colp[i] = csub(colp[i], cmul(lb[i], cj));
     }
     __syncthreads();
   }

@@ -2732,7 +2732,10 @@ void ensure_mc_values(afem_ctx* c) {
 int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, const afem_solve_opts* o,
                  afem_solve_stats* st, const SolveExtra* ex) {
   AFEM_REQUIRE(c->assembled, AFEM_ESTATE, "solve: system not assembled");
-  build_schedule(c);
+  // the multicolour paths never read the natural-order level schedules
+  const bool mc_only = o->precond == AFEM_PRECOND_HYBRID || o->precond == AFEM_PRECOND_SSOR_MC ||
+                       (o->precond == AFEM_PRECOND_LEARNED && mpnn_base(c) == 1);
+  build_schedule(c, !mc_only);
   ensure_mc_values(c);
   if (o->precond == AFEM_PRECOND_HYBRID || (o->precond == AFEM_PRECOND_LEARNED && mpnn_base(c) == 1))
     hybrid_prepare(c);
@@ -2756,7 +2759,7 @@ int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, cons
 void precond_apply_device(afem_ctx* c, double omega, const double2* r, double2* z) {
   AFEM_REQUIRE(c->assembled, AFEM_ESTATE, "preconditioner: system not assembled");
   AFEM_REQUIRE(c->nseg == 0, AFEM_EINVAL, "preconditioner: packed batches are not supported here");
-  build_schedule(c);
+  build_schedule(c, false);
   ensure_mc_values(c);
   hybrid_prepare(c);
   SolverWork* w = ensure_work<1, false>(c, 1, false);

@@ -467,11 +467,13 @@ def graded_levels(top: float, first: float, ratio: float, n: int) -> np.ndarray:
 
 
 def mt_box(nx: int, ny: int, n_air: int, n_earth: int, *, half_km: float = 50.0, air_km: float = 50.0,
-           earth_km: float = 50.0, first_km: float = 1.0, ratio: float = 1.25, sigma: float = 0.1,
+           earth_km: float = 50.0, first_km: float = 1.0, ratio: float = 1.25, ratio_air: float | None = None,
+           ratio_earth: float | None = None, sigma: float = 0.1,
            block_sigma: float | None = None, grf: bool = False, seed: int = 0, site_grid=None, freqs=None,
            name: str = "mt_box") -> TidalModel:
     """A magnetotelluric model on a Kuhn box over [-half_km, half_km]^2 with graded vertical cells
-    (n_air above z = 0 up to air_km, n_earth below down to -earth_km, finest at the surface).
+    (n_air above z = 0 up to air_km, n_earth below down to -earth_km, finest at the surface; each
+    region's cells grow by its ratio, scaled to fill the region, so the ratio sets the first cell).
 
     Physical tags as the MT program reads them (``n4flag(:,1)``,
     ``src/src_3DMT/forward_3DMT.f90:240``): air (centroid z > 0) tag 1 with
@@ -482,8 +484,8 @@ def mt_box(nx: int, ny: int, n_air: int, n_earth: int, *, half_km: float = 50.0,
     ``sigma(iele - nphys1)`` expects.  Sites 1 m below the surface on
     `site_grid` (default 5x5 over +-30 km); no tidal source (``nodes`` = 0).
     """
-    za = graded_levels(air_km, first_km, ratio, n_air)
-    ze = graded_levels(earth_km, first_km, ratio, n_earth)
+    za = graded_levels(air_km, first_km, ratio if ratio_air is None else ratio_air, n_air)
+    ze = graded_levels(earth_km, first_km, ratio if ratio_earth is None else ratio_earth, n_earth)
     zs = np.concatenate([0.0 - ze[::-1], za[1:]])
     xyz, tets, hex_of_tet, cen = kuhn_box(nx, ny, n_air + n_earth, (-half_km, half_km), (-half_km, half_km),
                                           zs=zs)

@@ -1,6 +1,7 @@
 """Train the learned preconditioner on the GPU and write its checkpoint.
 
   python -m actfemtide_b200.train_learned [--models 512] [--steps 2] [--lr 1e-3] [--base hybrid|jacobi] [--out PATH]
+  python -m actfemtide_b200.train_learned --eval-only [--eval 4]     (held-out evaluation and network time only)
 
 Training models: seeded log-normal conductivity on the 32x32x24 mesh (air and
 sea layers, M2 source); residuals from FP64 COCG with the network's base
@@ -51,11 +52,26 @@ def main():
     ap.add_argument("--base", choices=["jacobi", "hybrid"], default="hybrid",
                     help="jacobi: the network is the preconditioner; hybrid: it corrects the gradient-corrected SSOR")
     ap.add_argument("--out", default=None)
+    ap.add_argument("--eval-only", action="store_true",
+                    help="no training: evaluate the saved checkpoint, and time the network per iteration "
+                         "(zero output weights leave the iterations of the base, so the time difference is the network)")
     a = ap.parse_args()
     base = 1 if a.base == "hybrid" else 0
     out = a.out or (learned.HYBRID_CKPT if base else learned.DEFAULT_CKPT)
     freq = 1.0 / synth.M2_PERIOD_S
     t0 = time.time()
+    if a.eval_only:
+        with Forward(0) as fw:
+            held = [learned.training_model(100_000 + k) for k in range(a.eval)]
+            fw.load_model(held[0])
+            ev = evaluate(fw, learned.load(out), held, freq, base=base)
+            ev0 = evaluate(fw, learned.init_params(a.seed), held[:1], freq, base=base)
+        r0 = ev0[0]
+        ref = r0["hybrid" if base else "none"]
+        per_it = (r0["learned"]["seconds"] - ref["seconds"]) / max(1, r0["learned"]["iterations"])
+        print(json.dumps({"checkpoint": out, "held_out": ev, "zero_output_weights": r0,
+                          "network_ms_per_iteration": 1e3 * per_it, "wall_s": time.time() - t0}))
+        return
     with Forward(0) as fw:
         p, rec = learned.train(fw, a.models, a.steps, a.lr, a.seed, a.epochs, base=base)
         held = [learned.training_model(100_000 + k) for k in range(a.eval)]

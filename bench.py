@@ -710,7 +710,8 @@ def run_reference(args):
     per_it = timed / (16.0 * its)
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": 1e3 * timed / args.steps, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-           "dtype": "complex-f64", "data": "synthetic (seeded Kuhn-split boxes, log-normal subsurface, tidal sources)",
+           "dtype": "complex-f64" + (" COCG, complex-f32 preconditioner" if args.mt_precision == "pc32" else ""),
+           "data": "synthetic (seeded Kuhn-split boxes, log-normal subsurface, tidal sources)",
            "config": shared_config(c1_desc(), 16, ws, nnz),
            "method": {"name": "reference", "solver": "COCG13_single with SSOR (the reference's iterative solver; "
                                                      "its production solver, MKL PARDISO, is a closed binary)",
@@ -735,6 +736,93 @@ def run_reference(args):
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
            "wall_s": time.perf_counter() - t_all}
     print(json.dumps(out), flush=True)
+
+
+def mt_model(workload: str):
+    """The MT workload: a Kuhn box with graded vertical cells, a log-normal earth around 10 Ohm m
+    and a 2 Ohm m block, 8 frequencies from 1 mHz to 0.3 Hz, sites on a 20 x 20 grid."""
+    from actfemtide_b200 import synth
+    # cell growth per region chosen so the first cells at the surface are about 0.5 km (large),
+    # 1 km (medium) thick, near the horizontal cell size
+    dims, ra, re_ = {"large": ((96, 96, 24, 40), 1.11, 1.042), "medium": ((48, 48, 12, 20), 1.2, 1.1),
+                     "small": ((20, 20, 8, 12), 1.25, 1.15)}[workload]
+    freqs = np.logspace(-3, np.log10(0.3), 8)
+    grid = np.linspace(-40.0, 40.0, 20)
+    return synth.mt_box(*dims, ratio_air=ra, ratio_earth=re_, grf=True, seed=0, block_sigma=0.5, freqs=freqs,
+                        site_grid=grid, name="mt%dx%dx%d" % (dims[0], dims[1], dims[2] + dims[3]))
+
+
+def run_mt(args):
+    """The 3-D MT forward (afem_mt_forward): per call the four side faces' 2-D TM solves at every
+    frequency, the lifted 3-D systems of both polarisations, their batched solve, the sites and
+    the impedances.  Inputs resident on the device; the call returns the impedances to the host."""
+    import torch
+    from actfemtide_b200 import synth
+    from actfemtide_b200.forward import MTForward
+    from oracle import oracle as O
+    t_all = time.perf_counter()
+    m = mt_model(args.workload)
+    fw = MTForward(0)
+    fw.load_mt_model(m)
+    kw = dict(precond=args.precond or "HYBRID", precision=args.mt_precision, tol=TOL, maxit=args.maxit)
+    for _ in range(args.warmup):
+        r = fw.mt_forward(m.freqs, m.sites, **kw)
+    torch.cuda.synchronize()
+    clk = ClockSampler(0)
+    clk.start()
+    times, res = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = fw.mt_forward(m.freqs, m.sites, **kw)
+        times.append(time.perf_counter() - t0)
+        res.append(r.solve)
+    clocks = clk.stop()
+    # one more call with per-kernel events (outside the timed region)
+    fw._check(fw._L.afem_set_profiling(fw.ctx, 1))
+    fw.mt_forward(m.freqs, m.sites, **kw)
+    prof = {}
+    for i in range(fw._L.afem_profile_count(fw.ctx)):
+        import ctypes as C
+        buf = C.create_string_buffer(128); ms = C.c_double(); nl = C.c_long()
+        fw._L.afem_profile_entry(fw.ctx, i, buf, 128, C.byref(ms), C.byref(nl))
+        prof[buf.value.decode()] = round(ms.value, 3)
+    fw._check(fw._L.afem_set_profiling(fw.ctx, 0))
+    fw.close()
+    ok = all(x.ok for x in res)
+    pair = None
+    if args.mt_pair:
+        # a converged GPU / CPU pair on the 10 x 10 x 18 half-space model: the device against the oracle
+        # with a direct (SuperLU) solve, the PARDISO stand-in of the reference
+        ms_ = synth.mt_box(10, 10, 6, 12, sigma=0.1, freqs=[0.01], site_grid=(-20.0, 0.0, 20.0))
+        with MTForward(0) as f2:
+            f2.load_mt_model(ms_)
+            f2.mt_forward(ms_.freqs, ms_.sites, **kw)
+            t0 = time.perf_counter()
+            rg = f2.mt_forward(ms_.freqs, ms_.sites, **kw)
+            gpu_s = time.perf_counter() - t0
+        line, n6 = O.mkline(ms_.node, ms_.n4)
+        t0 = time.perf_counter()
+        ro = O.MTOracle(ms_, line, n6).forward(ms_.freqs, ms_.sites)
+        cpu_s = time.perf_counter() - t0
+        pair = {"workload": "10x10x18 half-space, 1 frequency, 9 sites", "gpu_s": gpu_s, "cpu_oracle_direct_s": cpu_s,
+                "z_rel_diff": float(np.abs(rg.z - ro["z"]).max() / np.abs(ro["z"]).max())}
+    value = statistics.mean(times)
+    out = {"metric": "s per 3-D MT forward (8 frequencies x 2 polarisations to 1e-8, 400 sites)",
+           "value": value, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": 1e3 * value, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+           "dtype": "complex-f64" + (" COCG, complex-f32 preconditioner" if args.mt_precision == "pc32" else ""),
+           "data": "synthetic (seeded graded Kuhn box, log-normal earth, 2 Ohm m block)",
+           "config": {"workload": f"{m.name}: {m.ntet} tets, 8 frequencies {m.freqs[0]:.3g}..{m.freqs[-1]:.3g} Hz, "
+                                  f"{m.sites.shape[0]} sites", "method": kw["precond"],
+                      "l2": "working set > 126 MB L2"},
+           "solver": {"iterations": [x.iterations for x in res], "resid_true_max": max(x.resid_true for x in res),
+                      "converged": ok},
+           "phases_ms": prof, "clocks": clocks,
+           "like_for_like_small": pair,
+           "wall_s": time.perf_counter() - t_all}
+    print(json.dumps(out), flush=True)
+    if not ok and not args.allow_unconverged:
+        sys.exit(3)
 
 
 def main():
@@ -767,8 +855,15 @@ def main():
     p.add_argument("--ckpt", default=None, help="learned methods: checkpoint path (without extension)")
     p.add_argument("--profile-case", action="store_true",
                    help="for profiler captures: one assembly and solve capped at --maxit, then exit (no bench line)")
+    p.add_argument("--mt", action="store_true",
+                   help="time the 3-D MT forward (afem_mt_forward) instead of the tidal step")
+    p.add_argument("--mt-precision", default="pc32", choices=["fp64", "pc32"],
+                   help="--mt: the preconditioner's precision (FP32 preconditioner by default, as the tidal step)")
+    p.add_argument("--mt-pair", type=int, default=1, help="--mt: 1 times the converged GPU/CPU pair on a small model")
     args = p.parse_args()
-    if args.impl == "reference":
+    if args.mt:
+        run_mt(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)
