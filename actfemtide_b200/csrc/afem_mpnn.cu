@@ -10,8 +10,8 @@
 //   a_ij = K_ij/(s_i s_j), b_ij = omega M_ij/(s_i s_j)
 //   h <- h + relu(X W_l + c_l)   (l = 0..5, GEMM 144 x 48 on the tensor cores)
 //   z_i = r_i/s_i^2 + rms * (o_i0 + i o_i1)/s_i,  o = h W_out  (Jacobi term + learned correction)
-// One fused kernel per layer: each warp aggregates its 16 rows' neighbours (five
-// rows at a time, 6 lanes per row, 16-byte loads) into a shared-memory tile, with the
+// One fused kernel per layer: the block aggregates its 64 rows' neighbours (all rows
+// at once, 2 lanes per row, 16-byte loads) into a shared-memory tile, with the
 // message weights of every matrix entry computed once per solve, then every warp
 // multiplies its 16 x 144 tile by W_l with
 // mma.sync.m16n8k16 (BF16 in, FP32 accumulate) and applies bias, ReLU and the
@@ -133,10 +133,10 @@ __global__ void k_encode(const V* __restrict__ r, int n, int ns, const float* __
 
 // One message-passing layer for rows x systems (blockIdx.y = system).
 // save_x / save_y (training) keep the layer input tile and the pre-activation.
-__device__ __forceinline__ void agg_add8(float (&aa)[8], float (&ab)[8], float2 w, uint4 u) {
-  const unsigned q[4] = {u.x, u.y, u.z, u.w};
+__device__ __forceinline__ void agg_add(float (&aa)[24], float (&ab)[24], float2 w, const uint4 (&u)[3]) {
+  const unsigned* q = reinterpret_cast<const unsigned*>(u);
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < 12; ++k) {
     const float2 hj = unpack_bf16(q[k]);
     aa[2 * k] += w.x * hj.x; aa[2 * k + 1] += w.x * hj.y;
     ab[2 * k] += w.y * hj.x; ab[2 * k + 1] += w.y * hj.y;
@@ -157,58 +157,51 @@ __global__ void __launch_bounds__(128)
   for (int k = threadIdx.x; k < H * XW; k += blockDim.x) ws[(k / XW) * XS + (k % XW)] = wt[k];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int r0 = blockIdx.x * ROWS + w * 16;
-  // ---- aggregate: each warp its own 16 rows, five at a time with six lanes per row; lane
-  // sub of a row owns features 8*sub .. 8*sub+7, one 16-byte word of the row's 96 bytes, so
-  // a neighbour's row is one load per lane (three full sectors); four neighbours in flight;
-  // each feature sums its neighbours in entry order
+  // ---- aggregate: all 64 rows of the block at once, two lanes per row, each lane owning
+  // features 24*half .. 24*half+23 (three 16-byte words of the row's 96 bytes), two
+  // neighbours' loads in flight; each feature sums its neighbours in entry order
   {
-    const int slot = lane / 6, sub = lane - 6 * (lane / 6);
-    const float2* ewr = ew + (long)sy * nnz;
-    for (int pass = 0; pass < 4; ++pass) {
-      const int rr = pass * 5 + slot;
-      if (slot >= 5 || rr >= 16) continue;
-      const int row = r0 + rr;
-      unsigned* xrow = reinterpret_cast<unsigned*>(xs + (w * 16 + rr) * XS);
-      if (row < n) {
-        float aa[8], ab[8];
+    const int rr = threadIdx.x >> 1, half = threadIdx.x & 1;
+    const int row = blockIdx.x * ROWS + rr;
+    unsigned* xrow = reinterpret_cast<unsigned*>(xs + rr * XS);
+    if (row < n) {
+      float aa[24], ab[24];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) { aa[q] = 0.f; ab[q] = 0.f; }
-        const uint4 o = reinterpret_cast<const uint4*>(h_in + (base + row) * H)[sub];
-        const int k1 = rowptr[row + 1];
-        int k = rowptr[row];
-        for (; k + 3 < k1; k += 4) {
-          int j[4];
-          float2 wk[4];
-          uint4 u[4];
+      for (int k = 0; k < 24; ++k) { aa[k] = 0.f; ab[k] = 0.f; }
+      const uint4* own = reinterpret_cast<const uint4*>(h_in + (base + row) * H) + 3 * half;
+      const uint4 o[3] = {own[0], own[1], own[2]};
+      const float2* ewr = ew + (long)sy * nnz;
+      const int k1 = rowptr[row + 1];
+      int k = rowptr[row];
+      for (; k + 1 < k1; k += 2) {
+        const int ja = col[k], jb = col[k + 1];
+        const float2 wa = ewr[k], wb = ewr[k + 1];
+        const uint4* pa = reinterpret_cast<const uint4*>(h_in + (base + ja) * H) + 3 * half;
+        const uint4* pb = reinterpret_cast<const uint4*>(h_in + (base + jb) * H) + 3 * half;
+        const uint4 ua[3] = {pa[0], pa[1], pa[2]}, ub[3] = {pb[0], pb[1], pb[2]};
+        agg_add(aa, ab, wa, ua);
+        agg_add(aa, ab, wb, ub);
+      }
+      if (k < k1) {
+        const int j = col[k];
+        const float2 wj = ewr[k];
+        const uint4* pj = reinterpret_cast<const uint4*>(h_in + (base + j) * H) + 3 * half;
+        const uint4 uj[3] = {pj[0], pj[1], pj[2]};
+        agg_add(aa, ab, wj, uj);
+      }
+      const unsigned* ow = reinterpret_cast<const unsigned*>(o);
 #pragma unroll
-          for (int q = 0; q < 4; ++q) { j[q] = col[k + q]; wk[q] = ewr[k + q]; }
+      for (int q = 0; q < 12; ++q) {
+        xrow[12 * half + q] = ow[q];
+        xrow[24 + 12 * half + q] = pack_bf16(aa[2 * q], aa[2 * q + 1]);
+        xrow[48 + 12 * half + q] = pack_bf16(ab[2 * q], ab[2 * q + 1]);
+      }
+    } else {
 #pragma unroll
-          for (int q = 0; q < 4; ++q) u[q] = reinterpret_cast<const uint4*>(h_in + (base + j[q]) * H)[sub];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) agg_add8(aa, ab, wk[q], u[q]);
-        }
-        for (; k < k1; ++k) {
-          const int j = col[k];
-          const float2 wk = ewr[k];
-          const uint4 u = reinterpret_cast<const uint4*>(h_in + (base + j) * H)[sub];
-          agg_add8(aa, ab, wk, u);
-        }
-        xrow[4 * sub] = o.x;
-        xrow[4 * sub + 1] = o.y;
-        xrow[4 * sub + 2] = o.z;
-        xrow[4 * sub + 3] = o.w;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          xrow[24 + 4 * sub + q] = pack_bf16(aa[2 * q], aa[2 * q + 1]);
-          xrow[48 + 4 * sub + q] = pack_bf16(ab[2 * q], ab[2 * q + 1]);
-        }
-      } else {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          xrow[4 * sub + q] = 0u;
-          xrow[24 + 4 * sub + q] = 0u;
-          xrow[48 + 4 * sub + q] = 0u;
-        }
+      for (int q = 0; q < 12; ++q) {
+        xrow[12 * half + q] = 0u;
+        xrow[24 + 12 * half + q] = 0u;
+        xrow[48 + 12 * half + q] = 0u;
       }
     }
   }

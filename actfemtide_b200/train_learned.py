@@ -1,7 +1,8 @@
 """Train the learned preconditioner on the GPU and write its checkpoint.
 
   python -m actfemtide_b200.train_learned [--models 512] [--steps 2] [--lr 1e-3] [--base hybrid|jacobi] [--out PATH]
-  python -m actfemtide_b200.train_learned --eval-only [--eval 4]     (held-out evaluation and network time only)
+  python -m actfemtide_b200.train_learned --eval-only [--eval 4]     (held-out evaluation against the base
+                                                                     alone, and the network's time per iteration)
 
 Training models: seeded log-normal conductivity on the 32x32x24 mesh (air and
 sea layers, M2 source); residuals from FP64 COCG with the network's base
@@ -22,13 +23,15 @@ from . import learned, synth
 from .forward import Forward
 
 
-def evaluate(fw, params, models, freq, tol=1e-8, maxit=20000, base=0):
+def evaluate(fw, params, models, freq, tol=1e-8, maxit=20000, base=0, with_ssor=True):
     """Iterations and time of flexible COCG with the network against its base and the reference's SSOR."""
     rows = []
     fw.mpnn_set_params(params)
     fw.mpnn_set_base(base == 1)
     runs = (("learned", "LEARNED"), ("hybrid", "HYBRID"), ("ssor", "SSOR")) if base == 1 else \
         (("learned", "LEARNED"), ("none", "NONE"), ("ssor", "SSOR"))
+    if not with_ssor:
+        runs = runs[:2]
     for m in models:
         fw.set_cond(m.sigma_air, m.sigma_ocean, 1, sigma_file=m.sigma_land)
         fw.assemble()
@@ -64,8 +67,8 @@ def main():
         with Forward(0) as fw:
             held = [learned.training_model(100_000 + k) for k in range(a.eval)]
             fw.load_model(held[0])
-            ev = evaluate(fw, learned.load(out), held, freq, base=base)
-            ev0 = evaluate(fw, learned.init_params(a.seed), held[:1], freq, base=base)
+            ev = evaluate(fw, learned.load(out), held, freq, base=base, with_ssor=False)
+            ev0 = evaluate(fw, learned.init_params(a.seed), held[:1], freq, base=base, with_ssor=False)
         r0 = ev0[0]
         ref = r0["hybrid" if base else "none"]
         per_it = (r0["learned"]["seconds"] - ref["seconds"]) / max(1, r0["learned"]["iterations"])
