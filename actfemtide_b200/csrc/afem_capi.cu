@@ -35,6 +35,19 @@ void check_status(afem_ctx* c, const char* what) {
   throw Error{code, buf};
 }
 
+HostTimer::HostTimer(afem_ctx* ctx, const char* nm) : c(ctx), name(nm), on(ctx->prof.on) {
+  if (on) {
+    cudaStreamSynchronize(c->stream);
+    t0 = std::chrono::steady_clock::now();
+  }
+}
+HostTimer::~HostTimer() {
+  if (!on) return;
+  cudaStreamSynchronize(c->stream);
+  const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  c->prof.add(name, ms);
+}
+
 std::atomic<long> g_launches{0};
 thread_local int g_capturing = 0;
 
@@ -185,6 +198,7 @@ int afem_set_mesh(afem_ctx* c, int node, const double* xyz, int ntet, const int3
   return guarded(c, [&]() {
     AFEM_REQUIRE(node > 0 && ntet > 0 && xyz && n4 && tag, AFEM_EINVAL, "set_mesh: empty mesh or null array");
     AFEM_REQUIRE(nline >= 0, AFEM_EINVAL, "set_mesh: negative nline");
+    afem::HostTimer ht(c, "host_set_mesh");
     for (long i = 0; i < 4L * ntet; ++i)
       AFEM_REQUIRE(n4[i] >= 1 && n4[i] <= node, AFEM_EINVAL, "set_mesh: node id outside 1..node in n4");
     if (nline > 0) {

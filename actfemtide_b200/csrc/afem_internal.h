@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -140,6 +141,17 @@ inline void count_launch(long n = 1) {
   if (e != cudaSuccess) throw Error{AFEM_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e)};
   if (!g_capturing) g_launches.fetch_add(n, std::memory_order_relaxed);
 }
+
+// Host wall time of a set-up phase, added to the profile table while profiling is on
+// (the stream is drained on both sides then, so the phase's device work is included).
+struct HostTimer {
+  afem_ctx* c;
+  const char* name;
+  std::chrono::steady_clock::time_point t0;
+  bool on;
+  HostTimer(afem_ctx* ctx, const char* nm);
+  ~HostTimer();
+};
 
 struct SolverWork;   // afem_solver.cu
 struct MpnnState;    // afem_mpnn.cu

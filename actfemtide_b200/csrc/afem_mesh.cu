@@ -6,6 +6,8 @@
 #include <algorithm>
 #include <vector>
 
+#include <memory>
+
 #include "afem_internal.h"
 
 namespace afem {
@@ -406,19 +408,63 @@ int compute_coloring(int n, const int32_t* rp, const int32_t* cl, uint8_t* color
   return nc;
 }
 
+namespace {
+
+// Colour-ordered split rows on the device: position p holds row perm[p]; lcnt/ucnt count its
+// entries of earlier / later colours, and the fill writes them in the row's CSR order.
+__global__ void k_split_count(const int32_t* __restrict__ rp, const int32_t* __restrict__ cl,
+                              const uint8_t* __restrict__ color, const int32_t* __restrict__ perm, int n,
+                              int32_t* __restrict__ lcnt, int32_t* __restrict__ ucnt) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int i = perm[p];
+    const int ci = color[i];
+    int nl = 0, nu = 0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      const int cj = color[cl[k]];
+      if (cj < ci) ++nl;
+      else if (cj > ci) ++nu;
+    }
+    lcnt[p] = nl;
+    ucnt[p] = nu;
+  }
+}
+
+__global__ void k_split_fill(const int32_t* __restrict__ rp, const int32_t* __restrict__ cl,
+                             const int32_t* __restrict__ dp, const uint8_t* __restrict__ color,
+                             const int32_t* __restrict__ perm, int n, const int32_t* __restrict__ lptr,
+                             const int32_t* __restrict__ uptr, int32_t* __restrict__ lcol, int32_t* __restrict__ lsrc,
+                             int32_t* __restrict__ ucol, int32_t* __restrict__ usrc, int32_t* __restrict__ dsrc) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int i = perm[p];
+    const int ci = color[i];
+    int a = lptr[p], b = uptr[p];
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      const int j = cl[k];
+      const int cj = color[j];
+      if (cj < ci) { lcol[a] = j; lsrc[a++] = k; }
+      else if (cj > ci) { ucol[b] = j; usrc[b++] = k; }
+    }
+    dsrc[p] = dp[i];
+  }
+}
+
+}  // namespace
+
 void build_schedule(afem_ctx* c, bool levels) {
   if (c->schedule_ready && (!levels || c->levels_ready)) return;
   const int n = c->nline;
   cudaStream_t s = c->stream;
-  std::vector<int32_t> rp(n + 1), dp(n), cl(c->nnz);
-  c->rowptr.download(rp.data(), n + 1, s);
-  c->diagpos.download(dp.data(), n, s);
-  c->col.download(cl.data(), c->nnz, s);
+  // host copies of the pattern for the colouring (left uninitialised: filled by the copies)
+  std::unique_ptr<int32_t[]> rp(new int32_t[n + 1]), cl(new int32_t[c->nnz]);
+  c->rowptr.download(rp.get(), n + 1, s);
+  c->col.download(cl.get(), c->nnz, s);
   AFEM_CUDA(cudaStreamSynchronize(s));
   if (levels && !c->levels_ready) {
     // the natural-order sweeps' dependency levels (IC, SSOR, DIAG, none)
-    std::vector<int32_t> pf(n), pb(n);
-    compute_schedule(n, rp.data(), dp.data(), cl.data(), pf.data(), pb.data(), &c->levels_f, &c->levels_b);
+    std::vector<int32_t> pf(n), pb(n), dp(n);
+    c->diagpos.download(dp.data(), n, s);
+    AFEM_CUDA(cudaStreamSynchronize(s));
+    compute_schedule(n, rp.get(), dp.data(), cl.get(), pf.data(), pb.data(), &c->levels_f, &c->levels_b);
     c->perm_f.upload(pf.data(), n, s);
     c->perm_b.upload(pb.data(), n, s);
     AFEM_CUDA(cudaStreamSynchronize(s));
@@ -427,7 +473,7 @@ void build_schedule(afem_ctx* c, bool levels) {
   if (c->schedule_ready) return;
   std::vector<uint8_t> color(n);
   std::vector<int32_t> pm(n), cptr(256);
-  const int nc = compute_coloring(n, rp.data(), cl.data(), color.data(), pm.data(), cptr.data(), 255);
+  const int nc = compute_coloring(n, rp.get(), cl.get(), color.data(), pm.data(), cptr.data(), 255);
   AFEM_REQUIRE(nc > 0, AFEM_EPATTERN, "colouring: more than 255 colours");
   c->ncolors = nc;
   c->color.upload(color.data(), n, s);
@@ -435,50 +481,29 @@ void build_schedule(afem_ctx* c, bool levels) {
   c->color_ptr.upload(cptr.data(), nc + 1, s);
   // colour-ordered split rows for the multicolour sweeps: position p holds row
   // perm[p]; its entries of earlier colours (the forward sweep's) and of later
-  // colours (the backward sweep's), each with the index of the entry in the CSR
+  // colours (the backward sweep's), each with the index of the entry in the CSR;
+  // built on the device from the colouring (counts, prefix sums, fill in CSR order)
   {
-    // two passes over the rows in parallel chunks (counts, then entries at the
-    // positions the prefix sums give), so the layout does not depend on the threads
-    std::vector<int32_t> lptr(n + 1), uptr(n + 1);
-    lptr[0] = uptr[0] = 0;
-    host_parallel_for(n, [&](long p0, long p1) {
-      for (long p = p0; p < p1; ++p) {
-        const int i = pm[p];
-        int nl = 0, nu = 0;
-        for (int k = rp[i]; k < rp[i + 1]; ++k) {
-          const int j = cl[k];
-          if (color[j] < color[i]) ++nl;
-          else if (color[j] > color[i]) ++nu;
-        }
-        lptr[p + 1] = nl;
-        uptr[p + 1] = nu;
-      }
-    });
-    for (int p = 0; p < n; ++p) {
-      lptr[p + 1] += lptr[p];
-      uptr[p + 1] += uptr[p];
-    }
-    std::vector<int32_t> lcol(lptr[n]), lsrc(lptr[n]), ucol(uptr[n]), usrc(uptr[n]);
-    host_parallel_for(n, [&](long p0, long p1) {
-      for (long p = p0; p < p1; ++p) {
-        const int i = pm[p];
-        int a = lptr[p], b = uptr[p];
-        for (int k = rp[i]; k < rp[i + 1]; ++k) {
-          const int j = cl[k];
-          if (color[j] < color[i]) { lcol[a] = j; lsrc[a++] = k; }
-          else if (color[j] > color[i]) { ucol[b] = j; usrc[b++] = k; }
-        }
-      }
-    });
-    c->mc_lptr.upload(lptr.data(), n + 1, s);
-    c->mc_lcol.upload(lcol.data(), lcol.size(), s);
-    c->mc_lsrc.upload(lsrc.data(), lsrc.size(), s);
-    c->mc_uptr.upload(uptr.data(), n + 1, s);
-    c->mc_ucol.upload(ucol.data(), ucol.size(), s);
-    c->mc_usrc.upload(usrc.data(), usrc.size(), s);
-    std::vector<int32_t> dsrc(n);
-    for (int p = 0; p < n; ++p) dsrc[p] = dp[pm[p]];
-    c->mc_dsrc.upload(dsrc.data(), n, s);
+    DBuf<int32_t> lcnt, ucnt;
+    lcnt.alloc(n);
+    ucnt.alloc(n);
+    const int nb = c->num_sms * 8;
+    k_split_count<<<nb, 256, 0, s>>>(c->rowptr.p, c->col.p, c->color.p, c->perm_mc.p, n, lcnt.p, ucnt.p);
+    count_launch();
+    c->mc_lptr.alloc(n + 1);
+    c->mc_uptr.alloc(n + 1);
+    long ltot = 0, utot = 0;
+    exclusive_scan(lcnt.p, c->mc_lptr.p, n, s, &ltot);
+    exclusive_scan(ucnt.p, c->mc_uptr.p, n, s, &utot);
+    c->mc_lcol.alloc(ltot);
+    c->mc_lsrc.alloc(ltot);
+    c->mc_ucol.alloc(utot);
+    c->mc_usrc.alloc(utot);
+    c->mc_dsrc.alloc(n);
+    k_split_fill<<<nb, 256, 0, s>>>(c->rowptr.p, c->col.p, c->diagpos.p, c->color.p, c->perm_mc.p, n, c->mc_lptr.p,
+                                    c->mc_uptr.p, c->mc_lcol.p, c->mc_lsrc.p, c->mc_ucol.p, c->mc_usrc.p,
+                                    c->mc_dsrc.p);
+    count_launch();
     c->mc_vals_gen = -1;
   }
   AFEM_CUDA(cudaStreamSynchronize(s));

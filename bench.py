@@ -409,6 +409,7 @@ def run_gpu(args):
     fw.set_profiling(True)
     step(maxit=args.prof_iters)
     prof = fw.profile()
+    prof = {k: v for k, v in prof.items() if not k.startswith("host_")}  # kernels only
     fw.set_profiling(False)
 
     # ---- end to end through the C ABI with pinned host buffers, copies inside the timed region
@@ -785,7 +786,8 @@ def run_mt(args):
         import ctypes as C
         buf = C.create_string_buffer(128); ms = C.c_double(); nl = C.c_long()
         fw._L.afem_profile_entry(fw.ctx, i, buf, 128, C.byref(ms), C.byref(nl))
-        prof[buf.value.decode()] = round(ms.value, 3)
+        if not buf.value.decode().startswith("host_"):
+            prof[buf.value.decode()] = round(ms.value, 3)
     fw._check(fw._L.afem_set_profiling(fw.ctx, 0))
     fw.close()
     ok = all(x.ok for x in res)
