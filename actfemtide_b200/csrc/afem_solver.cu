@@ -78,6 +78,7 @@ struct SolverWork {
   bool seg = false; // packed batch: vectors hold one system per row
   int nblocks = 0;  // persistent grid size (blocks of 256 threads)
   DBuf<double2> x, b;               // FP64 solution and right-hand side [row][sys]
+  DBuf<double2> xacc;               // FP64 solution accumulated over the refinement steps (kept between solves)
   DBuf<double2> r64;                // FP64 true residual
   DBuf<double2> r, z, p, q, dd;     // FP64 inner vectors
   DBuf<float2> rf, zf, pf, qf, ddf; // FP32 inner vectors
@@ -2275,7 +2276,10 @@ int inner_cocg(afem_ctx* c, SolverWork* w, const afem_solve_opts* o, int precond
   w->sd = o->sigma_diag > 0 ? o->sigma_diag : 1.0;
   setup_dd<T, PT, NS, SEG>(c, w, use_hyb ? AFEM_PRECOND_HYBRID : precond, w->sd);
   const int mode = precond;
-  tune_spmv<T, NS, SEG>(c, w);
+  {
+    HostTimer ht(c, "host_setup_spmv_tuner");
+    tune_spmv<T, NS, SEG>(c, w);
+  }
   const bool learned = mode == AFEM_PRECOND_LEARNED;
   if (learned) {
     using V = typename I::V;
@@ -2533,7 +2537,11 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
   const int nsys = SEG ? c->nseg : NS;
   const bool mixed = o->precision == AFEM_MIXED;
   const bool pc32 = o->precision == AFEM_FP32_PRECOND;
-  SolverWork* w = ensure_work<NS, SEG>(c, nsys, mixed, pc32);
+  SolverWork* w = nullptr;
+  {
+    HostTimer ht(c, "host_setup_work");
+    w = ensure_work<NS, SEG>(c, nsys, mixed, pc32);
+  }
   // ---- right-hand sides and omegas
   {
     DBuf<int> dsrc;
@@ -2569,7 +2577,7 @@ int solve_ns(afem_ctx* c, const double* freq, const int* srcs, const afem_solve_
   AFEM_CUDA(cudaEventCreate(&e1));
   AFEM_CUDA(cudaEventRecord(e0, s));
 
-  DBuf<double2> xacc;  // accumulated FP64 solution
+  DBuf<double2>& xacc = w->xacc;  // accumulated FP64 solution (allocated once per size)
   xacc.alloc(total);
   std::vector<double> rr, bb;
   double tol_scale = 1.0;  // inner tolerances are relative to ||r0||; the target is relative to ||b||
@@ -2735,10 +2743,18 @@ int solve_device(afem_ctx* c, int nsys, const double* freq, const int* src, cons
   // the multicolour paths never read the natural-order level schedules
   const bool mc_only = o->precond == AFEM_PRECOND_HYBRID || o->precond == AFEM_PRECOND_SSOR_MC ||
                        (o->precond == AFEM_PRECOND_LEARNED && mpnn_base(c) == 1);
-  build_schedule(c, !mc_only);
-  ensure_mc_values(c);
-  if (o->precond == AFEM_PRECOND_HYBRID || (o->precond == AFEM_PRECOND_LEARNED && mpnn_base(c) == 1))
+  {
+    HostTimer ht(c, "host_setup_schedule");
+    build_schedule(c, !mc_only);
+  }
+  {
+    HostTimer ht(c, "host_setup_mc_values");
+    ensure_mc_values(c);
+  }
+  if (o->precond == AFEM_PRECOND_HYBRID || (o->precond == AFEM_PRECOND_LEARNED && mpnn_base(c) == 1)) {
+    HostTimer ht(c, "host_setup_hybrid");
     hybrid_prepare(c);
+  }
   if (c->nseg > 0) {
     AFEM_REQUIRE(nsys == c->nseg, AFEM_EINVAL, "solve: a packed batch solves one system per mesh (nsys = nseg)");
     AFEM_REQUIRE(o->precond != AFEM_PRECOND_LEARNED, AFEM_EINVAL,
