@@ -1,7 +1,7 @@
 """CPU oracle checks: known answers from the reference sources, counts, identities, direct solves.
 
-The reference ships no tests or golden data for this path (SURVEY: no tests/,
-no CI), so the oracle is pinned by (i) the two known-answer examples written
+The reference ships no tests or golden data for this path (it has no tests/
+directory and no CI), so the oracle is pinned by (i) the two known-answer examples written
 in the reference's own sources, (ii) structural counts of the Kuhn meshes,
 (iii) mathematical identities of the edge-element system, (iv) a direct
 solve, and (v) the committed golden fixtures (regression).
