@@ -143,28 +143,11 @@ void hybrid_prepare(afem_ctx* c) {
     h->color.upload(color.data(), node, s);
     h->perm.upload(pm.data(), node, s);
     h->cptr.upload(cptr.data(), nc + 1, s);
-    {
-      std::vector<int32_t> lp(node + 1, 0), up(node + 1, 0), lc, ls, uc, us;
-      lc.reserve(nnz / 2); ls.reserve(nnz / 2); uc.reserve(nnz / 2); us.reserve(nnz / 2);
-      for (int p = 0; p < node; ++p) {
-        const int a = pm[p];
-        for (int k = rp[a]; k < rp[a + 1]; ++k) {
-          const int b = cl[k];
-          if (color[b] < color[a]) { lc.push_back(b); ls.push_back(k); }
-          else if (color[b] > color[a]) { uc.push_back(b); us.push_back(k); }
-        }
-        lp[p + 1] = (int32_t)lc.size();
-        up[p + 1] = (int32_t)uc.size();
-      }
-      h->lptr.upload(lp.data(), lp.size(), s);
-      h->lcol.upload(lc.data(), lc.size(), s);
-      h->lsrc.upload(ls.data(), ls.size(), s);
-      h->uptr.upload(up.data(), up.size(), s);
-      h->ucol.upload(uc.data(), uc.size(), s);
-      h->usrc.upload(us.data(), us.size(), s);
-      h->lkm.alloc(lc.size());
-      h->ukm.alloc(uc.size());
-    }
+    // colour-ordered split rows of the node graph, built on the device like the edges'
+    split_rows_device(c, h->rowptr.p, h->col.p, h->diagpos.p, h->color.p, h->perm.p, node, h->lptr, h->lcol, h->lsrc,
+                      h->uptr, h->ucol, h->usrc, nullptr);
+    h->lkm.alloc(h->lcol.n);
+    h->ukm.alloc(h->ucol.n);
     h->km.alloc(nnz);
     h->live.alloc(node);
     h->pattern_ready = true;

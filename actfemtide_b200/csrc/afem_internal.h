@@ -264,6 +264,13 @@ void build_schedule(afem_ctx* c, bool levels);  // colouring + split rows; the l
 void exclusive_scan(const int32_t* in, int32_t* out, int n, cudaStream_t s, long* total_host);
 int compute_coloring(int n, const int32_t* rp, const int32_t* cl, uint8_t* color, int32_t* perm, int32_t* cptr,
                      int max_colors);  // greedy distance-1 colouring, rows sorted by colour
+// Colour-ordered split rows of a CSR pattern on the device (rp, cl, dp, color, perm: device):
+// position p holds row perm[p], its entries of earlier colours (lptr/lcol/lsrc) and of later
+// colours (uptr/ucol/usrc) in the row's CSR order with their CSR indices; dsrc (optional)
+// the CSR index of the row's diagonal.
+void split_rows_device(afem_ctx* c, const int32_t* rp, const int32_t* cl, const int32_t* dp, const uint8_t* color,
+                       const int32_t* perm, int n, DBuf<int32_t>& lptr, DBuf<int32_t>& lcol, DBuf<int32_t>& lsrc,
+                       DBuf<int32_t>& uptr, DBuf<int32_t>& ucol, DBuf<int32_t>& usrc, DBuf<int32_t>* dsrc);
 
 // Host loop over [0, n) in contiguous chunks on up to 32 threads: f(begin, end).
 // Each index's work must be independent (and not throw); small n runs inline.

@@ -444,11 +444,39 @@ __global__ void k_split_fill(const int32_t* __restrict__ rp, const int32_t* __re
       if (cj < ci) { lcol[a] = j; lsrc[a++] = k; }
       else if (cj > ci) { ucol[b] = j; usrc[b++] = k; }
     }
-    dsrc[p] = dp[i];
+    if (dsrc) dsrc[p] = dp[i];
   }
 }
 
 }  // namespace
+
+void split_rows_device(afem_ctx* c, const int32_t* rp, const int32_t* cl, const int32_t* dp, const uint8_t* color,
+                       const int32_t* perm, int n, DBuf<int32_t>& lptr, DBuf<int32_t>& lcol, DBuf<int32_t>& lsrc,
+                       DBuf<int32_t>& uptr, DBuf<int32_t>& ucol, DBuf<int32_t>& usrc, DBuf<int32_t>* dsrc) {
+  cudaStream_t s = c->stream;
+  DBuf<int32_t> lcnt, ucnt;
+  lcnt.alloc(n);
+  ucnt.alloc(n);
+  const int nb = c->num_sms * 8;
+  k_split_count<<<nb, 256, 0, s>>>(rp, cl, color, perm, n, lcnt.p, ucnt.p);
+  count_launch();
+  lptr.alloc(n + 1);
+  uptr.alloc(n + 1);
+  long ltot = 0, utot = 0;
+  exclusive_scan(lcnt.p, lptr.p, n, s, &ltot);
+  exclusive_scan(ucnt.p, uptr.p, n, s, &utot);
+  lcol.alloc(ltot);
+  lsrc.alloc(ltot);
+  ucol.alloc(utot);
+  usrc.alloc(utot);
+  int32_t* ds = nullptr;
+  if (dsrc) {
+    dsrc->alloc(n);
+    ds = dsrc->p;
+  }
+  k_split_fill<<<nb, 256, 0, s>>>(rp, cl, dp, color, perm, n, lptr.p, uptr.p, lcol.p, lsrc.p, ucol.p, usrc.p, ds);
+  count_launch();
+}
 
 void build_schedule(afem_ctx* c, bool levels) {
   if (c->schedule_ready && (!levels || c->levels_ready)) return;
@@ -483,29 +511,9 @@ void build_schedule(afem_ctx* c, bool levels) {
   // perm[p]; its entries of earlier colours (the forward sweep's) and of later
   // colours (the backward sweep's), each with the index of the entry in the CSR;
   // built on the device from the colouring (counts, prefix sums, fill in CSR order)
-  {
-    DBuf<int32_t> lcnt, ucnt;
-    lcnt.alloc(n);
-    ucnt.alloc(n);
-    const int nb = c->num_sms * 8;
-    k_split_count<<<nb, 256, 0, s>>>(c->rowptr.p, c->col.p, c->color.p, c->perm_mc.p, n, lcnt.p, ucnt.p);
-    count_launch();
-    c->mc_lptr.alloc(n + 1);
-    c->mc_uptr.alloc(n + 1);
-    long ltot = 0, utot = 0;
-    exclusive_scan(lcnt.p, c->mc_lptr.p, n, s, &ltot);
-    exclusive_scan(ucnt.p, c->mc_uptr.p, n, s, &utot);
-    c->mc_lcol.alloc(ltot);
-    c->mc_lsrc.alloc(ltot);
-    c->mc_ucol.alloc(utot);
-    c->mc_usrc.alloc(utot);
-    c->mc_dsrc.alloc(n);
-    k_split_fill<<<nb, 256, 0, s>>>(c->rowptr.p, c->col.p, c->diagpos.p, c->color.p, c->perm_mc.p, n, c->mc_lptr.p,
-                                    c->mc_uptr.p, c->mc_lcol.p, c->mc_lsrc.p, c->mc_ucol.p, c->mc_usrc.p,
-                                    c->mc_dsrc.p);
-    count_launch();
-    c->mc_vals_gen = -1;
-  }
+  split_rows_device(c, c->rowptr.p, c->col.p, c->diagpos.p, c->color.p, c->perm_mc.p, n, c->mc_lptr, c->mc_lcol,
+                    c->mc_lsrc, c->mc_uptr, c->mc_ucol, c->mc_usrc, &c->mc_dsrc);
+  c->mc_vals_gen = -1;
   AFEM_CUDA(cudaStreamSynchronize(s));
   c->schedule_ready = true;
 }
