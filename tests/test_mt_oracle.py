@@ -5,8 +5,10 @@ pinned by: the surface extraction's counts on a box (EXTRACT6SURFACES,
 src/src_2D/m_surface_type.f90:189-502), the identities of the 2-D TM element
 (its curl-curl annihilates discrete gradients, its mass matrix is SPD;
 GENMAT2DTM, src/src_2D/forward_2DTM.f90:253-363), GENBCMT's assignment order
-(src/src_3DMT/forward_3DMT.f90:92-177) and the known answer of MT over a uniform
-half-space: apparent resistivity 1/sigma and phase 45 degrees (mod 180).
+(src/src_3DMT/forward_3DMT.f90:92-177) and the known answers of MT over a uniform
+half-space: apparent resistivity 1/sigma and phase 45 degrees (mod 180) where the skin
+depth is well above the bottom boundary, and the 1-D answer of a layer over a perfect
+conductor (the E = 0 bottom) where it is not.
 """
 import numpy as np
 import pytest
@@ -153,3 +155,30 @@ def test_halfspace_apparent_resistivity():
     np.testing.assert_allclose(pha[1], -135.0, atol=2.5)
     np.testing.assert_allclose(pha[2], 45.0, atol=2.5)
     assert np.abs(z[[0, 3]]).max() < 2e-2 * np.abs(z[[1, 2]]).min()
+
+
+def _z1d_over_conductor(f, sigma, depth_km):
+    """Impedance (SI, E/H) of a uniform earth of `depth_km` over a perfect conductor (E = 0), the
+    textbook 1-D layer recursion with a zero impedance below: Z = Z_i tanh(k h), k = sqrt(i w mu sigma)."""
+    mu = 4e-7 * np.pi
+    w = 2 * np.pi * f
+    k = np.sqrt(1j * w * mu * sigma)
+    return 1j * w * mu / k * np.tanh(k * depth_km * 1e3)
+
+
+def test_halfspace_over_the_bottom_boundary():
+    """At 1 mHz a 10 Ohm m earth's skin depth (50 km) reaches the E = 0 bottom at -50 km, so the
+    answer is that of a 50 km layer over a perfect conductor: rho_a = 12.44 Ohm m, phase 59.3
+    degrees, not 10 and 45.  The oracle's chain on a 10 x 10 x (6 + 18) mesh with 1.3 km surface
+    cells reproduces it (measured: 0.46 % and 1.0 degree)."""
+    f = 0.001
+    m = synth.mt_box(10, 10, 6, 18, ratio_earth=1.08, sigma=0.1, freqs=[f], site_grid=(-20.0, 0.0, 20.0))
+    line, n6 = O.mkline(m.node, m.n4)
+    r = O.MTOracle(m, line, n6).forward(m.freqs, m.sites)
+    Z = _z1d_over_conductor(f, 0.1, 50.0)
+    rho = abs(Z) ** 2 / (2 * np.pi * f * 4e-7 * np.pi)
+    pha = np.degrees(np.angle(Z))
+    assert abs(rho - 12.44) < 0.01 and abs(pha - 59.34) < 0.01
+    np.testing.assert_allclose(r["rho"][0][1:3], rho, rtol=0.01)
+    np.testing.assert_allclose(r["pha"][0][1] + 180.0, pha, atol=1.5)
+    np.testing.assert_allclose(r["pha"][0][2], pha, atol=1.5)
