@@ -182,3 +182,37 @@ def test_halfspace_over_the_bottom_boundary():
     np.testing.assert_allclose(r["rho"][0][1:3], rho, rtol=0.01)
     np.testing.assert_allclose(r["pha"][0][1] + 180.0, pha, atol=1.5)
     np.testing.assert_allclose(r["pha"][0][2], pha, atol=1.5)
+
+
+def test_layered_earth_converges_with_the_surface_cells():
+    """10 Ohm m over 100 Ohm m (below the mesh level near 9 km) at 0.01 Hz over the E = 0 bottom:
+    the oracle's apparent resistivity approaches the 1-D layered answer as the first cell under
+    the surface thins, about in proportion to it (B = curl A is constant in a tetrahedron, so a
+    site 1 m deep sees the top cell's average; measured 15.3, 8.2, 4.3 % for 1.34, 0.66, 0.32 km)."""
+    f = 0.01
+    mu = 4e-7 * np.pi
+    w = 2 * np.pi * f
+    errs, firsts = [], []
+    for ratio in (1.08, 1.15, 1.22):
+        m = synth.mt_box(10, 10, 6, 18, ratio_earth=ratio, sigma=0.1, freqs=[f], site_grid=(0.0,))
+        z = np.unique(m.xyz[:, 2])
+        zl = z[z < 0]
+        d = float(-zl[np.argmin(np.abs(zl + 10.0))])
+        cen = m.xyz[m.n4[m.nphys1:] - 1].mean(axis=1)
+        m.sigma_land = np.where(cen[:, 2] < -d, 0.01, m.sigma_land)
+        line, n6 = O.mkline(m.node, m.n4)
+        r = O.MTOracle(m, line, n6).forward(m.freqs, m.sites)
+        # the 1-D recursion: 100 Ohm m from -d to -50 km over the conductor, 10 Ohm m above
+        k = np.sqrt(1j * w * mu * np.array([0.1, 0.01]))
+        zi = 1j * w * mu / k
+        Z = zi[1] * np.tanh(k[1] * (50.0 - d) * 1e3)
+        t = np.tanh(k[0] * d * 1e3)
+        Z = zi[0] * (Z + zi[0] * t) / (zi[0] + Z * t)
+        rho = abs(Z) ** 2 / (w * mu)
+        errs.append(abs(r["rho"][0][1][0] / rho - 1.0))
+        firsts.append(-zl[-1])
+    assert firsts[0] > firsts[1] > firsts[2]
+    assert errs[0] > errs[1] > errs[2] and errs[2] < 0.06, errs
+    # first order: the error per km of the first cell stays within a factor 1.5
+    per_km = np.array(errs) / np.array(firsts)
+    assert per_km.max() <= 1.5 * per_km.min(), per_km
