@@ -216,3 +216,22 @@ def test_layered_earth_converges_with_the_surface_cells():
     # first order: the error per km of the first cell stays within a factor 1.5
     per_km = np.array(errs) / np.array(firsts)
     assert per_km.max() <= 1.5 * per_km.min(), per_km
+
+
+def test_mt_box_layout():
+    """The synthetic MT model: graded levels finest at the surface, air (tag 1) above and earth
+    (tag 3, 4 in the block) below z = 0 by centroid, the earth tetrahedra last with one
+    conductivity each, and each region's first cell set by its ratio."""
+    m = synth.mt_box(6, 5, 4, 6, ratio_air=1.3, ratio_earth=1.1, block_sigma=0.5, half_km=20.0)
+    z = np.unique(m.xyz[:, 2])
+    assert z[0] == -50.0 and z[-1] == 50.0 and 0.0 in z and z.size == 4 + 6 + 1
+    dz = np.diff(z)
+    i0 = int(np.searchsorted(z, 0.0))
+    assert np.all(np.diff(dz[i0:]) > 0) and np.all(np.diff(dz[:i0]) < 0)  # thicker away from 0
+    np.testing.assert_allclose(dz[i0 + 1] / dz[i0], 1.3)
+    np.testing.assert_allclose(dz[i0 - 2] / dz[i0 - 1], 1.1)
+    cz = m.xyz[m.n4 - 1].mean(axis=1)[:, 2]
+    assert np.all(m.tag[cz > 0] == 1) and np.all(m.tag[cz < 0] >= 3)
+    assert np.all(np.diff(m.tag >= 3) >= 0)  # earth last
+    assert m.sigma_land.shape[0] == int((m.tag >= 3).sum()) == m.ntet - m.nphys1
+    assert set(np.unique(m.sigma_land)) == {0.1, 0.5} and np.all(m.sigma_land[m.tag[m.nphys1:] == 4] == 0.5)
